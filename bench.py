@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""IASI spectra/s on B200: the line-by-line forward model on 400,000 synthetic lines.
+
+Workload ("iasi-400k"): 400,000 lines over H2O, CO2, O3, N2O, CO, CH4 in
+645-2760 cm^-1, IASI sounder (8461 channels, Gaussian apodization), 0.0025 cm^-1
+internal grid (858,801 points), the six AFGL 50-level profiles (49 layers) per
+step and per GPU, FullFaddeeva, 25 cm^-1 cutoff, DPTMIN 1e-6, :cim source,
+MT-CKD H2O and CO2 continua (CIA tables are not bundled and contribute zero, as
+in the reference without them).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1); every rank computes its own six
+profiles per step (weak scaling, no data-path collective).  `value` is the mixed
+(FP32 + Kahan) path with line lists resident in HBM, device-timed with CUDA
+events; `e2e` goes through the host C-ABI call with host buffers; the plain FP64
+kernel's spectra/s is reported beside it.  `--impl reference` times the
+reference algorithm's CPU implementation (the FP64 C++ restatement under
+oracle/, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+N_PROF = 6
+FAR_PAIR_FLOPS = 10     # d (2), d^2, d^2+b^2, rcp, pedestal FMA (2), value FMA (2), accumulate
+CORE_PAIR_FLOPS = 70    # far-pair ops + FP32 Faddeeva (continued fraction / Weideman-16 branch)
+FP32_LANES = 148 * 128  # B200: 148 SMs x 128 FP32 lanes
+
+
+def _package():
+    sys.path.insert(0, str(ROOT))
+    import __graft_entry__ as ge
+    return ge._package()
+
+
+def _workload_kw():
+    return dict(internal_dnu=0.0025, cutoff=25.0, dptmn=1e-6, apply_continuum=True,
+                with_ils=True, apodization="gaussian", T_method="logp_at_pcg",
+                source_function="cim")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(self.idx)],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                self.out = ""
+        else:
+            self.out = ""
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _physical_gpu(local_rank: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        try:
+            return int(vis.split(",")[local_rank])
+        except (ValueError, IndexError):
+            pass
+    return local_rank
+
+
+def _traffic_from_profiles():
+    """DRAM bytes per launch of the line-sum kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "linesum_mixed_iasi400k.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch_full:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_sample(seconds_target: float = 8.0):
+    """Oracle (reference algorithm, FP64, all host threads) on a channel window of the
+    same workload; scaled to full spectra by internal grid points."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+    pkg = _package()
+    o = orc.Oracle()
+    lists = pkg.synthetic.lists_iasi_400k()
+    prof = pkg.afgl_atmosphere("us_standard")
+    snd = orc.sounder(645.0, 2760.0, 0.25, opd_max=2.0, fwhm_gauss=0.5)
+    opt = orc.fm_options(**_workload_kw())
+    n_full = 858801
+    ll = {s: l.lines for s, l in lists.items()}
+    pr = dict(p=prof.pressure, T=prof.temperature, vmr=prof.vmr)
+    # size the window: time a small one first, then grow to about `seconds_target`
+    c0 = 3000
+    t0 = time.perf_counter()
+    o.forward_model(pr, ll, snd, opt, channels=(c0, c0 + 8))
+    t_small = time.perf_counter() - t0
+    n_small = 8 * 100 + 12800 + 1
+    per_pt = t_small / n_small
+    n_ch = max(8, int((seconds_target / per_pt - 12801) / 100))
+    n_ch = min(n_ch, 8461 - c0)
+    n_pts = n_ch * 100 + 12800 + 1
+
+    def run():
+        t = time.perf_counter()
+        o.forward_model(pr, ll, snd, opt, channels=(c0, c0 + n_ch))
+        return time.perf_counter() - t
+
+    return run, n_pts, n_full, orc.num_threads(), c0, n_ch
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    run, n_pts, n_full, cores, c0, n_ch = cpu_sample()
+    for _ in range(args.warmup):
+        run()
+    ts = [run() for _ in range(args.steps)]
+    t = sum(ts) / len(ts)
+    v = n_pts / n_full / t
+    line = {
+        "impl": "reference", "metric": "IASI spectra/s (line-by-line forward_model, 400k lines)",
+        "value": v, "unit": "spectra/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded line lists, AFGL profiles)",
+        "config": {"workload": "iasi-400k", "lines": 400000, "species": 6, "grid_dnu": 0.0025,
+                   "n_nu": n_full, "layers": 49, "profiles_per_step": 1, "method": "FullFaddeeva"},
+        "cpu_baseline": {"value": v, "unit": "spectra/s", "cores": cores, "kind": "port",
+                         "sample": f"one AFGL profile, channels {c0}..{c0 + n_ch - 1} ({n_pts} internal grid "
+                                   f"points of {n_full}), scaled by grid points"},
+        "e2e": {"value": v, "unit": "spectra/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    pkg = _package()
+    ctx = pkg.B200Context(local)
+    lists = pkg.synthetic.lists_iasi_400k()
+    profs = [pkg.afgl_atmosphere(a) for a in pkg.synthetic.AFGL][:N_PROF]
+    snd = pkg.IASIInstrument()
+    pkg._prepare(ctx, lists, None)
+    lib = ctx.lib
+
+    def options(prec):
+        return pkg.fm_options(precision=prec, method=pkg.FullFaddeeva, **_workload_kw())
+
+    batch = pkg._ProfileBatch(profs, [None] * N_PROF, [1.0] * N_PROF, [1.0] * N_PROF)
+    s = snd.c_struct()
+    nch = 8461
+    R = torch.empty((N_PROF, nch), dtype=torch.float64, device="cuda")
+    BT = torch.empty_like(R)
+    stream = torch.cuda.current_stream()
+
+    def step_device(opt):
+        pkg.check(lib.irs_forward_model_batch_device(ctx.h, batch.arr, N_PROF, C.byref(s), C.byref(opt),
+                                                     C.c_void_p(R.data_ptr()), C.c_void_p(BT.data_ptr()),
+                                                     C.c_void_p(stream.cuda_stream)))
+
+    # ---------------- value: mixed path, inputs resident, CUDA events
+    om = options("mixed")
+    for _ in range(args.warmup):
+        step_device(om)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(_physical_gpu(local)) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step_device(om)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    value = world * N_PROF / (ms / 1e3)
+
+    # per-stage device times (library events on its launching stream), averaged
+    acc = {"line_params_ms": 0.0, "line_sum_ms": 0.0, "rte_ms": 0.0, "ils_ms": 0.0}
+    for _ in range(args.steps):
+        step_device(om)
+        pkg.check(lib.irs_synchronize(ctx.h))
+        st = ctx.stage_times()
+        for k in acc:
+            acc[k] += getattr(st, k) / args.steps
+    pairs, core = st.pairs, st.core_pairs
+    launches_per_step = st.launches
+    t_ls = acc["line_sum_ms"] / 1e3
+    flops = FAR_PAIR_FLOPS * (pairs - core) + CORE_PAIR_FLOPS * core
+    clocks = clk.summary()
+    f_sm = (clocks["sm_mhz"] or 1965.0) * 1e6
+    peak = FP32_LANES * 2 * f_sm / 1e12
+    achieved = flops / t_ls / 1e12
+    traffic = _traffic_from_profiles()
+
+    # ---------------- e2e: host C-ABI call, host buffers in and out
+    Rh = (C.c_double * (N_PROF * nch))()
+    BTh = (C.c_double * (N_PROF * nch))()
+    for _ in range(2):
+        pkg.check(lib.irs_forward_model_batch(ctx.h, batch.arr, N_PROF, C.byref(s), C.byref(om), Rh, BTh))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        pkg.check(lib.irs_forward_model_batch(ctx.h, batch.arr, N_PROF, C.byref(s), C.byref(om), Rh, BTh))
+    t_e2e = max_over_ranks((time.perf_counter() - t0) / args.steps)
+    st = ctx.stage_times()
+    e2e = {"value": world * N_PROF / t_e2e, "unit": "spectra/s",
+           "h2d_bytes_per_step": int(st.h2d_bytes), "d2h_bytes_per_step": int(st.d2h_bytes),
+           "timing": "host wall clock around the synchronous C-ABI call, max over ranks"}
+
+    # ---------------- plain FP64 kernel on the same workload
+    op = options("fp64")
+    step_device(op)
+    barrier()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for _ in range(args.plain_steps):
+        step_device(op)
+    p1.record(stream)
+    torch.cuda.synchronize()
+    ms64 = max_over_ranks(p0.elapsed_time(p1) / args.plain_steps)
+    plain = world * N_PROF / (ms64 / 1e3)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        run, n_pts, n_full, cores, c0, n_ch = cpu_sample()
+        tc = run()
+        cpu = {"value": n_pts / n_full / tc, "unit": "spectra/s", "cores": cores, "kind": "port",
+               "sample": f"FP64 oracle, one AFGL profile, channels {c0}..{c0 + n_ch - 1} ({n_pts} of "
+                         f"{n_full} internal grid points), scaled by grid points"}
+
+    # consistency check of this run: mixed vs FP64 BT on the last batch
+    step_device(om)
+    torch.cuda.synchronize()
+    BTm = BT.clone()
+    step_device(op)
+    torch.cuda.synchronize()
+    d = (BTm - BT)
+    bt_rms = float(torch.sqrt(torch.mean(d * d)).item())
+    bt_max = float(d.abs().max().item())
+
+    if rank == 0:
+        line = {
+            "metric": "IASI spectra/s (line-by-line forward_model, 400k lines, mixed FP32+Kahan)",
+            "value": value, "unit": "spectra/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+kahan (fp64 transmittance/RTE)",
+            "data": "synthetic (seeded line lists, AFGL profiles)",
+            "config": {"workload": "iasi-400k", "lines": 400000, "species": 6, "grid_dnu": 0.0025,
+                       "n_nu": 858801, "layers": 49, "channels": nch, "profiles_per_step_per_gpu": N_PROF,
+                       "method": "FullFaddeeva", "cutoff": 25.0, "dptmn": 1e-6,
+                       "continua": "h2o,co2", "l2": "working set (line parameters ~4 GB, tau 1 GB) >> L2"},
+            "plain_fp64": {"value": plain, "unit": "spectra/s", "ms_per_step": ms64,
+                           "mixed_over_plain": value / plain},
+            "bt_mixed_vs_fp64_K": {"rms": bt_rms, "max": bt_max},
+            "stages_ms": acc,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "linesum_mixed_kernel<3>",
+                         "work": {"pairs": pairs, "core_pairs": core, "far_flops": FAR_PAIR_FLOPS,
+                                  "core_flops": CORE_PAIR_FLOPS},
+                         "peak_source": "148 SMs x 128 FP32 lanes x 2 FLOP x median sampled SM clock "
+                                        "(MEASURED_PEAKS.json has no FP32 figure)"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches_per_step * args.steps),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,174 @@
+/*
+ * irs_b200.h -- C ABI of libirs_b200.so, the B200 (sm_100a) line-by-line forward
+ * path of IRSounderLBL.jl.
+ *
+ * Plain C types only (pointers, sizes, doubles), so the Julia package binds it
+ * with `ccall` and Python with ctypes.  Every entry point returns an int status:
+ * 0 on success, a negative IRS_E* code on failure; irs_last_error() then returns
+ * a message for the calling thread (the Julia shim raises it as ErrorException,
+ * which is how the reference reports errors).  All host buffers are owned by the
+ * caller; the library never keeps a pointer to them after the call returns.
+ *
+ * Each declaration names the reference interface it replaces (paths are
+ * relative to the IRSounderLBL.jl project root).
+ */
+#ifndef IRS_B200_H
+#define IRS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IRS_ABI_VERSION 1
+
+/* status codes */
+#define IRS_OK            0
+#define IRS_E_ARG        -1   /* invalid argument (sizes, enums, ranges)      */
+#define IRS_E_CUDA       -2   /* CUDA runtime error                          */
+#define IRS_E_STATE      -3   /* missing table / line list / context         */
+#define IRS_E_NOMEM      -4   /* device allocation failed                    */
+
+/* VoigtMethod, src/CrossSections/voigt.jl:32-36 */
+#define IRS_WEIDEMAN      1
+#define IRS_PSEUDOVOIGT   2
+#define IRS_FULLFADDEEVA  3
+
+/* arithmetic of the line sum */
+#define IRS_FP64          0   /* FP64 everywhere: the plain GPU kernel                  */
+#define IRS_MIXED         1   /* FP32 Faddeeva + Kahan-compensated FP32 line sum        */
+
+/* HITRANLine, src/HITRAN/linelist.jl:20-31 (isbits, 56 bytes): a Julia
+ * Vector{HITRANLine} is passed as pointer(ll.lines) without a copy. */
+typedef struct {
+    int8_t  mol_id;
+    int8_t  iso_id;
+    uint8_t _pad[6];
+    double  wavenumber;
+    double  intensity;
+    double  a_coeff;
+    float   air_broad;
+    float   self_broad;
+    double  lower_energy;
+    float   temp_depend;
+    float   pressure_shift;
+} irs_line;
+
+/* Sounder, src/Sensor/sounder.jl:33-40 */
+typedef struct {
+    double  nu_min, nu_max, dnu;
+    int64_t n_channels;
+    double  opd_max, fwhm_gauss;
+} irs_sounder;
+
+/* forward_model keyword arguments, src/Sensor/sounder.jl:233-252.
+ * apodization: 0 :gaussian, 1/2/3 :norton_beer_weak/_medium/_strong (ils.jl:26-30)
+ * T_method: 0 :logp_at_pcg, 1 :mass_weighted (layers.jl:133)
+ * source_function: 0 :cim, 1 :toon (schwarzschild.jl:130)
+ * line_mixing: 0 nothing, 1 VPYLineMixing with per-line Y(T) = y0 (296/T)^0.75
+ *   (the y0 uploaded with the CO2 list; line_mixing.jl:1351-1369)
+ * continua: bit mask 1 :h2o, 2 :co2, 4 :co2_cia, 8 :n2, 16 :o2 (CIA tables are
+ *   not bundled and contribute zeros, as the reference does without them)
+ * method: VoigtMethod of the line sum (forward_model uses FullFaddeeva)
+ * precision: IRS_FP64 or IRS_MIXED */
+typedef struct {
+    double  internal_dnu;      /* <= 0: use high_res_factor (or 4) */
+    int32_t high_res_factor;   /* > 0 overrides internal_dnu       */
+    int32_t apply_continuum;
+    int32_t continua;
+    int32_t with_ils;
+    int32_t apodization;
+    int32_t line_mixing;
+    int32_t T_method;
+    int32_t source_function;
+    int32_t method;
+    int32_t precision;
+    double  cutoff, lm_cutoff, dptmn, x_far;
+} irs_fm_options;
+
+/* AtmosphericProfile (src/Atmosphere/profiles.jl:12-17) plus the per-scene
+ * surface and geometry kwargs of forward_model: levels surface-first, hPa, K;
+ * vmr is [n_species][n_lev] for the HITRAN molecule ids in species[]. */
+typedef struct {
+    int32_t       n_lev;
+    int32_t       n_species;
+    const double* pressure;
+    const double* temperature;
+    const int32_t* species;
+    const double* vmr;
+    double        T_sfc;       /* NaN: temperature[0] (sounder.jl:337) */
+    double        mu;          /* ViewingGeometry.mu, geometry.jl:18-34 */
+    double        eps_sfc;
+} irs_profile;
+
+/* per-stage device times of the last forward call, ms (CUDA events) */
+typedef struct {
+    double line_params_ms, line_sum_ms, rte_ms, ils_ms, total_ms;
+    double pairs;              /* (grid point, line, layer) pairs inside the cutoff after DPTMIN */
+    double core_pairs;         /* of which |x| <= x_far (Faddeeva evaluations) */
+    double h2d_bytes;          /* host->device bytes copied by the call */
+    double d2h_bytes;          /* device->host bytes copied by the call */
+    double launches;           /* kernels launched by the call */
+} irs_stage_times;
+
+typedef struct irs_ctx irs_ctx;
+
+int         irs_abi_version(void);
+const char* irs_last_error(void);
+
+/* Context on one GPU: device buffers, streams, uploaded tables and line lists.
+ * Not shared between host threads without external locking. */
+int irs_create(int device, irs_ctx** out);
+int irs_destroy(irs_ctx* ctx);
+
+/* TIPS-2024 Q(T) table for (mol, iso) at 1 K from t_min
+ * (replaces partition.jl:10-47 reading src/HITRAN/tips2024_data.jl). */
+int irs_set_partition_table(irs_ctx* ctx, int mol, int iso, int t_min, int n, const double* q);
+
+/* MT-CKD tables (replaces continuum.jl:49-99 reading data/mt_ckd_*). */
+int irs_set_continuum_h2o(irs_ctx* ctx, int n, const double* nu, const double* cs,
+                          const double* cf, const double* texp);
+int irs_set_continuum_co2(irs_ctx* ctx, int n, const double* nu, const double* s,
+                          const double* xfac, const double* tdep);
+
+/* Upload the line list of one species (HITRANLinelist, linelist.jl:51-56; lines
+ * sorted by wavenumber as HITRANLinelist guarantees -- unsorted input is sorted
+ * here).  y0 (nullable) holds per-line first-order mixing coefficients used when
+ * line_mixing = 1 (VPYLineMixing, line_mixing.jl:144-149). */
+int irs_upload_linelist(irs_ctx* ctx, int species, const irs_line* lines, int64_t n,
+                        const double* y0);
+
+/* compute_voigt_cross_sections(ν_grid, linelist, T, p_atm; vmr_self, cutoff,
+ * method, x_far) -- src/CrossSections/voigt.jl:375-462 -- for the uploaded list
+ * of `species`, on the host grid[n_nu]; sigma[n_nu] (cm^2/molecule) is written. */
+int irs_cross_sections(irs_ctx* ctx, int species, const double* grid, int64_t n_nu,
+                       double T, double p_atm, double vmr_self, double cutoff, int method,
+                       double x_far, int precision, double* sigma);
+
+/* forward_model(prof, linelists; sounder, geom, T_sfc, ε_sfc, kwargs...) for a
+ * batch of profiles -- src/Sensor/sounder.jl:233-360.  R and BT are host buffers
+ * [n_prof][n_channels] (mW/m^2/sr/cm^-1 and K). */
+int irs_forward_model_batch(irs_ctx* ctx, const irs_profile* profs, int n_prof,
+                            const irs_sounder* s, const irs_fm_options* o,
+                            double* R, double* BT);
+
+/* Same as irs_forward_model_batch, but R and BT are DEVICE pointers and the call
+ * returns once the work is enqueued on `stream` (a cudaStream_t; NULL = the
+ * context's stream).  Used when results stay in HBM. */
+int irs_forward_model_batch_device(irs_ctx* ctx, const irs_profile* profs, int n_prof,
+                                   const irs_sounder* s, const irs_fm_options* o,
+                                   double* R_dev, double* BT_dev, void* stream);
+
+/* Wait for the context's work; fill per-stage times of the last forward call. */
+int irs_synchronize(irs_ctx* ctx);
+int irs_last_stage_times(irs_ctx* ctx, irs_stage_times* out);
+
+/* Number of internal grid points and channels forward_model uses for (s, o). */
+int irs_grid_size(const irs_sounder* s, const irs_fm_options* o, int64_t* n_nu,
+                  int64_t* n_channels);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IRS_B200_H */

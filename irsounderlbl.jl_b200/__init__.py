@@ -1,0 +1,389 @@
+"""irsounderlbl.jl_b200 -- the line-by-line forward path of IRSounderLBL.jl on one B200.
+
+Host-side mirror of the reference interface (same names, argument meanings and
+error behaviour as the Julia package) over the C ABI of ``libirs_b200.so``:
+
+    compute_voigt_cross_sections   src/CrossSections/voigt.jl:375-462
+    forward_model                  src/Sensor/sounder.jl:233-360
+    Sounder / IASIInstrument ...   src/Sensor/sounder.jl:33-128
+    ViewingGeometry, scan angles   src/Sensor/geometry.jl:18-101
+    VoigtMethod, VPYLineMixing     voigt.jl:32-36, line_mixing.jl:144-149
+
+Every computation runs in the CUDA library; nothing here evaluates physics
+beyond argument marshalling and the scalar geometry helpers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from enum import IntEnum
+from pathlib import Path
+from typing import Dict, Iterable, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import (IRS_FP64, IRS_MIXED, LINE_DTYPE, FMOptions, IRSError, Profile, StageTimes,
+                   check, dptr)
+
+DATA = Path(__file__).resolve().parent / "data"
+
+
+class VoigtMethod(IntEnum):
+    """src/CrossSections/voigt.jl:32-36"""
+    Weideman = 1
+    PseudoVoigt = 2
+    FullFaddeeva = 3
+
+
+Weideman, PseudoVoigt, FullFaddeeva = VoigtMethod.Weideman, VoigtMethod.PseudoVoigt, VoigtMethod.FullFaddeeva
+
+
+class GasSpecies(IntEnum):
+    """src/Atmosphere/species.jl:6-16 (values are HITRAN molecule ids)"""
+    H2O = 1
+    CO2 = 2
+    O3 = 3
+    N2O = 4
+    CO = 5
+    CH4 = 6
+    O2 = 7
+    SO2 = 9
+    NH3 = 11
+
+
+H2O, CO2, O3, N2O, CO, CH4 = (GasSpecies.H2O, GasSpecies.CO2, GasSpecies.O3, GasSpecies.N2O,
+                              GasSpecies.CO, GasSpecies.CH4)
+
+PRECISION = {"fp64": IRS_FP64, "mixed": IRS_MIXED}
+APODIZATION = {"gaussian": 0, "norton_beer_weak": 1, "norton_beer_medium": 2, "norton_beer_strong": 3}
+CONTINUA = {"h2o": 1, "co2": 2, "co2_cia": 4, "n2": 8, "o2": 16}
+
+
+# ------------------------------------------------------------------ types
+class HITRANLinelist:
+    """HITRANLinelist (src/HITRAN/linelist.jl:51-56): lines sorted by wavenumber."""
+
+    def __init__(self, lines: np.ndarray):
+        lines = np.asarray(lines)
+        order = np.argsort(lines["wavenumber"], kind="stable")
+        out = np.zeros(len(lines), dtype=LINE_DTYPE)  # zeroed padding, 56-byte records
+        for name in LINE_DTYPE.names:
+            out[name] = lines[name][order]
+        self.lines = out
+        self.molecules = set(int(m) for m in np.unique(self.lines["mol_id"]))
+        self.nu_min = float(self.lines["wavenumber"].min()) if len(self.lines) else 0.0
+        self.nu_max = float(self.lines["wavenumber"].max()) if len(self.lines) else 0.0
+
+    def __len__(self):
+        return len(self.lines)
+
+
+@dataclass
+class AtmosphericProfile:
+    """src/Atmosphere/profiles.jl:12-17 (levels surface-first, hPa, K, km)."""
+    pressure: np.ndarray
+    temperature: np.ndarray
+    altitude: np.ndarray
+    vmr: Dict[int, np.ndarray]
+
+
+@dataclass
+class Sounder:
+    """src/Sensor/sounder.jl:33-56"""
+    nu_min: float
+    nu_max: float
+    dnu: float
+    n_channels: int
+    opd_max: float
+    fwhm_gauss: float
+
+    @staticmethod
+    def make(nu_min, nu_max, dnu, opd_max=None, fwhm_gauss=0.0, n_channels=None) -> "Sounder":
+        n = round((nu_max - nu_min) / dnu) + 1 if n_channels is None else int(n_channels)
+        return Sounder(float(nu_min), float(nu_max), float(dnu), n,
+                       1.0 / (2.0 * dnu) if opd_max is None else float(opd_max), float(fwhm_gauss))
+
+    def c_struct(self) -> _lib.Sounder:
+        s = _lib.Sounder()
+        s.nu_min, s.nu_max, s.dnu = self.nu_min, self.nu_max, self.dnu
+        s.n_channels, s.opd_max, s.fwhm_gauss = self.n_channels, self.opd_max, self.fwhm_gauss
+        return s
+
+
+def IASIInstrument(fwhm_gauss: float = 0.5) -> Sounder:  # sounder.jl:65-68
+    return Sounder.make(645.0, 2760.0, 0.25, opd_max=2.0, fwhm_gauss=fwhm_gauss)
+
+
+def IASINGInstrument(fwhm_gauss: float = 0.25) -> Sounder:  # sounder.jl:86-89
+    return Sounder.make(645.0, 2760.0, 0.125, opd_max=4.0, fwhm_gauss=fwhm_gauss)
+
+
+def CrISInstrument(band: str = "full", fwhm_gauss: float = 0.0) -> Sounder:  # sounder.jl:102-110
+    rng = {"full": (650.0, 2550.0), "lwir": (650.0, 1095.0), "mwir": (1210.0, 1750.0),
+           "swir": (2155.0, 2550.0)}
+    if band not in rng:
+        raise IRSError(f"CrIS band must be :full, :lwir, :mwir, or :swir; got :{band}")
+    return Sounder.make(*rng[band], 0.625, opd_max=0.8, fwhm_gauss=fwhm_gauss)
+
+
+def MTGIRSInstrument(band: str = "full", fwhm_gauss: float = 0.0) -> Sounder:  # sounder.jl:121-128
+    rng = {"full": (700.0, 2175.0), "lwir": (700.0, 1210.0), "mwir": (1600.0, 2175.0)}
+    if band not in rng:
+        raise IRSError(f"MTG-IRS band must be :full, :lwir, or :mwir; got :{band}")
+    return Sounder.make(*rng[band], 0.625, opd_max=0.8, fwhm_gauss=fwhm_gauss)
+
+
+@dataclass
+class ViewingGeometry:
+    """src/Sensor/geometry.jl:18-34"""
+    zenith_angle: float
+    azimuth_angle: float = 0.0
+    mu: float = field(init=False)
+
+    def __post_init__(self):
+        if not (0.0 <= self.zenith_angle < 90.0):
+            raise IRSError(f"Viewing zenith angle must be in [0, 90); got {self.zenith_angle}°")
+        self.mu = math.cos(math.radians(self.zenith_angle))
+
+
+def nadir_geometry() -> ViewingGeometry:
+    return ViewingGeometry(0.0)
+
+
+def scan_angle_to_local_zenith(scan_angle: float, h_sat_km: float = 817.0,
+                               R_earth_km: float = 6371.0) -> float:
+    """geometry.jl:92-101"""
+    s = (R_earth_km + h_sat_km) / R_earth_km * math.sin(math.radians(abs(scan_angle)))
+    if s > 1.0:
+        raise IRSError(f"scan_angle {scan_angle}° exceeds limb angle from h={h_sat_km} km")
+    return math.degrees(math.asin(s))
+
+
+@dataclass
+class VPYLineMixing:
+    """First-order (Rosenkranz) line mixing on the CO2 list (line_mixing.jl:144-149).
+
+    The reference derives Y(T) from the HITRAN2020 relaxation matrix, which is not
+    redistributable; here each CO2 line carries y0 and Y(T) = y0 (296/T)^0.75
+    (per atm), aligned with the CO2 HITRANLinelist order."""
+    y0: np.ndarray
+
+
+# ------------------------------------------------------------------ context
+def _read_tips(path=DATA / "tips2024_q.csv"):
+    out = {}
+    for line in open(path):
+        if line.startswith("#"):
+            continue
+        p = line.strip().split(",")
+        out[(int(p[0]), int(p[1]))] = np.array([float(v) for v in p[2:]])
+    return out
+
+
+def _read_cols(path):
+    rows = [l.strip().split(",") for l in open(path).readlines()[1:] if l.strip()]
+    return np.ascontiguousarray(np.array(rows, dtype=np.float64).T)
+
+
+class B200Context:
+    """One CUDA context of libirs_b200 on `device` with the bundled tables loaded.
+
+    Plays the role of the reference's `backend=` seam (strategy.jl:21-75): pass it
+    as `backend=` or let the module-level default be created on first use."""
+
+    def __init__(self, device: int = 0, load_tables: bool = True):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        check(self.lib.irs_create(device, C.byref(h)))
+        self.h = h
+        self.device = device
+        self._lists: Dict[int, tuple] = {}
+        if load_tables:
+            self.load_tables()
+
+    def load_tables(self):
+        for (mol, iso), q in _read_tips().items():
+            q = np.ascontiguousarray(q)
+            check(self.lib.irs_set_partition_table(self.h, mol, iso, 70, len(q), dptr(q)))
+        nu, cs, cf, te = _read_cols(DATA / "mt_ckd43_h2o_coeffs.csv")
+        self._h2o = (nu, cs, cf, te)
+        check(self.lib.irs_set_continuum_h2o(self.h, len(nu), *(dptr(a) for a in self._h2o)))
+        nu, s, xf, td = _read_cols(DATA / "mt_ckd_co2_coeffs.csv")
+        self._co2 = (nu, s, xf, td)
+        check(self.lib.irs_set_continuum_co2(self.h, len(nu), *(dptr(a) for a in self._co2)))
+
+    def upload_linelist(self, species: int, ll: HITRANLinelist, y0: Optional[np.ndarray] = None):
+        key = (id(ll), None if y0 is None else id(y0))
+        if self._lists.get(int(species), (None,))[0] == key:
+            return
+        lines = np.ascontiguousarray(ll.lines, dtype=LINE_DTYPE)
+        if lines.dtype.itemsize != 56:
+            raise IRSError("HITRANLine records must be 56 bytes (the isbits layout)")
+        yy = None if y0 is None else np.ascontiguousarray(y0, dtype=np.float64)
+        if yy is not None and len(yy) != len(lines):
+            raise IRSError("VPYLineMixing.y0 must have one entry per CO2 line")
+        check(self.lib.irs_upload_linelist(self.h, int(species), lines.ctypes.data, len(lines),
+                                           dptr(yy) if yy is not None else None))
+        self._lists[int(species)] = (key, ll, y0)
+
+    def stage_times(self) -> StageTimes:
+        t = StageTimes()
+        check(self.lib.irs_last_stage_times(self.h, C.byref(t)))
+        return t
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.irs_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default: Optional[B200Context] = None
+
+
+def default_context() -> B200Context:
+    global _default
+    if _default is None:
+        _default = B200Context()
+    return _default
+
+
+# ----------------------------------------------------------- operators
+def compute_voigt_cross_sections(nu_grid, linelist: HITRANLinelist, T: float, p_atm: float, *,
+                                 vmr_self: float = 0.0, cutoff: float = 25.0, backend=None,
+                                 method: VoigtMethod = FullFaddeeva, x_far: float = 122.0,
+                                 precision: str = "fp64") -> np.ndarray:
+    """compute_voigt_cross_sections (src/CrossSections/voigt.jl:375-462), cm^2/molecule."""
+    ctx = backend or default_context()
+    grid = np.ascontiguousarray(getattr(nu_grid, "nu", nu_grid), dtype=np.float64)
+    mols = linelist.molecules
+    if len(mols) != 1:
+        raise IRSError("compute_voigt_cross_sections takes a single-molecule line list here")
+    sp = next(iter(mols))
+    ctx.upload_linelist(sp, linelist)
+    out = np.empty(len(grid))
+    check(ctx.lib.irs_cross_sections(ctx.h, sp, dptr(grid), len(grid), float(T), float(p_atm),
+                                     float(vmr_self), float(cutoff), int(method), float(x_far),
+                                     PRECISION[precision], dptr(out)))
+    return out
+
+
+def fm_options(internal_dnu=0.001, high_res_factor=None, cutoff=25.0, lm_cutoff=None, dptmn=1e-6,
+               apply_continuum=True, continua=("h2o", "co2", "co2_cia", "n2", "o2"),
+               with_ils=True, apodization="gaussian", line_mixing=None,
+               T_method="logp_at_pcg", source_function="cim", method=FullFaddeeva,
+               x_far=122.0, precision="fp64") -> FMOptions:
+    """forward_model keyword arguments (src/Sensor/sounder.jl:233-252) as the C struct."""
+    if apodization not in APODIZATION:
+        raise IRSError(f"Unknown apodization {apodization}; expected :gaussian or one of "
+                       f"{[k for k in APODIZATION if k != 'gaussian']}")
+    if T_method not in ("logp_at_pcg", "mass_weighted"):
+        raise IRSError(f"T_method must be :logp_at_pcg or :mass_weighted, got :{T_method}")
+    if source_function not in ("cim", "toon"):
+        raise IRSError(f"source_function must be :toon or :cim, got :{source_function}")
+    o = FMOptions()
+    o.internal_dnu = -1.0 if internal_dnu is None else float(internal_dnu)
+    o.high_res_factor = int(high_res_factor or 0)
+    o.apply_continuum = int(bool(apply_continuum))
+    o.continua = sum(CONTINUA[c] for c in continua)
+    o.with_ils = int(bool(with_ils))
+    o.apodization = APODIZATION[apodization]
+    o.line_mixing = int(line_mixing is not None)
+    o.T_method = 0 if T_method == "logp_at_pcg" else 1
+    o.source_function = 0 if source_function == "cim" else 1
+    o.method = int(method)
+    o.precision = PRECISION[precision]
+    o.cutoff = float(cutoff)
+    o.lm_cutoff = float(cutoff if lm_cutoff is None else lm_cutoff)
+    o.dptmn = float(dptmn)
+    o.x_far = float(x_far)
+    return o
+
+
+class _ProfileBatch:
+    """Keeps the numpy buffers behind an array of irs_profile structs alive."""
+
+    def __init__(self, profs: Sequence[AtmosphericProfile], T_sfcs, mus, epss):
+        self.keep = []
+        self.arr = (Profile * len(profs))()
+        for k, pr in enumerate(profs):
+            p = np.ascontiguousarray(pr.pressure, dtype=np.float64)
+            T = np.ascontiguousarray(pr.temperature, dtype=np.float64)
+            sp = np.array(sorted(int(s) for s in pr.vmr), dtype=np.int32)
+            vmr = np.ascontiguousarray(np.stack([np.asarray(pr.vmr[s], dtype=np.float64) for s in sp])
+                                       if len(sp) else np.zeros((0, len(p))))
+            self.keep += [p, T, sp, vmr]
+            c = self.arr[k]
+            c.n_lev, c.n_species = len(p), len(sp)
+            c.pressure, c.temperature = dptr(p), dptr(T)
+            c.species = sp.ctypes.data_as(C.POINTER(C.c_int32))
+            c.vmr = dptr(vmr)
+            c.T_sfc = float("nan") if T_sfcs[k] is None else float(T_sfcs[k])
+            c.mu = float(mus[k])
+            c.eps_sfc = float(epss[k])
+
+
+def sounder_grid(s: Sounder) -> np.ndarray:
+    """Channel wavenumbers (sounder_grid, sounder.jl:135-137)."""
+    n_nu, n_ch = C.c_int64(), C.c_int64()
+    o = fm_options(with_ils=False, high_res_factor=1)
+    check(_lib.load().irs_grid_size(C.byref(s.c_struct()), C.byref(o), C.byref(n_nu), C.byref(n_ch)))
+    return np.array([s.nu_min + i * s.dnu for i in range(n_ch.value)])
+
+
+def _prepare(ctx, linelists, line_mixing):
+    for sp, ll in linelists.items():
+        y0 = line_mixing.y0 if (line_mixing is not None and int(sp) == 2) else None
+        ctx.upload_linelist(int(sp), ll, y0)
+    # species uploaded earlier but absent from this call must not contribute
+    for sp in list(ctx._lists):
+        if sp not in {int(s) for s in linelists}:
+            empty = HITRANLinelist(np.zeros(0, LINE_DTYPE))
+            ctx.upload_linelist(sp, empty)
+            del ctx._lists[sp]
+
+
+def forward_model_batch(profiles: Sequence[AtmosphericProfile], linelists, *, sounder: Sounder = None,
+                        geoms: Optional[Sequence[ViewingGeometry]] = None, T_sfcs=None, eps_sfcs=None,
+                        backend=None, line_mixing: Optional[VPYLineMixing] = None, **kw):
+    """forward_model for a batch of profiles sharing one sounder and options.
+
+    Returns (nu_out, R[n_prof, n_ch], BT[n_prof, n_ch])."""
+    ctx = backend or default_context()
+    sounder = sounder or IASIInstrument()
+    n = len(profiles)
+    geoms = geoms or [nadir_geometry()] * n
+    T_sfcs = T_sfcs if T_sfcs is not None else [None] * n
+    eps_sfcs = eps_sfcs if eps_sfcs is not None else [1.0] * n
+    _prepare(ctx, linelists, line_mixing)
+    o = fm_options(line_mixing=line_mixing, **kw)
+    batch = _ProfileBatch(profiles, T_sfcs, [g.mu for g in geoms], eps_sfcs)
+    s = sounder.c_struct()
+    nu_out = sounder_grid(sounder)
+    R = np.empty((n, len(nu_out)))
+    BT = np.empty((n, len(nu_out)))
+    check(ctx.lib.irs_forward_model_batch(ctx.h, batch.arr, n, C.byref(s), C.byref(o), dptr(R), dptr(BT)))
+    return nu_out, R, BT
+
+
+def forward_model(prof: AtmosphericProfile, linelists, *, sounder: Sounder = None,
+                  iasi: Sounder = None, geom: ViewingGeometry = None, T_sfc: Optional[float] = None,
+                  eps_sfc: float = 1.0, backend=None, line_mixing: Optional[VPYLineMixing] = None, **kw):
+    """forward_model (src/Sensor/sounder.jl:233-360) -> (nu, R, BT)."""
+    sounder = iasi if iasi is not None else sounder
+    nu, R, BT = forward_model_batch([prof], linelists, sounder=sounder, geoms=[geom or nadir_geometry()],
+                                    T_sfcs=[T_sfc], eps_sfcs=[eps_sfc], backend=backend,
+                                    line_mixing=line_mixing, **kw)
+    return nu, R[0], BT[0]
+
+
+iasi_forward_model = forward_model
+
+from .synthetic import afgl_atmosphere, synthetic_linelist  # noqa: E402,F401

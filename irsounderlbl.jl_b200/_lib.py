@@ -1,0 +1,114 @@
+"""ctypes binding of libirs_b200.so (the C ABI of include/irs_b200.h).
+
+The CUDA library is the only implementation: there is no CPU fallback, and a
+missing or unloadable library raises immediately.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+SO = HERE / "libirs_b200.so"
+
+IRS_WEIDEMAN, IRS_PSEUDOVOIGT, IRS_FULLFADDEEVA = 1, 2, 3
+IRS_FP64, IRS_MIXED = 0, 1
+
+# HITRANLine isbits layout (src/HITRAN/linelist.jl:20-31), 56 bytes
+LINE_DTYPE = np.dtype({
+    "names": ["mol_id", "iso_id", "wavenumber", "intensity", "a_coeff", "air_broad",
+              "self_broad", "lower_energy", "temp_depend", "pressure_shift"],
+    "formats": ["i1", "i1", "f8", "f8", "f8", "f4", "f4", "f8", "f4", "f4"],
+    "offsets": [0, 1, 8, 16, 24, 32, 36, 40, 48, 52],
+    "itemsize": 56,
+})
+
+
+class Sounder(C.Structure):
+    _fields_ = [("nu_min", C.c_double), ("nu_max", C.c_double), ("dnu", C.c_double),
+                ("n_channels", C.c_int64), ("opd_max", C.c_double), ("fwhm_gauss", C.c_double)]
+
+
+class FMOptions(C.Structure):
+    _fields_ = [("internal_dnu", C.c_double), ("high_res_factor", C.c_int32),
+                ("apply_continuum", C.c_int32), ("continua", C.c_int32), ("with_ils", C.c_int32),
+                ("apodization", C.c_int32), ("line_mixing", C.c_int32), ("T_method", C.c_int32),
+                ("source_function", C.c_int32), ("method", C.c_int32), ("precision", C.c_int32),
+                ("cutoff", C.c_double), ("lm_cutoff", C.c_double), ("dptmn", C.c_double),
+                ("x_far", C.c_double)]
+
+
+class Profile(C.Structure):
+    _fields_ = [("n_lev", C.c_int32), ("n_species", C.c_int32),
+                ("pressure", C.POINTER(C.c_double)), ("temperature", C.POINTER(C.c_double)),
+                ("species", C.POINTER(C.c_int32)), ("vmr", C.POINTER(C.c_double)),
+                ("T_sfc", C.c_double), ("mu", C.c_double), ("eps_sfc", C.c_double)]
+
+
+class StageTimes(C.Structure):
+    _fields_ = [("line_params_ms", C.c_double), ("line_sum_ms", C.c_double),
+                ("rte_ms", C.c_double), ("ils_ms", C.c_double), ("total_ms", C.c_double),
+                ("pairs", C.c_double), ("core_pairs", C.c_double), ("h2d_bytes", C.c_double),
+                ("d2h_bytes", C.c_double), ("launches", C.c_double)]
+
+
+# every symbol the header declares, with its ctypes signature
+_P = C.c_void_p
+_PD = C.POINTER(C.c_double)
+SIGNATURES = {
+    "irs_abi_version": ([], C.c_int),
+    "irs_last_error": ([], C.c_char_p),
+    "irs_create": ([C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "irs_destroy": ([_P], C.c_int),
+    "irs_set_partition_table": ([_P, C.c_int, C.c_int, C.c_int, C.c_int, _PD], C.c_int),
+    "irs_set_continuum_h2o": ([_P, C.c_int, _PD, _PD, _PD, _PD], C.c_int),
+    "irs_set_continuum_co2": ([_P, C.c_int, _PD, _PD, _PD, _PD], C.c_int),
+    "irs_upload_linelist": ([_P, C.c_int, _P, C.c_int64, _PD], C.c_int),
+    "irs_cross_sections": ([_P, C.c_int, _PD, C.c_int64, C.c_double, C.c_double, C.c_double,
+                            C.c_double, C.c_int, C.c_double, C.c_int, _PD], C.c_int),
+    "irs_forward_model_batch": ([_P, C.POINTER(Profile), C.c_int, C.POINTER(Sounder),
+                                 C.POINTER(FMOptions), _PD, _PD], C.c_int),
+    "irs_forward_model_batch_device": ([_P, C.POINTER(Profile), C.c_int, C.POINTER(Sounder),
+                                        C.POINTER(FMOptions), C.c_void_p, C.c_void_p, C.c_void_p],
+                                       C.c_int),
+    "irs_synchronize": ([_P], C.c_int),
+    "irs_last_stage_times": ([_P, C.POINTER(StageTimes)], C.c_int),
+    "irs_grid_size": ([C.POINTER(Sounder), C.POINTER(FMOptions), C.POINTER(C.c_int64),
+                       C.POINTER(C.c_int64)], C.c_int),
+}
+
+_lib = None
+
+
+def load(path: Path | str | None = None):
+    """Load libirs_b200.so (built in-tree by build.py); raise if it is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path or SO)
+    if not p.exists():
+        raise RuntimeError(f"{p} is missing: build it with `python irsounderlbl.jl_b200/build.py` "
+                           "(there is no CPU fallback)")
+    lib = C.CDLL(str(p))
+    for name, (args, res) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class IRSError(RuntimeError):
+    """Raised for a non-zero status of the C ABI (the reference raises ErrorException)."""
+
+
+def check(rc: int):
+    if rc != 0:
+        raise IRSError(f"[{rc}] " + (load().irs_last_error() or b"").decode())
+
+
+def dptr(a: np.ndarray):
+    return a.ctypes.data_as(_PD)

@@ -1,0 +1,583 @@
+// irs_b200.cu -- libirs_b200: context, uploads, stage orchestration and the C ABI
+// declared in include/irs_b200.h.  One translation unit holds every kernel so the
+// Faddeeva constants live in a single __constant__ block.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+#include "faddeeva.cuh"
+#include "irs_internal.h"
+#include "lineparams.cuh"
+#include "linesum.cuh"
+#include "rte_ils.cuh"
+
+namespace irs {
+const char* last_error();
+
+void* workspace(irs_ctx* ctx, const std::string& name, size_t bytes) {
+    DevBuf& b = ctx->work[name];
+    if (b.bytes >= bytes && b.p) return b.p;
+    if (b.p) IRS_CUDA(cudaFree(b.p));
+    b.p = nullptr;
+    b.bytes = 0;
+    const size_t want = std::max<size_t>(bytes, 256);
+    if (cudaMalloc(&b.p, want) != cudaSuccess) {
+        cudaGetLastError();
+        throw Error{IRS_E_NOMEM, "device allocation of " + std::to_string(want) + " bytes failed (" + name + ")"};
+    }
+    b.bytes = want;
+    return b.p;
+}
+
+template <typename T>
+static T* upload(irs_ctx* ctx, const std::string& name, const std::vector<T>& v) {
+    T* d = (T*)workspace(ctx, name, std::max<size_t>(v.size(), 1) * sizeof(T));
+    if (!v.empty()) IRS_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->n_h2d += (double)(v.size() * sizeof(T));
+    return d;
+}
+
+void upload_tables(irs_ctx* ctx) {
+    if (ctx->tips_dirty) {
+        const auto& tp = ctx->tables.tips;
+        int stride = 2;
+        for (auto& e : tp) stride = std::max<int>(stride, (int)e.second.second.size());
+        std::vector<double> q((size_t)std::max<size_t>(tp.size(), 1) * stride, 0.0);
+        std::vector<int> tmin(std::max<size_t>(tp.size(), 1), 0), n(std::max<size_t>(tp.size(), 1), 0);
+        ctx->tips_index.clear();
+        int idx = 0;
+        for (auto& e : tp) {
+            ctx->tips_index[e.first] = idx;
+            tmin[idx] = e.second.first;
+            n[idx] = (int)e.second.second.size();
+            std::copy(e.second.second.begin(), e.second.second.end(), q.begin() + (size_t)idx * stride);
+            ++idx;
+        }
+        ctx->n_tips = idx;
+        ctx->d_tips = upload(ctx, "tips_q", q);
+        ctx->d_tips_tmin = upload(ctx, "tips_tmin", tmin);
+        ctx->d_tips_n = upload(ctx, "tips_n", n);
+        ctx->tips_stride = stride;
+        ctx->tips_dirty = false;
+    }
+    if (ctx->cont_dirty) {
+        const Tables& t = ctx->tables;
+        std::vector<double> h;
+        h.insert(h.end(), t.h2o_nu.begin(), t.h2o_nu.end());
+        h.insert(h.end(), t.h2o_cs.begin(), t.h2o_cs.end());
+        h.insert(h.end(), t.h2o_cf.begin(), t.h2o_cf.end());
+        h.insert(h.end(), t.h2o_te.begin(), t.h2o_te.end());
+        std::vector<double> c;
+        c.insert(c.end(), t.co2_nu.begin(), t.co2_nu.end());
+        c.insert(c.end(), t.co2_s.begin(), t.co2_s.end());
+        c.insert(c.end(), t.co2_tdep.begin(), t.co2_tdep.end());
+        ctx->d_h2o = upload(ctx, "ckd_h2o", h);
+        ctx->d_co2 = upload(ctx, "ckd_co2", c);
+        ctx->n_h2o = (int)t.h2o_nu.size();
+        ctx->n_co2 = (int)t.co2_nu.size();
+        ctx->cont_dirty = false;
+    }
+}
+
+static TipsDev tips_dev(irs_ctx* ctx) {
+    TipsDev t;
+    t.q = ctx->d_tips;
+    t.tmin = ctx->d_tips_tmin;
+    t.n = ctx->d_tips_n;
+    t.stride = ctx->tips_stride;
+    return t;
+}
+
+static void check_launch(irs_ctx* ctx) {
+    ctx->n_launch += 1;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw Error{IRS_E_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e)};
+}
+
+static void validate_options(const irs_fm_options& o) {
+    IRS_REQUIRE(o.method >= 1 && o.method <= 3, "method must be 1 (Weideman), 2 (PseudoVoigt) or 3 (FullFaddeeva)");
+    IRS_REQUIRE(o.precision == IRS_FP64 || o.precision == IRS_MIXED, "precision must be IRS_FP64 or IRS_MIXED");
+    IRS_REQUIRE(o.cutoff > 0.0, "cutoff must be positive");
+    IRS_REQUIRE(o.apodization >= 0 && o.apodization <= 3, "unknown apodization");
+    IRS_REQUIRE(o.T_method == 0 || o.T_method == 1, "T_method must be :logp_at_pcg or :mass_weighted");
+    IRS_REQUIRE(o.source_function == 0 || o.source_function == 1, "source_function must be :cim or :toon");
+    IRS_REQUIRE(o.line_mixing == 0 || o.line_mixing == 1, "line_mixing must be 0 or 1 (VP_Y)");
+    if (o.line_mixing) {
+        IRS_REQUIRE(o.lm_cutoff == o.cutoff, "lm_cutoff must equal cutoff on this path");
+        IRS_REQUIRE(o.method == IRS_FULLFADDEEVA, "line mixing evaluates the Voigt part with FullFaddeeva");
+    }
+}
+
+// ------------------------------------------------------- the line-sum pipeline
+struct Plan {
+    std::vector<Segment> segs;
+    std::vector<int2> pl_segs;  // per (profile, layer): first segment, count
+    int n_prof = 0, L = 0;
+    int64_t slots = 0;
+    int64_t max_list = 0;
+};
+
+static std::vector<ListDev> list_descs(irs_ctx* ctx) {
+    std::vector<ListDev> v;
+    for (auto& l : ctx->lists) {
+        ListDev d;
+        d.nu = l.nu; d.S296 = l.S296; d.E = l.E; d.gair = l.gair; d.gself = l.gself;
+        d.nair = l.nair; d.delta = l.delta; d.y0 = l.y0; d.tips = l.tips;
+        d.n = l.n; d.mol = l.species; d.has_y0 = l.has_y0 ? 1 : 0;
+        v.push_back(d);
+    }
+    return v;
+}
+
+// Runs the line-parameter passes and the line sum for the plan; returns the
+// device tau buffer ([n_prof * L][n_nu], FP32 for mixed or FP64 for plain).
+static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n_nu, double grid0,
+                         double dnu_g, const irs_fm_options& o, int ev_mid) {
+    cudaStream_t st = ctx->stream;
+    const int nseg = (int)pl.segs.size();
+    std::vector<SegDev> sd(std::max(nseg, 1));
+    int64_t off = 0;
+    for (int s = 0; s < nseg; ++s) {
+        Segment& g = pl.segs[s];
+        g.out_off = off;
+        off += ctx->lists[g.list].n;
+        SegDev& d = sd[s];
+        d.T = g.T; d.p_atm = g.p_atm; d.vs = g.vmr_self; d.coef = g.coef; d.margin_g = g.margin_g;
+        d.off = g.out_off; d.list = g.list; d.flags = g.flags;
+        pl.max_list = std::max<int64_t>(pl.max_list, ctx->lists[g.list].n);
+    }
+    pl.slots = off;
+    SegDev* d_segs = upload(ctx, "segs", sd);
+    std::vector<ListDev> ld = list_descs(ctx);
+    ListDev* d_lists = upload(ctx, "list_descs", ld);
+    int2* d_pl = upload(ctx, "pl_segs", pl.pl_segs);
+    int* d_count = (int*)workspace(ctx, "seg_count", sizeof(int) * std::max(nseg, 1));
+    IRS_CUDA(cudaMemsetAsync(d_count, 0, sizeof(int) * std::max(nseg, 1), st));
+    unsigned long long* d_pairs = (unsigned long long*)workspace(ctx, "pair_counts", 16);
+    IRS_CUDA(cudaMemsetAsync(d_pairs, 0, 16, st));
+
+    const int mixed = o.precision == IRS_MIXED;
+    const size_t tau_elem = mixed ? sizeof(float) : sizeof(double);
+    void* d_tau = workspace(ctx, "tau", (size_t)pl.n_prof * pl.L * n_nu * tau_elem);
+    IRS_CUDA(cudaMemsetAsync(d_tau, 0, (size_t)pl.n_prof * pl.L * n_nu * tau_elem, st));
+    if (nseg == 0 || pl.slots == 0) {
+        IRS_CUDA(cudaEventRecord(ctx->ev[ev_mid], st));
+        return d_tau;
+    }
+    const int n_chunks = (int)((pl.max_list + kLpChunk - 1) / kLpChunk);
+    unsigned char* d_keep = (unsigned char*)workspace(ctx, "keep", (size_t)pl.slots);
+    int* d_chunk = (int*)workspace(ctx, "chunk_count", sizeof(int) * (size_t)nseg * n_chunks);
+    LpConfig cfg;
+    cfg.cutoff = o.cutoff; cfg.x_far = o.x_far; cfg.dptmn = o.dptmn;
+    cfg.grid0 = grid0; cfg.dnu_g = dnu_g; cfg.method = o.method;
+    const TipsDev tp = tips_dev(ctx);
+    dim3 g1(n_chunks, nseg);
+    lp_keep_kernel<<<g1, kLpThreads, 0, st>>>(d_segs, d_lists, tp, cfg, d_keep, d_chunk, n_chunks);
+    check_launch(ctx);
+    LpOutF64 o64{};
+    LpOutMixed om{};
+    const size_t S = (size_t)pl.slots;
+    if (!mixed) {
+        double* base = (double*)workspace(ctx, "lp64", S * 6 * sizeof(double));
+        o64.nu0 = base; o64.f = base + S; o64.y = base + 2 * S; o64.Sn = base + 3 * S;
+        o64.Hc = base + 4 * S; o64.YSn = base + 5 * S;
+        lp_write_kernel<0><<<g1, kLpThreads, 0, st>>>(d_segs, d_lists, tp, cfg, d_keep, d_chunk, n_chunks,
+                                                      d_count, o64, om, d_pairs);
+    } else {
+        char* base = (char*)workspace(ctx, "lpmx", S * (8 + 8 + 16 + 16 + 8));
+        om.V = (double*)base;
+        om.U = (double*)(base + S * 8);
+        om.p0 = (float4*)(base + S * 16);
+        om.p1 = (float4*)(base + S * 32);
+        om.p2 = (float2*)(base + S * 48);
+        lp_write_kernel<1><<<g1, kLpThreads, 0, st>>>(d_segs, d_lists, tp, cfg, d_keep, d_chunk, n_chunks,
+                                                      d_count, o64, om, d_pairs);
+    }
+    check_launch(ctx);
+    IRS_CUDA(cudaEventRecord(ctx->ev[ev_mid], st));
+    const int npl = pl.n_prof * pl.L;
+    if (!mixed) {
+        dim3 g2((unsigned)((n_nu + 255) / 256), npl);
+        if (o.method == 1)
+            linesum_f64_kernel<1><<<g2, 256, 0, st>>>(d_segs, d_count, d_pl, o64, d_grid, n_nu, o.cutoff, o.x_far, (double*)d_tau);
+        else if (o.method == 2)
+            linesum_f64_kernel<2><<<g2, 256, 0, st>>>(d_segs, d_count, d_pl, o64, d_grid, n_nu, o.cutoff, o.x_far, (double*)d_tau);
+        else
+            linesum_f64_kernel<3><<<g2, 256, 0, st>>>(d_segs, d_count, d_pl, o64, d_grid, n_nu, o.cutoff, o.x_far, (double*)d_tau);
+    } else {
+        dim3 g2((unsigned)((n_nu + kMxStrip - 1) / kMxStrip), npl);
+        const float cut_g = (float)(o.cutoff / dnu_g);
+        if (o.method == 1)
+            linesum_mixed_kernel<1><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau);
+        else if (o.method == 2)
+            linesum_mixed_kernel<2><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau);
+        else
+            linesum_mixed_kernel<3><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau);
+    }
+    check_launch(ctx);
+    return d_tau;
+}
+
+static void ensure_ils(irs_ctx* ctx, double dnu, double opd, double fwhm, int apod) {
+    const double key[4] = {dnu, opd, fwhm, (double)apod};
+    if (std::memcmp(key, ctx->ils_key, sizeof key) == 0) return;
+    const int64_t n_half = (int64_t)std::ceil(16.0 / dnu);
+    const int64_t n = 2 * n_half + 1;
+    double* k = (double*)workspace(ctx, "ils", n * sizeof(double));
+    ils_taps_kernel<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(dnu, opd, fwhm, apod, n_half, k);
+    check_launch(ctx);
+    ils_normalise_kernel<<<1, 1024, 0, ctx->stream>>>(k, n, dnu);
+    check_launch(ctx);
+    std::memcpy(ctx->ils_key, key, sizeof key);
+    ctx->ils_n = n;
+}
+
+static void forward_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder& s,
+                           const irs_fm_options& o, double* d_R, double* d_BT) {
+    IRS_REQUIRE(n_prof >= 1 && profs, "need at least one profile");
+    validate_options(o);
+    ctx->n_h2d = ctx->n_d2h = ctx->n_launch = 0;
+    upload_tables(ctx);
+    cudaStream_t st = ctx->stream;
+    const InternalGrid ig = internal_grid(s, o);
+    const GridSpec ch = make_grid(s.nu_min, s.nu_max, s.dnu);
+    const int64_t n_nu = ig.g.n;
+    const int L = profs[0].n_lev - 1;
+    Plan pl;
+    pl.n_prof = n_prof;
+    pl.L = L;
+    std::vector<int> list_sp;
+    std::vector<double> list_shift;
+    for (auto& l : ctx->lists) {  // empty lists produce no segments
+        list_sp.push_back(l.n > 0 ? l.species : -1);
+        list_shift.push_back(l.max_abs_shift);
+    }
+    std::vector<LayerRT> lrt;
+    std::vector<ProfileRT> prt(n_prof);
+    for (int p = 0; p < n_prof; ++p) {
+        IRS_REQUIRE(profs[p].n_lev == L + 1, "all profiles of a batch must have the same number of levels");
+        const size_t before = pl.segs.size();
+        layer_setup(profs[p], p, o, list_sp, list_shift, ig.dnu_hi, pl.segs, lrt, prt[p]);
+        (void)before;
+    }
+    // per (profile, layer) segment ranges (segments are emitted in p, layer order)
+    pl.pl_segs.assign((size_t)n_prof * L, make_int2(0, 0));
+    for (size_t i = 0; i < pl.segs.size(); ++i) {
+        const int key = pl.segs[i].prof * L + pl.segs[i].layer;
+        if (pl.pl_segs[key].y == 0) pl.pl_segs[key].x = (int)i;
+        pl.pl_segs[key].y++;
+    }
+    IRS_CUDA(cudaEventRecord(ctx->ev[0], st));
+    double* d_grid = (double*)workspace(ctx, "grid", n_nu * sizeof(double));
+    grid_values_kernel<<<(unsigned)((n_nu + 255) / 256), 256, 0, st>>>(to_dev(ig.g), d_grid);
+    check_launch(ctx);
+    if (o.with_ils) ensure_ils(ctx, ig.dnu_hi, s.opd_max, s.fwhm_gauss, o.apodization);
+    void* d_tau = run_linesum(ctx, pl, d_grid, n_nu, ig.g.at(0), ig.dnu_hi, o, 1);
+    IRS_CUDA(cudaEventRecord(ctx->ev[2], st));
+    LayerRT* d_lrt = upload(ctx, "lrt", lrt);
+    ProfileRT* d_prt = upload(ctx, "prt", prt);
+    double* d_I = (double*)workspace(ctx, "I", (size_t)n_prof * n_nu * sizeof(double));
+    ContDev cd;
+    cd.h2o = ctx->d_h2o; cd.co2 = ctx->d_co2; cd.n_h2o = ctx->n_h2o; cd.n_co2 = ctx->n_co2;
+    cd.mask = 0;
+    if (o.apply_continuum) {
+        if ((o.continua & 1) && ctx->n_h2o > 1) cd.mask |= 1;
+        if ((o.continua & 2) && ctx->n_co2 > 1) cd.mask |= 2;
+    }
+    dim3 g3((unsigned)((n_nu + 255) / 256), n_prof);
+    if (o.precision == IRS_MIXED)
+        rte_kernel<float><<<g3, 256, 0, st>>>((const float*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
+    else
+        rte_kernel<double><<<g3, 256, 0, st>>>((const double*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
+    check_launch(ctx);
+    IRS_CUDA(cudaEventRecord(ctx->ev[3], st));
+    const double* d_kern = o.with_ils ? (const double*)ctx->work["ils"].p : nullptr;
+    dim3 g4((unsigned)((ch.n * 32 + 255) / 256), n_prof);
+    ils_bt_kernel<<<g4, 256, 0, st>>>(d_I, n_nu, d_kern, o.with_ils ? ctx->ils_n : 0, ig.dnu_hi, to_dev(ig.g),
+                                       to_dev(ch), o.with_ils, d_R, d_BT);
+    check_launch(ctx);
+    IRS_CUDA(cudaEventRecord(ctx->ev[4], st));
+}
+
+static void collect_times(irs_ctx* ctx) {
+    float a = 0, b = 0, c = 0, d = 0;
+    IRS_CUDA(cudaEventSynchronize(ctx->ev[4]));
+    IRS_CUDA(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]));
+    IRS_CUDA(cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]));
+    IRS_CUDA(cudaEventElapsedTime(&c, ctx->ev[2], ctx->ev[3]));
+    IRS_CUDA(cudaEventElapsedTime(&d, ctx->ev[3], ctx->ev[4]));
+    ctx->last.line_params_ms = a;
+    ctx->last.line_sum_ms = b;
+    ctx->last.rte_ms = c;
+    ctx->last.ils_ms = d;
+    ctx->last.total_ms = a + b + c + d;
+    unsigned long long pc[2] = {0, 0};
+    DevBuf& pb = ctx->work["pair_counts"];
+    if (pb.p) IRS_CUDA(cudaMemcpy(pc, pb.p, 16, cudaMemcpyDeviceToHost));
+    ctx->last.pairs = (double)pc[0];
+    ctx->last.core_pairs = (double)pc[1];
+    ctx->last.h2d_bytes = ctx->n_h2d;
+    ctx->last.d2h_bytes = ctx->n_d2h;
+    ctx->last.launches = ctx->n_launch;
+}
+
+}  // namespace irs
+
+using namespace irs;
+
+#define IRS_API_BEGIN try {
+#define IRS_API_END                                  \
+    return IRS_OK;                                   \
+    }                                                \
+    catch (const Error& e) {                         \
+        set_error(e.msg);                            \
+        return e.code;                               \
+    }                                                \
+    catch (const std::exception& e) {                \
+        set_error(std::string("exception: ") + e.what()); \
+        return IRS_E_STATE;                          \
+    }
+
+extern "C" {
+
+int irs_abi_version(void) { return IRS_ABI_VERSION; }
+const char* irs_last_error(void) { return irs::last_error(); }
+
+int irs_create(int device, irs_ctx** out) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(out, "out is NULL");
+    *out = nullptr;
+    int n = 0;
+    IRS_CUDA(cudaGetDeviceCount(&n));
+    IRS_REQUIRE(device >= 0 && device < n, "no such CUDA device");
+    IRS_CUDA(cudaSetDevice(device));
+    std::unique_ptr<irs_ctx> c(new irs_ctx);
+    c->device = device;
+    IRS_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (auto& e : c->ev) IRS_CUDA(cudaEventCreate(&e));
+    FaddeevaConsts fc;
+    compute_faddeeva_consts(&fc);
+    IRS_CUDA(cudaMemcpyToSymbol(c_fad, &fc, sizeof fc));
+    *out = c.release();
+    IRS_API_END
+}
+
+int irs_destroy(irs_ctx* ctx) {
+    IRS_API_BEGIN
+    if (!ctx) return IRS_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& l : ctx->lists) {
+        cudaFree(l.nu);  // one allocation per list (see irs_upload_linelist)
+    }
+    for (auto& w : ctx->work) if (w.second.p) cudaFree(w.second.p);
+    for (auto& e : ctx->ev) cudaEventDestroy(e);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    IRS_API_END
+}
+
+int irs_set_partition_table(irs_ctx* ctx, int mol, int iso, int t_min, int n, const double* q) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && q && n >= 2, "invalid partition table");
+    ctx->tables.tips[{mol, iso}] = {t_min, std::vector<double>(q, q + n)};
+    ctx->tips_dirty = true;
+    IRS_API_END
+}
+
+int irs_set_continuum_h2o(irs_ctx* ctx, int n, const double* nu, const double* cs, const double* cf,
+                          const double* te) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && n >= 2 && nu && cs && cf && te, "invalid H2O continuum table");
+    for (int i = 1; i < n; ++i) IRS_REQUIRE(nu[i] > nu[i - 1], "continuum knots must increase");
+    Tables& t = ctx->tables;
+    t.h2o_nu.assign(nu, nu + n); t.h2o_cs.assign(cs, cs + n); t.h2o_cf.assign(cf, cf + n); t.h2o_te.assign(te, te + n);
+    ctx->cont_dirty = true;
+    IRS_API_END
+}
+
+int irs_set_continuum_co2(irs_ctx* ctx, int n, const double* nu, const double* s, const double* xf,
+                          const double* td) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && n >= 2 && nu && s && xf && td, "invalid CO2 continuum table");
+    for (int i = 1; i < n; ++i) IRS_REQUIRE(nu[i] > nu[i - 1], "continuum knots must increase");
+    Tables& t = ctx->tables;
+    t.co2_nu.assign(nu, nu + n);
+    t.co2_s.resize(n);
+    for (int i = 0; i < n; ++i) t.co2_s[i] = s[i] * xf[i];  // continuum.jl:90
+    t.co2_tdep.assign(td, td + n);
+    ctx->cont_dirty = true;
+    IRS_API_END
+}
+
+int irs_upload_linelist(irs_ctx* ctx, int species, const irs_line* lines, int64_t n, const double* y0) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && n >= 0 && (n == 0 || lines), "invalid line list");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    upload_tables(ctx);
+    // HITRANLinelist sorts by wavenumber (linelist.jl:51-56); keep that order.
+    std::vector<int64_t> ord(n);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) { return lines[a].wavenumber < lines[b].wavenumber; });
+    std::vector<double> h((size_t)n * 8);
+    std::vector<int> tips(n);
+    double max_shift = 0.0;
+    const double d_self = species == 1 ? 0.002 : (species == 2 ? -0.003 : 0.0);
+    for (int64_t k = 0; k < n; ++k) {
+        const irs_line& l = lines[ord[k]];
+        IRS_REQUIRE(l.mol_id == species, "line mol_id does not match the species of the list");
+        h[0 * n + k] = l.wavenumber;
+        h[1 * n + k] = l.intensity;
+        h[2 * n + k] = l.lower_energy;
+        h[3 * n + k] = (double)l.air_broad;
+        h[4 * n + k] = (double)l.self_broad;
+        h[5 * n + k] = (double)l.temp_depend;
+        h[6 * n + k] = (double)l.pressure_shift;
+        h[7 * n + k] = y0 ? y0[ord[k]] : 0.0;
+        auto it = ctx->tips_index.find({(int)l.mol_id, (int)l.iso_id});
+        tips[k] = it == ctx->tips_index.end() ? -1 : it->second;
+        max_shift = std::max(max_shift, std::fabs((double)l.pressure_shift) + std::fabs(d_self));
+    }
+    // replace an existing list of this species
+    int slot = -1;
+    for (size_t i = 0; i < ctx->lists.size(); ++i) if (ctx->lists[i].species == species) slot = (int)i;
+    if (slot >= 0) {
+        cudaFree(ctx->lists[slot].nu);
+        ctx->lists.erase(ctx->lists.begin() + slot);
+    }
+    DevLineList d;
+    d.species = species;
+    d.n = n;
+    d.has_y0 = y0 != nullptr;
+    d.max_abs_shift = max_shift;
+    const size_t bytes = (size_t)std::max<int64_t>(n, 1) * (8 * sizeof(double) + sizeof(int));
+    char* base = nullptr;
+    if (cudaMalloc((void**)&base, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        throw Error{IRS_E_NOMEM, "device allocation for the line list failed"};
+    }
+    double* b = (double*)base;
+    const size_t N = (size_t)std::max<int64_t>(n, 1);
+    d.nu = b; d.S296 = b + N; d.E = b + 2 * N; d.gair = b + 3 * N; d.gself = b + 4 * N;
+    d.nair = b + 5 * N; d.delta = b + 6 * N; d.y0 = b + 7 * N;
+    d.tips = (int*)(b + 8 * N);
+    if (n > 0) {
+        for (int f = 0; f < 8; ++f)
+            IRS_CUDA(cudaMemcpy(b + f * N, h.data() + (size_t)f * n, n * sizeof(double), cudaMemcpyHostToDevice));
+        IRS_CUDA(cudaMemcpy(d.tips, tips.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    ctx->lists.push_back(d);
+    std::sort(ctx->lists.begin(), ctx->lists.end(), [](const DevLineList& a, const DevLineList& b) { return a.species < b.species; });
+    IRS_API_END
+}
+
+int irs_cross_sections(irs_ctx* ctx, int species, const double* grid, int64_t n_nu, double T, double p_atm,
+                       double vmr_self, double cutoff, int method, double x_far, int precision, double* sigma) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && grid && sigma && n_nu >= 1, "invalid arguments");
+    IRS_REQUIRE(T > 0 && p_atm >= 0, "T must be positive and p_atm non-negative");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    int li = -1;
+    for (size_t i = 0; i < ctx->lists.size(); ++i) if (ctx->lists[i].species == species) li = (int)i;
+    IRS_REQUIRE(li >= 0, "no line list uploaded for this species");
+    irs_fm_options o{};
+    o.method = method; o.precision = precision; o.cutoff = cutoff; o.lm_cutoff = cutoff; o.x_far = x_far;
+    o.dptmn = 0.0;
+    validate_options(o);
+    upload_tables(ctx);
+    double dnu_g = n_nu > 1 ? (grid[n_nu - 1] - grid[0]) / double(n_nu - 1) : 1.0;
+    if (precision == IRS_MIXED) {
+        IRS_REQUIRE(n_nu > 1 && dnu_g > 0, "the mixed kernel needs a uniform increasing grid");
+        for (int64_t i = 0; i < n_nu; ++i)
+            IRS_REQUIRE(std::fabs(grid[i] - (grid[0] + double(i) * dnu_g)) <= 1e-9 * std::max(1.0, std::fabs(grid[i])),
+                        "the mixed kernel needs a uniform grid");
+    }
+    Plan pl;
+    pl.n_prof = 1;
+    pl.L = 1;
+    Segment s{};
+    s.T = T; s.p_atm = p_atm; s.vmr_self = vmr_self; s.coef = 1.0; s.list = li; s.flags = 0;
+    s.margin_g = ctx->lists[li].max_abs_shift * p_atm / dnu_g + 2.0;
+    pl.segs.push_back(s);
+    pl.pl_segs.push_back(make_int2(0, 1));
+    cudaStream_t st = ctx->stream;
+    IRS_CUDA(cudaEventRecord(ctx->ev[0], st));
+    double* d_grid = (double*)workspace(ctx, "grid", n_nu * sizeof(double));
+    IRS_CUDA(cudaMemcpyAsync(d_grid, grid, n_nu * sizeof(double), cudaMemcpyHostToDevice, st));
+    void* d_tau = run_linesum(ctx, pl, d_grid, n_nu, grid[0], dnu_g, o, 1);
+    IRS_CUDA(cudaEventRecord(ctx->ev[2], st));
+    if (precision == IRS_MIXED) {
+        std::vector<float> tmp(n_nu);
+        IRS_CUDA(cudaMemcpyAsync(tmp.data(), d_tau, n_nu * sizeof(float), cudaMemcpyDeviceToHost, st));
+        IRS_CUDA(cudaStreamSynchronize(st));
+        for (int64_t i = 0; i < n_nu; ++i) sigma[i] = tmp[i];
+    } else {
+        IRS_CUDA(cudaMemcpyAsync(sigma, d_tau, n_nu * sizeof(double), cudaMemcpyDeviceToHost, st));
+        IRS_CUDA(cudaStreamSynchronize(st));
+    }
+    IRS_API_END
+}
+
+int irs_forward_model_batch_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder* s,
+                                   const irs_fm_options* o, double* d_R, double* d_BT, void* stream) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && s && o && d_R && d_BT, "invalid arguments");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t user = (cudaStream_t)stream;
+    if (user) {  // order our stream after the caller's work, and the caller's after ours
+        IRS_CUDA(cudaEventRecord(ctx->ev[5], user));
+        IRS_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev[5], 0));
+    }
+    forward_device(ctx, profs, n_prof, *s, *o, d_R, d_BT);
+    if (user) {
+        IRS_CUDA(cudaEventRecord(ctx->ev[6], ctx->stream));
+        IRS_CUDA(cudaStreamWaitEvent(user, ctx->ev[6], 0));
+    }
+    IRS_API_END
+}
+
+int irs_forward_model_batch(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder* s,
+                            const irs_fm_options* o, double* R, double* BT) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && s && o && R && BT, "invalid arguments");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    const GridSpec ch = make_grid(s->nu_min, s->nu_max, s->dnu);
+    const size_t n = (size_t)n_prof * ch.n;
+    double* d_out = (double*)workspace(ctx, "fm_out", 2 * n * sizeof(double));
+    forward_device(ctx, profs, n_prof, *s, *o, d_out, d_out + n);
+    IRS_CUDA(cudaMemcpyAsync(R, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    IRS_CUDA(cudaMemcpyAsync(BT, d_out + n, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->n_d2h += 2.0 * n * sizeof(double);
+    IRS_CUDA(cudaStreamSynchronize(ctx->stream));
+    collect_times(ctx);
+    IRS_API_END
+}
+
+int irs_synchronize(irs_ctx* ctx) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx, "ctx is NULL");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    IRS_CUDA(cudaStreamSynchronize(ctx->stream));
+    collect_times(ctx);
+    IRS_API_END
+}
+
+int irs_last_stage_times(irs_ctx* ctx, irs_stage_times* out) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && out, "invalid arguments");
+    *out = ctx->last;
+    IRS_API_END
+}
+
+int irs_grid_size(const irs_sounder* s, const irs_fm_options* o, int64_t* n_nu, int64_t* n_ch) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(s && o && n_nu && n_ch, "invalid arguments");
+    *n_nu = internal_grid(*s, *o).g.n;
+    *n_ch = make_grid(s->nu_min, s->nu_max, s->dnu).n;
+    IRS_API_END
+}
+
+}  // extern "C"

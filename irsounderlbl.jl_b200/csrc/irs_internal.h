@@ -1,0 +1,150 @@
+// irs_internal.h -- shared declarations of libirs_b200 (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/irs_b200.h"
+
+namespace irs {
+
+// ------------------------------------------------------------------ errors
+void set_error(const std::string& msg);
+struct Error {
+    int code;
+    std::string msg;
+};
+#define IRS_CUDA(call)                                                                 \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            throw ::irs::Error{IRS_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+#define IRS_REQUIRE(cond, msg)                                        \
+    do {                                                              \
+        if (!(cond)) throw ::irs::Error{IRS_E_ARG, std::string(msg)}; \
+    } while (0)
+
+// ------------------------------------------------------------------ grids
+// Julia's float range a:s:b (src/Utils/wavenumber_grid.jl:23-26): start, step and
+// stop are rationalised (n/den) when they have exact small-denominator forms and the
+// elements are then (a_n + i s_n)/den, correctly rounded.
+struct GridSpec {
+    int64_t n = 0;
+    int64_t den = 0;  // 0: literal start + i*step
+    double a_n = 0, s_n = 0, start = 0, step = 0;
+    double at(int64_t i) const { return den ? (a_n + double(i) * s_n) / double(den) : start + double(i) * step; }
+};
+GridSpec make_grid(double a, double b, double s);
+
+// forward_model's internal monochromatic grid (src/Sensor/sounder.jl:155-161, 263-271)
+struct InternalGrid {
+    GridSpec g;
+    double dnu_hi;
+    int64_t hrf;
+};
+InternalGrid internal_grid(const irs_sounder& s, const irs_fm_options& o);
+
+// ------------------------------------------------------------ atmosphere
+// One (profile, layer, species) line-sum segment: Curtis-Godson state of the
+// layer for that species (src/Sensor/sounder.jl:283-307).
+struct Segment {
+    double T;         // T_cg (K)
+    double p_atm;     // p_cg / 1013.25
+    double vmr_self;  // vmr_cg for H2O, else 0
+    double coef;      // vmr_cg * dp * 2.1209e22 (molecules/cm^2)
+    double margin_g;  // window margin (grid units) covering the pressure shifts
+    int64_t out_off;  // first slot of this segment in the per-line parameter arrays
+    int32_t list;     // line-list index in the context
+    int32_t flags;    // SEG_DPTMIN | SEG_LM
+    int32_t prof, layer;
+};
+enum { SEG_DPTMIN = 1, SEG_LM = 2 };
+
+// Per (profile, layer) inputs of the fused RTE/continuum kernel.
+struct LayerRT {
+    double T_ave;     // cg_temperature_mass (TBAR), layers.jl:93-106
+    double T_top;     // T_levels[k+1]
+    double T_bot;     // T_levels[k]
+    double p_mid, T_mid, dz_cm;
+    double vmr_h2o, vmr_co2;  // mid-layer (continua)
+};
+struct ProfileRT {
+    double T_sfc, mu, eps;
+};
+
+// layers.jl:133-178 + sounder.jl:283-336 for one profile; appends to the vectors.
+void layer_setup(const irs_profile& prof, int prof_index, const irs_fm_options& o,
+                 const std::vector<int>& list_species, const std::vector<double>& list_max_shift,
+                 double dnu_grid, std::vector<Segment>& segs, std::vector<LayerRT>& lrt,
+                 ProfileRT& prt);
+
+// ------------------------------------------------------------ device data
+struct DevLineList {
+    int species = 0;
+    int64_t n = 0;
+    double max_abs_shift = 0;  // max |delta_air| + |delta_self| (cm^-1/atm)
+    bool has_y0 = false;
+    // SoA, sorted by wavenumber
+    double *nu = nullptr, *S296 = nullptr, *E = nullptr, *gair = nullptr, *gself = nullptr,
+           *nair = nullptr, *delta = nullptr, *y0 = nullptr;
+    int* tips = nullptr;  // table index or -1
+};
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+// Per-line parameter arrays for the line sum (one slot per (segment, line)).
+struct LineParamsF64 {  // plain FP64 kernel; PseudoVoigt reuses f=gV, y=eta, Sn=S, Hc=base
+    double *nu0, *f, *y, *Sn, *Hc, *YSn;
+};
+struct LineParamsMixed {  // FP32 kernel, grid units relative to the grid start
+    double* V;            // unshifted centre (sorted key)
+    double* U;            // shifted centre
+    float4* p0;           // b2, a, c1, c0        (PV: gV2, aPV, c1, c0)
+    float4* p1;           // dfar2, An, fx, y     (PV: kPV, gPV, -, -)
+    float2* p2;           // g, Yw (dispersive line mixing)
+};
+
+struct Tables {
+    std::map<std::pair<int, int>, std::pair<int, std::vector<double>>> tips;  // (tmin, q)
+    std::vector<double> h2o_nu, h2o_cs, h2o_cf, h2o_te;
+    std::vector<double> co2_nu, co2_s, co2_tdep;  // S already multiplied by xfac
+};
+
+}  // namespace irs
+
+struct irs_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[8] = {};
+    irs::Tables tables;
+    bool tips_dirty = true, cont_dirty = true;
+    // device copies of tables
+    double* d_tips = nullptr;  // [n_tab][331]
+    int* d_tips_tmin = nullptr;
+    int* d_tips_n = nullptr;
+    int n_tips = 0;
+    int tips_stride = 2;
+    std::map<std::pair<int, int>, int> tips_index;
+    double *d_h2o = nullptr, *d_co2 = nullptr;  // packed tables
+    int n_h2o = 0, n_co2 = 0;
+    std::vector<irs::DevLineList> lists;
+    std::map<std::string, irs::DevBuf> work;  // named growable workspaces
+    irs_stage_times last{};
+    double n_h2d = 0, n_d2h = 0, n_launch = 0;  // counters of the current call
+    // cached ILS kernel
+    double ils_key[4] = {-1, -1, -1, -1};
+    int64_t ils_n = 0;
+};
+
+namespace irs {
+void* workspace(irs_ctx* ctx, const std::string& name, size_t bytes);
+void upload_tables(irs_ctx* ctx);
+}

@@ -1,0 +1,274 @@
+// lineparams.cuh -- per-(profile, layer, species) line parameters, computed once
+// into SoA buffers, with DPTMIN rejection and compaction.
+//
+// Restates, per line (FP64, as the reference):
+//   pressure_shift                 src/HITRAN/broadening.jl:156-160
+//   pressure_broadened_width       broadening.jl:40-53
+//   temperature_scaled_intensity   broadening.jl:89-99, Q_ratio partition.jl:10-47
+//   Doppler factor, y, Snorm, pedestal H(cutoff)   src/CrossSections/voigt.jl:402-454
+//   DPTMIN peak test               voigt.jl:333-355
+//   VP_Y dispersive weight         line_mixing.jl:1193-1220 with Y(T) = y0 (296/T)^0.75
+//
+// Two passes over (segment, chunk of kLpChunk lines): pass A decides keep/reject
+// and counts per chunk; pass B recomputes the parameters of the kept lines and
+// writes them compacted (order preserved), so the line sums only see kept lines.
+#pragma once
+#include "faddeeva.cuh"
+
+namespace irs {
+
+constexpr int kLpThreads = 256;
+constexpr int kLpPerThread = 8;
+constexpr int kLpChunk = kLpThreads * kLpPerThread;  // lines per CTA
+
+struct ListDev {
+    const double *nu, *S296, *E, *gair, *gself, *nair, *delta, *y0;
+    const int* tips;
+    long long n;
+    int mol;
+    int has_y0;
+};
+struct SegDev {
+    double T, p_atm, vs, coef, margin_g;
+    long long off;
+    int list, flags;
+};
+struct TipsDev {
+    const double* q;
+    const int* tmin;
+    const int* n;
+    int stride;
+};
+struct LpConfig {
+    double cutoff, x_far, dptmn;
+    double grid0, dnu_g;  // grid start and spacing (mixed parameters are in grid units)
+    int method;           // 1 Weideman, 2 PseudoVoigt, 3 FullFaddeeva
+};
+
+__device__ __forceinline__ double tips_lookup(const TipsDev& t, int idx, double T) {
+    const double* q = t.q + (size_t)idx * t.stride;
+    const int n = t.n[idx];
+    int lo = (int)floor(T) - t.tmin[idx] + 1;  // 1-based, partition.jl:10-18
+    int hi = lo + 1;
+    lo = min(max(lo, 1), n);
+    hi = min(max(hi, 1), n);
+    const double fr = T - floor(T);
+    return q[lo - 1] * (1.0 - fr) + q[hi - 1] * fr;
+}
+
+__device__ __forceinline__ double mol_mass(int mol) {  // broadening.jl:131-148
+    switch (mol) {
+        case 1: return 18.010; case 2: return 44.010; case 3: return 47.998;
+        case 4: return 44.013; case 5: return 28.010; case 6: return 16.043;
+        case 7: return 31.999; case 8: return 34.015; case 9: return 64.065;
+        case 10: return 36.461; case 11: return 17.031; default: return 30.0;
+    }
+}
+
+struct LinePhys {
+    double nu0s, S, gl, gd;
+};
+
+__device__ __forceinline__ LinePhys line_phys(const ListDev& L, long long j, const TipsDev& tp,
+                                              double T, double p, double vs) {
+    const int mol = L.mol;
+    const double nu = L.nu[j];
+    const double n_air = L.nair[j];
+    const double n_self = mol == 1 ? 0.95 : (mol == 2 ? 0.75 : n_air);        // broadening.jl:17-20
+    const double d_self = mol == 1 ? 0.002 : (mol == 2 ? -0.003 : 0.0);        // :21-24
+    const double tr = 296.0 / T;
+    LinePhys o;
+    o.gl = pow(tr, n_air) * L.gair[j] * (1.0 - vs) * p + pow(tr, n_self) * L.gself[j] * vs * p;
+    o.gd = nu * 3.58126e-7 * sqrt(T / mol_mass(mol));
+    const int ti = L.tips[j];
+    const double Qr = ti >= 0 ? tips_lookup(tp, ti, 296.0) / tips_lookup(tp, ti, T) : 296.0 / T;
+    const double c2 = 1.4387752;
+    const double stim = (1.0 - exp(-c2 * nu / T)) / (1.0 - exp(-c2 * nu / 296.0));
+    const double boltz = exp(-c2 * L.E[j] * (1.0 / T - 1.0 / 296.0));
+    o.S = L.S296[j] * Qr * boltz * stim;
+    o.nu0s = nu + (L.delta[j] * (1.0 - vs) + d_self * vs) * p;
+    return o;
+}
+
+// Pass A: keep flags and per-chunk kept counts.  grid = (chunks, segments)
+__global__ void __launch_bounds__(kLpThreads) lp_keep_kernel(
+    const SegDev* __restrict__ segs, const ListDev* __restrict__ lists, TipsDev tp, LpConfig cfg,
+    unsigned char* __restrict__ keep, int* __restrict__ chunk_count, int n_chunks_max) {
+    const SegDev sg = segs[blockIdx.y];
+    const ListDev L = lists[sg.list];
+    const long long base = (long long)blockIdx.x * kLpChunk;
+    __shared__ int s_cnt;
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    if (base >= L.n) {
+        if (threadIdx.x == 0) chunk_count[(size_t)blockIdx.y * n_chunks_max + blockIdx.x] = 0;
+        return;
+    }
+    int cnt = 0;
+    for (int r = 0; r < kLpPerThread; ++r) {
+        const long long j = base + r * kLpThreads + threadIdx.x;
+        if (j >= L.n) break;
+        bool k = true;
+        if (sg.flags & 1) {  // DPTMIN, voigt.jl:340-349
+            const LinePhys ph = line_phys(L, j, tp, sg.T, sg.p_atm, sg.vs);
+            const double gd = fmax(ph.gd, 1e-10);
+            const double f = kSqrtLn2 / gd;
+            const double peak = (ph.S * f * kInvSqrtPi) * erfcx64(ph.gl * f);
+            k = peak * sg.coef > cfg.dptmn;
+        }
+        keep[sg.off + j] = k ? 1 : 0;
+        cnt += k;
+    }
+    atomicAdd(&s_cnt, cnt);
+    __syncthreads();
+    if (threadIdx.x == 0) chunk_count[(size_t)blockIdx.y * n_chunks_max + blockIdx.x] = s_cnt;
+}
+
+struct LpOutF64 {
+    double *nu0, *f, *y, *Sn, *Hc, *YSn;
+};
+struct LpOutMixed {
+    double *V, *U;
+    float4 *p0, *p1;
+    float2* p2;
+};
+
+// Pass B: compacted parameters.  PREC 0 -> FP64 arrays, 1 -> mixed arrays.
+template <int PREC>
+__global__ void __launch_bounds__(kLpThreads) lp_write_kernel(
+    const SegDev* __restrict__ segs, const ListDev* __restrict__ lists, TipsDev tp, LpConfig cfg,
+    const unsigned char* __restrict__ keep, const int* __restrict__ chunk_count, int n_chunks_max,
+    int* __restrict__ seg_count, LpOutF64 o64, LpOutMixed om, unsigned long long* __restrict__ pair_counts) {
+    const SegDev sg = segs[blockIdx.y];
+    const ListDev L = lists[sg.list];
+    const long long base = (long long)blockIdx.x * kLpChunk;
+    if (base >= L.n) return;
+    __shared__ int s_warp[kLpThreads / 32];
+    __shared__ long long s_off;
+    __shared__ unsigned long long s_pairs[2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x < 32) {  // offset of this chunk = kept lines of the earlier chunks
+        long long s = 0;
+        for (int c = lane; c < (int)blockIdx.x; c += 32) s += chunk_count[(size_t)blockIdx.y * n_chunks_max + c];
+        for (int d = 16; d; d >>= 1) s += __shfl_down_sync(0xffffffffu, s, d);
+        if (lane == 0) {
+            s_off = s;
+            s_pairs[0] = s_pairs[1] = 0;
+            if (blockIdx.x == gridDim.x - 1 || base + kLpChunk >= L.n) {
+                // last chunk of the segment publishes the segment's kept count
+                const long long last = (L.n - 1) / kLpChunk;
+                if ((long long)blockIdx.x == last)
+                    seg_count[blockIdx.y] = (int)(s + chunk_count[(size_t)blockIdx.y * n_chunks_max + blockIdx.x]);
+            }
+        }
+    }
+    __syncthreads();
+    long long run = s_off;
+    unsigned long long pairs = 0, core = 0;
+    const double isp = kInvSqrtPi;
+    for (int r = 0; r < kLpPerThread; ++r) {
+        const long long j = base + r * kLpThreads + threadIdx.x;
+        const bool valid = j < L.n;
+        const bool k = valid && keep[sg.off + j];
+        const unsigned bal = __ballot_sync(0xffffffffu, k);
+        if (lane == 0) s_warp[warp] = __popc(bal);
+        __syncthreads();
+        int before = 0, total = 0;
+#pragma unroll
+        for (int w = 0; w < kLpThreads / 32; ++w) {
+            before += w < warp ? s_warp[w] : 0;
+            total += s_warp[w];
+        }
+        const long long slot = sg.off + run + before + __popc(bal & ((1u << lane) - 1u));
+        if (k) {
+            const LinePhys ph = line_phys(L, j, tp, sg.T, sg.p_atm, sg.vs);
+            const double gd = fmax(ph.gd, 1e-10);
+            const double f = kSqrtLn2 / gd;
+            const double y = ph.gl * f;
+            const double Sn = ph.S * f * isp;
+            double YSn = 0.0;
+            if ((sg.flags & 2) && L.has_y0) {  // line_mixing.jl:1193-1220
+                const double Y = L.y0[j] * pow(296.0 / sg.T, 0.75);
+                if (Y != 0.0 && ph.S > 0.0) YSn = Y * sg.p_atm * Sn;
+            }
+            const double c = cfg.cutoff;
+            // pair counts inside the cutoff on the uniform grid (roofline work units)
+            {
+                const double lo = ceil((ph.nu0s - c - cfg.grid0) / cfg.dnu_g);
+                const double hi = floor((ph.nu0s + c - cfg.grid0) / cfg.dnu_g);
+                if (hi >= lo) pairs += (unsigned long long)(hi - lo + 1);
+                const double wc = fmin(cfg.x_far / f, c);
+                const double clo = ceil((ph.nu0s - wc - cfg.grid0) / cfg.dnu_g);
+                const double chi = floor((ph.nu0s + wc - cfg.grid0) / cfg.dnu_g);
+                if (chi >= clo) core += (unsigned long long)(chi - clo + 1);
+            }
+            if (cfg.method == 2) {  // PseudoVoigt, voigt.jl:422-441
+                const double fG = 2.0 * gd, fL = 2.0 * ph.gl;
+                const double fV = pow(pow(fG, 5.0) + 2.69269 * pow(fG, 4.0) * fL + 2.42843 * pow(fG, 3.0) * (fL * fL) +
+                                      4.47163 * (fG * fG) * pow(fL, 3.0) + 0.07842 * fG * pow(fL, 4.0) + pow(fL, 5.0), 0.2);
+                const double rr = fL / fV;
+                const double gV = 0.5 * fV;
+                const double eta = 1.36603 * rr - 0.47719 * (rr * rr) + 0.11116 * (rr * rr * rr);
+                const double cG = 0.46971863934982566;  // sqrt(log(2)/pi)
+                const double Gc = cG / gV * exp(-0.69314718055994531 * (c * c) / (gV * gV));
+                const double Lc = gV * 0.31830988618379067 / (c * c + gV * gV);
+                const double basev = ph.S * (eta * Lc + (1.0 - eta) * Gc);
+                if (PREC == 0) {
+                    o64.nu0[slot] = ph.nu0s; o64.f[slot] = gV; o64.y[slot] = eta;
+                    o64.Sn[slot] = ph.S; o64.Hc[slot] = basev; o64.YSn[slot] = YSn;
+                } else {
+                    const double dg = cfg.dnu_g, co = sg.coef;
+                    const double gVg = gV / dg;
+                    om.V[slot] = (L.nu[j] - cfg.grid0) / dg;
+                    om.U[slot] = (ph.nu0s - cfg.grid0) / dg;
+                    const double P = basev * co;
+                    om.p0[slot] = make_float4((float)(gVg * gVg), (float)(ph.S * co * eta * gVg / (M_PI * dg)),
+                                              (float)(P * (dg / c) * (dg / c)), (float)(-2.0 * P));
+                    om.p1[slot] = make_float4((float)(1.0 / (gVg * gVg)),
+                                              (float)(ph.S * co * (1.0 - eta) * cG / gV), 0.f, 0.f);
+                    om.p2[slot] = make_float2(0.f, 0.f);
+                }
+            } else {
+                const double xc = c * f;
+                double Hc;
+                if (fabs(xc) > cfg.x_far) Hc = y * isp / (xc * xc + y * y);
+                else Hc = cfg.method == 1 ? weideman24_64(xc, y) : faddeeva64(xc, y).x;
+                if (PREC == 0) {
+                    o64.nu0[slot] = ph.nu0s; o64.f[slot] = f; o64.y[slot] = y;
+                    o64.Sn[slot] = Sn; o64.Hc[slot] = Hc; o64.YSn[slot] = YSn;
+                } else {
+                    const double dg = cfg.dnu_g, co = sg.coef;
+                    const double fx = f * dg;         // x per grid unit
+                    const double An = Sn * co;        // tau per unit H
+                    const double P = An * Hc;         // pedestal scale
+                    const double Yw = YSn * co;
+                    om.V[slot] = (L.nu[j] - cfg.grid0) / dg;
+                    om.U[slot] = (ph.nu0s - cfg.grid0) / dg;
+                    const double b = y / fx;
+                    const double dfar = cfg.x_far / fx;
+                    om.p0[slot] = make_float4((float)(b * b), (float)(An * y * isp / (fx * fx)),
+                                              (float)(P * (dg / c) * (dg / c)), (float)(-2.0 * P));
+                    om.p1[slot] = make_float4((float)fmin(dfar * dfar, 3.0e38), (float)An, (float)fx, (float)y);
+                    om.p2[slot] = make_float2((float)(Yw * isp / fx), (float)Yw);
+                }
+            }
+        }
+        run += total;
+        __syncthreads();
+    }
+    for (int d = 16; d; d >>= 1) {
+        pairs += __shfl_down_sync(0xffffffffu, pairs, d);
+        core += __shfl_down_sync(0xffffffffu, core, d);
+    }
+    if (lane == 0) {
+        atomicAdd(&s_pairs[0], pairs);
+        atomicAdd(&s_pairs[1], core);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && pair_counts) {
+        atomicAdd(&pair_counts[0], s_pairs[0]);
+        atomicAdd(&pair_counts[1], s_pairs[1]);
+    }
+}
+
+}  // namespace irs

@@ -1,0 +1,266 @@
+// rte_ils.cuh -- continuum + Schwarzschild RTE per grid point, then the ILS and
+// brightness temperature at the channel nodes only.
+//
+//  rte_kernel (one thread per grid point and profile) restates
+//    continua added to the layer optical depth   src/Sensor/sounder.jl:310-322,
+//      h2o_continuum / co2_continuum              src/CrossSections/continuum.jl:169-250
+//    level_transmittances (FP64 product)          src/Solver/transmittance.jl:26-43
+//    schwarzschild_rte, :cim and :toon sources    src/Solver/schwarzschild.jl:130-209
+//    add_reflected_downwelling! when eps < 1      schwarzschild.jl:228-274
+//    planck_radiance                              src/Solver/planck.jl:22-24
+//  The per-layer tau is FP32 (mixed) or FP64 (plain); the cumulative transmittance
+//  product and the radiance sum are FP64.
+//
+//  ils_bt_kernel (one warp per channel and profile) restates apply_ils
+//  (src/Sensor/ils.jl:131-153) evaluated at the grid nodes that the linear channel
+//  resampling reads (sounder.jl:372-377), then brightness_temperature
+//  (planck.jl:53-57).  Channel nodes are grid nodes for every sounder, so this is the
+//  full convolution sampled where it is used, not an approximation.
+#pragma once
+#include "irs_internal.h"
+
+namespace irs {
+
+struct GridDev {
+    long long n, den;
+    double a_n, s_n, start, step;
+    __host__ __device__ double at(long long i) const {
+        return den ? (a_n + double(i) * s_n) / double(den) : start + double(i) * step;
+    }
+};
+inline GridDev to_dev(const GridSpec& g) {
+    GridDev d;
+    d.n = g.n; d.den = g.den; d.a_n = g.a_n; d.s_n = g.s_n; d.start = g.start; d.step = g.step;
+    return d;
+}
+
+struct ContDev {
+    const double* h2o;  // nu[n], cs[n], cf[n], te[n]
+    const double* co2;  // nu[n], seff[n], tdep[n]
+    int n_h2o, n_co2;
+    int mask;           // 1 h2o, 2 co2 (only when apply_continuum)
+};
+
+__global__ void grid_values_kernel(GridDev g, double* out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < g.n) out[i] = g.at(i);
+}
+
+__device__ __forceinline__ double planck64(double nu, double T) {
+    return 1.191042953e-5 * (nu * nu * nu) / expm1(1.4387769 * nu / T);
+}
+__device__ __forceinline__ double cim_corr(double s) {  // schwarzschild.jl:59-63
+    if (s < 0.06) return s / 6.0;
+    const double e = exp(-s);
+    return 1.0 - 2.0 * (e / (e - 1.0) + 1.0 / s);
+}
+__device__ __forceinline__ double lit_corr(double s) {  // schwarzschild.jl:43-47
+    if (s < 1e-4) return s * (0.5 - s * (1.0 / 3.0 - s * 0.125));
+    const double e = exp(-s);
+    return (1.0 - e) / s - e;
+}
+__device__ __forceinline__ double radfn(double nu, double T) {  // continuum.jl:169-174
+    const double x = 1.4387769 * nu / T;
+    if (x <= 0.01) return 0.5 * x * nu;
+    if (x <= 10.0) return nu * (1.0 - exp(-x)) / (1.0 + exp(-x));
+    return nu;
+}
+// Interpolations.jl linear interpolation, Flat() extrapolation
+struct Lerp {
+    int i;
+    double w;
+    int edge;  // -1 below, +1 above, 0 inside
+};
+__device__ __forceinline__ Lerp lerp_at(const double* k, int n, double x) {
+    Lerp r{0, 0.0, 0};
+    if (x <= k[0]) { r.edge = -1; return r; }
+    if (x >= k[n - 1]) { r.edge = 1; r.i = n - 1; return r; }
+    int lo = 0, hi = n;  // upper_bound
+    while (lo < hi) { const int mid = (lo + hi) >> 1; if (k[mid] <= x) lo = mid + 1; else hi = mid; }
+    r.i = min(max(lo - 1, 0), n - 2);
+    r.w = (x - k[r.i]) / (k[r.i + 1] - k[r.i]);
+    return r;
+}
+__device__ __forceinline__ double lerp_val(const double* v, const Lerp& l) {
+    if (l.edge) return v[l.i];
+    return v[l.i] * (1.0 - l.w) + v[l.i + 1] * l.w;
+}
+
+template <typename TT>
+__device__ __forceinline__ double layer_tau(const TT* tau_l, long long i, double nu, const LayerRT& r,
+                                            const ContDev& c, double Cs, double Cf, double te, double Se,
+                                            double td) {
+    double t = (double)tau_l[i];
+    if (c.mask) {
+        const double T = r.T_mid, p = r.p_mid;
+        const double rho = (p / 1013.0) * (296.0 / T);
+        const double rad = radfn(nu, T);
+        if (c.mask & 1) {
+            const double n = r.vmr_h2o * p * 100.0 / (1.380649e-23 * T) * 1e-6;
+            const double ks = Cs * pow(296.0 / T, te) * r.vmr_h2o * rho * rad * n;
+            const double kf = Cf * (1.0 - r.vmr_h2o) * rho * rad * n;
+            t += (ks + kf) * r.dz_cm;
+        }
+        if (c.mask & 2) {
+            const double n = r.vmr_co2 * p * 100.0 / (1.380649e-23 * T) * 1e-6;
+            const double pref = 1e-20 * n * rho;
+            const double tc = td == 0.0 ? 1.0 : pow(T / 246.0, td);
+            t += Se * tc * pref * rad * r.dz_cm;
+        }
+    }
+    return t;
+}
+
+template <typename TT>
+__global__ void __launch_bounds__(256) rte_kernel(const TT* __restrict__ tau, const LayerRT* __restrict__ lrt,
+                                                  const ProfileRT* __restrict__ prt, int L,
+                                                  const double* __restrict__ grid, long long n_nu, int src,
+                                                  ContDev cont, double* __restrict__ I) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = blockIdx.y;
+    if (i >= n_nu) return;
+    const double nu = grid[i];
+    double Cs = 0, Cf = 0, te = 0, Se = 0, td = 0;
+    if (cont.mask & 1) {
+        const Lerp l = lerp_at(cont.h2o, cont.n_h2o, nu);
+        Cs = lerp_val(cont.h2o + cont.n_h2o, l);
+        Cf = lerp_val(cont.h2o + 2 * cont.n_h2o, l);
+        te = lerp_val(cont.h2o + 3 * cont.n_h2o, l);
+    }
+    if (cont.mask & 2) {
+        const Lerp l = lerp_at(cont.co2, cont.n_co2, nu);
+        Se = lerp_val(cont.co2 + cont.n_co2, l);
+        td = lerp_val(cont.co2 + 2 * cont.n_co2, l);
+    }
+    const ProfileRT pr = prt[p];
+    const LayerRT* lr = lrt + (size_t)p * L;
+    const TT* tp = tau + (size_t)p * L * n_nu;
+    double Tr_up = 1.0;   // transmittance of the level above (TOA = 1)
+    double I_atm = 0.0;
+    for (int k = L - 1; k >= 0; --k) {
+        const LayerRT r = lr[k];
+        const double s = layer_tau(tp + (size_t)k * n_nu, i, nu, r, cont, Cs, Cf, te, Se, td) / pr.mu;
+        const double Tr_k = Tr_up * exp(-s);
+        const double dT = Tr_up - Tr_k;
+        if (src == 0) {
+            const double Ba = planck64(nu, r.T_ave), Bt = planck64(nu, r.T_top);
+            I_atm += Ba * dT + (Bt - Ba) * (dT * cim_corr(s));
+        } else {
+            const double Bb = planck64(nu, r.T_bot), Bt = planck64(nu, r.T_top);
+            I_atm += Bt * dT + (Bb - Bt) * (Tr_up * lit_corr(s));
+        }
+        Tr_up = Tr_k;
+    }
+    const double Tr0 = Tr_up;
+    double Iv = pr.eps * planck64(nu, pr.T_sfc) * Tr0 + I_atm;
+    if (pr.eps < 1.0) {
+        double Id = 0.0, g = 1.0;
+        for (int k = 0; k < L; ++k) {
+            const LayerRT r = lr[k];
+            const double s = layer_tau(tp + (size_t)k * n_nu, i, nu, r, cont, Cs, Cf, te, Se, td) / pr.mu;
+            double em;
+            if (src == 0) {
+                const double Ba = planck64(nu, r.T_ave), Bb = planck64(nu, r.T_bot);
+                em = (1.0 - exp(-s)) * (Ba + (Bb - Ba) * cim_corr(s));
+            } else {
+                const double Bb = planck64(nu, r.T_bot), Bt = planck64(nu, r.T_top);
+                em = Bb * (1.0 - exp(-s)) + (Bt - Bb) * lit_corr(s);
+            }
+            Id += g * em;
+            g *= exp(-s);
+        }
+        Iv += (1.0 - pr.eps) * Id * Tr0;
+    }
+    I[(size_t)p * n_nu + i] = Iv;
+}
+
+// ---------------------------------------------------------------- ILS
+// ils.jl:80-114: raw taps, then area normalisation
+__global__ void ils_taps_kernel(double dnu, double opd_max, double fwhm, int apod, long long n_half,
+                                double* __restrict__ kern) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > 2 * n_half) return;
+    const int n_pts = 2048;
+    const double dL = opd_max / (n_pts - 1);
+    const double dv = double(k - n_half) * dnu;
+    const double sg = fwhm / (2.0 * sqrt(2.0 * log(2.0)));
+    const double nb[3][3] = {{0.384093, 0.087577, 0.528330},
+                             {0.152442, 0.136176, 0.711382},
+                             {0.045335, 0.554883, 0.399782}};
+    double s = 0.0;
+    for (int j = 0; j < n_pts; ++j) {
+        const double L = (double(j) / double(n_pts - 1)) * opd_max;
+        double A;
+        if (apod == 0) A = exp(-(2.0 * (M_PI * M_PI)) * (sg * sg) * (L * L));
+        else {
+            const double x = L / opd_max;
+            const double t = 1.0 - x * x;
+            A = fabs(x) > 1.0 ? 0.0 : nb[apod - 1][0] + nb[apod - 1][1] * t * t + nb[apod - 1][2] * (t * t) * (t * t);
+        }
+        s += A * cos(2.0 * M_PI * L * dv);
+    }
+    kern[k] = 2.0 * s * dL;
+}
+__global__ void ils_normalise_kernel(double* kern, long long n, double dnu) {
+    __shared__ double part[1024];
+    double s = 0.0;
+    for (long long k = threadIdx.x; k < n; k += blockDim.x) s += kern[k];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int d = blockDim.x / 2; d; d >>= 1) {
+        if ((int)threadIdx.x < d) part[threadIdx.x] += part[threadIdx.x + d];
+        __syncthreads();
+    }
+    const double tot = part[0] * dnu;
+    __syncthreads();
+    for (long long k = threadIdx.x; k < n; k += blockDim.x) kern[k] /= tot;
+}
+
+__device__ double apod_at(const double* __restrict__ Ip, long long n_nu, const double* __restrict__ kern,
+                          long long n_taps, long long i, int lane) {
+    const long long half = (n_taps - 1) / 2;
+    double acc = 0.0;
+    for (long long k = lane; k < n_taps; k += 32) {
+        const long long j = i + k - half;
+        if (j >= 0 && j < n_nu) acc = fma(Ip[j], kern[k], acc);
+    }
+    for (int d = 16; d; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
+    return acc;
+}
+
+__global__ void __launch_bounds__(256) ils_bt_kernel(const double* __restrict__ I, long long n_nu,
+                                                     const double* __restrict__ kern, long long n_taps,
+                                                     double dnu_hi, GridDev g, GridDev ch, int with_ils,
+                                                     double* __restrict__ R, double* __restrict__ BT) {
+    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int p = blockIdx.y;
+    if (wid >= ch.n) return;
+    const double nu = ch.at(wid);
+    const double* Ip = I + (size_t)p * n_nu;
+    auto value = [&](long long i) -> double {
+        if (!with_ils) return Ip[i];
+        return apod_at(Ip, n_nu, kern, n_taps, i, lane) * dnu_hi;
+    };
+    double Rv;
+    const double g0 = g.at(0), gl = g.at(n_nu - 1);
+    if (nu <= g0) Rv = value(0);
+    else if (nu >= gl) Rv = value(n_nu - 1);
+    else {
+        long long i = (long long)floor((nu - g0) / dnu_hi);
+        i = max(0LL, min(i, n_nu - 2));
+        while (i > 0 && g.at(i) > nu) --i;
+        while (i + 2 < n_nu && g.at(i + 1) <= nu) ++i;
+        const double a = g.at(i), b = g.at(i + 1);
+        const double w = (nu - a) / (b - a);
+        const double r0 = value(i);
+        Rv = w == 0.0 ? r0 : r0 * (1.0 - w) + value(i + 1) * w;
+    }
+    if (lane == 0) {
+        R[(size_t)p * ch.n + wid] = Rv;
+        BT[(size_t)p * ch.n + wid] =
+            Rv <= 0.0 ? 0.0 : 1.4387769 * nu / log1p(1.191042953e-5 * (nu * nu * nu) / Rv);
+    }
+}
+
+}  // namespace irs

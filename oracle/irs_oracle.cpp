@@ -1,0 +1,913 @@
+// irs_oracle.cpp -- TEST INFRASTRUCTURE ONLY (see irs_oracle.h).
+//
+// FP64 C++ restatement of IRSounderLBL.jl's line-by-line forward path.  Each
+// function names the reference file:line it restates.  OpenMP parallelises the
+// loops over grid points exactly where the reference's KernelAbstractions CPU
+// backend does (one work item per grid point), so per-point arithmetic order is
+// the reference's.
+#include "irs_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <string>
+#include <utility>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+using cplx = std::complex<double>;
+thread_local std::string g_err;
+
+int fail(const std::string& m) { g_err = m; return -1; }
+
+// ---------------------------------------------------------------- constants
+const double SQRT_LN2 = std::sqrt(std::log(2.0));          // voigt.jl:4
+const double INV_SQRT_PI = 1.0 / std::sqrt(M_PI);          // voigt.jl:5
+const double C2_LINE = 1.4387752;                           // broadening.jl:10
+const double T_REF = 296.0;                                 // partition.jl:6
+const double PLANCK_C1 = 1.191042953e-5;                    // planck.jl:11
+const double PLANCK_C2 = 1.4387769;                         // planck.jl:12
+const double ILS_HALFWIDTH_CM = 16.0;                       // ils.jl:24
+const double NAIR_PER_VMR = 2.1209e22;                      // sounder.jl:280
+
+// broadening.jl:17-24 (species-average n_self, delta_self)
+double n_self_of(int mol, double n_air) {
+    if (mol == 1) return 0.95;
+    if (mol == 2) return 0.75;
+    return n_air;
+}
+double delta_self_of(int mol) {
+    if (mol == 1) return 0.002;
+    if (mol == 2) return -0.003;
+    return 0.0;
+}
+// broadening.jl:131-148
+double molecular_mass_amu(int mol) {
+    static const double m[11] = {18.010, 44.010, 47.998, 44.013, 28.010, 16.043,
+                                 31.999, 34.015, 64.065, 36.461, 17.031};
+    if (mol < 1 || mol > 11) return 30.0;
+    return m[mol - 1];
+}
+
+// ------------------------------------------------------------------ tables
+struct Tips { int tmin; std::vector<double> q; };
+std::map<std::pair<int, int>, Tips> g_tips;
+struct Table1D { std::vector<double> x; std::vector<std::vector<double>> y; };
+Table1D g_ckd_h2o;  // y: Cs, Cf, texp
+Table1D g_ckd_co2;  // y: S*xfac, tdep
+bool g_have_h2o = false, g_have_co2 = false;
+
+// Interpolations.jl linear_interpolation(knots, v; extrapolation_bc=Flat()),
+// as used at continuum.jl:64-66, :94-95 and interpolation.jl:20.
+double interp_flat(const std::vector<double>& k, const std::vector<double>& v, double x) {
+    const size_t n = k.size();
+    if (x <= k[0]) return v[0];
+    if (x >= k[n - 1]) return v[n - 1];
+    size_t i = std::upper_bound(k.begin(), k.end(), x) - k.begin() - 1;
+    if (i >= n - 1) i = n - 2;
+    const double w = (x - k[i]) / (k[i + 1] - k[i]);
+    return v[i] * (1.0 - w) + v[i + 1] * w;
+}
+
+// partition.jl:10-18 (_tips_lookup: linear at 1 K, clamped indices)
+double tips_lookup(const Tips& t, double T) {
+    const long n = (long)t.q.size();
+    long i_lo = (long)std::floor(T) - t.tmin + 1;  // 1-based
+    long i_hi = i_lo + 1;
+    i_lo = std::min(std::max(i_lo, 1L), n);
+    i_hi = std::min(std::max(i_hi, 1L), n);
+    const double frac = T - std::floor(T);
+    return t.q[i_lo - 1] * (1.0 - frac) + t.q[i_hi - 1] * frac;
+}
+
+// ------------------------------------------------------------ Faddeeva w(z)
+// The reference evaluates Re/Im erfcx(y - i x) = w(x + i y) through
+// SpecialFunctions.jl -> OpenSpecFun (voigt.jl:158-160, line_mixing.jl:1182).
+// Restated here from two published methods (no third-party source):
+//   * |x| + y >= 8: Laplace continued fraction
+//       w(z) = (i/sqrt(pi)) / (z - (1/2)/(z - 1/(z - (3/2)/(z - ...)))), 24 levels;
+//   * otherwise: Weideman, SIAM J. Numer. Anal. 31 (1994) 1497-1518, rational
+//       series with N = 40 terms, w = 2 p(Z)/(L - i z)^2 + (1/sqrt(pi))/(L - i z),
+//       Z = (L + i z)/(L - i z), L = sqrt(N/sqrt(2)); the coefficients of p are
+//       the DFT of exp(-t^2)(L^2 + t^2) at t = L tan(theta/2).
+// Checked against scipy.special.wofz to ~2e-14 of |w| in tests/test_oracle_pins.py.
+struct WeidemanW {
+    static const int N = 40;
+    double L;
+    double a[N];  // highest power first (polyval order)
+    WeidemanW() {
+        const int M = 2 * N, M2 = 2 * M;
+        L = std::sqrt(N / std::sqrt(2.0));
+        // f sampled at k = -M+1..M-1, prefixed with 0 -> length 2M; fftshift;
+        // real part of the DFT divided by 2M; keep entries 1..N reversed.
+        std::vector<double> f(M2, 0.0);
+        for (int k = -M + 1; k <= M - 1; ++k) {
+            const double th = k * M_PI / M;
+            const double t = L * std::tan(th / 2.0);
+            f[k + M] = std::exp(-t * t) * (L * L + t * t);
+        }
+        // fftshift of length-2M vector: element m moves to (m + M) mod 2M
+        std::vector<double> g(M2);
+        for (int m = 0; m < M2; ++m) g[(m + M) % M2] = f[m];
+        for (int n = 1; n <= N; ++n) {
+            long double s = 0.0L;
+            for (int m = 0; m < M2; ++m)
+                s += (long double)g[m] * std::cos(2.0L * (long double)M_PI * n * m / M2);
+            a[N - n] = (double)(s / M2);
+        }
+    }
+    cplx eval(cplx z) const {
+        const cplx iz(-z.imag(), z.real());
+        const cplx den = L - iz;
+        const cplx Z = (L + iz) / den;
+        cplx p = a[0];
+        for (int n = 1; n < N; ++n) p = p * Z + a[n];
+        return 2.0 * p / (den * den) + INV_SQRT_PI / den;
+    }
+};
+const WeidemanW& weid_w() { static const WeidemanW w; return w; }
+
+cplx faddeeva(double x, double y) {
+    if (std::fabs(x) + y >= 8.0) {
+        const cplx z(x, y);
+        cplx r = 0.0;
+        for (int k = 24; k >= 1; --k) r = (0.5 * k) / (z - r);
+        return cplx(0.0, INV_SQRT_PI) / (z - r);
+    }
+    return weid_w().eval(cplx(x, y));
+}
+
+// voigt.jl:56-64, 89-117: the reference's "Weideman" evaluator -- a 24-node
+// trapezoid rule on the tan-substituted integral with a two-sum correction.
+struct Weid24 {
+    double t[24], w[24], c[24], scale;
+    float t32[24], w32[24], c32[24], scale32;
+    Weid24() {
+        const int N = 24;
+        const double L = std::sqrt(double(N) / std::log(2.0));
+        for (int n = 1; n <= N; ++n) {
+            t[n - 1] = L * std::tan(double(2 * n - 1 - N) * M_PI / double(2 * N));
+            w[n - 1] = L * L + t[n - 1] * t[n - 1];
+            c[n - 1] = w[n - 1] * std::exp(-t[n - 1] * t[n - 1]);
+            t32[n - 1] = (float)t[n - 1]; w32[n - 1] = (float)w[n - 1]; c32[n - 1] = (float)c[n - 1];
+        }
+        scale = double(N) * L;
+        scale32 = (float)scale;
+    }
+};
+const Weid24& weid24() { static const Weid24 w; return w; }
+
+double weideman_voigt(double x, double y) {
+    const Weid24& W = weid24();
+    double A = 0.0, B = 0.0;
+    for (int n = 0; n < 24; ++n) {
+        const double d = (x - W.t[n]) * (x - W.t[n]) + y * y;
+        A += W.c[n] / d;
+        B += W.w[n] / d;
+    }
+    const double sc = y / W.scale;
+    return std::max(0.0, std::exp(-(x * x)) * (1.0 - B * sc) + A * sc);
+}
+float weideman_voigt32(float x, float y) {
+    const Weid24& W = weid24();
+    float A = 0.0f, B = 0.0f;
+    for (int n = 0; n < 24; ++n) {
+        const float dx = x - W.t32[n];
+        const float d = dx * dx + y * y;
+        A += W.c32[n] / d;
+        B += W.w32[n] / d;
+    }
+    const float sc = y / W.scale32;
+    return std::max(0.0f, std::exp(-(x * x)) * (1.0f - B * sc) + A * sc);
+}
+
+double faddeeva_voigt(double x, double y) { return faddeeva(x, y).real(); }
+
+// voigt.jl:134-147
+double pseudo_voigt_profile(double nu, double nu0, double gl, double gd) {
+    const double fG = 2.0 * gd, fL = 2.0 * gl;
+    const double fV = std::pow(std::pow(fG, 5) + 2.69269 * std::pow(fG, 4) * fL +
+                               2.42843 * std::pow(fG, 3) * fL * fL +
+                               4.47163 * fG * fG * std::pow(fL, 3) +
+                               0.07842 * fG * std::pow(fL, 4) + std::pow(fL, 5), 0.2);
+    const double gV = 0.5 * fV, r = fL / fV;
+    const double eta = 1.36603 * r - 0.47719 * r * r + 0.11116 * r * r * r;
+    const double d = nu - nu0;
+    const double G = std::sqrt(std::log(2.0) / M_PI) / gV * std::exp(-std::log(2.0) * d * d / (gV * gV));
+    const double Lz = gV / (M_PI * (d * d + gV * gV));
+    return eta * Lz + (1.0 - eta) * G;
+}
+
+// --------------------------------------------------------- line parameters
+struct LineParams { double nu0, S, gl, gd; };
+
+// broadening.jl:40-53 (pressure_broadened_width), :89-99 (S(T)),
+// :156-160 (pressure_shift); partition.jl:41-47 (Q_ratio)
+double Q_ratio(int mol, int iso, double T) {
+    auto it = g_tips.find({mol, iso});
+    if (it == g_tips.end()) return T_REF / T;
+    return tips_lookup(it->second, T_REF) / tips_lookup(it->second, T);
+}
+double partition_function(int mol, int iso, double T) {
+    auto it = g_tips.find({mol, iso});
+    if (it == g_tips.end()) return T / T_REF;
+    return tips_lookup(it->second, T);
+}
+LineParams line_params(const orc_line& l, double T, double p, double vs) {
+    LineParams o;
+    const int mol = l.mol_id;
+    const double n_air = (double)l.temp_depend;
+    const double n_self = n_self_of(mol, n_air);
+    const double tr = T_REF / T;
+    o.gl = std::pow(tr, n_air) * (double)l.air_broad * (1.0 - vs) * p +
+           std::pow(tr, n_self) * (double)l.self_broad * vs * p;
+    o.gd = l.wavenumber * 3.58126e-7 * std::sqrt(T / molecular_mass_amu(mol));
+    const double Qr = Q_ratio(mol, l.iso_id, T);
+    const double stim = (1.0 - std::exp(-C2_LINE * l.wavenumber / T)) /
+                        (1.0 - std::exp(-C2_LINE * l.wavenumber / T_REF));
+    const double boltz = std::exp(-C2_LINE * l.lower_energy * (1.0 / T - 1.0 / T_REF));
+    o.S = l.intensity * Qr * boltz * stim;
+    o.nu0 = l.wavenumber + ((double)l.pressure_shift * (1.0 - vs) + delta_self_of(mol) * vs) * p;
+    return o;
+}
+
+// voigt.jl:220-236 (1-based lower/upper bound on possibly unsorted shifted centres)
+long lower_bound1(const double* a, double v, long n) {
+    long lo = 1, hi = n + 1;
+    while (lo < hi) { long mid = (lo + hi) >> 1; if (a[mid - 1] < v) lo = mid + 1; else hi = mid; }
+    return lo;
+}
+long upper_bound1(const double* a, double v, long n) {
+    long lo = 0, hi = n;
+    while (lo < hi) { long mid = (lo + hi + 1) >> 1; if (a[mid - 1] > v) hi = mid - 1; else lo = mid; }
+    return lo;
+}
+
+// voigt.jl:375-462 compute_voigt_cross_sections (host prep + kernels :243-313)
+void voigt_xsec(const orc_line* lines, long nL, const double* grid, long n_nu, double T,
+                double p, double vs, double cutoff, int method, double x_far, double* sigma) {
+    std::vector<double> nu0(nL), S(nL), gl(nL), gd(nL), f(nL), y(nL), Sn(nL);
+    for (long j = 0; j < nL; ++j) {
+        LineParams lp = line_params(lines[j], T, p, vs);
+        nu0[j] = lp.nu0;
+        S[j] = lp.S;
+        gl[j] = lp.gl;
+        gd[j] = std::max(lp.gd, 1e-10);
+        f[j] = SQRT_LN2 / gd[j];
+        y[j] = lp.gl * f[j];
+        Sn[j] = lp.S * f[j] * INV_SQRT_PI;
+    }
+    const double rc = 1.0 / cutoff;
+    if (method == 2) {  // PseudoVoigt, voigt.jl:422-441, kernel :281-313
+        std::vector<double> gV(nL), eta(nL), base(nL);
+        const double cG = std::sqrt(std::log(2.0) / M_PI);
+        for (long j = 0; j < nL; ++j) {
+            const double fG = 2 * gd[j], fL = 2 * gl[j];
+            const double fV = std::pow(std::pow(fG, 5) + 2.69269 * std::pow(fG, 4) * fL +
+                                       2.42843 * std::pow(fG, 3) * (fL * fL) +
+                                       4.47163 * (fG * fG) * std::pow(fL, 3) +
+                                       0.07842 * fG * std::pow(fL, 4) + std::pow(fL, 5), 0.2);
+            const double r = fL / fV;
+            gV[j] = 0.5 * fV;
+            eta[j] = 1.36603 * r - 0.47719 * (r * r) + 0.11116 * (r * r * r);
+            const double Gc = cG / gV[j] * std::exp(-std::log(2.0) * (cutoff * cutoff) / (gV[j] * gV[j]));
+            const double Lc = gV[j] * (1.0 / M_PI) / (cutoff * cutoff + gV[j] * gV[j]);
+            base[j] = S[j] * (eta[j] * Lc + (1.0 - eta[j]) * Gc);
+        }
+        const double cln2 = std::log(2.0), invpi = 1.0 / M_PI;
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < n_nu; ++i) {
+            const double nu = grid[i];
+            const long jlo = lower_bound1(nu0.data(), nu - cutoff, nL);
+            const long jhi = upper_bound1(nu0.data(), nu + cutoff, nL);
+            double acc = 0.0;
+            for (long j = jlo; j <= jhi; ++j) {
+                const long q = j - 1;
+                const double d = nu - nu0[q];
+                const double G = cG / gV[q] * std::exp(-cln2 * d * d / (gV[q] * gV[q]));
+                const double Lz = gV[q] * invpi / (d * d + gV[q] * gV[q]);
+                const double zr = d * rc;
+                acc += S[q] * (eta[q] * Lz + (1.0 - eta[q]) * G) - (2.0 - zr * zr) * base[q];
+            }
+            sigma[i] = std::max(acc, 0.0);
+        }
+        return;
+    }
+    // Weideman (1) or FullFaddeeva (3): voigt.jl:442-458, kernel :243-277
+    auto Hcore = [method](double x, double yy) {
+        return method == 3 ? faddeeva_voigt(x, yy) : weideman_voigt(x, yy);
+    };
+    std::vector<double> Hc(nL);
+    for (long j = 0; j < nL; ++j) {
+        const double xc = cutoff * f[j];
+        Hc[j] = std::fabs(xc) > x_far ? y[j] * INV_SQRT_PI / (xc * xc + y[j] * y[j]) : Hcore(xc, y[j]);
+    }
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n_nu; ++i) {
+        const double nu = grid[i];
+        const long jlo = lower_bound1(nu0.data(), nu - cutoff, nL);
+        const long jhi = upper_bound1(nu0.data(), nu + cutoff, nL);
+        double acc = 0.0;
+        for (long j = jlo; j <= jhi; ++j) {
+            const long q = j - 1;
+            const double d = nu - nu0[q];
+            const double x = d * f[q];
+            const double yy = y[q];
+            const double zr = d * rc;
+            const double ped = (2.0 - zr * zr) * Hc[q];
+            const double H = (std::fabs(x) > x_far ? yy * INV_SQRT_PI / (x * x + yy * yy) : Hcore(x, yy)) - ped;
+            acc += Sn[q] * H;
+        }
+        sigma[i] = std::max(acc, 0.0);
+    }
+}
+
+// voigt.jl:333-355 (_reject_weak_lines; DPTMIN)
+long reject_weak(const orc_line* lines, long nL, double T, double p, double coef, double vs,
+                 double dptmn, uint8_t* keep) {
+    long nk = 0;
+    for (long j = 0; j < nL; ++j) {
+        if (dptmn <= 0.0) { keep[j] = 1; ++nk; continue; }
+        LineParams lp = line_params(lines[j], T, p, vs);
+        const double gd = std::max(lp.gd, 1e-10);
+        const double f = SQRT_LN2 / gd;
+        const double peak = (lp.S * f * INV_SQRT_PI) * faddeeva_voigt(0.0, lp.gl * f);
+        keep[j] = (peak * coef > dptmn) ? 1 : 0;
+        nk += keep[j];
+    }
+    return nk;
+}
+
+// line_mixing.jl:1166-1236 (dispersive kernel and its flat SoA build), with the
+// relaxation-matrix Y replaced by a per-line Y(T) = y0 (296/T)^0.75 and the
+// per-line centre, widths and S(T) of the Voigt line itself.
+void lm_dispersive(const orc_line* lines, long nL, const double* y0, const double* grid,
+                   long n_nu, double T, double p, double cutoff, double x_far, double* ds) {
+    struct DL { double nu0, f, y, ysn; };
+    std::vector<DL> dl;
+    dl.reserve(nL);
+    for (long j = 0; j < nL; ++j) {
+        const double Y = y0[j] * std::pow(T_REF / T, 0.75);
+        if (Y == 0.0) continue;
+        LineParams lp = line_params(lines[j], T, p, 0.0);
+        if (lp.S <= 0.0) continue;
+        const double f = SQRT_LN2 / std::max(lp.gd, 1e-10);
+        dl.push_back({lp.nu0, f, lp.gl * f, Y * p * lp.S * f * INV_SQRT_PI});
+    }
+    std::stable_sort(dl.begin(), dl.end(), [](const DL& a, const DL& b) { return a.nu0 < b.nu0; });
+    const long n = (long)dl.size();
+    std::vector<double> c(n);
+    for (long j = 0; j < n; ++j) c[j] = dl[j].nu0;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n_nu; ++i) {
+        const double nu = grid[i];
+        const long jlo = lower_bound1(c.data(), nu - cutoff, n);
+        const long jhi = upper_bound1(c.data(), nu + cutoff, n);
+        double acc = 0.0;
+        for (long j = jlo; j <= jhi; ++j) {
+            const DL& L = dl[j - 1];
+            const double x = (nu - L.nu0) * L.f;
+            const double imw = std::fabs(x) > x_far ? x * INV_SQRT_PI / (x * x + L.y * L.y)
+                                                    : faddeeva(x, L.y).imag();
+            acc += L.ysn * imw;
+        }
+        ds[i] = acc;
+    }
+}
+
+// ------------------------------------------------------------ atmosphere
+bool approx_eq(double a, double b) {  // Julia isapprox default rtol = sqrt(eps)
+    return std::fabs(a - b) <= 1.4901161193847656e-8 * std::max(std::fabs(a), std::fabs(b));
+}
+// layers.jl:36-45
+double cg_column_vmr(double v1, double v2, double p1, double p2) {
+    if (v1 <= 0.0 || v2 <= 0.0) return 0.5 * (v1 + v2);
+    if (approx_eq(v1, v2)) return v1;
+    const double a = std::log(v2 / v1) / std::log(p2 / p1);
+    const double r = p2 / p1, b = a + 1;
+    if (std::fabs(b) < 1e-8) return (v1 - v2) / std::log(v1 / v2);
+    return v1 * p1 * (1.0 - std::pow(r, b)) / (b * std::fabs(p1 - p2));
+}
+// layers.jl:60-72
+double cg_pressure(double v1, double v2, double p1, double p2) {
+    if (v1 <= 0.0 || v2 <= 0.0) return 0.5 * (p1 + p2);
+    if (approx_eq(v1, v2)) return 0.5 * (p1 + p2);
+    const double a = std::log(v2 / v1) / std::log(p2 / p1);
+    const double r = p2 / p1, b1 = a + 1, b2 = a + 2;
+    if (std::fabs(b1) < 1e-8) return std::fabs(p1 - p2) / std::log(p1 / p2);
+    if (std::fabs(b2) < 1e-8) return p2 * std::log(p2 / p1) / (p2 / p1 - 1.0);
+    return p1 * b1 / b2 * (1.0 - std::pow(r, b2)) / (1.0 - std::pow(r, b1));
+}
+// layers.jl:93-106
+double cg_temperature_mass(double T1, double T2, double p1, double p2) {
+    if (approx_eq(T1, T2)) return T1;
+    if (approx_eq(p1, p2)) return 0.5 * (T1 + T2);
+    const double a = std::log(p2 / p1);
+    double frac;
+    if (std::fabs(a) < 1e-3) frac = 0.5 + a / 12.0;
+    else { const double b = p2 / p1; frac = ((a - 1.0) * b + 1.0) / (a * (b - 1.0)); }
+    return T1 + (T2 - T1) * frac;
+}
+// interpolation.jl:10-22 (linear in log p, flat outside)
+struct LogPInterp {
+    std::vector<double> k, v;
+    LogPInterp(int n, const double* p, const double* x) {
+        std::vector<std::pair<double, double>> kv(n);
+        for (int i = 0; i < n; ++i) kv[i] = {std::log(p[i]), x[i]};
+        bool sorted = true;
+        for (int i = 1; i < n; ++i) if (kv[i].first < kv[i - 1].first) sorted = false;
+        if (!sorted) std::stable_sort(kv.begin(), kv.end(),
+                                      [](auto& a, auto& b) { return a.first < b.first; });
+        for (auto& e : kv) { k.push_back(e.first); v.push_back(e.second); }
+    }
+    double operator()(double p) const { return interp_flat(k, v, std::log(p)); }
+};
+
+// ------------------------------------------------------------ continua
+// continuum.jl:169-174
+double radfn(double nu, double T) {
+    const double x = 1.4387769 * nu / T;
+    if (x <= 0.01) return 0.5 * x * nu;
+    if (x <= 10.0) return nu * (1.0 - std::exp(-x)) / (1.0 + std::exp(-x));
+    return nu;
+}
+// optical_depth.jl:123-130
+double dp_to_dz_cm(double dp, double pmid, double T) {
+    const double H = 8.314462 * T / (0.028964 * 9.80665);
+    return H * dp / pmid * 100.0;
+}
+// continuum.jl:183-209
+void h2o_continuum_add(const double* grid, long n, double vmr, double p, double T, double dz, double* tau) {
+    if (!g_have_h2o) return;  // missing table: zeros (continuum.jl:190-194)
+    const double rho = (p / 1013.0) * (296.0 / T);
+    const double nh2o = vmr * p * 100.0 / (1.380649e-23 * T) * 1e-6;
+    for (long i = 0; i < n; ++i) {
+        const double nu = grid[i];
+        const double Cs = interp_flat(g_ckd_h2o.x, g_ckd_h2o.y[0], nu);
+        const double Cf = interp_flat(g_ckd_h2o.x, g_ckd_h2o.y[1], nu);
+        const double te = interp_flat(g_ckd_h2o.x, g_ckd_h2o.y[2], nu);
+        const double rad = radfn(nu, T);
+        const double ks = Cs * std::pow(296.0 / T, te) * vmr * rho * rad * nh2o;
+        const double kf = Cf * (1.0 - vmr) * rho * rad * nh2o;
+        tau[i] += (ks + kf) * dz;
+    }
+}
+// continuum.jl:227-250
+void co2_continuum_add(const double* grid, long n, double vmr, double p, double T, double dz, double* tau) {
+    if (!g_have_co2) return;
+    const double rho = (p / 1013.0) * (296.0 / T);
+    const double nco2 = vmr * p * 100.0 / (1.380649e-23 * T) * 1e-6;
+    const double pref = 1e-20 * nco2 * rho;
+    const double tr = T / 246.0;
+    for (long i = 0; i < n; ++i) {
+        const double nu = grid[i];
+        const double td = interp_flat(g_ckd_co2.x, g_ckd_co2.y[1], nu);
+        const double tc = td == 0.0 ? 1.0 : std::pow(tr, td);
+        tau[i] += interp_flat(g_ckd_co2.x, g_ckd_co2.y[0], nu) * tc * pref * radfn(nu, T) * dz;
+    }
+}
+
+// ------------------------------------------------------------- solver
+double planck(double nu, double T) { return PLANCK_C1 * (nu * nu * nu) / std::expm1(PLANCK_C2 * nu / T); }
+double bt(double nu, double R) {
+    if (R <= 0.0) return 0.0;
+    return PLANCK_C2 * nu / std::log1p(PLANCK_C1 * (nu * nu * nu) / R);
+}
+// schwarzschild.jl:43-63
+double lit_corr(double s) {
+    if (s < 1e-4) return s * (0.5 - s * (1.0 / 3.0 - s * 0.125));
+    const double e = std::exp(-s);
+    return (1.0 - e) / s - e;
+}
+double cim_corr(double s) {
+    if (s < 0.06) return s / 6.0;
+    const double e = std::exp(-s);
+    return 1.0 - 2.0 * (e / (e - 1.0) + 1.0 / s);
+}
+
+// transmittance.jl:26-43 and schwarzschild.jl:130-274, for one grid point.
+// tau is [layer][nu] with stride n_nu.
+double rte_point(double nu, long i, long n_nu, int L, const double* tau, const double* T_lev,
+                 double T_sfc, double mu, double eps, int src, const double* T_ave) {
+    std::vector<double> Tr(L + 1);
+    Tr[L] = 1.0;
+    for (int k = L - 1; k >= 0; --k) Tr[k] = Tr[k + 1] * std::exp(-tau[(long)k * n_nu + i] / mu);
+    double I = eps * planck(nu, T_sfc) * Tr[0];
+    for (int k = 0; k < L; ++k) {
+        const double s = tau[(long)k * n_nu + i] / mu;
+        const double dT = Tr[k + 1] - Tr[k];
+        if (src == 1) {  // :toon
+            const double Bb = planck(nu, T_lev[k]), Bt = planck(nu, T_lev[k + 1]);
+            const double C = Tr[k + 1] * lit_corr(s);
+            I += Bt * dT + (Bb - Bt) * C;
+        } else {  // :cim
+            const double Ba = planck(nu, T_ave[k]), Bt = planck(nu, T_lev[k + 1]);
+            const double C = dT * cim_corr(s);
+            I += Ba * dT + (Bt - Ba) * C;
+        }
+    }
+    if (eps < 1.0) {  // schwarzschild.jl:203-206, 228-274
+        double Id = 0.0, g = 1.0;
+        for (int k = 0; k < L; ++k) {
+            const double s = tau[(long)k * n_nu + i] / mu;
+            double em;
+            if (src == 1) {
+                const double Bb = planck(nu, T_lev[k]), Bt = planck(nu, T_lev[k + 1]);
+                em = Bb * (1.0 - std::exp(-s)) + (Bt - Bb) * lit_corr(s);
+            } else {
+                const double Ba = planck(nu, T_ave[k]), Bb = planck(nu, T_lev[k]);
+                em = (1.0 - std::exp(-s)) * (Ba + (Bb - Ba) * cim_corr(s));
+            }
+            Id += g * em;
+            g *= std::exp(-s);
+        }
+        I += (1.0 - eps) * Id * Tr[0];
+    }
+    return I;
+}
+
+// ils.jl:38-44, 80-114
+const double NB[3][3] = {{0.384093, 0.087577, 0.528330},
+                         {0.152442, 0.136176, 0.711382},
+                         {0.045335, 0.554883, 0.399782}};
+void ils_kernel(double dnu, double opd_max, double fwhm, int apod, std::vector<double>& kern) {
+    const int n_pts = 2048;
+    const double dL = opd_max / (n_pts - 1);
+    std::vector<double> opd(n_pts), A(n_pts);
+    for (int j = 0; j < n_pts; ++j) {
+        // LinRange(0, opd_max, n): (1 - t)*0 + t*opd_max with t = j/(n-1)
+        opd[j] = (double(j) / double(n_pts - 1)) * opd_max;
+        if (apod == 0) {
+            const double sg = fwhm / (2.0 * std::sqrt(2.0 * std::log(2.0)));
+            A[j] = std::exp(-(2.0 * (M_PI * M_PI)) * (sg * sg) * (opd[j] * opd[j]));
+        } else {
+            const double x = opd[j] / opd_max;
+            const double* c = NB[apod - 1];
+            if (std::fabs(x) > 1.0) A[j] = 0.0;
+            else { const double t = 1.0 - x * x; A[j] = c[0] + c[1] * t * t + c[2] * (t * t) * (t * t); }
+        }
+    }
+    const long n_half = (long)std::ceil(ILS_HALFWIDTH_CM / dnu);
+    kern.assign(2 * n_half + 1, 0.0);
+    double tot = 0.0;
+    for (long k = -n_half; k <= n_half; ++k) {
+        const double dv = double(k) * dnu;
+        double s = 0.0;
+        for (int j = 0; j < n_pts; ++j) s += A[j] * std::cos(2.0 * M_PI * opd[j] * dv);
+        kern[k + n_half] = 2.0 * s * dL;
+    }
+    for (double v : kern) tot += v;
+    for (double& v : kern) v /= (tot * dnu);
+}
+
+// ------------------------------------------------------------- grid
+// Julia's float range a:s:b (utils/wavenumber_grid.jl:23-26) rationalises
+// start, step and stop and evaluates (a_n + i s_n)/den in extended precision.
+long rat_den(double x) {
+    for (long d = 1; d <= 1000000; ++d) {
+        const double n = std::nearbyint(x * d);
+        if (n / d == x) return d;
+    }
+    return 0;
+}
+struct Grid { double start, step; long den, n; double a_n, s_n; };
+Grid make_grid(double a, double b, double s) {
+    Grid g{a, s, 0, 0, 0, 0};
+    const long ds = rat_den(s), da = rat_den(a), db = rat_den(b);
+    if (ds && da && db) {
+        long den = std::lcm(da, ds);
+        den = std::lcm(den, db);
+        g.den = den;
+        g.a_n = std::nearbyint(a * den);
+        g.s_n = std::nearbyint(s * den);
+        const double b_n = std::nearbyint(b * den);
+        g.n = (long)std::floor((b_n - g.a_n) / g.s_n) + 1;
+    } else {
+        const double lf = (b - a) / s;
+        g.n = (long)std::nearbyint(lf) + 1;
+        if (a + (g.n - 1) * s > b) g.n -= 1;
+    }
+    return g;
+}
+double grid_at(const Grid& g, long i) {
+    if (g.den) return (g.a_n + double(i) * g.s_n) / double(g.den);
+    return g.start + double(i) * g.step;
+}
+
+struct InternalGrid { Grid g; double dnu_hi; };
+InternalGrid internal_grid(const orc_sounder& s, const orc_fm_options& o) {
+    // sounder.jl:263-271, :155-161
+    long hrf;
+    if (o.high_res_factor > 0) hrf = o.high_res_factor;
+    else if (o.internal_dnu > 0) hrf = std::max(1L, (long)std::ceil(s.dnu / o.internal_dnu));
+    else hrf = 4;
+    const double dhi = s.dnu / double(hrf);
+    InternalGrid ig;
+    ig.dnu_hi = dhi;
+    if (o.with_ils) {
+        const double pad = std::ceil(ILS_HALFWIDTH_CM / dhi) * dhi;
+        ig.g = make_grid(s.nu_min - pad, s.nu_max + pad, dhi);
+    } else {
+        ig.g = make_grid(s.nu_min, s.nu_max, dhi);
+    }
+    return ig;
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+extern "C" {
+
+const char* orc_last_error(void) { return g_err.c_str(); }
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void orc_clear_tables(void) {
+    g_tips.clear();
+    g_have_h2o = g_have_co2 = false;
+}
+int orc_set_tips(int mol, int iso, int tmin, int n, const double* q) {
+    if (n < 2) return fail("TIPS table needs at least 2 points");
+    g_tips[{mol, iso}] = Tips{tmin, std::vector<double>(q, q + n)};
+    return 0;
+}
+int orc_set_ckd_h2o(int n, const double* nu, const double* cs, const double* cf, const double* te) {
+    g_ckd_h2o.x.assign(nu, nu + n);
+    g_ckd_h2o.y = {std::vector<double>(cs, cs + n), std::vector<double>(cf, cf + n),
+                   std::vector<double>(te, te + n)};
+    g_have_h2o = true;
+    return 0;
+}
+int orc_set_ckd_co2(int n, const double* nu, const double* s, const double* xf, const double* td) {
+    g_ckd_co2.x.assign(nu, nu + n);
+    std::vector<double> se(n);
+    for (int i = 0; i < n; ++i) se[i] = s[i] * xf[i];
+    g_ckd_co2.y = {se, std::vector<double>(td, td + n)};
+    g_have_co2 = true;
+    return 0;
+}
+
+void orc_faddeeva(double x, double y, double* re, double* im) {
+    cplx w = faddeeva(x, y);
+    *re = w.real();
+    *im = w.imag();
+}
+double orc_weideman_voigt(double x, double y) { return weideman_voigt(x, y); }
+float orc_weideman_voigt32(float x, float y) { return weideman_voigt32(x, y); }
+double orc_pseudo_voigt_profile(double nu, double nu0, double gl, double gd) {
+    return pseudo_voigt_profile(nu, nu0, gl, gd);
+}
+double orc_voigt_profile(double nu, double nu0, double gl, double gd, int method) {
+    if (method == 2) return pseudo_voigt_profile(nu, nu0, gl, gd);
+    const double f = SQRT_LN2 / gd, x = (nu - nu0) * f, y = gl * f;
+    const double H = method == 1 ? weideman_voigt(x, y) : faddeeva_voigt(x, y);
+    return f * H * INV_SQRT_PI;
+}
+double orc_Q_ratio(int mol, int iso, double T) { return Q_ratio(mol, iso, T); }
+double orc_partition_function(int mol, int iso, double T) { return partition_function(mol, iso, T); }
+void orc_line_params(const orc_line* l, double T, double p, double vs, double* nu0, double* S,
+                     double* gl, double* gd) {
+    LineParams lp = line_params(*l, T, p, vs);
+    *nu0 = lp.nu0; *S = lp.S; *gl = lp.gl; *gd = lp.gd;
+}
+double orc_planck(double nu, double T) { return planck(nu, T); }
+double orc_bt(double nu, double R) { return bt(nu, R); }
+double orc_dB_dT(double nu, double T) {  // planck.jl:67-71
+    const double x = PLANCK_C2 * nu / T, ex = std::exp(x);
+    return PLANCK_C1 * PLANCK_C2 * (nu * nu * nu * nu) * ex / ((T * T) * (ex - 1.0) * (ex - 1.0));
+}
+double orc_cim_correction(double s) { return cim_corr(s); }
+double orc_lit_correction(double s) { return lit_corr(s); }
+void orc_layer_cg(double v1, double v2, double p1, double p2, double* vc, double* pc) {
+    *vc = cg_column_vmr(v1, v2, p1, p2);
+    *pc = cg_pressure(v1, v2, p1, p2);
+}
+double orc_cg_temperature_mass(double T1, double T2, double p1, double p2) {
+    return cg_temperature_mass(T1, T2, p1, p2);
+}
+double orc_scan_angle_to_local_zenith(double scan) {  // geometry.jl:92-101
+    const double s = (6371.0 + 817.0) / 6371.0 * std::sin(std::fabs(scan) * M_PI / 180.0);
+    if (s > 1.0) return NAN;
+    return std::asin(s) * 180.0 / M_PI;
+}
+
+int64_t orc_internal_grid(const orc_sounder* s, const orc_fm_options* o, double* nu0,
+                          double* dnu_hi, int64_t* den) {
+    InternalGrid ig = internal_grid(*s, *o);
+    *nu0 = grid_at(ig.g, 0);
+    *dnu_hi = ig.dnu_hi;
+    *den = ig.g.den;
+    return ig.g.n;
+}
+void orc_grid_values(double nu_start, double dnu_hi, int64_t den, int64_t i0, int64_t n, double* out) {
+    Grid g{nu_start, dnu_hi, den, 0, 0, 0};
+    if (den) { g.a_n = std::nearbyint(nu_start * den); g.s_n = std::nearbyint(dnu_hi * den); }
+    for (int64_t i = 0; i < n; ++i) out[i] = grid_at(g, i0 + i);
+}
+
+int orc_voigt_xsec(const orc_line* lines, int64_t nL, const double* grid, int64_t n_nu, double T,
+                   double p, double vs, double cutoff, int method, double x_far, double* sigma) {
+    if (method < 1 || method > 3) return fail("method must be 1 (Weideman), 2 (PseudoVoigt) or 3 (FullFaddeeva)");
+    voigt_xsec(lines, nL, grid, n_nu, T, p, vs, cutoff, method, x_far, sigma);
+    return 0;
+}
+int64_t orc_reject_weak_lines(const orc_line* lines, int64_t nL, double T, double p, double coef,
+                              double vs, double dptmn, uint8_t* keep) {
+    return reject_weak(lines, nL, T, p, coef, vs, dptmn, keep);
+}
+int orc_lm_dispersive(const orc_line* lines, int64_t nL, const double* y0, const double* grid,
+                      int64_t n_nu, double T, double p, double cutoff, double x_far, double* ds) {
+    lm_dispersive(lines, nL, y0, grid, n_nu, T, p, cutoff, x_far, ds);
+    return 0;
+}
+int orc_ils_kernel(double dnu, double opd, double fwhm, int apod, int64_t n_taps, double* out) {
+    if (apod < 0 || apod > 3) return fail("unknown apodization");
+    std::vector<double> k;
+    ils_kernel(dnu, opd, fwhm, apod, k);
+    if ((int64_t)k.size() != n_taps) return fail("n_taps mismatch");
+    std::copy(k.begin(), k.end(), out);
+    return 0;
+}
+int orc_rte(const double* grid, int64_t n_nu, int L, const double* tau, const double* T_lev,
+            double T_sfc, double mu, double eps, int src, const double* T_ave, double* I) {
+    if (!(mu > 0.0 && mu <= 1.0)) return fail("mu must be in (0, 1]");
+    if (src != 0 && src != 1) return fail("source_function must be :cim or :toon");
+    if (src == 0 && !T_ave) return fail(":cim source_function requires T_ave");
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n_nu; ++i)
+        I[i] = rte_point(grid[i], i, n_nu, L, tau, T_lev, T_sfc, mu, eps, src, T_ave);
+    return 0;
+}
+
+// sounder.jl:233-360
+int orc_forward_model(int n_lev, const double* p_lev, const double* T_lev, int nps,
+                      const int* psp, const double* pvmr, int n_lists, const int* lsp,
+                      const int64_t* loff, const orc_line* lines, const double* y0,
+                      const orc_sounder* s, const orc_fm_options* o, int64_t ch_begin,
+                      int64_t ch_end, double* R_out, double* BT_out, double* tau_out,
+                      int64_t* n_nu_window) {
+    if (n_lev < 2) return fail("profile needs at least 2 levels");
+    if (!(o->mu > 0.0 && o->mu <= 1.0)) return fail("mu must be in (0, 1]");
+    if (o->T_method != 0 && o->T_method != 1) return fail("T_method must be :logp_at_pcg or :mass_weighted");
+    if (o->source_function != 0 && o->source_function != 1) return fail("source_function must be :cim or :toon");
+    if (o->apodization < 0 || o->apodization > 3) return fail("unknown apodization");
+    const int L = n_lev - 1;
+    InternalGrid ig = internal_grid(*s, *o);
+    const Grid ch = make_grid(s->nu_min, s->nu_max, s->dnu);
+    if (ch_end <= 0) { ch_begin = 0; ch_end = ch.n; }
+    if (ch_begin < 0 || ch_end > ch.n || ch_begin >= ch_end) return fail("bad channel window");
+    // channel wavenumbers and the hi-res index interval the window needs
+    std::vector<double> nu_ch(ch_end - ch_begin);
+    for (long c = ch_begin; c < ch_end; ++c) nu_ch[c - ch_begin] = grid_at(ch, c);
+    const double dhi = ig.dnu_hi;
+    const long n_hi = ig.g.n;
+    const double nu_first = grid_at(ig.g, 0);
+    auto idx_floor = [&](double nu) {
+        long i = (long)std::floor((nu - nu_first) / dhi);
+        i = std::max(0L, std::min(i, n_hi - 1));
+        while (i > 0 && grid_at(ig.g, i) > nu) --i;
+        while (i + 1 < n_hi && grid_at(ig.g, i + 1) <= nu) ++i;
+        return i;
+    };
+    std::vector<double> kern;
+    long n_half = 0;
+    if (o->with_ils) {
+        ils_kernel(dhi, s->opd_max, s->fwhm_gauss, o->apodization, kern);
+        n_half = ((long)kern.size() - 1) / 2;
+    }
+    const long i_lo_ch = idx_floor(nu_ch.front());
+    const long i_hi_ch = std::min(n_hi - 1, idx_floor(nu_ch.back()) + 1);
+    const long w0 = std::max(0L, i_lo_ch - n_half);
+    const long w1 = std::min(n_hi - 1, i_hi_ch + n_half);
+    const long nw = w1 - w0 + 1;
+    std::vector<double> grid(nw);
+    for (long i = 0; i < nw; ++i) grid[i] = grid_at(ig.g, w0 + i);
+    if (n_nu_window) *n_nu_window = nw;
+
+    // layers.jl:133-178
+    std::vector<double> p_mid(L), dp(L);
+    for (int k = 0; k < L; ++k) { p_mid[k] = 0.5 * (p_lev[k] + p_lev[k + 1]); dp[k] = std::fabs(p_lev[k] - p_lev[k + 1]); }
+    LogPInterp Ti(n_lev, p_lev, T_lev);
+    std::vector<double> T_mid(L);
+    for (int k = 0; k < L; ++k) T_mid[k] = Ti(p_mid[k]);
+    std::vector<double> T_mass(L);
+    for (int k = 0; k < L; ++k) T_mass[k] = cg_temperature_mass(T_lev[k], T_lev[k + 1], p_lev[k], p_lev[k + 1]);
+    auto prof_index = [&](int sp) { for (int q = 0; q < nps; ++q) if (psp[q] == sp) return q; return -1; };
+
+    std::vector<double> tau((size_t)L * nw, 0.0), sig(nw), ds(nw);
+    for (int k = 0; k < L; ++k) {
+        double* tk = tau.data() + (size_t)k * nw;
+        for (int li = 0; li < n_lists; ++li) {
+            const int sp = lsp[li];
+            const int q = prof_index(sp);
+            if (q < 0) continue;
+            const double* v = pvmr + (size_t)q * n_lev;
+            const double vmr = cg_column_vmr(v[k], v[k + 1], p_lev[k], p_lev[k + 1]);
+            if (vmr == 0.0) continue;
+            const double pcg = cg_pressure(v[k], v[k + 1], p_lev[k], p_lev[k + 1]);
+            const double p_atm = pcg / 1013.25;
+            const double Tcg = o->T_method == 1 ? T_mass[k] : Ti(pcg);
+            const double vs = sp == 1 ? vmr : 0.0;
+            const double coef = vmr * dp[k] * NAIR_PER_VMR;
+            const orc_line* ll = lines + loff[li];
+            const long nL = (long)(loff[li + 1] - loff[li]);
+            const bool lm_co2 = sp == 2 && o->line_mixing == 1;
+            std::vector<orc_line> kept;
+            const orc_line* use = ll;
+            long nuse = nL;
+            if (o->dptmn > 0.0 && !lm_co2) {
+                std::vector<uint8_t> keep(nL);
+                reject_weak(ll, nL, Tcg, p_atm, coef, vs, o->dptmn, keep.data());
+                for (long j = 0; j < nL; ++j) if (keep[j]) kept.push_back(ll[j]);
+                use = kept.data();
+                nuse = (long)kept.size();
+            }
+            if (lm_co2) {
+                voigt_xsec(use, nuse, grid.data(), nw, Tcg, p_atm, 0.0, o->cutoff, 3, o->x_far, sig.data());
+                if (y0) {
+                    lm_dispersive(use, nuse, y0 + loff[li], grid.data(), nw, Tcg, p_atm, o->lm_cutoff, o->x_far, ds.data());
+                    for (long i = 0; i < nw; ++i) sig[i] = std::max(sig[i] + ds[i], 0.0);
+                }
+            } else if (nuse > 0) {
+                voigt_xsec(use, nuse, grid.data(), nw, Tcg, p_atm, vs, o->cutoff, o->method, o->x_far, sig.data());
+            } else {
+                std::fill(sig.begin(), sig.end(), 0.0);
+            }
+            for (long i = 0; i < nw; ++i) tk[i] += sig[i] * coef;
+        }
+    }
+    if (o->apply_continuum) {  // sounder.jl:310-322
+        const int qh = prof_index(1), qc = prof_index(2);
+        for (int k = 0; k < L; ++k) {
+            double* tk = tau.data() + (size_t)k * nw;
+            LogPInterp* dummy = nullptr; (void)dummy;
+            auto vmid = [&](int q) {
+                const double* v = pvmr + (size_t)q * n_lev;
+                LogPInterp vi(n_lev, p_lev, v);
+                return vi(p_mid[k]);
+            };
+            const double vh = qh >= 0 ? vmid(qh) : 0.0;
+            const double vc = qc >= 0 ? vmid(qc) : 4.15e-4;
+            const double dz = dp_to_dz_cm(dp[k], p_mid[k], T_mid[k]);
+            if (o->continua & 1) h2o_continuum_add(grid.data(), nw, vh, p_mid[k], T_mid[k], dz, tk);
+            if (o->continua & 2) co2_continuum_add(grid.data(), nw, vc, p_mid[k], T_mid[k], dz, tk);
+            // CIA tables (:co2_cia, :n2, :o2) are not bundled: they contribute zeros
+            // exactly as the reference does when the data is absent (continuum.jl:268-272).
+        }
+    }
+    if (tau_out) std::copy(tau.begin(), tau.end(), tau_out);
+
+    std::vector<double> T_ave(L);
+    for (int k = 0; k < L; ++k) T_ave[k] = cg_temperature_mass(T_lev[k], T_lev[k + 1], p_lev[k], p_lev[k + 1]);
+    const double Tsfc = std::isnan(o->T_sfc) ? T_lev[0] : o->T_sfc;
+    std::vector<double> I(nw);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < nw; ++i)
+        I[i] = rte_point(grid[i], i, nw, L, tau.data(), T_lev, Tsfc, o->mu, o->eps_sfc,
+                         o->source_function, T_ave.data());
+
+    // ils.jl:131-153 evaluated at the nodes the channel interpolation reads,
+    // then sounder.jl:372-377 (linear interpolation, flat outside) and planck.jl:53-57
+    auto ils_at = [&](long ig_idx) {
+        if (!o->with_ils) return I[ig_idx - w0];
+        double acc = 0.0;
+        for (long k = 0; k < (long)kern.size(); ++k) {
+            const long j = ig_idx + (k - n_half);
+            if (j < 0 || j >= n_hi) continue;
+            acc += I[j - w0] * kern[k];
+        }
+        return acc * dhi;
+    };
+    const long nch = ch_end - ch_begin;
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < nch; ++c) {
+        const double nu = nu_ch[c];
+        double R;
+        if (nu <= nu_first) R = ils_at(0);
+        else if (nu >= grid_at(ig.g, n_hi - 1)) R = ils_at(n_hi - 1);
+        else {
+            const long i = idx_floor(nu);
+            const double a = grid_at(ig.g, i), b = grid_at(ig.g, i + 1);
+            const double w = (nu - a) / (b - a);
+            const double r0 = ils_at(i);
+            R = w == 0.0 ? r0 : r0 * (1.0 - w) + ils_at(i + 1) * w;
+        }
+        R_out[c] = R;
+        BT_out[c] = bt(nu, R);
+    }
+    return 0;
+}
+
+}  // extern "C"
