@@ -187,12 +187,12 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
         lp_write_kernel<0><<<g1, kLpThreads, 0, st>>>(d_segs, d_lists, tp, cfg, d_keep, d_chunk, n_chunks,
                                                       d_count, o64, om, d_pairs);
     } else {
-        char* base = (char*)workspace(ctx, "lpmx", S * (8 + 8 + 16 + 16 + 8));
+        char* base = (char*)workspace(ctx, "lpmx", S * (8 + 8 + 16 + 16 + 16));
         om.V = (double*)base;
         om.U = (double*)(base + S * 8);
         om.p0 = (float4*)(base + S * 16);
         om.p1 = (float4*)(base + S * 32);
-        om.p2 = (float2*)(base + S * 48);
+        om.p2 = (float4*)(base + S * 48);
         lp_write_kernel<1><<<g1, kLpThreads, 0, st>>>(d_segs, d_lists, tp, cfg, d_keep, d_chunk, n_chunks,
                                                       d_count, o64, om, d_pairs);
     }

@@ -109,7 +109,7 @@ struct LineParamsMixed {  // FP32 kernel, grid units relative to the grid start
     double* U;            // shifted centre
     float4* p0;           // b2, a, c1, c0        (PV: gV2, aPV, c1, c0)
     float4* p1;           // dfar2, An, fx, y     (PV: kPV, gPV, -, -)
-    float2* p2;           // g, Yw (dispersive line mixing)
+    float4* p2;           // g, Yw, dfar, - (dispersive line mixing, core reach)
 };
 
 struct Tables {

@@ -130,7 +130,7 @@ struct LpOutF64 {
 struct LpOutMixed {
     double *V, *U;
     float4 *p0, *p1;
-    float2* p2;
+    float4* p2;
 };
 
 // Pass B: compacted parameters.  PREC 0 -> FP64 arrays, 1 -> mixed arrays.
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(kLpThreads) lp_write_kernel(
                                               (float)(P * (dg / c) * (dg / c)), (float)(-2.0 * P));
                     om.p1[slot] = make_float4((float)(1.0 / (gVg * gVg)),
                                               (float)(ph.S * co * (1.0 - eta) * cG / gV), 0.f, 0.f);
-                    om.p2[slot] = make_float2(0.f, 0.f);
+                    om.p2[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
                 }
             } else {
                 const double xc = c * f;
@@ -244,12 +244,15 @@ __global__ void __launch_bounds__(kLpThreads) lp_write_kernel(
                     const double Yw = YSn * co;
                     om.V[slot] = (L.nu[j] - cfg.grid0) / dg;
                     om.U[slot] = (ph.nu0s - cfg.grid0) / dg;
-                    const double b = y / fx;
+                    // b^2 floored at 1e-12 grid units^2 (gamma_L ~ 1e-9 cm^-1) so the far-wing
+                    // denominators stay normal in FP32 even at p -> 0
+                    const double b2 = fmax((y / fx) * (y / fx), 1e-12);
                     const double dfar = cfg.x_far / fx;
-                    om.p0[slot] = make_float4((float)(b * b), (float)(An * y * isp / (fx * fx)),
-                                              (float)(P * (dg / c) * (dg / c)), (float)(-2.0 * P));
+                    const double c1 = P * (dg / c) * (dg / c);
+                    om.p0[slot] = make_float4((float)b2, (float)(An * y * isp / (fx * fx)), (float)c1,
+                                              (float)(-2.0 * P - c1 * b2));
                     om.p1[slot] = make_float4((float)fmin(dfar * dfar, 3.0e38), (float)An, (float)fx, (float)y);
-                    om.p2[slot] = make_float2((float)(Yw * isp / fx), (float)Yw);
+                    om.p2[slot] = make_float4((float)(Yw * isp / fx), (float)Yw, (float)fmin(dfar, 1.0e30), 0.f);
                 }
             }
         }

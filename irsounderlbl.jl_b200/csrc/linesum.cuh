@@ -114,43 +114,101 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
     s = t;
 }
 
-template <int METHOD, bool CHECKED>
-__device__ __forceinline__ void mixed_tile(int nt, const float2* su, const float4* s0, const float4* s1,
-                                           const float2* s2, bool lm, const float* pt, float wlo, float whi,
-                                           float cut2, float* tacc, float* tdsp) {
+// 1/x with the MUFU approximation (max 1 ulp); x > 0 and finite here
+__device__ __forceinline__ float rcp_fast(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// One tile of lines against the warp's 8 x 32 points.  For each line the warp
+// decides (uniformly, every lane reads the same line) whether it is
+//   out   -- beyond the cutoff for all of the warp's points: skipped;
+//   fast  -- inside the cutoff and in the Lorentz far wing (|x| > x_far) for all
+//            points: branch-free, one reciprocal per two pairs, pedestal folded
+//            as c1*(d^2 + b^2) + c0' with the constant c0' summed once per line;
+//   slow  -- anything else (Faddeeva core, cutoff edge): per-pair tests.
+// p0 = (b2, a, c1, c0'), p1 = (dfar2, An, fx, y), p2 = (g, Yw, dfar, -), all in
+// grid units relative to the CTA strip; see lp_write_kernel.
+template <int METHOD, bool LM>
+__device__ __forceinline__ void mixed_tile(int nt, const float2* __restrict__ su, const float4* __restrict__ s0,
+                                           const float4* __restrict__ s1, const float4* __restrict__ s2,
+                                           const float* pt, float wc, float cut, float cut2, float* tacc,
+                                           float* tdsp, float& csum) {
+    constexpr float kHalf = 0.5f * kMxWarpPts + 0.5f;
     for (int k = 0; k < nt; ++k) {
         const float2 u = su[k];
-        if (CHECKED && (u.x < wlo || u.x > whi)) continue;  // warp-uniform: line outside this warp's window
+        const float dist = fabsf(u.x - wc);
+        if (dist > cut + kHalf) continue;
         const float4 a0 = s0[k];
-        const float4 a1 = s1[k];
-        const float2 a2 = lm ? s2[k] : make_float2(0.f, 0.f);
+        const float4 a2 = s2[k];
+        if (dist + kHalf <= cut && dist > a2.z + kHalf) {
+            csum += a0.w;
 #pragma unroll
-        for (int q = 0; q < kMxQ; ++q) {
-            const float d = (pt[q] - u.x) - u.y;
-            const float d2 = d * d;
-            if (CHECKED && d2 > cut2) continue;
-            const float ped = fmaf(a0.z, d2, a0.w);
-            if (METHOD == 2) {
-                const float r = __frcp_rn(d2 + a0.x);
-                tacc[q] += fmaf(a0.y, r, fmaf(a1.y, exp2f(-a1.x * d2), ped));
-            } else {
-                const float r = __frcp_rn(d2 + a0.x);
-                float v = fmaf(a0.y, r, ped);
-                float vd = a2.x * d * r;
+            for (int q = 0; q < kMxQ; q += 2) {
+                const float d0 = (pt[q] - u.x) - u.y;
+                const float d1 = (pt[q + 1] - u.x) - u.y;
+                const float e0 = fmaf(d0, d0, a0.x);
+                const float e1 = fmaf(d1, d1, a0.x);
+                const float R = rcp_fast(e0 * e1);
+                const float r0 = e1 * R, r1 = e0 * R;
+                tacc[q] = fmaf(a0.y, r0, fmaf(a0.z, e0, tacc[q]));
+                tacc[q + 1] = fmaf(a0.y, r1, fmaf(a0.z, e1, tacc[q + 1]));
+                if (LM) {
+                    tdsp[q] = fmaf(a2.x * d0, r0, tdsp[q]);
+                    tdsp[q + 1] = fmaf(a2.x * d1, r1, tdsp[q + 1]);
+                }
+            }
+        } else {
+            const float4 a1 = s1[k];
+#pragma unroll
+            for (int q = 0; q < kMxQ; ++q) {
+                const float d = (pt[q] - u.x) - u.y;
+                const float d2 = d * d;
+                if (d2 > cut2) continue;
+                const float e = d2 + a0.x;
+                const float ped = fmaf(a0.z, e, a0.w);
+                float v, vd = 0.f;
                 if (d2 <= a1.x) {  // |x| <= x_far: Faddeeva core
                     const float x = d * a1.z;
                     if (METHOD == 1) {
                         v = fmaf(a1.y, weideman24_32(x, a1.w), ped);
-                        if (lm) vd = a2.y * faddeeva32(x, a1.w).y;
                     } else {
                         const float2 w = faddeeva32(x, a1.w);
                         v = fmaf(a1.y, w.x, ped);
                         vd = a2.y * w.y;
                     }
+                } else {
+                    const float r = __frcp_rn(e);
+                    v = fmaf(a0.y, r, ped);
+                    vd = a2.x * d * r;
                 }
                 tacc[q] += v;
-                if (lm) tdsp[q] += vd;
+                if (LM) tdsp[q] += vd;
             }
+        }
+    }
+}
+
+// PseudoVoigt (voigt.jl:281-313): no far-wing shortcut; p0 = (gV2, aPV, c1, c0),
+// p1 = (kPV, gPV, -, -): value = aPV/(d^2 + gV2) + gPV 2^(-kPV d^2) + c1 d^2 + c0.
+__device__ __forceinline__ void mixed_tile_pv(int nt, const float2* __restrict__ su, const float4* __restrict__ s0,
+                                              const float4* __restrict__ s1, const float* pt, float wc, float cut,
+                                              float cut2, float* tacc) {
+    constexpr float kHalf = 0.5f * kMxWarpPts + 0.5f;
+    for (int k = 0; k < nt; ++k) {
+        const float2 u = su[k];
+        const float dist = fabsf(u.x - wc);
+        if (dist > cut + kHalf) continue;
+        const float4 a0 = s0[k];
+        const float4 a1 = s1[k];
+        const bool inside = dist + kHalf <= cut;
+#pragma unroll
+        for (int q = 0; q < kMxQ; ++q) {
+            const float d = (pt[q] - u.x) - u.y;
+            const float d2 = d * d;
+            if (!inside && d2 > cut2) continue;
+            tacc[q] += fmaf(a0.y, __frcp_rn(d2 + a0.x), fmaf(a1.y, exp2f(-a1.x * d2), fmaf(a0.z, d2, a0.w)));
         }
     }
 }
@@ -162,16 +220,15 @@ __global__ void __launch_bounds__(kMxThreads) linesum_mixed_kernel(
     __shared__ float2 su[kMxTile];
     __shared__ float4 s0[kMxTile];
     __shared__ float4 s1[kMxTile];
-    __shared__ float2 s2[kMxTile];
-    __shared__ long long s_rng[4];
+    __shared__ float4 s2[kMxTile];
+    __shared__ long long s_rng[2];
     const int pl = blockIdx.y;
     const long long strip0 = (long long)blockIdx.x * kMxStrip;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float pt[kMxQ];
 #pragma unroll
     for (int q = 0; q < kMxQ; ++q) pt[q] = (float)(warp * kMxWarpPts + q * 32 + lane);
-    const float wlo = (float)(warp * kMxWarpPts) - cut_g - 1.0f;
-    const float whi = (float)(warp * kMxWarpPts + kMxWarpPts - 1) + cut_g + 1.0f;
+    const float wc = (float)(warp * kMxWarpPts) + 0.5f * (kMxWarpPts - 1);
     const float cut2 = cut_g * cut_g;
     float tsum[kMxQ];
 #pragma unroll
@@ -183,21 +240,14 @@ __global__ void __launch_bounds__(kMxThreads) linesum_mixed_kernel(
         const long long cnt = seg_count[s];
         const bool lm = (sg.flags & 2) != 0;
         if (threadIdx.x == 0) {
-            // window on the sorted unshifted centres, widened by the largest shift;
-            // [i1, i2) are lines within the cutoff of every point of the strip
+            // lines whose shifted centre can be within the cutoff of the strip: search
+            // the sorted unshifted centres, widened by the largest pressure shift
             const double* V = lp.V + sg.off;
-            const double a = (double)strip0, b = (double)(strip0 + kMxStrip - 1);
-            const double m = sg.margin_g;
-            s_rng[0] = lower_bound0(V, a - cut_g - m, cnt);
-            s_rng[3] = lower_bound0(V, b + cut_g + m + 1e-9, cnt);
-            s_rng[1] = lower_bound0(V, b - cut_g + m, cnt);
-            s_rng[2] = lower_bound0(V, a + cut_g - m + 1e-9, cnt);
-            if (s_rng[1] < s_rng[0]) s_rng[1] = s_rng[0];
-            if (s_rng[2] < s_rng[1]) s_rng[2] = s_rng[1];
-            if (s_rng[2] > s_rng[3]) s_rng[2] = s_rng[3];
+            s_rng[0] = lower_bound0(V, (double)strip0 - cut_g - sg.margin_g, cnt);
+            s_rng[1] = lower_bound0(V, (double)(strip0 + kMxStrip - 1) + cut_g + sg.margin_g + 1e-9, cnt);
         }
         __syncthreads();
-        const long long jlo = s_rng[0], i1 = s_rng[1], i2 = s_rng[2], jhi = s_rng[3];
+        const long long jlo = s_rng[0], jhi = s_rng[1];
         __syncthreads();
         float sum[kMxQ], comp[kMxQ], sumD[kMxQ], compD[kMxQ];
 #pragma unroll
@@ -211,20 +261,22 @@ __global__ void __launch_bounds__(kMxThreads) linesum_mixed_kernel(
                 su[threadIdx.x] = make_float2(uh, (float)(u - (double)uh));
                 s0[threadIdx.x] = lp.p0[q];
                 s1[threadIdx.x] = lp.p1[q];
-                if (lm) s2[threadIdx.x] = lp.p2[q];
+                s2[threadIdx.x] = lp.p2[q];
             }
             __syncthreads();
             float tacc[kMxQ], tdsp[kMxQ];
 #pragma unroll
             for (int q = 0; q < kMxQ; ++q) tacc[q] = tdsp[q] = 0.f;
-            const bool interior = t0 >= i1 && t0 + nt <= i2;
-            if (interior)
-                mixed_tile<METHOD, false>(nt, su, s0, s1, s2, lm, pt, wlo, whi, cut2, tacc, tdsp);
+            float csum = 0.f;
+            if (METHOD == 2)
+                mixed_tile_pv(nt, su, s0, s1, pt, wc, cut_g, cut2, tacc);
+            else if (lm)
+                mixed_tile<METHOD, true>(nt, su, s0, s1, s2, pt, wc, cut_g, cut2, tacc, tdsp, csum);
             else
-                mixed_tile<METHOD, true>(nt, su, s0, s1, s2, lm, pt, wlo, whi, cut2, tacc, tdsp);
+                mixed_tile<METHOD, false>(nt, su, s0, s1, s2, pt, wc, cut_g, cut2, tacc, tdsp, csum);
 #pragma unroll
             for (int q = 0; q < kMxQ; ++q) {
-                kahan_add(sum[q], comp[q], tacc[q]);
+                kahan_add(sum[q], comp[q], tacc[q] + csum);
                 if (lm) kahan_add(sumD[q], compD[q], tdsp[q]);
             }
             __syncthreads();
