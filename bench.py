@@ -236,7 +236,10 @@ def main():
     nch = 8461
     R = torch.empty((N_PROF, nch), dtype=torch.float64, device="cuda")
     BT = torch.empty_like(R)
-    stream = torch.cuda.current_stream()
+    # a real (non-default) stream: the library orders its own stream after this one
+    # on entry and this one after its work on exit, so events here bracket the work
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
 
     def step_device(opt):
         pkg.check(lib.irs_forward_model_batch_device(ctx.h, batch.arr, N_PROF, C.byref(s), C.byref(opt),

@@ -154,8 +154,10 @@ int irs_forward_model_batch(irs_ctx* ctx, const irs_profile* profs, int n_prof,
                             double* R, double* BT);
 
 /* Same as irs_forward_model_batch, but R and BT are DEVICE pointers and the call
- * returns once the work is enqueued on `stream` (a cudaStream_t; NULL = the
- * context's stream).  Used when results stay in HBM. */
+ * returns once the work is enqueued.  The work runs on the context's stream,
+ * ordered after the work already queued on `stream` (a cudaStream_t) and with
+ * `stream` ordered after it.  With stream = NULL no ordering is set up: the
+ * results are complete after irs_synchronize(ctx).  Used when results stay in HBM. */
 int irs_forward_model_batch_device(irs_ctx* ctx, const irs_profile* profs, int n_prof,
                                    const irs_sounder* s, const irs_fm_options* o,
                                    double* R_dev, double* BT_dev, void* stream);

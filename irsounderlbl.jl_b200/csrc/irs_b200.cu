@@ -172,7 +172,7 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
     int* d_chunk = (int*)workspace(ctx, "chunk_count", sizeof(int) * (size_t)nseg * n_chunks);
     LpConfig cfg;
     cfg.cutoff = o.cutoff; cfg.x_far = o.x_far; cfg.dptmn = o.dptmn;
-    cfg.grid0 = grid0; cfg.dnu_g = dnu_g; cfg.method = o.method;
+    cfg.grid0 = grid0; cfg.dnu_g = dnu_g; cfg.method = o.method; cfg.n_nu = n_nu;
     const TipsDev tp = tips_dev(ctx);
     dim3 g1(n_chunks, nseg);
     lp_keep_kernel<<<g1, kLpThreads, 0, st>>>(d_segs, d_lists, tp, cfg, d_keep, d_chunk, n_chunks);
@@ -211,11 +211,13 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
         dim3 g2((unsigned)((n_nu + kMxStrip - 1) / kMxStrip), npl);
         const float cut_g = (float)(o.cutoff / dnu_g);
         if (o.method == 1)
-            linesum_mixed_kernel<1><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau);
+            linesum_mixed_kernel<1, false><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau);
         else if (o.method == 2)
-            linesum_mixed_kernel<2><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau);
+            linesum_mixed_kernel<2, false><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau);
+        else if (o.line_mixing)
+            linesum_mixed_kernel<3, true><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau);
         else
-            linesum_mixed_kernel<3><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau);
+            linesum_mixed_kernel<3, false><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau);
     }
     check_launch(ctx);
     return d_tau;

@@ -42,6 +42,7 @@ struct TipsDev {
 struct LpConfig {
     double cutoff, x_far, dptmn;
     double grid0, dnu_g;  // grid start and spacing (mixed parameters are in grid units)
+    long long n_nu;       // grid points (for the pair counts)
     int method;           // 1 Weideman, 2 PseudoVoigt, 3 FullFaddeeva
 };
 
@@ -194,12 +195,13 @@ __global__ void __launch_bounds__(kLpThreads) lp_write_kernel(
             const double c = cfg.cutoff;
             // pair counts inside the cutoff on the uniform grid (roofline work units)
             {
-                const double lo = ceil((ph.nu0s - c - cfg.grid0) / cfg.dnu_g);
-                const double hi = floor((ph.nu0s + c - cfg.grid0) / cfg.dnu_g);
+                const double last = (double)(cfg.n_nu - 1);
+                const double lo = fmax(ceil((ph.nu0s - c - cfg.grid0) / cfg.dnu_g), 0.0);
+                const double hi = fmin(floor((ph.nu0s + c - cfg.grid0) / cfg.dnu_g), last);
                 if (hi >= lo) pairs += (unsigned long long)(hi - lo + 1);
                 const double wc = fmin(cfg.x_far / f, c);
-                const double clo = ceil((ph.nu0s - wc - cfg.grid0) / cfg.dnu_g);
-                const double chi = floor((ph.nu0s + wc - cfg.grid0) / cfg.dnu_g);
+                const double clo = fmax(ceil((ph.nu0s - wc - cfg.grid0) / cfg.dnu_g), 0.0);
+                const double chi = fmin(floor((ph.nu0s + wc - cfg.grid0) / cfg.dnu_g), last);
                 if (chi >= clo) core += (unsigned long long)(chi - clo + 1);
             }
             if (cfg.method == 2) {  // PseudoVoigt, voigt.jl:422-441
@@ -250,7 +252,7 @@ __global__ void __launch_bounds__(kLpThreads) lp_write_kernel(
                     const double dfar = cfg.x_far / fx;
                     const double c1 = P * (dg / c) * (dg / c);
                     om.p0[slot] = make_float4((float)b2, (float)(An * y * isp / (fx * fx)), (float)c1,
-                                              (float)(-2.0 * P - c1 * b2));
+                                              (float)(-2.0 * P));
                     om.p1[slot] = make_float4((float)fmin(dfar * dfar, 3.0e38), (float)An, (float)fx, (float)y);
                     om.p2[slot] = make_float4((float)(Yw * isp / fx), (float)Yw, (float)fmin(dfar, 1.0e30), 0.f);
                 }

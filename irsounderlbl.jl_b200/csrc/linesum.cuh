@@ -92,11 +92,24 @@ __global__ void __launch_bounds__(256) linesum_f64_kernel(
 }
 
 // ----------------------------------------------------------------- mixed
-constexpr int kMxThreads = 256;
-constexpr int kMxQ = 8;                          // points per lane
-constexpr int kMxWarpPts = 32 * kMxQ;            // 256 points per warp
-constexpr int kMxStrip = kMxThreads * kMxQ;      // 2048 points per CTA
-constexpr int kMxTile = 256;                     // lines per shared-memory tile
+// Each warp owns 256 consecutive grid points (8 per lane, point = 32 q + lane)
+// and walks its own window of lines in tiles of 32 staged in warp-private shared
+// memory (no block-wide barriers).  The staging lane of each line precomputes,
+// once per (warp, line): the FP32 position split u = uh + ul relative to the
+// warp, the class of the line for this warp (outside the cutoff / fast / slow),
+// and, for fast lines, the line's pedestal as a quadratic in the point index, so
+// the 32 pedestals of a tile reduce to three numbers.
+//   fast: inside the cutoff and in the Lorentz far wing (|x| > x_far) for all 256
+//         points: d by one FADD from a per-line origin, one MUFU reciprocal per
+//         two pairs, one FMA into the tile sum;
+//   slow: Faddeeva core or cutoff edge: per-pair tests.
+// Tile sums go into a Kahan-compensated FP32 accumulator per point.
+constexpr int kMxWarps = 8;
+constexpr int kMxThreads = 32 * kMxWarps;
+constexpr int kMxQ = 8;                               // points per lane
+constexpr int kMxWarpPts = 32 * kMxQ;                 // 256 points per warp
+constexpr int kMxStrip = kMxWarps * kMxWarpPts;       // 2048 points per CTA
+constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ long long lower_bound0(const double* a, double v, long long n) {
     long long lo = 0, hi = n;
@@ -121,177 +134,218 @@ __device__ __forceinline__ float rcp_fast(float x) {
     return r;
 }
 
-// One tile of lines against the warp's 8 x 32 points.  For each line the warp
-// decides (uniformly, every lane reads the same line) whether it is
-//   out   -- beyond the cutoff for all of the warp's points: skipped;
-//   fast  -- inside the cutoff and in the Lorentz far wing (|x| > x_far) for all
-//            points: branch-free, one reciprocal per two pairs, pedestal folded
-//            as c1*(d^2 + b^2) + c0' with the constant c0' summed once per line;
-//   slow  -- anything else (Faddeeva core, cutoff edge): per-pair tests.
-// p0 = (b2, a, c1, c0'), p1 = (dfar2, An, fx, y), p2 = (g, Yw, dfar, -), all in
-// grid units relative to the CTA strip; see lp_write_kernel.
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int d = 16; d; d >>= 1) v += __shfl_xor_sync(kFull, v, d);
+    return v;
+}
+
+struct WarpTile {
+    float4 su[32];  // uh, ul, g, class (0 outside, 1 fast, 2 slow)
+    float4 s0[32];  // b2, a, c1, c0          (PV: gV2, aPV, c1, c0)
+    float4 s1[32];  // dfar2, An, fx, y       (PV: kPV, gPV, -, -)
+    float sy[32];   // Yw
+};
+
+// window [jlo, jhi) of the lines that can reach this warp's points [wb, wb + 255]
+__device__ __forceinline__ void warp_window(const LpOutMixed& lp, const SegDev& sg, long long cnt,
+                                            long long wb, float cut, int lane, long long& jlo, long long& jhi) {
+    long long a = 0, b = 0;
+    if (lane == 0) {
+        const double* V = lp.V + sg.off;
+        a = lower_bound0(V, (double)wb - cut - sg.margin_g, cnt);
+        b = lower_bound0(V, (double)(wb + kMxWarpPts - 1) + cut + sg.margin_g + 1e-9, cnt);
+    }
+    jlo = __shfl_sync(kFull, a, 0);
+    jhi = __shfl_sync(kFull, b, 0);
+}
+
 template <int METHOD, bool LM>
-__device__ __forceinline__ void mixed_tile(int nt, const float2* __restrict__ su, const float4* __restrict__ s0,
-                                           const float4* __restrict__ s1, const float4* __restrict__ s2,
-                                           const float* pt, float wc, float cut, float cut2, float* tacc,
-                                           float* tdsp, float& csum) {
+__device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, const LpOutMixed& lp, long long wb,
+                                             float cut, float cut2, int lane, WarpTile& T, float* tsum) {
+    constexpr float kCentre = 0.5f * (kMxWarpPts - 1);
     constexpr float kHalf = 0.5f * kMxWarpPts + 0.5f;
-    for (int k = 0; k < nt; ++k) {
-        const float2 u = su[k];
-        const float dist = fabsf(u.x - wc);
-        if (dist > cut + kHalf) continue;
-        const float4 a0 = s0[k];
-        const float4 a2 = s2[k];
-        if (dist + kHalf <= cut && dist > a2.z + kHalf) {
-            csum += a0.w;
+    long long jlo, jhi;
+    warp_window(lp, sg, cnt, wb, cut, lane, jlo, jhi);
+    const float pl0 = (float)lane;
+    float sum[kMxQ], comp[kMxQ], sumD[kMxQ], compD[kMxQ];
 #pragma unroll
-            for (int q = 0; q < kMxQ; q += 2) {
-                const float d0 = (pt[q] - u.x) - u.y;
-                const float d1 = (pt[q + 1] - u.x) - u.y;
-                const float e0 = fmaf(d0, d0, a0.x);
-                const float e1 = fmaf(d1, d1, a0.x);
-                const float R = rcp_fast(e0 * e1);
-                const float r0 = e1 * R, r1 = e0 * R;
-                tacc[q] = fmaf(a0.y, r0, fmaf(a0.z, e0, tacc[q]));
-                tacc[q + 1] = fmaf(a0.y, r1, fmaf(a0.z, e1, tacc[q + 1]));
-                if (LM) {
-                    tdsp[q] = fmaf(a2.x * d0, r0, tdsp[q]);
-                    tdsp[q + 1] = fmaf(a2.x * d1, r1, tdsp[q + 1]);
-                }
+    for (int q = 0; q < kMxQ; ++q) sum[q] = comp[q] = sumD[q] = compD[q] = 0.f;
+    for (long long t0 = jlo; t0 < jhi; t0 += 32) {
+        const int nt = (int)min(32LL, jhi - t0);
+        float pa = 0.f, pb = 0.f, pc = 0.f;  // this line's pedestal quadratic (fast lines)
+        __syncwarp();
+        if (lane < nt) {
+            const long long q = sg.off + t0 + lane;
+            const double u = lp.U[q] - (double)wb;
+            const float uh = (float)u;
+            const float ul = (float)(u - (double)uh);
+            const float4 a0 = lp.p0[q];
+            const float4 a2 = lp.p2[q];
+            const float dist = fabsf(uh - kCentre);
+            float cls = 2.f;
+            if (dist > cut + kHalf) cls = 0.f;
+            else if (dist + kHalf <= cut && dist > a2.z + kHalf) {
+                cls = 1.f;
+                // sum over points p of c1 (p - u)^2 + c0 = p^2 c1 - 2 p c1 u + (c1 u^2 + c0)
+                pa = a0.z;
+                pb = a0.z * uh;
+                pc = fmaf(pb, uh, a0.w);
             }
-        } else {
-            const float4 a1 = s1[k];
+            T.su[lane] = make_float4(uh, ul, a2.x, cls);
+            T.s0[lane] = a0;
+            T.s1[lane] = lp.p1[q];
+            if (LM) T.sy[lane] = a2.y;
+        }
+        const float A = warp_sum(pa), B = warp_sum(pb), Cc = warp_sum(pc);
+        __syncwarp();
+        float tacc[kMxQ], tdsp[kMxQ];
 #pragma unroll
-            for (int q = 0; q < kMxQ; ++q) {
-                const float d = (pt[q] - u.x) - u.y;
-                const float d2 = d * d;
-                if (d2 > cut2) continue;
-                const float e = d2 + a0.x;
-                const float ped = fmaf(a0.z, e, a0.w);
-                float v, vd = 0.f;
-                if (d2 <= a1.x) {  // |x| <= x_far: Faddeeva core
-                    const float x = d * a1.z;
-                    if (METHOD == 1) {
-                        v = fmaf(a1.y, weideman24_32(x, a1.w), ped);
-                    } else {
-                        const float2 w = faddeeva32(x, a1.w);
-                        v = fmaf(a1.y, w.x, ped);
-                        vd = a2.y * w.y;
+        for (int q = 0; q < kMxQ; ++q) tacc[q] = tdsp[q] = 0.f;
+        for (int k = 0; k < nt; ++k) {
+            const float4 u = T.su[k];
+            if (u.w == 0.f) continue;
+            const float4 a0 = T.s0[k];
+            if (u.w == 1.f) {
+                const float d0 = (pl0 - u.x) - u.y;
+#pragma unroll
+                for (int q = 0; q < kMxQ; q += 2) {
+                    const float da = d0 + 32.f * q;
+                    const float db = d0 + 32.f * (q + 1);
+                    const float e0 = fmaf(da, da, a0.x);
+                    const float e1 = fmaf(db, db, a0.x);
+                    const float R = rcp_fast(e0 * e1);
+                    const float r0 = e1 * R, r1 = e0 * R;
+                    tacc[q] = fmaf(a0.y, r0, tacc[q]);
+                    tacc[q + 1] = fmaf(a0.y, r1, tacc[q + 1]);
+                    if (LM) {
+                        tdsp[q] = fmaf(u.z * da, r0, tdsp[q]);
+                        tdsp[q + 1] = fmaf(u.z * db, r1, tdsp[q + 1]);
                     }
-                } else {
-                    const float r = __frcp_rn(e);
-                    v = fmaf(a0.y, r, ped);
-                    vd = a2.x * d * r;
                 }
-                tacc[q] += v;
-                if (LM) tdsp[q] += vd;
+            } else {
+                const float4 a1 = T.s1[k];
+                const float yw = LM ? T.sy[k] : 0.f;
+#pragma unroll
+                for (int q = 0; q < kMxQ; ++q) {
+                    const float d = ((pl0 + 32.f * q) - u.x) - u.y;
+                    const float d2 = d * d;
+                    if (d2 > cut2) continue;
+                    const float ped = fmaf(a0.z, d2, a0.w);
+                    float v, vd;
+                    if (d2 <= a1.x) {  // |x| <= x_far: Faddeeva core
+                        const float x = d * a1.z;
+                        if (METHOD == 1) {
+                            v = fmaf(a1.y, weideman24_32(x, a1.w), ped);
+                            vd = 0.f;
+                        } else {
+                            const float2 w = faddeeva32(x, a1.w);
+                            v = fmaf(a1.y, w.x, ped);
+                            vd = yw * w.y;
+                        }
+                    } else {
+                        const float r = rcp_fast(d2 + a0.x);
+                        v = fmaf(a0.y, r, ped);
+                        vd = u.z * d * r;
+                    }
+                    tacc[q] += v;
+                    if (LM) tdsp[q] += vd;
+                }
             }
         }
+#pragma unroll
+        for (int q = 0; q < kMxQ; ++q) {
+            const float p = pl0 + 32.f * q;
+            kahan_add(sum[q], comp[q], tacc[q] + fmaf(p, fmaf(p, A, -2.f * B), Cc));
+            if (LM) kahan_add(sumD[q], compD[q], tdsp[q]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kMxQ; ++q) {
+        float sig = fmaxf(sum[q], 0.f);
+        if (LM) sig = fmaxf(sig + sumD[q], 0.f);
+        tsum[q] += sig;
     }
 }
 
 // PseudoVoigt (voigt.jl:281-313): no far-wing shortcut; p0 = (gV2, aPV, c1, c0),
 // p1 = (kPV, gPV, -, -): value = aPV/(d^2 + gV2) + gPV 2^(-kPV d^2) + c1 d^2 + c0.
-__device__ __forceinline__ void mixed_tile_pv(int nt, const float2* __restrict__ su, const float4* __restrict__ s0,
-                                              const float4* __restrict__ s1, const float* pt, float wc, float cut,
-                                              float cut2, float* tacc) {
+__device__ __forceinline__ void warp_segment_pv(const SegDev& sg, long long cnt, const LpOutMixed& lp, long long wb,
+                                                float cut, float cut2, int lane, WarpTile& T, float* tsum) {
+    constexpr float kCentre = 0.5f * (kMxWarpPts - 1);
     constexpr float kHalf = 0.5f * kMxWarpPts + 0.5f;
-    for (int k = 0; k < nt; ++k) {
-        const float2 u = su[k];
-        const float dist = fabsf(u.x - wc);
-        if (dist > cut + kHalf) continue;
-        const float4 a0 = s0[k];
-        const float4 a1 = s1[k];
-        const bool inside = dist + kHalf <= cut;
+    long long jlo, jhi;
+    warp_window(lp, sg, cnt, wb, cut, lane, jlo, jhi);
+    const float pl0 = (float)lane;
+    float sum[kMxQ], comp[kMxQ];
 #pragma unroll
-        for (int q = 0; q < kMxQ; ++q) {
-            const float d = (pt[q] - u.x) - u.y;
-            const float d2 = d * d;
-            if (!inside && d2 > cut2) continue;
-            tacc[q] += fmaf(a0.y, __frcp_rn(d2 + a0.x), fmaf(a1.y, exp2f(-a1.x * d2), fmaf(a0.z, d2, a0.w)));
+    for (int q = 0; q < kMxQ; ++q) sum[q] = comp[q] = 0.f;
+    for (long long t0 = jlo; t0 < jhi; t0 += 32) {
+        const int nt = (int)min(32LL, jhi - t0);
+        __syncwarp();
+        if (lane < nt) {
+            const long long q = sg.off + t0 + lane;
+            const double u = lp.U[q] - (double)wb;
+            const float uh = (float)u;
+            const float dist = fabsf(uh - kCentre);
+            const float cls = dist > cut + kHalf ? 0.f : (dist + kHalf <= cut ? 1.f : 2.f);
+            T.su[lane] = make_float4(uh, (float)(u - (double)uh), 0.f, cls);
+            T.s0[lane] = lp.p0[q];
+            T.s1[lane] = lp.p1[q];
         }
+        __syncwarp();
+        float tacc[kMxQ];
+#pragma unroll
+        for (int q = 0; q < kMxQ; ++q) tacc[q] = 0.f;
+        for (int k = 0; k < nt; ++k) {
+            const float4 u = T.su[k];
+            if (u.w == 0.f) continue;
+            const float4 a0 = T.s0[k];
+            const float4 a1 = T.s1[k];
+#pragma unroll
+            for (int q = 0; q < kMxQ; ++q) {
+                const float d = ((pl0 + 32.f * q) - u.x) - u.y;
+                const float d2 = d * d;
+                if (u.w == 2.f && d2 > cut2) continue;
+                tacc[q] += fmaf(a0.y, rcp_fast(d2 + a0.x), fmaf(a1.y, exp2f(-a1.x * d2), fmaf(a0.z, d2, a0.w)));
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kMxQ; ++q) kahan_add(sum[q], comp[q], tacc[q]);
     }
+#pragma unroll
+    for (int q = 0; q < kMxQ; ++q) tsum[q] += fmaxf(sum[q], 0.f);
 }
 
-template <int METHOD>
-__global__ void __launch_bounds__(kMxThreads) linesum_mixed_kernel(
+template <int METHOD, bool ANY_LM>
+__global__ void __launch_bounds__(kMxThreads, ANY_LM ? 2 : 3) linesum_mixed_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const int2* __restrict__ pl_segs,
     LpOutMixed lp, long long n_nu, float cut_g, float* __restrict__ tau) {
-    __shared__ float2 su[kMxTile];
-    __shared__ float4 s0[kMxTile];
-    __shared__ float4 s1[kMxTile];
-    __shared__ float4 s2[kMxTile];
-    __shared__ long long s_rng[2];
-    const int pl = blockIdx.y;
-    const long long strip0 = (long long)blockIdx.x * kMxStrip;
+    __shared__ WarpTile tiles[kMxWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float pt[kMxQ];
-#pragma unroll
-    for (int q = 0; q < kMxQ; ++q) pt[q] = (float)(warp * kMxWarpPts + q * 32 + lane);
-    const float wc = (float)(warp * kMxWarpPts) + 0.5f * (kMxWarpPts - 1);
+    const int pl = blockIdx.y;
+    const long long wb = (long long)blockIdx.x * kMxStrip + (long long)warp * kMxWarpPts;
+    if (wb >= n_nu) return;  // no block-wide barriers below: whole warps may leave
     const float cut2 = cut_g * cut_g;
+    WarpTile& T = tiles[warp];
     float tsum[kMxQ];
 #pragma unroll
     for (int q = 0; q < kMxQ; ++q) tsum[q] = 0.f;
-
     const int2 rng = pl_segs[pl];
     for (int s = rng.x; s < rng.x + rng.y; ++s) {
         const SegDev sg = segs[s];
         const long long cnt = seg_count[s];
-        const bool lm = (sg.flags & 2) != 0;
-        if (threadIdx.x == 0) {
-            // lines whose shifted centre can be within the cutoff of the strip: search
-            // the sorted unshifted centres, widened by the largest pressure shift
-            const double* V = lp.V + sg.off;
-            s_rng[0] = lower_bound0(V, (double)strip0 - cut_g - sg.margin_g, cnt);
-            s_rng[1] = lower_bound0(V, (double)(strip0 + kMxStrip - 1) + cut_g + sg.margin_g + 1e-9, cnt);
-        }
-        __syncthreads();
-        const long long jlo = s_rng[0], jhi = s_rng[1];
-        __syncthreads();
-        float sum[kMxQ], comp[kMxQ], sumD[kMxQ], compD[kMxQ];
-#pragma unroll
-        for (int q = 0; q < kMxQ; ++q) sum[q] = comp[q] = sumD[q] = compD[q] = 0.f;
-        for (long long t0 = jlo; t0 < jhi; t0 += kMxTile) {
-            const int nt = (int)min((long long)kMxTile, jhi - t0);
-            if (threadIdx.x < nt) {
-                const long long q = sg.off + t0 + threadIdx.x;
-                const double u = lp.U[q] - (double)strip0;
-                const float uh = (float)u;
-                su[threadIdx.x] = make_float2(uh, (float)(u - (double)uh));
-                s0[threadIdx.x] = lp.p0[q];
-                s1[threadIdx.x] = lp.p1[q];
-                s2[threadIdx.x] = lp.p2[q];
-            }
-            __syncthreads();
-            float tacc[kMxQ], tdsp[kMxQ];
-#pragma unroll
-            for (int q = 0; q < kMxQ; ++q) tacc[q] = tdsp[q] = 0.f;
-            float csum = 0.f;
-            if (METHOD == 2)
-                mixed_tile_pv(nt, su, s0, s1, pt, wc, cut_g, cut2, tacc);
-            else if (lm)
-                mixed_tile<METHOD, true>(nt, su, s0, s1, s2, pt, wc, cut_g, cut2, tacc, tdsp, csum);
-            else
-                mixed_tile<METHOD, false>(nt, su, s0, s1, s2, pt, wc, cut_g, cut2, tacc, tdsp, csum);
-#pragma unroll
-            for (int q = 0; q < kMxQ; ++q) {
-                kahan_add(sum[q], comp[q], tacc[q] + csum);
-                if (lm) kahan_add(sumD[q], compD[q], tdsp[q]);
-            }
-            __syncthreads();
-        }
-#pragma unroll
-        for (int q = 0; q < kMxQ; ++q) {
-            float sig = fmaxf(sum[q], 0.f);
-            if (lm) sig = fmaxf(sig + sumD[q], 0.f);
-            tsum[q] += sig;
-        }
+        if (METHOD == 2)
+            warp_segment_pv(sg, cnt, lp, wb, cut_g, cut2, lane, T, tsum);
+        else if (ANY_LM && (sg.flags & 2))
+            warp_segment<METHOD, true>(sg, cnt, lp, wb, cut_g, cut2, lane, T, tsum);
+        else
+            warp_segment<METHOD, false>(sg, cnt, lp, wb, cut_g, cut2, lane, T, tsum);
     }
     float* out = tau + (size_t)pl * n_nu;
 #pragma unroll
     for (int q = 0; q < kMxQ; ++q) {
-        const long long i = strip0 + warp * kMxWarpPts + q * 32 + lane;
+        const long long i = wb + q * 32 + lane;
         if (i < n_nu) out[i] = tsum[q];
     }
 }
