@@ -272,6 +272,23 @@ static void forward_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, c
         if (pl.pl_segs[key].y == 0) pl.pl_segs[key].x = (int)i;
         pl.pl_segs[key].y++;
     }
+    {  // size every workspace up front so no (synchronising) reallocation falls inside a timed stage
+        int64_t slots = 0, max_list = 0;
+        for (auto& g : pl.segs) { slots += ctx->lists[g.list].n; max_list = std::max<int64_t>(max_list, ctx->lists[g.list].n); }
+        const bool mixed = o.precision == IRS_MIXED;
+        const int nseg = std::max<int>((int)pl.segs.size(), 1);
+        workspace(ctx, "tau", (size_t)n_prof * L * n_nu * (mixed ? sizeof(float) : sizeof(double)));
+        workspace(ctx, "I", (size_t)n_prof * n_nu * sizeof(double));
+        workspace(ctx, "grid", n_nu * sizeof(double));
+        if (slots > 0) {
+            workspace(ctx, mixed ? "lpmx" : "lp64", (size_t)slots * (mixed ? 64 : 48));
+            workspace(ctx, "keep", (size_t)slots);
+            workspace(ctx, "chunk_count", sizeof(int) * (size_t)nseg * ((max_list + kLpChunk - 1) / kLpChunk));
+        }
+        workspace(ctx, "seg_count", sizeof(int) * nseg);
+        workspace(ctx, "lrt", std::max<size_t>(lrt.size(), 1) * sizeof(LayerRT));
+        workspace(ctx, "prt", std::max<size_t>(prt.size(), 1) * sizeof(ProfileRT));
+    }
     IRS_CUDA(cudaEventRecord(ctx->ev[0], st));
     double* d_grid = (double*)workspace(ctx, "grid", n_nu * sizeof(double));
     grid_values_kernel<<<(unsigned)((n_nu + 255) / 256), 256, 0, st>>>(to_dev(ig.g), d_grid);

@@ -141,10 +141,11 @@ __device__ __forceinline__ float warp_sum(float v) {
 }
 
 struct WarpTile {
-    float4 su[32];  // uh, ul, g, class (0 outside, 1 fast, 2 slow)
-    float4 s0[32];  // b2, a, c1, c0          (PV: gV2, aPV, c1, c0)
-    float4 s1[32];  // dfar2, An, fx, y       (PV: kPV, gPV, -, -)
-    float sy[32];   // Yw
+    float4 fu[32];  // fast lines: uh, ul, b2, a               (PV: uh, ul, -, class)
+    float4 su[32];  // slow lines: uh, ul, b2, a               (PV: gV2, aPV, c1, c0)
+    float4 sp[32];  // slow lines: c1, c0, dfar2, An           (PV: kPV, gPV, -, -)
+    float4 sq[32];  // slow lines: fx, y, g, Yw
+    float fg[32];   // fast lines: g (dispersive line mixing)
 };
 
 // window [jlo, jhi) of the lines that can reach this warp's points [wb, wb + 255]
@@ -160,6 +161,18 @@ __device__ __forceinline__ void warp_window(const LpOutMixed& lp, const SegDev& 
     jhi = __shfl_sync(kFull, b, 0);
 }
 
+// Fast line, two points q and q+1 with packed FP32x2 arithmetic.  The squared
+// distances are formed in swapped order es = (e[q+1], e[q]) so one reciprocal of
+// their product gives both reciprocals with a single packed multiply:
+//   r = es * (1/(e[q] e[q+1])) = (1/e[q], 1/e[q+1]).
+__device__ __forceinline__ void fast_pair(float2 d0s, float2 offs, float2 b2, float2 a, float2& acc) {
+    const float2 dds = __fadd2_rn(d0s, offs);       // (d[q+1], d[q])
+    const float2 es = __ffma2_rn(dds, dds, b2);     // (e[q+1], e[q])
+    const float R = rcp_fast(es.x * es.y);
+    const float2 r = __fmul2_rn(es, make_float2(R, R));
+    acc = __ffma2_rn(a, r, acc);
+}
+
 template <int METHOD, bool LM>
 __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, const LpOutMixed& lp, long long wb,
                                              float cut, float cut2, int lane, WarpTile& T, float* tsum) {
@@ -168,95 +181,116 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
     long long jlo, jhi;
     warp_window(lp, sg, cnt, wb, cut, lane, jlo, jhi);
     const float pl0 = (float)lane;
+    // per-lane constant offsets of the point pairs, swapped: (32(q+1), 32q)
+    float2 offs[kMxQ / 2];
+#pragma unroll
+    for (int h = 0; h < kMxQ / 2; ++h) offs[h] = make_float2(32.f * (2 * h + 1), 32.f * (2 * h));
     float sum[kMxQ], comp[kMxQ], sumD[kMxQ], compD[kMxQ];
 #pragma unroll
     for (int q = 0; q < kMxQ; ++q) sum[q] = comp[q] = sumD[q] = compD[q] = 0.f;
+    const unsigned lt = (1u << lane) - 1u;
     for (long long t0 = jlo; t0 < jhi; t0 += 32) {
         const int nt = (int)min(32LL, jhi - t0);
         float pa = 0.f, pb = 0.f, pc = 0.f;  // this line's pedestal quadratic (fast lines)
-        __syncwarp();
+        int cls = 0;
+        float4 a0, a1, a2;
+        float uh = 0.f, ul = 0.f;
         if (lane < nt) {
             const long long q = sg.off + t0 + lane;
             const double u = lp.U[q] - (double)wb;
-            const float uh = (float)u;
-            const float ul = (float)(u - (double)uh);
-            const float4 a0 = lp.p0[q];
-            const float4 a2 = lp.p2[q];
+            uh = (float)u;
+            ul = (float)(u - (double)uh);
+            a0 = lp.p0[q];
+            a2 = lp.p2[q];
             const float dist = fabsf(uh - kCentre);
-            float cls = 2.f;
-            if (dist > cut + kHalf) cls = 0.f;
+            if (dist > cut + kHalf) cls = 0;
             else if (dist + kHalf <= cut && dist > a2.z + kHalf) {
-                cls = 1.f;
+                cls = 1;
                 // sum over points p of c1 (p - u)^2 + c0 = p^2 c1 - 2 p c1 u + (c1 u^2 + c0)
                 pa = a0.z;
                 pb = a0.z * uh;
                 pc = fmaf(pb, uh, a0.w);
+            } else {
+                cls = 2;
+                a1 = lp.p1[q];
             }
-            T.su[lane] = make_float4(uh, ul, a2.x, cls);
-            T.s0[lane] = a0;
-            T.s1[lane] = lp.p1[q];
-            if (LM) T.sy[lane] = a2.y;
+        }
+        const unsigned fm = __ballot_sync(kFull, cls == 1), sm = __ballot_sync(kFull, cls == 2);
+        __syncwarp();
+        if (cls == 1) {
+            const int pos = __popc(fm & lt);
+            T.fu[pos] = make_float4(uh, ul, a0.x, a0.y);
+            if (LM) T.fg[pos] = a2.x;
+        } else if (cls == 2) {
+            const int pos = __popc(sm & lt);
+            T.su[pos] = make_float4(uh, ul, a0.x, a0.y);
+            T.sp[pos] = make_float4(a0.z, a0.w, a1.x, a1.y);
+            T.sq[pos] = make_float4(a1.z, a1.w, a2.x, a2.y);
         }
         const float A = warp_sum(pa), B = warp_sum(pb), Cc = warp_sum(pc);
         __syncwarp();
-        float tacc[kMxQ], tdsp[kMxQ];
+        const int nf = __popc(fm), ns = __popc(sm);
+        float2 acc2[kMxQ / 2];
+        float tdsp[kMxQ];
 #pragma unroll
-        for (int q = 0; q < kMxQ; ++q) tacc[q] = tdsp[q] = 0.f;
-        for (int k = 0; k < nt; ++k) {
-            const float4 u = T.su[k];
-            if (u.w == 0.f) continue;
-            const float4 a0 = T.s0[k];
-            if (u.w == 1.f) {
-                const float d0 = (pl0 - u.x) - u.y;
+        for (int h = 0; h < kMxQ / 2; ++h) acc2[h] = make_float2(0.f, 0.f);
 #pragma unroll
-                for (int q = 0; q < kMxQ; q += 2) {
-                    const float da = d0 + 32.f * q;
-                    const float db = d0 + 32.f * (q + 1);
-                    const float e0 = fmaf(da, da, a0.x);
-                    const float e1 = fmaf(db, db, a0.x);
-                    const float R = rcp_fast(e0 * e1);
-                    const float r0 = e1 * R, r1 = e0 * R;
-                    tacc[q] = fmaf(a0.y, r0, tacc[q]);
-                    tacc[q + 1] = fmaf(a0.y, r1, tacc[q + 1]);
-                    if (LM) {
-                        tdsp[q] = fmaf(u.z * da, r0, tdsp[q]);
-                        tdsp[q + 1] = fmaf(u.z * db, r1, tdsp[q + 1]);
-                    }
-                }
-            } else {
-                const float4 a1 = T.s1[k];
-                const float yw = LM ? T.sy[k] : 0.f;
+        for (int q = 0; q < kMxQ; ++q) tdsp[q] = 0.f;
+        for (int k = 0; k < nf; ++k) {
+            const float4 f = T.fu[k];
+            const float d0 = (pl0 - f.x) - f.y;
+            const float2 d0s = make_float2(d0, d0), b2 = make_float2(f.z, f.z), a = make_float2(f.w, f.w);
+#pragma unroll
+            for (int h = 0; h < kMxQ / 2; ++h) fast_pair(d0s, offs[h], b2, a, acc2[h]);
+            if (LM) {
+                const float g = T.fg[k];
 #pragma unroll
                 for (int q = 0; q < kMxQ; ++q) {
-                    const float d = ((pl0 + 32.f * q) - u.x) - u.y;
-                    const float d2 = d * d;
-                    if (d2 > cut2) continue;
-                    const float ped = fmaf(a0.z, d2, a0.w);
-                    float v, vd;
-                    if (d2 <= a1.x) {  // |x| <= x_far: Faddeeva core
-                        const float x = d * a1.z;
-                        if (METHOD == 1) {
-                            v = fmaf(a1.y, weideman24_32(x, a1.w), ped);
-                            vd = 0.f;
-                        } else {
-                            const float2 w = faddeeva32(x, a1.w);
-                            v = fmaf(a1.y, w.x, ped);
-                            vd = yw * w.y;
-                        }
-                    } else {
-                        const float r = rcp_fast(d2 + a0.x);
-                        v = fmaf(a0.y, r, ped);
-                        vd = u.z * d * r;
-                    }
-                    tacc[q] += v;
-                    if (LM) tdsp[q] += vd;
+                    const float d = d0 + 32.f * q;
+                    tdsp[q] = fmaf(g * d, rcp_fast(fmaf(d, d, f.z)), tdsp[q]);
                 }
+            }
+        }
+        float tacc[kMxQ];
+#pragma unroll
+        for (int h = 0; h < kMxQ / 2; ++h) {
+            tacc[2 * h] = acc2[h].x;
+            tacc[2 * h + 1] = acc2[h].y;
+        }
+        for (int k = 0; k < ns; ++k) {
+            const float4 u = T.su[k];
+            const float4 p = T.sp[k];
+            const float4 w = T.sq[k];
+#pragma unroll
+            for (int q = 0; q < kMxQ; ++q) {
+                const float d = ((pl0 + 32.f * q) - u.x) - u.y;
+                const float d2 = d * d;
+                if (d2 > cut2) continue;
+                const float ped = fmaf(p.x, d2, p.y);
+                float v, vd;
+                if (d2 <= p.z) {  // |x| <= x_far: Faddeeva core
+                    const float x = d * w.x;
+                    if (METHOD == 1) {
+                        v = fmaf(p.w, weideman24_32(x, w.y), ped);
+                        vd = 0.f;
+                    } else {
+                        const float2 fw = faddeeva32(x, w.y);
+                        v = fmaf(p.w, fw.x, ped);
+                        vd = w.w * fw.y;
+                    }
+                } else {
+                    const float r = rcp_fast(d2 + u.z);
+                    v = fmaf(u.w, r, ped);
+                    vd = w.z * d * r;
+                }
+                tacc[q] += v;
+                if (LM) tdsp[q] += vd;
             }
         }
 #pragma unroll
         for (int q = 0; q < kMxQ; ++q) {
-            const float p = pl0 + 32.f * q;
-            kahan_add(sum[q], comp[q], tacc[q] + fmaf(p, fmaf(p, A, -2.f * B), Cc));
+            const float pp = pl0 + 32.f * q;
+            kahan_add(sum[q], comp[q], tacc[q] + fmaf(pp, fmaf(pp, A, -2.f * B), Cc));
             if (LM) kahan_add(sumD[q], compD[q], tdsp[q]);
         }
     }
@@ -289,19 +323,19 @@ __device__ __forceinline__ void warp_segment_pv(const SegDev& sg, long long cnt,
             const float uh = (float)u;
             const float dist = fabsf(uh - kCentre);
             const float cls = dist > cut + kHalf ? 0.f : (dist + kHalf <= cut ? 1.f : 2.f);
-            T.su[lane] = make_float4(uh, (float)(u - (double)uh), 0.f, cls);
-            T.s0[lane] = lp.p0[q];
-            T.s1[lane] = lp.p1[q];
+            T.fu[lane] = make_float4(uh, (float)(u - (double)uh), 0.f, cls);
+            T.su[lane] = lp.p0[q];
+            T.sp[lane] = lp.p1[q];
         }
         __syncwarp();
         float tacc[kMxQ];
 #pragma unroll
         for (int q = 0; q < kMxQ; ++q) tacc[q] = 0.f;
         for (int k = 0; k < nt; ++k) {
-            const float4 u = T.su[k];
+            const float4 u = T.fu[k];
             if (u.w == 0.f) continue;
-            const float4 a0 = T.s0[k];
-            const float4 a1 = T.s1[k];
+            const float4 a0 = T.su[k];
+            const float4 a1 = T.sp[k];
 #pragma unroll
             for (int q = 0; q < kMxQ; ++q) {
                 const float d = ((pl0 + 32.f * q) - u.x) - u.y;

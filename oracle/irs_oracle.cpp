@@ -620,6 +620,176 @@ InternalGrid internal_grid(const orc_sounder& s, const orc_fm_options& o) {
     return ig;
 }
 
+// ======================================================== Jacobian pieces
+// partition.jl:52-66 (staircase slope of the 1 K TIPS table)
+double partition_derivative(int mol, int iso, double T) {
+    auto it = g_tips.find({mol, iso});
+    if (it == g_tips.end()) return 1.0 / T_REF;
+    const Tips& t = it->second;
+    const long i_lo = (long)std::floor(T) - t.tmin + 1, i_hi = i_lo + 1;
+    if (i_lo < 1 || i_hi > (long)t.q.size()) return 0.0;
+    return t.q[i_hi - 1] - t.q[i_lo - 1];
+}
+
+// schwarzschild.jl:71-90
+double lit_corr_deriv(double s) {
+    if (s < 1e-4) return 0.5 - s * (2.0 / 3.0 - s * 0.375);
+    const double e = std::exp(-s);
+    return (e * (s + 1.0) - 1.0) / (s * s) + e;
+}
+double cim_corr_deriv(double s) {
+    if (s < 0.06) return 1.0 / 6.0;
+    const double w = std::exp(-s);
+    return 2.0 / (s * s) - 2.0 * w / ((w - 1.0) * (w - 1.0));
+}
+double dB_dT(double nu, double T) {  // planck.jl:67-71
+    const double x = PLANCK_C2 * nu / T, ex = std::exp(x);
+    return PLANCK_C1 * PLANCK_C2 * (nu * nu * nu * nu) * ex / ((T * T) * (ex - 1.0) * (ex - 1.0));
+}
+// schwarzschild_jacobian.jl:47-53
+double cg_mass_frac(double p1, double p2) {
+    if (approx_eq(p1, p2)) return 0.5;
+    const double a = std::log(p2 / p1);
+    if (std::fabs(a) < 1e-3) return 0.5 + a / 12.0;
+    const double b = p2 / p1;
+    return ((a - 1.0) * b + 1.0) / (a * (b - 1.0));
+}
+// vmr_jacobian.jl:81-107
+void cg_column_vmr_grad(double v1, double v2, double p1, double p2, double& g1, double& g2) {
+    if (v1 <= 0.0 || v2 <= 0.0) { g1 = g2 = 0.5; return; }
+    if (approx_eq(v1, v2)) { const double fr = cg_mass_frac(p1, p2); g1 = 1.0 - fr; g2 = fr; return; }
+    const double L = std::log(p2 / p1), al = std::log(v2 / v1) / L, be = al + 1.0, dp = std::fabs(p1 - p2);
+    if (std::fabs(be) < 1e-6) {
+        const double h1 = std::max(std::fabs(v1), 1e-300) * 1e-6, h2 = std::max(std::fabs(v2), 1e-300) * 1e-6;
+        g1 = (cg_column_vmr(v1 + h1, v2, p1, p2) - cg_column_vmr(v1 - h1, v2, p1, p2)) / (2 * h1);
+        g2 = (cg_column_vmr(v1, v2 + h2, p1, p2) - cg_column_vmr(v1, v2 - h2, p1, p2)) / (2 * h2);
+        return;
+    }
+    const double r = p2 / p1, rb = std::pow(r, be);
+    const double c = v1 * p1 * (1.0 - rb) / (be * dp);
+    const double J = (v1 * p1 / L) * ((rb - 1.0) / (be * be) - rb * L / be);
+    g1 = c / v1 - J / (v1 * dp);
+    g2 = J / (v2 * dp);
+}
+// vmr_jacobian.jl:120-125
+double dBT_dR(double nu, double R) {
+    if (R <= 0.0) return 0.0;
+    const double A = PLANCK_C1 * (nu * nu * nu), L = std::log1p(A / R);
+    return PLANCK_C2 * nu * A / ((L * L) * R * (R + A));
+}
+
+// cross_section_jacobian.jl:43-56
+void voigt_H_and_grad(double x, double y, double x_far, double& H, double& Hx, double& Hy) {
+    if (std::fabs(x) > x_far) {
+        const double d = x * x + y * y, d2 = d * d;
+        H = y * INV_SQRT_PI / d;
+        Hx = -2.0 * x * y * INV_SQRT_PI / d2;
+        Hy = INV_SQRT_PI * (x * x - y * y) / d2;
+        return;
+    }
+    const cplx w = faddeeva(x, y);
+    const double K = w.real(), L = w.imag();
+    H = K;
+    Hx = -2.0 * x * K + 2.0 * y * L;
+    Hy = 2.0 * (x * L + y * K) - 2.0 * INV_SQRT_PI;
+}
+
+struct Grad { std::vector<double> s, dT, dp, dv; };
+
+// cross_section_jacobian.jl:155-240 (sigma, dsigma/dT, dsigma/dp_atm, dsigma/dvmr_self)
+void voigt_xsec_grad(const orc_line* lines, long nL, const double* grid, long n_nu, double T, double p,
+                     double vs, double cutoff, double x_far, Grad& g) {
+    std::vector<double> nu0(nL), f(nL), df(nL), y(nL), dyT(nL), dyp(nL), dyv(nL), dn0p(nL), dn0v(nL),
+        Sn(nL), dSnT(nL), Hc(nL), dHcT(nL), dHcp(nL), dHcv(nL);
+    for (long j = 0; j < nL; ++j) {
+        const orc_line& l = lines[j];
+        const int mol = l.mol_id;
+        const double n_air = (double)l.temp_depend, n_self = n_self_of(mol, n_air);
+        const double d_air = (double)l.pressure_shift, d_self = delta_self_of(mol);
+        LineParams lp = line_params(l, T, p, vs);
+        nu0[j] = lp.nu0;
+        dn0p[j] = d_air * (1.0 - vs) + d_self * vs;
+        dn0v[j] = (d_self - d_air) * p;
+        // temperature_scaled_intensity_deriv, broadening.jl:112-128
+        const double QT = partition_function(mol, l.iso_id, T), dQT = partition_derivative(mol, l.iso_id, T);
+        const double a = C2_LINE * l.wavenumber;
+        const double dlnS = -dQT / QT + C2_LINE * l.lower_energy / (T * T) - (a / (T * T)) / (std::exp(a / T) - 1.0);
+        const double S = lp.S, dS = S * dlnS;
+        // pressure_broadened_width_deriv, broadening.jl:62-78
+        const double tr = T_REF / T;
+        const double A = std::pow(tr, n_air) * (double)l.air_broad * (1.0 - vs) * p;
+        const double B = std::pow(tr, n_self) * (double)l.self_broad * vs * p;
+        const double gl = A + B, dglT = -(n_air * A + n_self * B) / T;
+        double gd = lp.gd;
+        const double dgd = gd / (2.0 * T);
+        gd = std::max(gd, 1e-10);
+        const double fj = SQRT_LN2 / gd, dfj = -fj * (dgd / gd);
+        const double ac = std::pow(tr, n_air) * (double)l.air_broad, bc = std::pow(tr, n_self) * (double)l.self_broad;
+        const double dglp = gl / p, dglv = (bc - ac) * p;
+        f[j] = fj; df[j] = dfj; y[j] = gl * fj;
+        dyT[j] = dglT * fj + gl * dfj; dyp[j] = dglp * fj; dyv[j] = dglv * fj;
+        Sn[j] = S * fj * INV_SQRT_PI;
+        dSnT[j] = (dS * fj + S * dfj) * INV_SQRT_PI;
+        double hc, hx, hy;
+        voigt_H_and_grad(cutoff * fj, y[j], x_far, hc, hx, hy);
+        Hc[j] = hc;
+        dHcT[j] = hx * (cutoff * dfj) + hy * dyT[j];
+        dHcp[j] = hy * dyp[j];
+        dHcv[j] = hy * dyv[j];
+    }
+    g.s.assign(n_nu, 0.0); g.dT.assign(n_nu, 0.0); g.dp.assign(n_nu, 0.0); g.dv.assign(n_nu, 0.0);
+    const double invc = 1.0 / cutoff, invc2 = invc * invc;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n_nu; ++i) {
+        const double nu = grid[i];
+        const long jlo = lower_bound1(nu0.data(), nu - cutoff, nL), jhi = upper_bound1(nu0.data(), nu + cutoff, nL);
+        double acc = 0, aT = 0, ap = 0, av = 0;
+        for (long jj = jlo; jj <= jhi; ++jj) {
+            const long j = jj - 1;
+            const double d = nu - nu0[j], fj = f[j], x = d * fj;
+            double H, Hx, Hy;
+            voigt_H_and_grad(x, y[j], x_far, H, Hx, Hy);
+            const double dHt = Hx * (d * df[j]) + Hy * dyT[j];
+            const double dHp = Hx * (-dn0p[j] * fj) + Hy * dyp[j];
+            const double dHv = Hx * (-dn0v[j] * fj) + Hy * dyv[j];
+            const double pedfac = 2.0 - (d * invc) * (d * invc);
+            const double dpfp = 2.0 * d * dn0p[j] * invc2, dpfv = 2.0 * d * dn0v[j] * invc2;
+            const double dpedT = pedfac * dHcT[j];
+            const double dpedp = dpfp * Hc[j] + pedfac * dHcp[j];
+            const double dpedv = dpfv * Hc[j] + pedfac * dHcv[j];
+            const double Hm = H - pedfac * Hc[j];
+            acc += Sn[j] * Hm;
+            aT += dSnT[j] * Hm + Sn[j] * (dHt - dpedT);
+            ap += Sn[j] * (dHp - dpedp);
+            av += Sn[j] * (dHv - dpedv);
+        }
+        if (acc > 0.0) { g.s[i] = acc; g.dT[i] = aT; g.dp[i] = ap; g.dv[i] = av; }
+    }
+}
+
+// cross_section_jacobian.jl:255-322 for VP_Y: analytic Voigt baseline plus the
+// dispersive perturbation central-differenced in (T, p)
+void species_grad(const orc_line* ll, long nL, const double* y0, bool lm, const double* grid, long n,
+                  double T, double p, double vs, double cutoff, double lm_cutoff, double x_far, Grad& g) {
+    voigt_xsec_grad(ll, nL, grid, n, T, p, vs, cutoff, x_far, g);
+    if (!lm || !y0) return;
+    std::vector<double> d0(n), a(n), b(n);
+    lm_dispersive(ll, nL, y0, grid, n, T, p, lm_cutoff, x_far, d0.data());
+    const double hT = 0.02;
+    lm_dispersive(ll, nL, y0, grid, n, T + hT, p, lm_cutoff, x_far, a.data());
+    lm_dispersive(ll, nL, y0, grid, n, T - hT, p, lm_cutoff, x_far, b.data());
+    std::vector<double> dT(n);
+    for (long i = 0; i < n; ++i) dT[i] = (a[i] - b[i]) / (2 * hT);
+    const double hp = std::max(p, 1e-6) * 1e-4;
+    lm_dispersive(ll, nL, y0, grid, n, T, p + hp, lm_cutoff, x_far, a.data());
+    lm_dispersive(ll, nL, y0, grid, n, T, p - hp, lm_cutoff, x_far, b.data());
+    for (long i = 0; i < n; ++i) {
+        const double s = g.s[i] + d0[i];
+        if (s <= 0.0) { g.s[i] = 0; g.dT[i] = 0; g.dp[i] = 0; }
+        else { g.s[i] = s; g.dT[i] += dT[i]; g.dp[i] += (a[i] - b[i]) / (2 * hp); }
+    }
+}
+
 }  // namespace
 
 // =================================================================== C ABI
@@ -907,6 +1077,330 @@ int orc_forward_model(int n_lev, const double* p_lev, const double* T_lev, int n
         R_out[c] = R;
         BT_out[c] = bt(nu, R);
     }
+    return 0;
+}
+
+// vmr_jacobian.jl:152-505 (analytic_jacobian) with schwarzschild_jacobian.jl:66-266
+// on channels [ch_begin, ch_end).  State layout (state_vector.jl:253-309):
+// [T (n_lev) if include_T][per retrieved species: VMR or log VMR (n_lev)][T_sfc][eps].
+// K is [n_state][n_window_channels] (the column-major n_ch x n_state Jacobian.K).
+int orc_analytic_jacobian(int n_lev, const double* p_lev, const double* T_lev, int nps, const int* psp,
+                          const double* pvmr, int n_lists, const int* lsp, const int64_t* loff,
+                          const orc_line* lines, const double* y0, const orc_sounder* s,
+                          const orc_fm_options* o, int n_retr, const int* retr, int include_T,
+                          int include_tsfc, int include_eps, int log_vmr, int vmr_coupling, int observable,
+                          int64_t ch_begin, int64_t ch_end, double* K, double* y_out) {
+    if (n_lev < 2) return fail("profile needs at least 2 levels");
+    if (!(o->mu > 0.0 && o->mu <= 1.0)) return fail("mu must be in (0, 1]");
+    const int L = n_lev - 1;
+    const int src = o->source_function;
+    InternalGrid ig = internal_grid(*s, *o);
+    const Grid ch = make_grid(s->nu_min, s->nu_max, s->dnu);
+    if (ch_end <= 0) { ch_begin = 0; ch_end = ch.n; }
+    if (ch_begin < 0 || ch_end > ch.n || ch_begin >= ch_end) return fail("bad channel window");
+    const double dhi = ig.dnu_hi;
+    const long n_hi = ig.g.n;
+    const double nu_first = grid_at(ig.g, 0);
+    auto idx_floor = [&](double nu) {
+        long i = (long)std::floor((nu - nu_first) / dhi);
+        i = std::max(0L, std::min(i, n_hi - 1));
+        while (i > 0 && grid_at(ig.g, i) > nu) --i;
+        while (i + 1 < n_hi && grid_at(ig.g, i + 1) <= nu) ++i;
+        return i;
+    };
+    std::vector<double> kern;
+    long n_half = 0;
+    if (o->with_ils) { ils_kernel(dhi, s->opd_max, s->fwhm_gauss, o->apodization, kern); n_half = ((long)kern.size() - 1) / 2; }
+    const long nch = ch_end - ch_begin;
+    std::vector<double> nu_ch(nch);
+    for (long c = 0; c < nch; ++c) nu_ch[c] = grid_at(ch, ch_begin + c);
+    const long w0 = std::max(0L, idx_floor(nu_ch.front()) - n_half);
+    const long w1 = std::min(n_hi - 1, std::min(n_hi - 1, idx_floor(nu_ch.back()) + 1) + n_half);
+    const long nw = w1 - w0 + 1;
+    std::vector<double> grid(nw);
+    for (long i = 0; i < nw; ++i) grid[i] = grid_at(ig.g, w0 + i);
+
+    // layer properties (layers.jl:133-178)
+    std::vector<double> p_mid(L), dp(L), T_mid(L), T_ave(L), fracs(L);
+    LogPInterp Ti(n_lev, p_lev, T_lev);
+    for (int k = 0; k < L; ++k) {
+        p_mid[k] = 0.5 * (p_lev[k] + p_lev[k + 1]);
+        dp[k] = std::fabs(p_lev[k] - p_lev[k + 1]);
+        T_mid[k] = Ti(p_mid[k]);
+        T_ave[k] = cg_temperature_mass(T_lev[k], T_lev[k + 1], p_lev[k], p_lev[k + 1]);
+        fracs[k] = cg_mass_frac(p_lev[k], p_lev[k + 1]);
+    }
+    auto prof_index = [&](int sp) { for (int q = 0; q < nps; ++q) if (psp[q] == sp) return q; return -1; };
+    auto is_retr = [&](int sp) { for (int r = 0; r < n_retr; ++r) if (retr[r] == sp) return true; return false; };
+
+    const size_t NL = (size_t)L * nw;
+    std::vector<double> tau(NL, 0.0);
+    std::map<int, std::vector<double>> tau_sp, dTcg, dtdp, dtdTc, dtdvs, wT;
+    for (int li = 0; li < n_lists; ++li) {
+        const int sp = lsp[li];
+        if (include_T) { dTcg[sp].assign(NL, 0.0); wT[sp].assign(L, 0.0); }
+        if (is_retr(sp)) {
+            tau_sp[sp].assign(NL, 0.0);
+            if (vmr_coupling) { dtdp[sp].assign(NL, 0.0); dtdTc[sp].assign(NL, 0.0); dtdvs[sp].assign(NL, 0.0); }
+        }
+    }
+    for (int k = 0; k < L; ++k) {
+        for (int li = 0; li < n_lists; ++li) {
+            const int sp = lsp[li];
+            const int q = prof_index(sp);
+            if (q < 0) continue;
+            const double* v = pvmr + (size_t)q * n_lev;
+            const double vmr = cg_column_vmr(v[k], v[k + 1], p_lev[k], p_lev[k + 1]);
+            if (vmr == 0.0) continue;
+            const double pcg = cg_pressure(v[k], v[k + 1], p_lev[k], p_lev[k + 1]);
+            const double p_atm = pcg / 1013.25;
+            const double Tcg = o->T_method == 1 ? T_ave[k] : Ti(pcg);
+            const double vs = sp == 1 ? vmr : 0.0;
+            const double coef = vmr * dp[k] * NAIR_PER_VMR;
+            const orc_line* ll = lines + loff[li];
+            const long nL = (long)(loff[li + 1] - loff[li]);
+            const bool lm = sp == 2 && o->line_mixing == 1;
+            Grad g;
+            species_grad(ll, nL, y0 ? y0 + loff[li] : nullptr, lm, grid.data(), nw, Tcg, p_atm, vs, o->cutoff,
+                         o->lm_cutoff, o->x_far, g);
+            const size_t base = (size_t)k * nw;
+            if (include_T) {
+                for (long i = 0; i < nw; ++i) dTcg[sp][base + i] = g.dT[i] * coef;
+                wT[sp][k] = o->T_method == 1 ? cg_mass_frac(p_lev[k], p_lev[k + 1])
+                                             : std::log(pcg / p_lev[k]) / std::log(p_lev[k + 1] / p_lev[k]);
+            }
+            if (vmr_coupling && is_retr(sp))
+                for (long i = 0; i < nw; ++i) {
+                    dtdp[sp][base + i] = g.dp[i] * (coef / 1013.25);
+                    dtdTc[sp][base + i] = g.dT[i] * coef;
+                    dtdvs[sp][base + i] = g.dv[i] * coef;
+                }
+            for (long i = 0; i < nw; ++i) {
+                const double c = g.s[i] * coef;
+                tau[base + i] += c;
+                if (is_retr(sp)) tau_sp[sp][base + i] = c;
+            }
+        }
+    }
+    // continua and their central differences (vmr_jacobian.jl:294-345)
+    const int qh = prof_index(1), qc = prof_index(2);
+    auto vmid = [&](int q, int k, double dflt) {
+        if (q < 0) return dflt;
+        LogPInterp vi(n_lev, p_lev, pvmr + (size_t)q * n_lev);
+        return vi(p_mid[k]);
+    };
+    auto cont_layer = [&](int k, double vh, double vc, double Tm, std::vector<double>& out) {
+        out.assign(nw, 0.0);
+        const double dz = dp_to_dz_cm(dp[k], p_mid[k], Tm);
+        if (o->continua & 1) h2o_continuum_add(grid.data(), nw, vh, p_mid[k], Tm, dz, out.data());
+        if (o->continua & 2) co2_continuum_add(grid.data(), nw, vc, p_mid[k], Tm, dz, out.data());
+    };
+    const bool cvh = o->apply_continuum && vmr_coupling && is_retr(1);
+    const bool cvc = o->apply_continuum && vmr_coupling && is_retr(2);
+    const bool cT = o->apply_continuum && include_T;
+    std::vector<double> dcvh(cvh ? NL : 0), dcvc(cvc ? NL : 0), dcT(cT ? NL : 0), wM(L, 0.0), t1, t2;
+    if (o->apply_continuum)
+        for (int k = 0; k < L; ++k) {
+            const double vh = vmid(qh, k, 0.0), vc = vmid(qc, k, 4.15e-4);
+            cont_layer(k, vh, vc, T_mid[k], t1);
+            for (long i = 0; i < nw; ++i) tau[(size_t)k * nw + i] += t1[i];
+            wM[k] = std::log(p_mid[k] / p_lev[k]) / std::log(p_lev[k + 1] / p_lev[k]);
+            if (cvh) {
+                const double h = std::max(std::fabs(vh), 1e-30) * 1e-6;
+                cont_layer(k, vh + h, vc, T_mid[k], t1); cont_layer(k, vh - h, vc, T_mid[k], t2);
+                for (long i = 0; i < nw; ++i) dcvh[(size_t)k * nw + i] = (t1[i] - t2[i]) / (2 * h);
+            }
+            if (cvc) {
+                const double h = std::max(std::fabs(vc), 1e-30) * 1e-6;
+                cont_layer(k, vh, vc + h, T_mid[k], t1); cont_layer(k, vh, vc - h, T_mid[k], t2);
+                for (long i = 0; i < nw; ++i) dcvc[(size_t)k * nw + i] = (t1[i] - t2[i]) / (2 * h);
+            }
+            if (cT) {
+                const double h = 0.05;
+                cont_layer(k, vh, vc, T_mid[k] + h, t1); cont_layer(k, vh, vc, T_mid[k] - h, t2);
+                for (long i = 0; i < nw; ++i) dcT[(size_t)k * nw + i] = (t1[i] - t2[i]) / (2 * h);
+            }
+        }
+
+    // schwarzschild_rte_jacobian (schwarzschild_jacobian.jl:66-266)
+    const double Tsfc = std::isnan(o->T_sfc) ? T_lev[0] : o->T_sfc;
+    const double mu = o->mu, eps = o->eps_sfc, invmu = 1.0 / mu;
+    std::vector<double> I(nw), dIdtau(NL), dIdTl((size_t)n_lev * nw, 0.0), dIdTs(nw), dIde(nw);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < nw; ++i) {
+        const double nu = grid[i];
+        std::vector<double> Tr(L + 1), gk(L), em(L), dem(L);
+        Tr[L] = 1.0;
+        for (int k = L - 1; k >= 0; --k) Tr[k] = Tr[k + 1] * std::exp(-tau[(size_t)k * nw + i] / mu);
+        const double Bs = planck(nu, Tsfc);
+        double Ii = eps * Bs * Tr[0];
+        dIde[i] = Bs * Tr[0];
+        dIdTs[i] = eps * dB_dT(nu, Tsfc) * Tr[0];
+        double Ib = eps * Bs * Tr[0];
+        for (int m = 0; m < L; ++m) {
+            const double a = tau[(size_t)m * nw + i] * invmu, w = std::exp(-a), u = 1.0 - w, Tt = Tr[m + 1];
+            double e, dea;
+            if (src == 0) {
+                const double Ba = planck(nu, T_ave[m]), Bt = planck(nu, T_lev[m + 1]);
+                const double f = cim_corr(a), fp = cim_corr_deriv(a), core = Ba + (Bt - Ba) * f;
+                e = u * core;
+                dea = w * core + u * (Bt - Ba) * fp;
+                const double cavg = Tt * u * (1.0 - f) * dB_dT(nu, T_ave[m]);
+                dIdTl[(size_t)m * nw + i] += cavg * (1.0 - fracs[m]);
+                dIdTl[(size_t)(m + 1) * nw + i] += cavg * fracs[m] + Tt * u * f * dB_dT(nu, T_lev[m + 1]);
+            } else {
+                const double Bb = planck(nu, T_lev[m]), Bt = planck(nu, T_lev[m + 1]);
+                const double fl = lit_corr(a), flp = lit_corr_deriv(a);
+                e = Bt * u + (Bb - Bt) * fl;
+                dea = Bt * w + (Bb - Bt) * flp;
+                dIdTl[(size_t)m * nw + i] += Tt * fl * dB_dT(nu, T_lev[m]);
+                dIdTl[(size_t)(m + 1) * nw + i] += Tt * (u - fl) * dB_dT(nu, T_lev[m + 1]);
+            }
+            dIdtau[(size_t)m * nw + i] = invmu * (-Ib + Tt * dea);
+            Ii += Tt * e;
+            Ib += Tt * e;
+        }
+        if (eps < 1.0) {  // schwarzschild_jacobian.jl:189-266
+            const double refl = 1.0 - eps, T1 = Tr[0];
+            double g = 1.0, Id = 0.0;
+            for (int k = 0; k < L; ++k) {
+                const double a = tau[(size_t)k * nw + i] * invmu, w = std::exp(-a), u = 1.0 - w;
+                gk[k] = g;
+                if (src == 0) {
+                    const double Ba = planck(nu, T_ave[k]), Bb = planck(nu, T_lev[k]);
+                    const double f = cim_corr(a), fp = cim_corr_deriv(a), core = Ba + (Bb - Ba) * f;
+                    em[k] = u * core;
+                    dem[k] = w * core + u * (Bb - Ba) * fp;
+                    const double cavg = refl * T1 * g * u * (1.0 - f) * dB_dT(nu, T_ave[k]);
+                    dIdTl[(size_t)k * nw + i] += cavg * (1.0 - fracs[k]) + refl * T1 * g * u * f * dB_dT(nu, T_lev[k]);
+                    dIdTl[(size_t)(k + 1) * nw + i] += cavg * fracs[k];
+                } else {
+                    const double Bb = planck(nu, T_lev[k]), Bt = planck(nu, T_lev[k + 1]);
+                    const double fl = lit_corr(a), flp = lit_corr_deriv(a);
+                    em[k] = Bb * u + (Bt - Bb) * fl;
+                    dem[k] = Bb * w + (Bt - Bb) * flp;
+                    dIdTl[(size_t)k * nw + i] += refl * T1 * g * (u - fl) * dB_dT(nu, T_lev[k]);
+                    dIdTl[(size_t)(k + 1) * nw + i] += refl * T1 * g * fl * dB_dT(nu, T_lev[k + 1]);
+                }
+                Id += g * em[k];
+                g *= w;
+            }
+            Ii += refl * Id * T1;
+            dIde[i] += -Id * T1;
+            double above = 0.0;
+            for (int m = L - 1; m >= 0; --m) {
+                dIdtau[(size_t)m * nw + i] += refl * invmu * T1 * (-above + gk[m] * dem[m] - Id);
+                above += gk[m] * em[m];
+            }
+        }
+        I[i] = Ii;
+    }
+
+    // channel tail (vmr_jacobian.jl:359-380): ILS at the nodes the resampling reads
+    std::vector<long> c_i(nch);
+    std::vector<double> c_w(nch);
+    for (long c = 0; c < nch; ++c) {
+        const double nu = nu_ch[c];
+        if (nu <= nu_first) { c_i[c] = 0; c_w[c] = -1; }
+        else if (nu >= grid_at(ig.g, n_hi - 1)) { c_i[c] = n_hi - 1; c_w[c] = -1; }
+        else {
+            const long i = idx_floor(nu);
+            const double a = grid_at(ig.g, i), b = grid_at(ig.g, i + 1);
+            c_i[c] = i;
+            c_w[c] = (nu - a) / (b - a);
+        }
+    }
+    auto ils_at = [&](const std::vector<double>& col, long gi) {
+        if (!o->with_ils) return col[gi - w0];
+        double acc = 0.0;
+        for (long k = 0; k < (long)kern.size(); ++k) {
+            const long j = gi + (k - n_half);
+            if (j < 0 || j >= n_hi) continue;
+            acc += col[j - w0] * kern[k];
+        }
+        return acc * dhi;
+    };
+    auto resample = [&](const std::vector<double>& col, long c) {
+        const double r0 = ils_at(col, c_i[c]);
+        if (c_w[c] <= 0.0) return r0;
+        return r0 * (1.0 - c_w[c]) + ils_at(col, c_i[c] + 1) * c_w[c];
+    };
+    std::vector<double> Rc(nch), dbt(nch);
+    for (long c = 0; c < nch; ++c) {
+        Rc[c] = resample(I, c);
+        dbt[c] = observable == 0 ? dBT_dR(nu_ch[c], Rc[c]) : 1.0;
+        y_out[c] = observable == 0 ? bt(nu_ch[c], Rc[c]) : Rc[c];
+    }
+    int col = 0;
+    auto emit = [&](const std::vector<double>& dI, double scale) {
+#pragma omp parallel for schedule(static)
+        for (long c = 0; c < nch; ++c) K[(size_t)col * nch + c] = resample(dI, c) * dbt[c] * scale;
+        ++col;
+    };
+    std::vector<double> dI(nw);
+    if (include_T) {
+        for (int j = 0; j < n_lev; ++j) {
+            for (long i = 0; i < nw; ++i) dI[i] = dIdTl[(size_t)j * nw + i];
+            for (auto& e : dTcg) {
+                const std::vector<double>& M = e.second;
+                const std::vector<double>& w = wT[e.first];
+                if (j < L) for (long i = 0; i < nw; ++i) dI[i] += dIdtau[(size_t)j * nw + i] * M[(size_t)j * nw + i] * (1.0 - w[j]);
+                if (j >= 1) for (long i = 0; i < nw; ++i) dI[i] += dIdtau[(size_t)(j - 1) * nw + i] * M[(size_t)(j - 1) * nw + i] * w[j - 1];
+            }
+            if (cT) {
+                if (j < L) for (long i = 0; i < nw; ++i) dI[i] += dIdtau[(size_t)j * nw + i] * dcT[(size_t)j * nw + i] * (1.0 - wM[j]);
+                if (j >= 1) for (long i = 0; i < nw; ++i) dI[i] += dIdtau[(size_t)(j - 1) * nw + i] * dcT[(size_t)(j - 1) * nw + i] * wM[j - 1];
+            }
+            emit(dI, 1.0);
+        }
+    }
+    for (int r = 0; r < n_retr; ++r) {
+        const int sp = retr[r];
+        const int q = prof_index(sp);
+        if (q < 0) return fail("profile is missing a retrieved species");
+        const double* vl = pvmr + (size_t)q * n_lev;
+        const bool has_lbl = tau_sp.count(sp) > 0;
+        std::vector<double> vcg(L), gV1(L), gV2(L), gP1(L, 0.0), gP2(L, 0.0), gT1(L, 0.0), gT2(L, 0.0);
+        for (int k = 0; k < L; ++k) {
+            const double v1 = vl[k], v2 = vl[k + 1], p1 = p_lev[k], p2 = p_lev[k + 1];
+            vcg[k] = cg_column_vmr(v1, v2, p1, p2);
+            cg_column_vmr_grad(v1, v2, p1, p2, gV1[k], gV2[k]);
+            if (vmr_coupling) {
+                const double h1 = std::max(std::fabs(v1), 1e-300) * 1e-6, h2 = std::max(std::fabs(v2), 1e-300) * 1e-6;
+                gP1[k] = (cg_pressure(v1 + h1, v2, p1, p2) - cg_pressure(v1 - h1, v2, p1, p2)) / (2 * h1);
+                gP2[k] = (cg_pressure(v1, v2 + h2, p1, p2) - cg_pressure(v1, v2 - h2, p1, p2)) / (2 * h2);
+                if (o->T_method != 1) {
+                    const double dTdp = (T_lev[k + 1] - T_lev[k]) / (cg_pressure(v1, v2, p1, p2) * std::log(p2 / p1));
+                    gT1[k] = dTdp * gP1[k];
+                    gT2[k] = dTdp * gP2[k];
+                }
+            }
+        }
+        const std::vector<double>* dcv = sp == 1 ? (cvh ? &dcvh : nullptr) : (sp == 2 ? (cvc ? &dcvc : nullptr) : nullptr);
+        for (int j = 0; j < n_lev; ++j) {
+            std::fill(dI.begin(), dI.end(), 0.0);
+            auto add_layer = [&](int k, double gV, double gP, double gT) {
+                if (!has_lbl || vcg[k] == 0.0) return;
+                const std::vector<double>& ts = tau_sp[sp];
+                for (long i = 0; i < nw; ++i) dI[i] += dIdtau[(size_t)k * nw + i] * ts[(size_t)k * nw + i] * (gV / vcg[k]);
+                if (vmr_coupling) {
+                    for (long i = 0; i < nw; ++i)
+                        dI[i] += dIdtau[(size_t)k * nw + i] * (dtdp[sp][(size_t)k * nw + i] * gP + dtdTc[sp][(size_t)k * nw + i] * gT);
+                    if (sp == 1)
+                        for (long i = 0; i < nw; ++i) dI[i] += dIdtau[(size_t)k * nw + i] * dtdvs[sp][(size_t)k * nw + i] * gV;
+                }
+            };
+            if (j < L) add_layer(j, gV1[j], gP1[j], gT1[j]);
+            if (j >= 1) add_layer(j - 1, gV2[j - 1], gP2[j - 1], gT2[j - 1]);
+            if (dcv) {
+                if (j < L) for (long i = 0; i < nw; ++i) dI[i] += dIdtau[(size_t)j * nw + i] * (*dcv)[(size_t)j * nw + i] * (1.0 - wM[j]);
+                if (j >= 1) for (long i = 0; i < nw; ++i) dI[i] += dIdtau[(size_t)(j - 1) * nw + i] * (*dcv)[(size_t)(j - 1) * nw + i] * wM[j - 1];
+            }
+            emit(dI, log_vmr ? vl[j] : 1.0);
+        }
+    }
+    if (include_tsfc) emit(dIdTs, 1.0);
+    if (include_eps) emit(dIde, 1.0);
     return 0;
 }
 
