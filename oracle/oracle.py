@@ -161,6 +161,10 @@ class Oracle:
                                         C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.POINTER(Sounder), C.POINTER(FMOptions), i64, i64,
                                         pd, pd, C.c_void_p, C.POINTER(C.c_int64)]
+        L.orc_analytic_jacobian.argtypes = [i32, pd, pd, i32, C.c_void_p, pd, i32, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.POINTER(Sounder), C.POINTER(FMOptions), i32, C.c_void_p,
+                                            i32, i32, i32, i32, i32, i32, i64, i64, pd, pd]
         L.orc_last_error.restype = C.c_char_p
         if load_tables:
             self.load_tables()
@@ -298,6 +302,105 @@ class Oracle:
         if return_tau:
             return R, BT, tau[:(len(p) - 1) * nw.value].reshape(len(p) - 1, nw.value)
         return R, BT
+
+    # -- Jacobians -----------------------------------------------------------
+    def analytic_jacobian(self, profile, linelists, snd: Sounder, opt: FMOptions, retrieved=(),
+                          include_T=True, include_tsfc=True, include_eps=True, log_vmr=True,
+                          vmr_coupling=True, observable="bt", channels=None, y0=None):
+        """analytic_jacobian (src/Estimation/vmr_jacobian.jl:152-505) -> (K [n_ch, n_state], y).
+
+        State layout as StateVectorSpec (state_vector.jl:253-309): [T][VMR blocks in
+        `retrieved` order][T_sfc][eps]."""
+        p = np.ascontiguousarray(profile["p"], dtype=np.float64)
+        T = np.ascontiguousarray(profile["T"], dtype=np.float64)
+        psp = np.array(sorted(profile["vmr"]), dtype=np.int32)
+        pv = np.ascontiguousarray(np.stack([np.asarray(profile["vmr"][s], dtype=np.float64)
+                                            for s in psp]))
+        lsp = np.array(sorted(linelists), dtype=np.int32)
+        lists = [_lines(linelists[s]) for s in lsp]
+        off = np.zeros(len(lists) + 1, dtype=np.int64)
+        off[1:] = np.cumsum([len(l) for l in lists])
+        lines = np.zeros(int(off[-1]), dtype=LINE_DTYPE)
+        for k, l in enumerate(lists):
+            lines[off[k]:off[k + 1]] = l
+        yy = None
+        if y0 is not None:
+            yy = np.zeros(len(lines))
+            for k, s in enumerate(lsp):
+                if s in y0:
+                    yy[off[k]:off[k + 1]] = y0[s]
+        retr = np.array(list(retrieved), dtype=np.int32)
+        n_lev = len(p)
+        n_state = (n_lev if include_T else 0) + n_lev * len(retr) + int(include_tsfc) + int(include_eps)
+        c0, c1 = (0, 0) if channels is None else channels
+        nch = snd.n_channels if channels is None else c1 - c0
+        K = np.zeros((n_state, nch))
+        y = np.empty(nch)
+        self._check(self.lib.orc_analytic_jacobian(
+            n_lev, _dp(p), _dp(T), len(psp), psp.ctypes.data, _dp(pv), len(lsp), lsp.ctypes.data,
+            off.ctypes.data, lines.ctypes.data, yy.ctypes.data if yy is not None else None,
+            C.byref(snd), C.byref(opt), len(retr), retr.ctypes.data if len(retr) else None,
+            int(include_T), int(include_tsfc), int(include_eps), int(log_vmr), int(vmr_coupling),
+            0 if observable == "bt" else 1, c0, c1, _dp(K), _dp(y)))
+        return np.ascontiguousarray(K.T), y
+
+    def fd_jacobian(self, profile, linelists, snd: Sounder, opt_kw: dict, retrieved=(),
+                    include_T=True, include_tsfc=True, include_eps=True, T_sfc=None, eps_sfc=1.0,
+                    steps=None, observable="bt", channels=None, y0=None):
+        """finite_difference_jacobian (src/Estimation/jacobian_fd.jl:111-165), central,
+        with dptmn = 0 unless opt_kw overrides it.  Log-VMR state for retrieved species."""
+        n_lev = len(profile["p"])
+        base_T = np.asarray(profile["T"], dtype=np.float64)
+        labels = []
+        x0 = []
+        if include_T:
+            labels += [("T", j) for j in range(n_lev)]
+            x0 += list(base_T)
+        for s in retrieved:
+            labels += [("v", s, j) for j in range(n_lev)]
+            x0 += list(np.log(np.maximum(profile["vmr"][s], 1e-30)))
+        Ts0 = base_T[0] if T_sfc is None else T_sfc
+        if include_tsfc:
+            labels.append(("Ts",))
+            x0.append(Ts0)
+        if include_eps:
+            labels.append(("e",))
+            x0.append(eps_sfc)
+        x0 = np.array(x0)
+        kw = dict(dptmn=0.0)
+        kw.update(opt_kw)
+
+        def run(x):
+            T = base_T.copy()
+            vmr = {s: np.asarray(v, dtype=np.float64).copy() for s, v in profile["vmr"].items()}
+            Ts, es = (x[0] if include_T else base_T[0]), eps_sfc
+            i = 0
+            if include_T:
+                T = x[:n_lev].copy()
+                i = n_lev
+            for s in retrieved:
+                vmr[s] = np.exp(x[i:i + n_lev])
+                i += n_lev
+            Ts = T[0]
+            if include_tsfc:
+                Ts = x[i]
+                i += 1
+            if include_eps:
+                es = x[i]
+            o = fm_options(T_sfc=Ts, eps_sfc=es, **kw)
+            R, BT = self.forward_model(dict(p=profile["p"], T=T, vmr=vmr), linelists, snd, o,
+                                       channels=channels, y0=y0)
+            return BT if observable == "bt" else R
+
+        y_0 = run(x0)
+        K = np.zeros((len(y_0), len(x0)))
+        for i in range(len(x0)):
+            h = steps[i]
+            xp, xm = x0.copy(), x0.copy()
+            xp[i] += h
+            xm[i] -= h
+            K[:, i] = (run(xp) - run(xm)) / (2 * h)
+        return K, y_0, labels
 
 
 def build(force: bool = False):
