@@ -166,6 +166,20 @@ int irs_forward_model_batch_device(irs_ctx* ctx, const irs_profile* profs, int n
 int irs_synchronize(irs_ctx* ctx);
 int irs_last_stage_times(irs_ctx* ctx, irs_stage_times* out);
 
+/* No counterpart in the reference.  compute_voigt_cross_sections in FP64 for callers
+ * that cannot allocate device memory (hosts whose allocator already owns the device,
+ * such as a CUDA.jl memory pool, or hosts that forbid allocation after start-up):
+ * it allocates nothing.  d_lines (56-byte records sorted by wavenumber), d_tips_q
+ * (Q(T) at 1 K from tips_t_min, or NULL for Q proportional to T), d_grid and d_sigma
+ * are device pointers owned by the caller; the work is queued on `stream`.  At most
+ * 131072 lines (IRS_E_ARG beyond).  Its per-line scratch is one file-scope device
+ * array shared by all calls, so calls that overlap on the GPU race; the first call
+ * on each device does a one-time set-up and should come before any stream capture. */
+int irs_cross_sections_noalloc(const irs_line* d_lines, int64_t n_lines, const double* d_tips_q,
+                               int tips_t_min, int tips_n, const double* d_grid, int64_t n_nu,
+                               double T, double p_atm, double vmr_self, double cutoff, int method,
+                               double x_far, double* d_sigma, void* stream);
+
 /* Number of internal grid points and channels forward_model uses for (s, o). */
 int irs_grid_size(const irs_sounder* s, const irs_fm_options* o, int64_t* n_nu,
                   int64_t* n_channels);

@@ -75,6 +75,9 @@ SIGNATURES = {
                                        C.c_int),
     "irs_synchronize": ([_P], C.c_int),
     "irs_last_stage_times": ([_P, C.POINTER(StageTimes)], C.c_int),
+    "irs_cross_sections_noalloc": ([_P, C.c_int64, _P, C.c_int, C.c_int, _P, C.c_int64, C.c_double,
+                                    C.c_double, C.c_double, C.c_double, C.c_int, C.c_double, _P, _P],
+                                   C.c_int),
     "irs_grid_size": ([C.POINTER(Sounder), C.POINTER(FMOptions), C.POINTER(C.c_int64),
                        C.POINTER(C.c_int64)], C.c_int),
 }

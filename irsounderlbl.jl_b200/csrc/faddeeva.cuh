@@ -42,7 +42,7 @@ void compute_faddeeva_consts(FaddeevaConsts* c);
 }  // namespace irs
 
 #ifdef __CUDACC__
-__constant__ irs::FaddeevaConsts c_fad;
+static __constant__ irs::FaddeevaConsts c_fad;  // one copy per translation unit
 
 namespace irs {
 
@@ -55,7 +55,7 @@ __device__ __forceinline__ double2 cmul64(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-__device__ __noinline__ double2 faddeeva64(double x, double y) {
+static __device__ __noinline__ double2 faddeeva64(double x, double y) {
     if (fabs(x) + y >= 8.0) {
         const double2 z = make_double2(x, y);
         double2 r = make_double2(0.0, 0.0);
@@ -82,7 +82,7 @@ __device__ __noinline__ double2 faddeeva64(double x, double y) {
 
 // erfcx(y) = w(i y) for real y >= 0 (the DPTMIN peak, voigt.jl:345); the same two
 // methods as faddeeva64 restricted to the imaginary axis, in real arithmetic.
-__device__ double erfcx64(double y) {
+static __device__ double erfcx64(double y) {
     if (y >= 8.0) {
         double rho = 0.0;
 #pragma unroll 1
@@ -99,7 +99,7 @@ __device__ double erfcx64(double y) {
 }
 
 // voigt.jl:89-101
-__device__ __noinline__ double weideman24_64(double x, double y) {
+static __device__ __noinline__ double weideman24_64(double x, double y) {
     double A = 0.0, B = 0.0;
 #pragma unroll 4
     for (int n = 0; n < 24; ++n) {
@@ -128,7 +128,7 @@ __device__ __forceinline__ float2 cmul32(float2 a, float2 b) {
     return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 
-__device__ __noinline__ float2 faddeeva32(float x, float y) {
+static __device__ __noinline__ float2 faddeeva32(float x, float y) {
     const float s = fabsf(x) + y;
     const float2 z = make_float2(x, y);
     if (s >= 8.0f) {
@@ -155,7 +155,7 @@ __device__ __noinline__ float2 faddeeva32(float x, float y) {
 }
 
 // voigt.jl:105-117 (Float32 Weideman-24, IEEE division as Julia's Float32 `/`)
-__device__ __noinline__ float weideman24_32(float x, float y) {
+static __device__ __noinline__ float weideman24_32(float x, float y) {
     float A = 0.0f, B = 0.0f;
 #pragma unroll 4
     for (int n = 0; n < 24; ++n) {
