@@ -190,8 +190,24 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run a small case of the line-sum kernels for ncu: the 400k-line list, one "
+                         "profile, 645-1000 cm^-1, mixed then plain FP64, twice each")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.profile_case:
+        pkg = _package()
+        ctx = pkg.B200Context(0)
+        lists = pkg.synthetic.lists_iasi_400k()
+        snd = pkg.Sounder.make(645.0, 1000.0, 0.25, opd_max=2.0, fwhm_gauss=0.5)
+        for prec in ("mixed", "mixed", "fp64", "fp64"):
+            pkg.forward_model(pkg.afgl_atmosphere(), lists, sounder=snd, backend=ctx, precision=prec,
+                              method=pkg.FullFaddeeva, **_workload_kw())
+            t = ctx.stage_times()
+            print(json.dumps({"precision": prec, "line_sum_ms": t.line_sum_ms, "pairs": t.pairs,
+                              "core_pairs": t.core_pairs}), flush=True)
+        ctx.close()
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -162,6 +162,42 @@ int irs_forward_model_batch_device(irs_ctx* ctx, const irs_profile* profs, int n
                                    const irs_sounder* s, const irs_fm_options* o,
                                    double* R_dev, double* BT_dev, void* stream);
 
+/* StateVectorSpec (src/Estimation/state_vector.jl:253-309) with full-profile VMR
+ * blocks: state = [T (n_lev) if include_temperature][VMR or log VMR (n_lev) per
+ * retrieved species, in order][T_sfc][eps].  observable: 0 :bt, 1 :radiance.
+ * vmr_coupling as analytic_jacobian's keyword (vmr_jacobian.jl:152-172).
+ * At most 4 retrieved species. */
+typedef struct {
+    int32_t        n_retrieved;
+    const int32_t* retrieved;
+    int32_t        include_temperature;
+    int32_t        include_tsfc;
+    int32_t        include_emissivity;
+    int32_t        log_vmr;
+    int32_t        vmr_coupling;
+    int32_t        observable;
+} irs_state_spec;
+
+/* Length of the state vector for `spec` on n_lev levels. */
+int irs_state_size(const irs_state_spec* spec, int n_lev, int64_t* n_state);
+
+/* analytic_jacobian(prof, linelists, spec; sounder, geom, T_sfc, ε_sfc, observable,
+ * kwargs...) -- src/Estimation/vmr_jacobian.jl:152-505 -- for a batch of profiles.
+ * K is [n_prof][n_state][n_channels] (per profile the column-major Jacobian.K,
+ * jacobian_fd.jl:43-50); y is [n_prof][n_channels], the observable at the
+ * linearisation point.  The line set is frozen (no DPTMIN), as the reference does.
+ * The line sum runs in FP32 with Kahan-compensated tile sums (o->precision is
+ * ignored); transmittances and radiance derivatives are FP64. */
+int irs_jacobian_batch(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder* s,
+                       const irs_fm_options* o, const irs_state_spec* spec, double* K, double* y);
+
+/* Vector-Jacobian product dx = K^T dy for each profile (the pullback behind the
+ * ChainRulesCore.rrule of forward_model): dy is [n_prof][n_channels], dx is
+ * [n_prof][n_state]; y receives the observable. */
+int irs_vjp_batch(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder* s,
+                  const irs_fm_options* o, const irs_state_spec* spec, const double* dy, double* dx,
+                  double* y);
+
 /* Wait for the context's work; fill per-stage times of the last forward call. */
 int irs_synchronize(irs_ctx* ctx);
 int irs_last_stage_times(irs_ctx* ctx, irs_stage_times* out);

@@ -387,3 +387,7 @@ def forward_model(prof: AtmosphericProfile, linelists, *, sounder: Sounder = Non
 iasi_forward_model = forward_model
 
 from .synthetic import afgl_atmosphere, synthetic_linelist  # noqa: E402,F401
+from .estimation import (ColumnScale, FullProfile, Jacobian, PartialColumns, StateVectorSpec,  # noqa: E402,F401
+                         analytic_jacobian, analytic_jacobian_batch, column, default_fd_steps, dfs_partition,
+                         finite_difference_jacobian, forward_model_rrule, pack_state, partial_column_basis,
+                         state_labels, unpack_state, vmr_range)

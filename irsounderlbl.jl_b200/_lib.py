@@ -47,6 +47,13 @@ class Profile(C.Structure):
                 ("T_sfc", C.c_double), ("mu", C.c_double), ("eps_sfc", C.c_double)]
 
 
+class StateSpec(C.Structure):
+    _fields_ = [("n_retrieved", C.c_int32), ("retrieved", C.POINTER(C.c_int32)),
+                ("include_temperature", C.c_int32), ("include_tsfc", C.c_int32),
+                ("include_emissivity", C.c_int32), ("log_vmr", C.c_int32),
+                ("vmr_coupling", C.c_int32), ("observable", C.c_int32)]
+
+
 class StageTimes(C.Structure):
     _fields_ = [("line_params_ms", C.c_double), ("line_sum_ms", C.c_double),
                 ("rte_ms", C.c_double), ("ils_ms", C.c_double), ("total_ms", C.c_double),
@@ -73,6 +80,11 @@ SIGNATURES = {
     "irs_forward_model_batch_device": ([_P, C.POINTER(Profile), C.c_int, C.POINTER(Sounder),
                                         C.POINTER(FMOptions), C.c_void_p, C.c_void_p, C.c_void_p],
                                        C.c_int),
+    "irs_state_size": ([C.POINTER(StateSpec), C.c_int, C.POINTER(C.c_int64)], C.c_int),
+    "irs_jacobian_batch": ([_P, C.POINTER(Profile), C.c_int, C.POINTER(Sounder), C.POINTER(FMOptions),
+                            C.POINTER(StateSpec), _PD, _PD], C.c_int),
+    "irs_vjp_batch": ([_P, C.POINTER(Profile), C.c_int, C.POINTER(Sounder), C.POINTER(FMOptions),
+                       C.POINTER(StateSpec), _PD, _PD, _PD], C.c_int),
     "irs_synchronize": ([_P], C.c_int),
     "irs_last_stage_times": ([_P, C.POINTER(StageTimes)], C.c_int),
     "irs_cross_sections_noalloc": ([_P, C.c_int64, _P, C.c_int, C.c_int, _P, C.c_int64, C.c_double,

@@ -13,6 +13,7 @@
 #include "lineparams.cuh"
 #include "linesum.cuh"
 #include "rte_ils.cuh"
+#include "jacobian.cuh"
 
 namespace irs {
 const char* last_error();
@@ -237,11 +238,8 @@ static void ensure_ils(irs_ctx* ctx, double dnu, double opd, double fwhm, int ap
     ctx->ils_n = n;
 }
 
-static void forward_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder& s,
-                           const irs_fm_options& o, double* d_R, double* d_BT) {
-    IRS_REQUIRE(n_prof >= 1 && profs, "need at least one profile");
-    validate_options(o);
-    ctx->n_h2d = ctx->n_d2h = ctx->n_launch = 0;
+static void forward_pass(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder& s,
+                         const irs_fm_options& o, double* d_R, double* d_BT) {
     upload_tables(ctx);
     cudaStream_t st = ctx->stream;
     const InternalGrid ig = internal_grid(s, o);
@@ -321,6 +319,192 @@ static void forward_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, c
     IRS_CUDA(cudaEventRecord(ctx->ev[4], st));
 }
 
+// ------------------------------------------------------------ Jacobian
+static int profiles_per_pass(irs_ctx* ctx, int n_prof, int L, size_t per_prof);
+
+static int64_t state_size(const irs_state_spec& sp, int n_lev) {
+    return (sp.include_temperature ? n_lev : 0) + (int64_t)sp.n_retrieved * n_lev + (sp.include_tsfc ? 1 : 0) +
+           (sp.include_emissivity ? 1 : 0);
+}
+
+// vmr_jacobian.jl:152-505 for profiles [0, n_prof): K_h [n_prof][n_state][n_ch], y_h [n_prof][n_ch]
+static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder& s,
+                            const irs_fm_options& o_in, const irs_state_spec& sp, double* K_h, double* y_h) {
+    IRS_REQUIRE(n_prof >= 1 && profs, "need at least one profile");
+    IRS_REQUIRE(sp.n_retrieved >= 0 && sp.n_retrieved <= 4 && (sp.n_retrieved == 0 || sp.retrieved),
+                "at most 4 retrieved species");
+    IRS_REQUIRE(sp.observable == 0 || sp.observable == 1, "observable must be :bt or :radiance");
+    irs_fm_options o = o_in;
+    o.dptmn = 0.0;               // frozen line set (vmr_jacobian.jl:188-201)
+    o.precision = IRS_MIXED;
+    validate_options(o);
+    upload_tables(ctx);
+    cudaStream_t st = ctx->stream;
+    const InternalGrid ig = internal_grid(s, o);
+    const GridSpec ch = make_grid(s.nu_min, s.nu_max, s.dnu);
+    const int64_t n_nu = ig.g.n, n_ch = ch.n;
+    const int L = profs[0].n_lev - 1;
+    const int64_t n_state = state_size(sp, L + 1);
+    const int n_out = 3 + 2 * sp.n_retrieved;
+    for (int r = 0; r < sp.n_retrieved; ++r)
+        for (int p = 0; p < n_prof; ++p) {
+            bool found = false;
+            for (int q = 0; q < profs[p].n_species; ++q) found |= profs[p].species[q] == sp.retrieved[r];
+            IRS_REQUIRE(found, "profile is missing a retrieved species");
+        }
+    std::vector<int> list_sp;
+    std::vector<double> list_shift;
+    std::vector<bool> has_list(64, false);
+    for (auto& l : ctx->lists) {
+        list_sp.push_back(l.n > 0 ? l.species : -1);
+        list_shift.push_back(l.max_abs_shift);
+        if (l.n > 0 && l.species >= 0 && l.species < 64) has_list[l.species] = true;
+    }
+    if (o.with_ils) ensure_ils(ctx, ig.dnu_hi, s.opd_max, s.fwhm_gauss, o.apodization);
+    double* d_grid = (double*)workspace(ctx, "grid", n_nu * sizeof(double));
+    grid_values_kernel<<<(unsigned)((n_nu + 255) / 256), 256, 0, st>>>(to_dev(ig.g), d_grid);
+    check_launch(ctx);
+    // profiles in chunks that fit the device
+    int64_t max_list = 1;
+    for (auto& l : ctx->lists) max_list = std::max<int64_t>(max_list, l.n);
+    int64_t total_lines = 0;
+    for (auto& l : ctx->lists) total_lines += l.n;
+    const size_t per_prof = (size_t)L * total_lines * 96 + (size_t)n_out * L * n_nu * 4 + (size_t)n_state * n_nu * 4 +
+                            (size_t)n_nu * 8 + (size_t)n_state * n_ch * 4;
+    const int chunk = profiles_per_pass(ctx, n_prof, L, per_prof);
+    std::vector<float> Kf;
+    for (int p0 = 0; p0 < n_prof; p0 += chunk) {
+        const int np = std::min(chunk, n_prof - p0);
+        Plan pl;
+        std::vector<LayerRT> lrt;
+        std::vector<ProfileRT> prt(np);
+        std::vector<JgLayer> jl;
+        std::vector<JgProfile> jp(np);
+        std::vector<double> vlev((size_t)np * 4 * (L + 1), 0.0);
+        for (int p = 0; p < np; ++p) {
+            const irs_profile& P = profs[p0 + p];
+            IRS_REQUIRE(P.n_lev == L + 1, "all profiles of a batch must have the same number of levels");
+            layer_setup(P, p, o, list_sp, list_shift, ig.dnu_hi, pl.segs, lrt, prt[p]);
+            for (int k = 0; k < L; ++k) {
+                JgLayer y;
+                y.frac = cg_mass_frac(P.pressure[k], P.pressure[k + 1]);
+                const double pm = 0.5 * (P.pressure[k] + P.pressure[k + 1]);
+                y.wM = std::log(pm / P.pressure[k]) / std::log(P.pressure[k + 1] / P.pressure[k]);
+                y.dp = std::fabs(P.pressure[k] - P.pressure[k + 1]);
+                jl.push_back(y);
+            }
+            JgProfile& g = jp[p];
+            g.n_retr = sp.n_retrieved;
+            g.retr_h2o = g.retr_co2 = -1;
+            for (int r = 0; r < sp.n_retrieved; ++r) {
+                const int spc = sp.retrieved[r];
+                const bool cont_vmr = o.apply_continuum && sp.vmr_coupling && spc < 64 && has_list[spc];
+                if (spc == 1 && cont_vmr) g.retr_h2o = r;
+                if (spc == 2 && cont_vmr) g.retr_co2 = r;
+                for (int q = 0; q < P.n_species; ++q)
+                    if (P.species[q] == spc)
+                        for (int j = 0; j <= L; ++j) vlev[((size_t)p * 4 + r) * (L + 1) + j] = P.vmr[(size_t)q * P.n_lev + j];
+            }
+            g.include_T = sp.include_temperature;
+            g.include_tsfc = sp.include_tsfc;
+            g.include_eps = sp.include_emissivity;
+            g.log_vmr = sp.log_vmr;
+            g.n_state = (int)n_state;
+        }
+        pl.n_prof = np;
+        pl.L = L;
+        pl.pl_segs.assign((size_t)np * L, make_int2(0, 0));
+        std::vector<SegDev> sd(std::max<size_t>(pl.segs.size(), 1));
+        std::vector<SegW> sw(std::max<size_t>(pl.segs.size(), 1));
+        std::vector<int> sn(std::max<size_t>(pl.segs.size(), 1), 0);
+        int64_t off = 0;
+        for (size_t i = 0; i < pl.segs.size(); ++i) {
+            Segment& g = pl.segs[i];
+            const int key = g.prof * L + g.layer;
+            if (pl.pl_segs[key].y == 0) pl.pl_segs[key].x = (int)i;
+            pl.pl_segs[key].y++;
+            g.out_off = off;
+            sn[i] = (int)ctx->lists[g.list].n;
+            off += sn[i];
+            SegDev& d = sd[i];
+            d.T = g.T; d.p_atm = g.p_atm; d.vs = g.vmr_self; d.coef = g.coef; d.margin_g = g.margin_g;
+            d.off = g.out_off; d.list = g.list; d.flags = g.flags;
+            std::memset(&sw[i], 0, sizeof(SegW));
+            jacobian_weights(profs[p0 + g.prof], o, ctx->lists[g.list].species, g.layer, sp, sw[i].w);
+        }
+        const int nseg = (int)pl.segs.size();
+        const size_t S = (size_t)std::max<int64_t>(off, 1);
+        char* base = (char*)workspace(ctx, "jg_params", S * 96);
+        JgOut go;
+        go.V = (double*)base; go.U = (double*)(base + S * 8);
+        go.q0 = (float4*)(base + S * 16); go.q1 = (float4*)(base + S * 32); go.q2 = (float4*)(base + S * 48);
+        go.q3 = (float4*)(base + S * 64); go.q4 = (float4*)(base + S * 80);
+        float* d_out = (float*)workspace(ctx, "jg_out", (size_t)np * L * n_out * n_nu * sizeof(float));
+        float* d_D = (float*)workspace(ctx, "jg_D", (size_t)np * n_state * n_nu * sizeof(float));
+        double* d_I = (double*)workspace(ctx, "I", (size_t)np * n_nu * sizeof(double));
+        double* d_RB = (double*)workspace(ctx, "jg_RB", (size_t)2 * np * n_ch * sizeof(double));
+        float* d_K = (float*)workspace(ctx, "jg_K", (size_t)np * n_state * n_ch * sizeof(float));
+        SegDev* d_segs = upload(ctx, "segs", sd);
+        SegW* d_sw = upload(ctx, "jg_w", sw);
+        int* d_sn = upload(ctx, "jg_n", sn);
+        std::vector<ListDev> ld = list_descs(ctx);
+        ListDev* d_lists = upload(ctx, "list_descs", ld);
+        int2* d_pl = upload(ctx, "pl_segs", pl.pl_segs);
+        LayerRT* d_lrt = upload(ctx, "lrt", lrt);
+        ProfileRT* d_prt = upload(ctx, "prt", prt);
+        JgLayer* d_jl = upload(ctx, "jg_layer", jl);
+        JgProfile* d_jp = upload(ctx, "jg_prof", jp);
+        double* d_vlev = upload(ctx, "jg_vlev", vlev);
+        IRS_CUDA(cudaMemsetAsync(d_out, 0, (size_t)np * L * n_out * n_nu * sizeof(float), st));
+        if (nseg > 0) {
+            LpConfig cfg;
+            cfg.cutoff = o.cutoff; cfg.x_far = o.x_far; cfg.dptmn = 0.0; cfg.grid0 = ig.g.at(0);
+            cfg.dnu_g = ig.dnu_hi; cfg.method = o.method; cfg.n_nu = n_nu;
+            jg_params_kernel<<<dim3((unsigned)((max_list + 255) / 256), nseg), 256, 0, st>>>(d_segs, d_lists, tips_dev(ctx), cfg, go);
+            check_launch(ctx);
+            const dim3 g2((unsigned)((n_nu + kJgStrip - 1) / kJgStrip), np * L);
+            const float cut_g = (float)(o.cutoff / ig.dnu_hi);
+            const bool lm = o.line_mixing == 1;
+#define IRS_JG(NO)                                                                                                   \
+    if (lm) jg_linesum_kernel<true, NO><<<g2, kJgWarps * 32, 0, st>>>(d_segs, d_sn, d_sw, d_pl, go, n_nu, cut_g, d_out); \
+    else jg_linesum_kernel<false, NO><<<g2, kJgWarps * 32, 0, st>>>(d_segs, d_sn, d_sw, d_pl, go, n_nu, cut_g, d_out)
+            switch (n_out) {
+                case 3: IRS_JG(3); break;
+                case 5: IRS_JG(5); break;
+                case 7: IRS_JG(7); break;
+                case 9: IRS_JG(9); break;
+                default: IRS_JG(11); break;
+            }
+#undef IRS_JG
+            check_launch(ctx);
+        }
+        ContDev cd;
+        cd.h2o = ctx->d_h2o; cd.co2 = ctx->d_co2; cd.n_h2o = ctx->n_h2o; cd.n_co2 = ctx->n_co2; cd.mask = 0;
+        if (o.apply_continuum) {
+            if ((o.continua & 1) && ctx->n_h2o > 1) cd.mask |= 1;
+            if ((o.continua & 2) && ctx->n_co2 > 1) cd.mask |= 2;
+        }
+        jg_rte_kernel<<<dim3((unsigned)((n_nu + 127) / 128), np), 128, 0, st>>>(
+            d_out, n_out, d_lrt, d_jl, d_prt, d_jp, d_vlev, L, d_grid, n_nu, o.source_function, cd, d_I, d_D);
+        check_launch(ctx);
+        const double* d_kern = o.with_ils ? (const double*)ctx->work["ils"].p : nullptr;
+        const int64_t n_taps = o.with_ils ? ctx->ils_n : 0;
+        ils_bt_kernel<<<dim3((unsigned)((n_ch * 32 + 255) / 256), np), 256, 0, st>>>(
+            d_I, n_nu, d_kern, n_taps, ig.dnu_hi, to_dev(ig.g), to_dev(ch), o.with_ils, d_RB, d_RB + (size_t)np * n_ch);
+        check_launch(ctx);
+        jg_channel_kernel<<<dim3((unsigned)((n_ch * 32 + 255) / 256), (unsigned)n_state, np), 256, 0, st>>>(
+            d_D, n_nu, (int)n_state, d_kern, n_taps, ig.dnu_hi, to_dev(ig.g), to_dev(ch), o.with_ils, d_RB,
+            sp.observable, d_K);
+        check_launch(ctx);
+        Kf.resize((size_t)np * n_state * n_ch);
+        IRS_CUDA(cudaMemcpyAsync(Kf.data(), d_K, Kf.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+        IRS_CUDA(cudaMemcpyAsync(y_h + (size_t)p0 * n_ch, d_RB + (sp.observable == 0 ? (size_t)np * n_ch : 0),
+                                 (size_t)np * n_ch * sizeof(double), cudaMemcpyDeviceToHost, st));
+        IRS_CUDA(cudaStreamSynchronize(st));
+        for (size_t k = 0; k < Kf.size(); ++k) K_h[(size_t)p0 * n_state * n_ch + k] = (double)Kf[k];
+    }
+}
+
 static void collect_times(irs_ctx* ctx) {
     float a = 0, b = 0, c = 0, d = 0;
     IRS_CUDA(cudaEventSynchronize(ctx->ev[4]));
@@ -328,19 +512,77 @@ static void collect_times(irs_ctx* ctx) {
     IRS_CUDA(cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]));
     IRS_CUDA(cudaEventElapsedTime(&c, ctx->ev[2], ctx->ev[3]));
     IRS_CUDA(cudaEventElapsedTime(&d, ctx->ev[3], ctx->ev[4]));
-    ctx->last.line_params_ms = a;
-    ctx->last.line_sum_ms = b;
-    ctx->last.rte_ms = c;
-    ctx->last.ils_ms = d;
-    ctx->last.total_ms = a + b + c + d;
+    ctx->last.line_params_ms = a + ctx->prior.line_params_ms;
+    ctx->last.line_sum_ms = b + ctx->prior.line_sum_ms;
+    ctx->last.rte_ms = c + ctx->prior.rte_ms;
+    ctx->last.ils_ms = d + ctx->prior.ils_ms;
+    ctx->last.total_ms = a + b + c + d + ctx->prior.total_ms;
     unsigned long long pc[2] = {0, 0};
     DevBuf& pb = ctx->work["pair_counts"];
     if (pb.p) IRS_CUDA(cudaMemcpy(pc, pb.p, 16, cudaMemcpyDeviceToHost));
-    ctx->last.pairs = (double)pc[0];
-    ctx->last.core_pairs = (double)pc[1];
+    ctx->last.pairs = (double)pc[0] + ctx->prior.pairs;
+    ctx->last.core_pairs = (double)pc[1] + ctx->prior.core_pairs;
     ctx->last.h2d_bytes = ctx->n_h2d;
     ctx->last.d2h_bytes = ctx->n_d2h;
     ctx->last.launches = ctx->n_launch;
+}
+
+// Device bytes the library may use: what is free plus its own workspaces (reused or
+// grown in place).
+static size_t device_budget(irs_ctx* ctx) {
+    size_t free_b = 0, tot_b = 0;
+    IRS_CUDA(cudaMemGetInfo(&free_b, &tot_b));
+    size_t own = 0;
+    for (auto& w : ctx->work) own += w.second.bytes;
+    return free_b + own;
+}
+
+// Profiles per pass: bounded by device memory (60% of the budget) and by the grid
+// limits of the per-segment and per-(profile, layer) launches (65535 in y).
+static int profiles_per_pass(irs_ctx* ctx, int n_prof, int L, size_t per_prof) {
+    int n_lists = 0;
+    for (auto& l : ctx->lists) n_lists += l.n > 0 ? 1 : 0;
+    const size_t by_mem = std::max<size_t>(1, device_budget(ctx) * 6 / 10 / std::max<size_t>(per_prof, 1));
+    const size_t by_grid = std::max<size_t>(1, 65535 / (size_t)std::max(1, L * std::max(n_lists, 1)));
+    return (int)std::min<size_t>((size_t)n_prof, std::min(by_mem, by_grid));
+}
+
+// forward_model for a batch: one pass when the batch fits, else sequential passes
+// (each pass but the last is waited for so its stage times can be added up).
+static void forward_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder& s,
+                           const irs_fm_options& o, double* d_R, double* d_BT) {
+    IRS_REQUIRE(n_prof >= 1 && profs, "need at least one profile");
+    validate_options(o);
+    ctx->n_h2d = ctx->n_d2h = ctx->n_launch = 0;
+    ctx->prior = irs_stage_times{};
+    const InternalGrid ig = internal_grid(s, o);
+    const GridSpec ch = make_grid(s.nu_min, s.nu_max, s.dnu);
+    const int L = profs[0].n_lev - 1;
+    IRS_REQUIRE(L >= 1, "a profile needs at least two levels");
+    int64_t total_lines = 0;
+    for (auto& l : ctx->lists) total_lines += l.n;
+    const bool mixed = o.precision == IRS_MIXED;
+    const size_t per_prof = (size_t)L * total_lines * (mixed ? 65 : 49) + (size_t)L * ig.g.n * (mixed ? 4 : 8) +
+                            (size_t)ig.g.n * 8;
+    const int chunk = profiles_per_pass(ctx, n_prof, L, per_prof);
+    for (int p0 = 0; p0 < n_prof; p0 += chunk) {
+        const int np = std::min(chunk, n_prof - p0);
+        forward_pass(ctx, profs + p0, np, s, o, d_R + (size_t)p0 * ch.n, d_BT + (size_t)p0 * ch.n);
+        if (p0 + np < n_prof) {
+            const double h2d = ctx->n_h2d, d2h = ctx->n_d2h, nl = ctx->n_launch;
+            const irs_stage_times keep = ctx->prior;
+            collect_times(ctx);
+            ctx->prior = ctx->last;
+            ctx->prior.line_params_ms += keep.line_params_ms;
+            ctx->prior.line_sum_ms += keep.line_sum_ms;
+            ctx->prior.rte_ms += keep.rte_ms;
+            ctx->prior.ils_ms += keep.ils_ms;
+            ctx->prior.total_ms += keep.total_ms;
+            ctx->prior.pairs += keep.pairs;
+            ctx->prior.core_pairs += keep.core_pairs;
+            ctx->n_h2d = h2d, ctx->n_d2h = d2h, ctx->n_launch = nl;
+        }
+    }
 }
 
 }  // namespace irs
@@ -588,6 +830,43 @@ int irs_last_stage_times(irs_ctx* ctx, irs_stage_times* out) {
     IRS_API_BEGIN
     IRS_REQUIRE(ctx && out, "invalid arguments");
     *out = ctx->last;
+    IRS_API_END
+}
+
+int irs_state_size(const irs_state_spec* spec, int n_lev, int64_t* n_state) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(spec && n_state && n_lev >= 2, "invalid arguments");
+    *n_state = state_size(*spec, n_lev);
+    IRS_API_END
+}
+
+int irs_jacobian_batch(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder* s,
+                       const irs_fm_options* o, const irs_state_spec* spec, double* K, double* y) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && s && o && spec && K && y, "invalid arguments");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    jacobian_device(ctx, profs, n_prof, *s, *o, *spec, K, y);
+    IRS_API_END
+}
+
+int irs_vjp_batch(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder* s,
+                  const irs_fm_options* o, const irs_state_spec* spec, const double* dy, double* dx,
+                  double* y) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && s && o && spec && dy && dx && y && profs && n_prof >= 1, "invalid arguments");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    const int64_t n_state = state_size(*spec, profs[0].n_lev);
+    const int64_t n_ch = make_grid(s->nu_min, s->nu_max, s->dnu).n;
+    std::vector<double> Kh((size_t)n_prof * n_state * n_ch);
+    jacobian_device(ctx, profs, n_prof, *s, *o, *spec, Kh.data(), y);
+    for (int p = 0; p < n_prof; ++p)
+        for (int64_t x = 0; x < n_state; ++x) {
+            const double* row = Kh.data() + ((size_t)p * n_state + x) * n_ch;
+            const double* d = dy + (size_t)p * n_ch;
+            double acc = 0.0;
+            for (int64_t c = 0; c < n_ch; ++c) acc += row[c] * d[c];
+            dx[(size_t)p * n_state + x] = acc;
+        }
     IRS_API_END
 }
 

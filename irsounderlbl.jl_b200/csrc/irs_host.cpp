@@ -187,6 +187,75 @@ void layer_setup(const irs_profile& P, int pi, const irs_fm_options& o,
     prt.eps = P.eps_sfc;
 }
 
+// ------------------------------------------------------ Jacobian chains
+// schwarzschild_jacobian.jl:47-53
+double cg_mass_frac(double p1, double p2) {
+    if (approx_eq(p1, p2)) return 0.5;
+    const double al = std::log(p2 / p1);
+    if (std::fabs(al) < 1e-3) return 0.5 + al / 12.0;
+    const double be = p2 / p1;
+    return ((al - 1.0) * be + 1.0) / (al * (be - 1.0));
+}
+// vmr_jacobian.jl:81-107
+static void cg_column_vmr_grad(double v1, double v2, double p1, double p2, double& g1, double& g2) {
+    if (v1 <= 0.0 || v2 <= 0.0) { g1 = g2 = 0.5; return; }
+    if (approx_eq(v1, v2)) { const double fr = cg_mass_frac(p1, p2); g1 = 1.0 - fr; g2 = fr; return; }
+    const double Lg = std::log(p2 / p1), al = std::log(v2 / v1) / Lg, be = al + 1.0, dp = std::fabs(p1 - p2);
+    if (std::fabs(be) < 1e-6) {
+        const double h1 = std::max(std::fabs(v1), 1e-300) * 1e-6, h2 = std::max(std::fabs(v2), 1e-300) * 1e-6;
+        g1 = (cg_column_vmr(v1 + h1, v2, p1, p2) - cg_column_vmr(v1 - h1, v2, p1, p2)) / (2 * h1);
+        g2 = (cg_column_vmr(v1, v2 + h2, p1, p2) - cg_column_vmr(v1, v2 - h2, p1, p2)) / (2 * h2);
+        return;
+    }
+    const double r = p2 / p1, rb = std::pow(r, be);
+    const double c = v1 * p1 * (1.0 - rb) / (be * dp);
+    const double J = (v1 * p1 / Lg) * ((rb - 1.0) / (be * be) - rb * Lg / be);
+    g1 = c / v1 - J / (v1 * dp);
+    g2 = J / (v2 * dp);
+}
+
+// Weights of one (profile, layer, species) segment onto the layer Jacobian channels
+// (vmr_jacobian.jl:230-290, 392-430): channel 0 tau; 1/2 the T_cg derivative split
+// onto the layer's lower/upper level; 3+2r/4+2r the retrieved species r's level
+// derivatives (column amount, CG pressure, CG temperature, self broadening).
+void jacobian_weights(const irs_profile& P, const irs_fm_options& o, int species, int layer,
+                      const irs_state_spec& sp, float w[][4]) {
+    const int k = layer;
+    const double p1 = P.pressure[k], p2 = P.pressure[k + 1];
+    const double* v = nullptr;
+    for (int q = 0; q < P.n_species; ++q) if (P.species[q] == species) v = P.vmr + (size_t)q * P.n_lev;
+    const double pcg = cg_pressure(v[k], v[k + 1], p1, p2);
+    w[0][0] = 1.f;
+    if (sp.include_temperature) {
+        const double wT = o.T_method == 1 ? cg_mass_frac(p1, p2) : std::log(pcg / p1) / std::log(p2 / p1);
+        w[1][1] = (float)(1.0 - wT);
+        w[2][1] = (float)wT;
+    }
+    for (int r = 0; r < sp.n_retrieved; ++r) {
+        if (sp.retrieved[r] != species) continue;
+        const double v1 = v[k], v2 = v[k + 1];
+        const double vcg = cg_column_vmr(v1, v2, p1, p2);
+        double gV1, gV2;
+        cg_column_vmr_grad(v1, v2, p1, p2, gV1, gV2);
+        double gP1 = 0, gP2 = 0, gT1 = 0, gT2 = 0;
+        if (sp.vmr_coupling) {
+            const double h1 = std::max(std::fabs(v1), 1e-300) * 1e-6, h2 = std::max(std::fabs(v2), 1e-300) * 1e-6;
+            gP1 = (cg_pressure(v1 + h1, v2, p1, p2) - cg_pressure(v1 - h1, v2, p1, p2)) / (2 * h1);
+            gP2 = (cg_pressure(v1, v2 + h2, p1, p2) - cg_pressure(v1, v2 - h2, p1, p2)) / (2 * h2);
+            if (o.T_method != 1) {
+                const double dTdp = (P.temperature[k + 1] - P.temperature[k]) / (pcg * std::log(p2 / p1));
+                gT1 = dTdp * gP1;
+                gT2 = dTdp * gP2;
+            }
+        }
+        const bool self = species == 1 && sp.vmr_coupling;
+        float* lo = w[3 + 2 * r];
+        float* hi = w[4 + 2 * r];
+        lo[0] = (float)(gV1 / vcg); lo[1] = (float)gT1; lo[2] = (float)(gP1 / 1013.25); lo[3] = self ? (float)gV1 : 0.f;
+        hi[0] = (float)(gV2 / vcg); hi[1] = (float)gT2; hi[2] = (float)(gP2 / 1013.25); hi[3] = self ? (float)gV2 : 0.f;
+    }
+}
+
 // --------------------------------------------------- Faddeeva constants
 static void weideman_coefficients(int N, double* L_out, double* a_out) {
     const int M = 2 * N, M2 = 2 * M;

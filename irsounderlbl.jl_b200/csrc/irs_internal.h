@@ -83,6 +83,11 @@ void layer_setup(const irs_profile& prof, int prof_index, const irs_fm_options& 
                  double dnu_grid, std::vector<Segment>& segs, std::vector<LayerRT>& lrt,
                  ProfileRT& prt);
 
+// Jacobian: schwarzschild_jacobian.jl:47-53 and the per-segment state-chain weights
+double cg_mass_frac(double p1, double p2);
+void jacobian_weights(const irs_profile& P, const irs_fm_options& o, int species, int layer,
+                      const irs_state_spec& sp, float w[][4]);
+
 // ------------------------------------------------------------ device data
 struct DevLineList {
     int species = 0;
@@ -138,6 +143,7 @@ struct irs_ctx {
     std::vector<irs::DevLineList> lists;
     std::map<std::string, irs::DevBuf> work;  // named growable workspaces
     irs_stage_times last{};
+    irs_stage_times prior{};  // stage times of the earlier passes of a multi-pass batch
     double n_h2d = 0, n_d2h = 0, n_launch = 0;  // counters of the current call
     // cached ILS kernel
     double ils_key[4] = {-1, -1, -1, -1};

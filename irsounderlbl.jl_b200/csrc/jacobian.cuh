@@ -1,0 +1,589 @@
+// jacobian.cuh -- the analytic Jacobian of forward_model on the GPU.
+//
+// Restates vmr_jacobian.jl:152-505 with its atoms:
+//   cross-section derivatives (sigma, d/dT, d/dp, d/dvmr_self) in one pass
+//                                cross_section_jacobian.jl:68-240 (jg_params_kernel,
+//                                jg_linesum_kernel); VP_Y dispersive term with its
+//                                analytic derivatives (the reference central-
+//                                differences it, :255-322)
+//   RTE Jacobian                 schwarzschild_jacobian.jl:66-266 (jg_rte_kernel)
+//   channel tail K = dBT/dR . resample . ILS . dI/dx      vmr_jacobian.jl:359-503
+//                                (jg_channel_kernel)
+// The line sum and the channel contraction are FP32 (Kahan-compensated tile sums);
+// the optical-depth sums, transmittances and radiance derivatives are FP64.
+#pragma once
+#include "faddeeva.cuh"
+#include "lineparams.cuh"
+#include "linesum.cuh"
+#include "rte_ils.cuh"
+
+namespace irs {
+
+constexpr int kJgMaxOut = 11;  // tau, T_lo, T_hi, and (lo, hi) for up to 4 retrieved species
+
+// Per-line primitives (FP64 physics, stored FP32 except the centres), grid units.
+struct JgOut {
+    double *V, *U;          // sorted key, shifted centre
+    float4 *q0;             // An, fx, y, Hc
+    float4 *q1;             // An_T, fx_T, y_T, Hc_T
+    float4 *q2;             // y_p, u_p, Hc_p, dfar
+    float4 *q3;             // y_v, u_v, Hc_v, -
+    float4 *q4;             // Yw, Yw_T, Yw_p, -
+};
+
+// cross_section_jacobian.jl:43-56 in FP64 (H and its x, y gradient)
+__device__ __forceinline__ void h_and_grad64(double x, double y, double x_far, double& H, double& Hx, double& Hy) {
+    if (fabs(x) > x_far) {
+        const double d = x * x + y * y, d2 = d * d;
+        H = y * kInvSqrtPi / d;
+        Hx = -2.0 * x * y * kInvSqrtPi / d2;
+        Hy = kInvSqrtPi * (x * x - y * y) / d2;
+        return;
+    }
+    const double2 w = faddeeva64(x, y);
+    H = w.x;
+    Hx = -2.0 * x * w.x + 2.0 * y * w.y;
+    Hy = 2.0 * (x * w.y + y * w.x) - 2.0 * kInvSqrtPi;
+}
+
+// partition.jl:52-66
+__device__ __forceinline__ double tips_slope(const TipsDev& t, int idx, double T) {
+    const double* q = t.q + (size_t)idx * t.stride;
+    const int lo = (int)floor(T) - t.tmin[idx] + 1, hi = lo + 1;
+    if (lo < 1 || hi > t.n[idx]) return 0.0;
+    return q[hi - 1] - q[lo - 1];
+}
+
+// One thread per (line, segment); no DPTMIN (the Jacobian freezes the line set,
+// vmr_jacobian.jl:188-201).  cross_section_jacobian.jl:198-236.
+__global__ void __launch_bounds__(256) jg_params_kernel(const SegDev* __restrict__ segs,
+                                                        const ListDev* __restrict__ lists, TipsDev tp,
+                                                        LpConfig cfg, JgOut o) {
+    const SegDev sg = segs[blockIdx.y];
+    const ListDev L = lists[sg.list];
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= L.n) return;
+    const long long slot = sg.off + j;
+    const int mol = L.mol;
+    const double T = sg.T, p = sg.p_atm, vs = sg.vs, c = cfg.cutoff, dg = cfg.dnu_g, co = sg.coef;
+    const double nu = L.nu[j], n_air = L.nair[j];
+    const double n_self = mol == 1 ? 0.95 : (mol == 2 ? 0.75 : n_air);
+    const double d_air = L.delta[j], d_self = mol == 1 ? 0.002 : (mol == 2 ? -0.003 : 0.0);
+    const double nu0 = nu + (d_air * (1.0 - vs) + d_self * vs) * p;
+    const double dn0p = d_air * (1.0 - vs) + d_self * vs, dn0v = (d_self - d_air) * p;
+    // temperature_scaled_intensity_deriv, broadening.jl:112-128
+    const int ti = L.tips[j];
+    const double c2 = 1.4387752;
+    double Qr, dlnQ;
+    if (ti >= 0) {
+        const double QT = tips_lookup(tp, ti, T);
+        Qr = tips_lookup(tp, ti, 296.0) / QT;
+        dlnQ = tips_slope(tp, ti, T) / QT;
+    } else {
+        Qr = 296.0 / T;
+        dlnQ = (1.0 / 296.0) / (T / 296.0);
+    }
+    const double stim = (1.0 - exp(-c2 * nu / T)) / (1.0 - exp(-c2 * nu / 296.0));
+    const double S = L.S296[j] * Qr * exp(-c2 * L.E[j] * (1.0 / T - 1.0 / 296.0)) * stim;
+    const double a = c2 * nu;
+    const double dS = S * (-dlnQ + c2 * L.E[j] / (T * T) - (a / (T * T)) / (exp(a / T) - 1.0));
+    // pressure_broadened_width_deriv, broadening.jl:62-78
+    const double tr = 296.0 / T;
+    const double ac = pow(tr, n_air) * L.gair[j], bc = pow(tr, n_self) * L.gself[j];
+    const double A = ac * (1.0 - vs) * p, B = bc * vs * p;
+    const double gl = A + B, dglT = -(n_air * A + n_self * B) / T;
+    const double gd0 = nu * 3.58126e-7 * sqrt(T / mol_mass(mol)), dgd = gd0 / (2.0 * T);
+    const double gd = fmax(gd0, 1e-10);
+    const double f = kSqrtLn2 / gd, df = -f * (dgd / gd);
+    const double dglp = p > 0.0 ? gl / p : ac * (1.0 - vs) + bc * vs, dglv = (bc - ac) * p;
+    const double y = gl * f, dyT = dglT * f + gl * df, dyp = dglp * f, dyv = dglv * f;
+    const double Sn = S * f * kInvSqrtPi, dSnT = (dS * f + S * df) * kInvSqrtPi;
+    double Hc, Hcx, Hcy;
+    h_and_grad64(c * f, y, cfg.x_far, Hc, Hcx, Hcy);
+    const double dHcT = Hcx * (c * df) + Hcy * dyT, dHcp = Hcy * dyp, dHcv = Hcy * dyv;
+    double Yw = 0.0, YwT = 0.0, Ywp = 0.0;
+    if ((sg.flags & SEG_LM) && L.has_y0) {  // line_mixing.jl:1193-1220 with Y(T) = y0 (296/T)^0.75
+        const double Y = L.y0[j] * pow(296.0 / T, 0.75);
+        if (Y != 0.0 && S > 0.0) {
+            const double YT = -0.75 * Y / T;
+            Yw = Y * p * Sn * co;
+            YwT = (YT * Sn + Y * dSnT) * p * co;
+            Ywp = Y * Sn * co;
+        }
+    }
+    o.V[slot] = (nu - cfg.grid0) / dg;
+    o.U[slot] = (nu0 - cfg.grid0) / dg;
+    o.q0[slot] = make_float4((float)(Sn * co), (float)(f * dg), (float)y, (float)Hc);
+    o.q1[slot] = make_float4((float)(dSnT * co), (float)(df * dg), (float)dyT, (float)dHcT);
+    o.q2[slot] = make_float4((float)dyp, (float)(dn0p / dg), (float)dHcp, (float)fmin(cfg.x_far / (f * dg), 1.0e30));
+    o.q3[slot] = make_float4((float)dyv, (float)(dn0v / dg), (float)dHcv, 0.f);
+    o.q4[slot] = make_float4((float)Yw, (float)YwT, (float)Ywp, 0.f);
+}
+
+// ------------------------------------------------------------------ line sum
+constexpr int kJgQ = 4;                        // points per lane
+constexpr int kJgWarpPts = 32 * kJgQ;          // 128 points per warp
+constexpr int kJgWarps = 8;
+constexpr int kJgStrip = kJgWarps * kJgWarpPts;
+
+struct JgTile {
+    float4 u[32];   // uh, ul, class, dfar2
+    float4 q0[32], q1[32], q2[32], q3[32], q4[32];
+};
+
+// Per pair: the value and derivative terms of one line at offset d (grid units).
+// H-ped and its derivatives; x = d fx, y; c1 = P/cut^2, c0 = -2P with P = An Hc.
+// Far wing: H = y/(sqrt(pi)(x^2+y^2)); core: FP32 Faddeeva with w' = -2 z w + 2i/sqrt(pi).
+template <bool LM>
+__device__ __forceinline__ void jg_pair(float d, bool core, const float4& q0, const float4& q1, const float4& q2,
+                                        const float4& q3, const float4& q4, float icut2, float& s, float& sT,
+                                        float& sp, float& sv, float& D, float& DT, float& Dp) {
+    const float An = q0.x, fx = q0.y, y = q0.z, Hc = q0.w;
+    const float x = d * fx;
+    const float xT = d * q1.y;          // u_T = 0
+    const float xp = -fx * q2.y, xv = -fx * q3.y;
+    float H, Hx, Hy, Lw = 0.f, Lx = 0.f, Ly = 0.f;
+    if (core) {
+        const float2 w = faddeeva32(x, y);
+        H = w.x;
+        Hx = -2.f * x * w.x + 2.f * y * w.y;
+        Hy = 2.f * (x * w.y + y * w.x) - 2.f * (float)kInvSqrtPi;
+        if (LM) {
+            Lw = w.y;
+            Lx = -2.f * (x * w.y + y * w.x) + 2.f * (float)kInvSqrtPi;
+            Ly = Hx;
+        }
+    } else {
+        const float e = fmaf(x, x, y * y);
+        const float r = __frcp_rn(e);
+        const float r2 = r * r;
+        const float k = (float)kInvSqrtPi;
+        H = y * k * r;
+        Hx = -2.f * x * y * k * r2;
+        Hy = k * (x * x - y * y) * r2;
+        if (LM) {
+            Lw = x * k * r;
+            Lx = k * (y * y - x * x) * r2;
+            Ly = -2.f * x * y * k * r2;
+        }
+    }
+    // pedestal (2 - (d/cut)^2) Hc and its derivatives; the factor moves with the centre
+    const float pf = 2.f - d * d * icut2;
+    const float pfp = 2.f * d * q2.y * icut2, pfv = 2.f * d * q3.y * icut2;
+    const float Hm = H - pf * Hc;
+    s += An * Hm;
+    sT += q1.x * Hm + An * (Hx * xT + Hy * q1.z - pf * q1.w);
+    sp += An * (Hx * xp + Hy * q2.x - (pfp * Hc + pf * q2.z));
+    sv += An * (Hx * xv + Hy * q3.x - (pfv * Hc + pf * q3.z));
+    if (LM) {
+        D += q4.x * Lw;
+        DT += q4.y * Lw + q4.x * (Lx * xT + Ly * q1.z);
+        Dp += q4.z * Lw + q4.x * (Lx * xp + Ly * q2.x);
+    }
+}
+
+template <bool LM>
+__device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long long wb, float cut, int lane,
+                           JgTile& T, float sum[4][kJgQ], float dsum[3][kJgQ]) {
+    constexpr float kCentre = 0.5f * (kJgWarpPts - 1);
+    constexpr float kHalf = 0.5f * kJgWarpPts + 0.5f;
+    const float cut2 = cut * cut, icut2 = 1.f / cut2;
+    long long jlo = 0, jhi = 0;
+    if (lane == 0) {
+        jlo = lower_bound0(g.V + sg.off, (double)wb - cut - sg.margin_g, cnt);
+        jhi = lower_bound0(g.V + sg.off, (double)(wb + kJgWarpPts - 1) + cut + sg.margin_g + 1e-9, cnt);
+    }
+    jlo = __shfl_sync(kFull, jlo, 0);
+    jhi = __shfl_sync(kFull, jhi, 0);
+    float comp[4][kJgQ], dcomp[3][kJgQ];
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int q = 0; q < kJgQ; ++q) sum[c][q] = comp[c][q] = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int q = 0; q < kJgQ; ++q) dsum[c][q] = dcomp[c][q] = 0.f;
+    for (long long t0 = jlo; t0 < jhi; t0 += 32) {
+        const int nt = (int)min(32LL, jhi - t0);
+        __syncwarp();
+        if (lane < nt) {
+            const long long q = sg.off + t0 + lane;
+            const double u = g.U[q] - (double)wb;
+            const float uh = (float)u;
+            const float4 q2 = g.q2[q];
+            const float dist = fabsf(uh - kCentre);
+            float cls = 2.f;
+            if (dist > cut + kHalf) cls = 0.f;
+            else if (dist + kHalf <= cut && dist > q2.w + kHalf) cls = 1.f;
+            T.u[lane] = make_float4(uh, (float)(u - (double)uh), cls, q2.w * q2.w);
+            T.q0[lane] = g.q0[q];
+            T.q1[lane] = g.q1[q];
+            T.q2[lane] = q2;
+            T.q3[lane] = g.q3[q];
+            if (LM) T.q4[lane] = g.q4[q];
+        }
+        __syncwarp();
+        float t[4][kJgQ], td[3][kJgQ];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int q = 0; q < kJgQ; ++q) t[c][q] = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int q = 0; q < kJgQ; ++q) td[c][q] = 0.f;
+        for (int k = 0; k < nt; ++k) {
+            const float4 u = T.u[k];
+            if (u.z == 0.f) continue;
+            const float4 q0 = T.q0[k], q1 = T.q1[k], q2 = T.q2[k], q3 = T.q3[k];
+            const float4 q4 = LM ? T.q4[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const bool fast = u.z == 1.f;
+#pragma unroll
+            for (int q = 0; q < kJgQ; ++q) {
+                const float d = (((float)lane + 32.f * q) - u.x) - u.y;
+                const float d2 = d * d;
+                if (!fast && d2 > cut2) continue;
+                jg_pair<LM>(d, !fast && d2 <= u.w, q0, q1, q2, q3, q4, icut2, t[0][q], t[1][q], t[2][q], t[3][q],
+                            td[0][q], td[1][q], td[2][q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kJgQ; ++q) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) kahan_add(sum[c][q], comp[c][q], t[c][q]);
+            if (LM)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) kahan_add(dsum[c][q], dcomp[c][q], td[c][q]);
+        }
+    }
+}
+
+// Segment weights: out[o] += W[o][0] s + W[o][1] s_T + W[o][2] s_p + W[o][3] s_v
+struct SegW {
+    float w[kJgMaxOut][4];
+};
+
+template <bool ANY_LM, int NOUT>
+__global__ void __launch_bounds__(kJgWarps * 32) jg_linesum_kernel(
+    const SegDev* __restrict__ segs, const int* __restrict__ seg_n, const SegW* __restrict__ wts,
+    const int2* __restrict__ pl_segs, JgOut g, long long n_nu, float cut_g, float* __restrict__ out) {
+    __shared__ JgTile tiles[kJgWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int pl = blockIdx.y;
+    const long long wb = (long long)blockIdx.x * kJgStrip + (long long)warp * kJgWarpPts;
+    if (wb >= n_nu) return;
+    constexpr int n_out = NOUT;
+    float acc[NOUT][kJgQ];
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+        for (int q = 0; q < kJgQ; ++q) acc[o][q] = 0.f;
+    const int2 rng = pl_segs[pl];
+    for (int si = rng.x; si < rng.x + rng.y; ++si) {
+        const SegDev sg = segs[si];
+        float s[4][kJgQ], ds[3][kJgQ];
+        const long long nl = seg_n[si];
+        const bool lm = ANY_LM && (sg.flags & SEG_LM);
+        if (lm)
+            jg_segment<true>(sg, nl, g, wb, cut_g, lane, tiles[warp], s, ds);
+        else
+            jg_segment<false>(sg, nl, g, wb, cut_g, lane, tiles[warp], s, ds);
+        // clamps (voigt.jl:276, line_mixing.jl:1368, cross_section_jacobian.jl:107-113, :312-319)
+#pragma unroll
+        for (int q = 0; q < kJgQ; ++q) {
+            float v = s[0][q], vT = s[1][q], vp = s[2][q], vv = s[3][q];
+            if (!(v > 0.f)) v = vT = vp = vv = 0.f;
+            if (lm) {
+                v += ds[0][q];
+                vT += ds[1][q];
+                vp += ds[2][q];
+                if (!(v > 0.f)) v = vT = vp = 0.f;
+            }
+            const SegW& W = wts[si];
+#pragma unroll
+            for (int o = 0; o < NOUT; ++o)
+                acc[o][q] += W.w[o][0] * v + W.w[o][1] * vT + W.w[o][2] * vp + W.w[o][3] * vv;
+        }
+    }
+    float* base = out + (size_t)pl * n_out * n_nu;
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+        for (int q = 0; q < kJgQ; ++q) {
+            const long long i = wb + 32 * q + lane;
+            if (i < n_nu) base[(size_t)o * n_nu + i] = acc[o][q];
+        }
+}
+
+// ------------------------------------------------------------------ RTE Jacobian
+struct JgLayer {       // per (profile, layer), beyond LayerRT
+    double frac;       // _cg_mass_frac (T_ave weight on the upper level)
+    double wM;         // log-p weight of p_mid on the upper level
+    double dp;         // layer thickness, hPa
+};
+struct JgProfile {     // per profile
+    int n_retr;
+    int retr_h2o, retr_co2;  // retrieved index of H2O / CO2 whose continuum VMR derivative is used, or -1
+    int include_T, include_tsfc, include_eps, log_vmr;
+    int n_state;
+};
+
+__device__ __forceinline__ double dB_dT64(double nu, double T) {  // planck.jl:67-71
+    const double x = 1.4387769 * nu / T, ex = exp(x);
+    return 1.191042953e-5 * 1.4387769 * (nu * nu * nu * nu) * ex / ((T * T) * (ex - 1.0) * (ex - 1.0));
+}
+__device__ __forceinline__ double cim_corr_d(double s) {
+    if (s < 0.06) return 1.0 / 6.0;
+    const double w = exp(-s);
+    return 2.0 / (s * s) - 2.0 * w / ((w - 1.0) * (w - 1.0));
+}
+__device__ __forceinline__ double lit_corr_d(double s) {
+    if (s < 1e-4) return 0.5 - s * (2.0 / 3.0 - s * 0.375);
+    const double e = exp(-s);
+    return (e * (s + 1.0) - 1.0) / (s * s) + e;
+}
+
+// continuum optical depth of one layer at (vh, vc, Tm), continuum.jl:183-250 and
+// the dz(Tm) of optical_depth.jl:123-130 (vmr_jacobian.jl:300-311)
+__device__ __forceinline__ double cont_tau(double nu, const LayerRT& r, double dp, const ContDev& c, double Cs,
+                                          double Cf, double te, double Se, double td, double vh, double vc,
+                                          double Tm) {
+    const double p = r.p_mid;
+    const double dz = 8.314462 * Tm / (0.028964 * 9.80665) * dp / p * 100.0;
+    const double rho = (p / 1013.0) * (296.0 / Tm);
+    const double rad = radfn(nu, Tm);
+    double t = 0.0;
+    if (c.mask & 1) {
+        const double n = vh * p * 100.0 / (1.380649e-23 * Tm) * 1e-6;
+        const double ks = Cs * pow(296.0 / Tm, te) * vh * rho * rad * n;
+        const double kf = Cf * (1.0 - vh) * rho * rad * n;
+        t += (ks + kf) * dz;
+    }
+    if (c.mask & 2) {
+        const double n = vc * p * 100.0 / (1.380649e-23 * Tm) * 1e-6;
+        const double tc = td == 0.0 ? 1.0 : pow(Tm / 246.0, td);
+        t += Se * tc * (1e-20 * n * rho) * rad * dz;
+    }
+    return t;
+}
+
+// One thread per (profile, grid point): the monochromatic Jacobian columns
+// D[x][nu] = dI/dx (FP32) for every state element, and I (FP64).
+// schwarzschild_jacobian.jl:66-266 with the state chains of vmr_jacobian.jl:383-503.
+// Transmittances come from the FP64 cumulative optical depth: the top-of-layer
+// transmittance of layer m is exp(-(OD_total - OD_below_and_m)).
+__global__ void __launch_bounds__(128) jg_rte_kernel(
+    const float* __restrict__ jl, int n_out, const LayerRT* __restrict__ lrt, const JgLayer* __restrict__ jlay,
+    const ProfileRT* __restrict__ prt, const JgProfile* __restrict__ jprof, const double* __restrict__ vlev,
+    int L, const double* __restrict__ grid, long long n_nu, int src, ContDev cont, double* __restrict__ I,
+    float* __restrict__ D) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = blockIdx.y;
+    if (i >= n_nu) return;
+    const double nu = grid[i];
+    const ProfileRT pr = prt[p];
+    const JgProfile jp = jprof[p];
+    const LayerRT* lr = lrt + (size_t)p * L;
+    const JgLayer* jy = jlay + (size_t)p * L;
+    const float* out = jl + (size_t)p * L * n_out * n_nu;
+    const double* vl = vlev + (size_t)p * 4 * (L + 1);  // level VMR of the retrieved species
+    double Cs = 0, Cf = 0, te = 0, Se = 0, td = 0;
+    if (cont.mask & 1) {
+        const Lerp l = lerp_at(cont.h2o, cont.n_h2o, nu);
+        Cs = lerp_val(cont.h2o + cont.n_h2o, l);
+        Cf = lerp_val(cont.h2o + 2 * cont.n_h2o, l);
+        te = lerp_val(cont.h2o + 3 * cont.n_h2o, l);
+    }
+    if (cont.mask & 2) {
+        const Lerp l = lerp_at(cont.co2, cont.n_co2, nu);
+        Se = lerp_val(cont.co2 + cont.n_co2, l);
+        td = lerp_val(cont.co2 + 2 * cont.n_co2, l);
+    }
+    const double invmu = 1.0 / pr.mu, eps = pr.eps;
+    auto layer_s = [&](int k) {
+        double t = (double)out[((size_t)k * n_out) * n_nu + i];
+        if (cont.mask) t += cont_tau(nu, lr[k], jy[k].dp, cont, Cs, Cf, te, Se, td, lr[k].vmr_h2o, lr[k].vmr_co2, lr[k].T_mid);
+        return t * invmu;
+    };
+    auto emission_down = [&](int k, double s, double& em, double& dem) {  // schwarzschild_jacobian.jl:221-243
+        const double w = exp(-s), u = 1.0 - w;
+        if (src == 0) {
+            const double Ba = planck64(nu, lr[k].T_ave), Bb = planck64(nu, lr[k].T_bot);
+            const double f = cim_corr(s), fp = cim_corr_d(s), core = Ba + (Bb - Ba) * f;
+            em = u * core;
+            dem = w * core + u * (Bb - Ba) * fp;
+        } else {
+            const double Bb = planck64(nu, lr[k].T_bot), Bt = planck64(nu, lr[k].T_top);
+            const double fl = lit_corr(s), flp = lit_corr_d(s);
+            em = Bb * u + (Bt - Bb) * fl;
+            dem = Bb * w + (Bt - Bb) * flp;
+        }
+    };
+    // pass 1: total optical depth and the downwelling radiance at the surface
+    double OD = 0.0, Id = 0.0, gk = 1.0;
+    for (int k = 0; k < L; ++k) {
+        const double s = layer_s(k);
+        OD += s;
+        if (eps < 1.0) {
+            double em, dem;
+            emission_down(k, s, em, dem);
+            Id += gk * em;
+            gk *= exp(-s);
+        }
+    }
+    const double Tr0 = exp(-OD), refl = 1.0 - eps;
+    const double Bs = planck64(nu, pr.T_sfc);
+    double Iv = eps * Bs * Tr0, Ib = eps * Bs * Tr0;
+    const double dIde = Bs * Tr0 - (eps < 1.0 ? Id * Tr0 : 0.0);
+    const double dIdTs = eps * dB_dT64(nu, pr.T_sfc) * Tr0;
+    // pass 2, surface to top
+    const int nT = jp.include_T ? L + 1 : 0;
+    double cum = 0.0, gdn = 1.0, Id_below = 0.0;
+    double carryT = 0.0, carryV[4] = {0, 0, 0, 0};
+    const size_t nn = (size_t)n_nu;
+    float* Dp = D + (size_t)p * jp.n_state * nn;
+    for (int m = 0; m < L; ++m) {
+        const LayerRT r = lr[m];
+        const JgLayer jm = jy[m];
+        const double s = layer_s(m);
+        cum += s;
+        const double Tt = exp(-(OD - cum));  // transmittance from the top of layer m to space
+        const double w = exp(-s), u = 1.0 - w;
+        double e, dea, dTl_lo, dTl_hi;
+        if (src == 0) {
+            const double Ba = planck64(nu, r.T_ave), Bt = planck64(nu, r.T_top);
+            const double f = cim_corr(s), fp = cim_corr_d(s), core = Ba + (Bt - Ba) * f;
+            e = u * core;
+            dea = w * core + u * (Bt - Ba) * fp;
+            const double cavg = Tt * u * (1.0 - f) * dB_dT64(nu, r.T_ave);
+            dTl_lo = cavg * (1.0 - jm.frac);
+            dTl_hi = cavg * jm.frac + Tt * u * f * dB_dT64(nu, r.T_top);
+        } else {
+            const double Bb = planck64(nu, r.T_bot), Bt = planck64(nu, r.T_top);
+            const double fl = lit_corr(s), flp = lit_corr_d(s);
+            e = Bt * u + (Bb - Bt) * fl;
+            dea = Bt * w + (Bb - Bt) * flp;
+            dTl_lo = Tt * fl * dB_dT64(nu, r.T_bot);
+            dTl_hi = Tt * (u - fl) * dB_dT64(nu, r.T_top);
+        }
+        double dIdtau = invmu * (-Ib + Tt * dea);
+        if (eps < 1.0) {  // reflected downwelling, schwarzschild_jacobian.jl:210-264
+            double em, dem;
+            emission_down(m, s, em, dem);
+            const double above = Id - Id_below - gdn * em;  // emitted above layer m
+            dIdtau += refl * invmu * Tr0 * (-above + gdn * dem - Id);
+            if (src == 0) {
+                const double f = cim_corr(s);
+                const double cavg = refl * Tr0 * gdn * u * (1.0 - f) * dB_dT64(nu, r.T_ave);
+                dTl_lo += cavg * (1.0 - jm.frac) + refl * Tr0 * gdn * u * f * dB_dT64(nu, r.T_bot);
+                dTl_hi += cavg * jm.frac;
+            } else {
+                const double fl = lit_corr(s);
+                dTl_lo += refl * Tr0 * gdn * (u - fl) * dB_dT64(nu, r.T_bot);
+                dTl_hi += refl * Tr0 * gdn * fl * dB_dT64(nu, r.T_top);
+            }
+            Id_below += gdn * em;
+            gdn *= w;
+        }
+        Iv += Tt * e;
+        Ib += Tt * e;
+        // continuum derivatives by central differences (vmr_jacobian.jl:322-344)
+        const float* om = out + (size_t)m * n_out * nn;
+        double cT = 0.0, cvh = 0.0, cvc = 0.0;
+        if (cont.mask) {
+            const double vh = r.vmr_h2o, vc = r.vmr_co2, Tm = r.T_mid;
+            if (jp.include_T)
+                cT = (cont_tau(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh, vc, Tm + 0.05) -
+                      cont_tau(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh, vc, Tm - 0.05)) / 0.1;
+            if (jp.retr_h2o >= 0) {
+                const double h = fmax(fabs(vh), 1e-30) * 1e-6;
+                cvh = (cont_tau(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh + h, vc, Tm) -
+                       cont_tau(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh - h, vc, Tm)) / (2 * h);
+            }
+            if (jp.retr_co2 >= 0) {
+                const double h = fmax(fabs(vc), 1e-30) * 1e-6;
+                cvc = (cont_tau(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh, vc + h, Tm) -
+                       cont_tau(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh, vc - h, Tm)) / (2 * h);
+            }
+        }
+        if (jp.include_T) {
+            const double tlo = (double)om[1 * nn + i] + cT * (1.0 - jm.wM);
+            const double thi = (double)om[2 * nn + i] + cT * jm.wM;
+            Dp[(size_t)m * nn + i] = (float)(carryT + dTl_lo + dIdtau * tlo);
+            carryT = dTl_hi + dIdtau * thi;
+        }
+        for (int rr = 0; rr < jp.n_retr; ++rr) {
+            const double cv = rr == jp.retr_h2o ? cvh : (rr == jp.retr_co2 ? cvc : 0.0);
+            const double vlo = (double)om[(size_t)(3 + 2 * rr) * nn + i] + cv * (1.0 - jm.wM);
+            const double vhi = (double)om[(size_t)(4 + 2 * rr) * nn + i] + cv * jm.wM;
+            const double sc = jp.log_vmr ? vl[rr * (L + 1) + m] : 1.0;
+            Dp[(size_t)(nT + rr * (L + 1) + m) * nn + i] = (float)(sc * (carryV[rr] + dIdtau * vlo));
+            carryV[rr] = dIdtau * vhi;
+        }
+    }
+    if (jp.include_T) Dp[(size_t)L * nn + i] = (float)carryT;
+    for (int rr = 0; rr < jp.n_retr; ++rr) {
+        const double sc = jp.log_vmr ? vl[rr * (L + 1) + L] : 1.0;
+        Dp[(size_t)(nT + rr * (L + 1) + L) * nn + i] = (float)(sc * carryV[rr]);
+    }
+    int col = nT + jp.n_retr * (L + 1);
+    if (jp.include_tsfc) Dp[(size_t)(col++) * nn + i] = (float)dIdTs;
+    if (jp.include_eps) Dp[(size_t)(col++) * nn + i] = (float)dIde;
+    if (eps < 1.0) Iv += refl * Id * Tr0;
+    I[(size_t)p * nn + i] = Iv;
+}
+
+// ------------------------------------------------------------------ channel tail
+// K[x][c] = dBT/dR_c * resample(ILS(D[x]))_c, vmr_jacobian.jl:359-380.  One warp per
+// (state element, channel); the ILS taps run over lanes (FP32 products, FP32 sums).
+__global__ void __launch_bounds__(256) jg_channel_kernel(const float* __restrict__ D, long long n_nu, int n_state,
+                                                         const double* __restrict__ kern, long long n_taps,
+                                                         double dnu_hi, GridDev g, GridDev ch, int with_ils,
+                                                         const double* __restrict__ R, int observable,
+                                                         float* __restrict__ K) {
+    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int x = blockIdx.y, p = blockIdx.z;
+    if (wid >= ch.n) return;
+    const double nu = ch.at(wid);
+    const float* Dx = D + ((size_t)p * n_state + x) * n_nu;
+    auto value = [&](long long i) -> double {
+        if (!with_ils) return (double)Dx[i];
+        const long long half = (n_taps - 1) / 2;
+        float acc = 0.f;
+        for (long long k = lane; k < n_taps; k += 32) {
+            const long long j = i + k - half;
+            if (j >= 0 && j < n_nu) acc = fmaf(Dx[j], (float)kern[k], acc);
+        }
+        for (int d = 16; d; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
+        return (double)acc * dnu_hi;
+    };
+    double v;
+    const double g0 = g.at(0), gl = g.at(n_nu - 1);
+    if (nu <= g0) v = value(0);
+    else if (nu >= gl) v = value(n_nu - 1);
+    else {
+        long long i = (long long)floor((nu - g0) / dnu_hi);
+        i = max(0LL, min(i, n_nu - 2));
+        while (i > 0 && g.at(i) > nu) --i;
+        while (i + 2 < n_nu && g.at(i + 1) <= nu) ++i;
+        const double a = g.at(i), b = g.at(i + 1), w = (nu - a) / (b - a);
+        const double r0 = value(i);
+        v = w == 0.0 ? r0 : r0 * (1.0 - w) + value(i + 1) * w;
+    }
+    if (lane == 0) {
+        double scale = 1.0;
+        if (observable == 0) {  // vmr_jacobian.jl:120-125
+            const double Rc = R[(size_t)p * ch.n + wid];
+            if (Rc <= 0.0) scale = 0.0;
+            else {
+                const double A = 1.191042953e-5 * (nu * nu * nu), Lg = log1p(A / Rc);
+                scale = 1.4387769 * nu * A / ((Lg * Lg) * Rc * (Rc + A));
+            }
+        }
+        K[((size_t)p * n_state + x) * ch.n + wid] = (float)(v * scale);
+    }
+}
+
+}  // namespace irs
