@@ -193,8 +193,31 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="run a small case of the line-sum kernels for ncu: the 400k-line list, one "
                          "profile, 645-1000 cm^-1, mixed then plain FP64, twice each")
+    ap.add_argument("--profile-jacobian", action="store_true",
+                    help="run a small case of the Jacobian kernels for ncu: the 400k-line list with VP_Y "
+                         "line mixing on CO2, two perturbed profiles, 645-1000 cm^-1, state T + log H2O + "
+                         "log O3 + T_sfc, twice")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.profile_jacobian:
+        pkg = _package()
+        ctx = pkg.B200Context(0)
+        lists = pkg.synthetic.lists_iasi_400k()
+        lm = pkg.VPYLineMixing(pkg.synthetic.vpy_y0(len(lists[2])))
+        snd = pkg.Sounder.make(645.0, 1000.0, 0.25, opd_max=2.0, fwhm_gauss=0.5)
+        profs, ang = pkg.synthetic.perturbed_profiles(2)
+        geoms = [pkg.ViewingGeometry(pkg.scan_angle_to_local_zenith(a)) for a in ang]
+        spec = pkg.StateVectorSpec(len(profs[0].pressure), [pkg.H2O, pkg.O3], include_emissivity=False)
+        kw = _workload_kw()
+        kw.pop("dptmn")
+        for _ in range(2):
+            t0 = time.perf_counter()
+            _, K, _ = pkg.analytic_jacobian_batch(profs, lists, spec, sounder=snd, geoms=geoms, backend=ctx,
+                                                  line_mixing=lm, **kw)
+            print(json.dumps({"jacobians": len(profs), "n_state": K.shape[2], "n_ch": K.shape[1],
+                              "wall_s": time.perf_counter() - t0}), flush=True)
+        ctx.close()
+        return
     if args.profile_case:
         pkg = _package()
         ctx = pkg.B200Context(0)

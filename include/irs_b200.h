@@ -198,6 +198,30 @@ int irs_vjp_batch(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_
                   const irs_fm_options* o, const irs_state_spec* spec, const double* dy, double* dx,
                   double* y);
 
+/* optimal_estimation keyword arguments (optimal_estimation.jl:142-156): method 0
+ * :levenberg_marquardt, 1 :gauss_newton; eps_fixed = ε_fixed. */
+typedef struct {
+    int32_t max_iter, max_linesearch, method;
+    double  gamma0, gamma_factor, gamma_min, conv_factor, eps_fixed;
+} irs_oe_params;
+
+/* optimal_estimation(y, spec, base_prof, linelists; xa, Sa, Se, x0, ...) --
+ * src/Estimation/optimal_estimation.jl:142-291 -- for a batch of scenes with diagonal
+ * Se (se_inv = 1/σ² per channel; 0 drops a channel, as channel_mask does).  Each scene
+ * iterates on its own (LM damping, line search, convergence d²/n < conv_factor); every
+ * stage is one batched GPU call over the scenes still iterating: FP64 normal equations
+ * from the Jacobian, FP64 Cholesky solves, the forward model at trial states (dptmn = 0,
+ * o->precision) and the analytic Jacobian at accepted states.
+ * Arrays: base [n_scene]; y_obs, se_inv, y_fit [n_scene][n_channels]; xa, x0, x_out
+ * [n_scene][n_state]; Sa_inv [n_state][n_state] (shared); M_out [n_scene][n_state]
+ * [n_state] = K^T Se^-1 K at the solution; n_iter, converged, cost [n_scene].
+ * At most 127 state elements. */
+int irs_oe_batch(irs_ctx* ctx, const irs_profile* base, int n_scene, const irs_sounder* s,
+                 const irs_fm_options* o, const irs_state_spec* spec, const double* y_obs,
+                 const double* se_inv, const double* xa, const double* Sa_inv, const double* x0,
+                 const irs_oe_params* prm, double* x_out, double* y_fit, double* M_out,
+                 int32_t* n_iter, int32_t* converged, double* cost);
+
 /* Wait for the context's work; fill per-stage times of the last forward call. */
 int irs_synchronize(irs_ctx* ctx);
 int irs_last_stage_times(irs_ctx* ctx, irs_stage_times* out);
@@ -215,6 +239,43 @@ int irs_cross_sections_noalloc(const irs_line* d_lines, int64_t n_lines, const d
                                int tips_t_min, int tips_n, const double* d_grid, int64_t n_nu,
                                double T, double p_atm, double vmr_self, double cutoff, int method,
                                double x_far, double* d_sigma, void* stream);
+
+/* ------------------------------------------------------------------------------
+ * MLP surrogate of forward_model.  No counterpart in the reference: it maps a
+ * profile plus scan angle (n_in floats) to channel brightness temperatures through
+ * n_layers hidden GELU layers of n_hidden units, on the tcgen05 tensor cores (BF16
+ * weights and activations, FP32 accumulation, FP32 master weights and Adam).  It is
+ * trained on spectra of irs_forward_model_batch, and its callers fall back to that
+ * path for inputs whose OOD score exceeds their threshold.  All X / Y / out buffers
+ * are row-major [n][n_in] / [n][n_out] FP32; host pointers unless named _dev.
+ * ------------------------------------------------------------------------------ */
+typedef struct irs_surrogate irs_surrogate;
+
+int irs_surrogate_create(irs_ctx* ctx, int n_in, int n_hidden, int n_layers, int n_out, uint64_t seed,
+                         irs_surrogate** out);
+int irs_surrogate_destroy(irs_surrogate* s);
+/* parameters as one FP32 vector: per layer W [n_out_l][n_in_l] row-major, then b [n_out_l] */
+int irs_surrogate_param_count(irs_surrogate* s, int64_t* n);
+int irs_surrogate_get_params(irs_surrogate* s, float* params);
+int irs_surrogate_set_params(irs_surrogate* s, const float* params);
+/* input scaling x' = (x - x_mean) / x_sd, output y = y' y_sd + y_mean */
+int irs_surrogate_set_scaling(irs_surrogate* s, const float* x_mean, const float* x_sd, const float* y_mean,
+                              const float* y_sd);
+/* OOD score of a sample = |W x'|^2 / n_in with W [n_in][n_in] the whitening matrix */
+int irs_surrogate_set_whitening(irs_surrogate* s, const float* W);
+/* epochs of Adam on 0.5 mean((y' - t')^2) over full mini-batches of a shuffled set */
+int irs_surrogate_train(irs_surrogate* s, const float* X, const float* Y, int64_t n, int batch, int epochs,
+                        float lr, uint64_t seed, double* loss_per_epoch);
+/* loss and its gradient (same layout as the parameters) on one batch, no update */
+int irs_surrogate_gradients(irs_surrogate* s, const float* X, const float* Y, int64_t n, float* grads,
+                            double* loss);
+/* predictions [n][n_out] and OOD scores [n] (ood nullable) */
+int irs_surrogate_infer(irs_surrogate* s, const float* X, int64_t n, float* out, float* ood);
+/* same with device buffers; ordered after and before the work on `stream` (a cudaStream_t) */
+int irs_surrogate_infer_device(irs_surrogate* s, const float* X_dev, int64_t n, float* out_dev,
+                               float* ood_dev, void* stream);
+/* C [M][N] = A [M][K] B [N][K]^T with BF16 inputs (uint16 bit patterns), FP32 output */
+int irs_gemm_bf16(irs_ctx* ctx, const uint16_t* A, const uint16_t* B, int M, int N, int K, float* C);
 
 /* Number of internal grid points and channels forward_model uses for (s, o). */
 int irs_grid_size(const irs_sounder* s, const irs_fm_options* o, int64_t* n_nu,

@@ -390,4 +390,6 @@ from .synthetic import afgl_atmosphere, synthetic_linelist  # noqa: E402,F401
 from .estimation import (ColumnScale, FullProfile, Jacobian, PartialColumns, StateVectorSpec,  # noqa: E402,F401
                          analytic_jacobian, analytic_jacobian_batch, column, default_fd_steps, dfs_partition,
                          finite_difference_jacobian, forward_model_rrule, pack_state, partial_column_basis,
-                         state_labels, unpack_state, vmr_range)
+                         state_labels, unpack_state, vmr_range, build_sa, scene_nedt, exclude_channels,
+                         RetrievalResult, optimal_estimation, optimal_estimation_batch, oe_diagnostics)
+from .surrogate import Surrogate, surrogate_features, surrogate_forward_batch  # noqa: E402,F401

@@ -54,6 +54,12 @@ class StateSpec(C.Structure):
                 ("vmr_coupling", C.c_int32), ("observable", C.c_int32)]
 
 
+class OEParams(C.Structure):
+    _fields_ = [("max_iter", C.c_int32), ("max_linesearch", C.c_int32), ("method", C.c_int32),
+                ("gamma0", C.c_double), ("gamma_factor", C.c_double), ("gamma_min", C.c_double),
+                ("conv_factor", C.c_double), ("eps_fixed", C.c_double)]
+
+
 class StageTimes(C.Structure):
     _fields_ = [("line_params_ms", C.c_double), ("line_sum_ms", C.c_double),
                 ("rte_ms", C.c_double), ("ils_ms", C.c_double), ("total_ms", C.c_double),
@@ -64,6 +70,7 @@ class StageTimes(C.Structure):
 # every symbol the header declares, with its ctypes signature
 _P = C.c_void_p
 _PD = C.POINTER(C.c_double)
+_PF = C.POINTER(C.c_float)
 SIGNATURES = {
     "irs_abi_version": ([], C.c_int),
     "irs_last_error": ([], C.c_char_p),
@@ -85,11 +92,27 @@ SIGNATURES = {
                             C.POINTER(StateSpec), _PD, _PD], C.c_int),
     "irs_vjp_batch": ([_P, C.POINTER(Profile), C.c_int, C.POINTER(Sounder), C.POINTER(FMOptions),
                        C.POINTER(StateSpec), _PD, _PD, _PD], C.c_int),
+    "irs_oe_batch": ([_P, C.POINTER(Profile), C.c_int, C.POINTER(Sounder), C.POINTER(FMOptions),
+                      C.POINTER(StateSpec), _PD, _PD, _PD, _PD, _PD, C.POINTER(OEParams), _PD, _PD, _PD,
+                      C.POINTER(C.c_int32), C.POINTER(C.c_int32), _PD], C.c_int),
     "irs_synchronize": ([_P], C.c_int),
     "irs_last_stage_times": ([_P, C.POINTER(StageTimes)], C.c_int),
     "irs_cross_sections_noalloc": ([_P, C.c_int64, _P, C.c_int, C.c_int, _P, C.c_int64, C.c_double,
                                     C.c_double, C.c_double, C.c_double, C.c_int, C.c_double, _P, _P],
                                    C.c_int),
+    "irs_surrogate_create": ([_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)],
+                             C.c_int),
+    "irs_surrogate_destroy": ([_P], C.c_int),
+    "irs_surrogate_param_count": ([_P, C.POINTER(C.c_int64)], C.c_int),
+    "irs_surrogate_get_params": ([_P, _PF], C.c_int),
+    "irs_surrogate_set_params": ([_P, _PF], C.c_int),
+    "irs_surrogate_set_scaling": ([_P, _PF, _PF, _PF, _PF], C.c_int),
+    "irs_surrogate_set_whitening": ([_P, _PF], C.c_int),
+    "irs_surrogate_train": ([_P, _PF, _PF, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_uint64, _PD], C.c_int),
+    "irs_surrogate_gradients": ([_P, _PF, _PF, C.c_int64, _PF, _PD], C.c_int),
+    "irs_surrogate_infer": ([_P, _PF, C.c_int64, _PF, _PF], C.c_int),
+    "irs_surrogate_infer_device": ([_P, _P, C.c_int64, _P, _P, _P], C.c_int),
+    "irs_gemm_bf16": ([_P, _P, _P, C.c_int, C.c_int, C.c_int, _PF], C.c_int),
     "irs_grid_size": ([C.POINTER(Sounder), C.POINTER(FMOptions), C.POINTER(C.c_int64),
                        C.POINTER(C.c_int64)], C.c_int),
 }
@@ -127,3 +150,8 @@ def check(rc: int):
 
 def dptr(a: np.ndarray):
     return a.ctypes.data_as(_PD)
+
+
+def fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_PF)

@@ -14,6 +14,7 @@
 #include "linesum.cuh"
 #include "rte_ils.cuh"
 #include "jacobian.cuh"
+#include "oe.cuh"
 
 namespace irs {
 const char* last_error();
@@ -328,8 +329,11 @@ static int64_t state_size(const irs_state_spec& sp, int n_lev) {
 }
 
 // vmr_jacobian.jl:152-505 for profiles [0, n_prof): K_h [n_prof][n_state][n_ch], y_h [n_prof][n_ch]
+// Outputs: host K_h/y_h (double), or with K_dev non-null the device K_dev (float
+// [n_prof][n_state][n_ch]) and host y_h.
 static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder& s,
-                            const irs_fm_options& o_in, const irs_state_spec& sp, double* K_h, double* y_h) {
+                            const irs_fm_options& o_in, const irs_state_spec& sp, double* K_h, double* y_h,
+                            float* K_dev = nullptr) {
     IRS_REQUIRE(n_prof >= 1 && profs, "need at least one profile");
     IRS_REQUIRE(sp.n_retrieved >= 0 && sp.n_retrieved <= 4 && (sp.n_retrieved == 0 || sp.retrieved),
                 "at most 4 retrieved species");
@@ -443,7 +447,8 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
         float* d_D = (float*)workspace(ctx, "jg_D", (size_t)np * n_state * n_nu * sizeof(float));
         double* d_I = (double*)workspace(ctx, "I", (size_t)np * n_nu * sizeof(double));
         double* d_RB = (double*)workspace(ctx, "jg_RB", (size_t)2 * np * n_ch * sizeof(double));
-        float* d_K = (float*)workspace(ctx, "jg_K", (size_t)np * n_state * n_ch * sizeof(float));
+        float* d_K = K_dev ? K_dev + (size_t)p0 * n_state * n_ch
+                           : (float*)workspace(ctx, "jg_K", (size_t)np * n_state * n_ch * sizeof(float));
         SegDev* d_segs = upload(ctx, "segs", sd);
         SegW* d_sw = upload(ctx, "jg_w", sw);
         int* d_sn = upload(ctx, "jg_n", sn);
@@ -465,9 +470,14 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
             const dim3 g2((unsigned)((n_nu + kJgStrip - 1) / kJgStrip), np * L);
             const float cut_g = (float)(o.cutoff / ig.dnu_hi);
             const bool lm = o.line_mixing == 1;
-#define IRS_JG(NO)                                                                                                   \
-    if (lm) jg_linesum_kernel<true, NO><<<g2, kJgWarps * 32, 0, st>>>(d_segs, d_sn, d_sw, d_pl, go, n_nu, cut_g, d_out); \
-    else jg_linesum_kernel<false, NO><<<g2, kJgWarps * 32, 0, st>>>(d_segs, d_sn, d_sw, d_pl, go, n_nu, cut_g, d_out)
+#define IRS_JG(NO)                                                                                          \
+    do {                                                                                                    \
+        const size_t sm = jg_smem_bytes(NO);                                                                \
+        IRS_CUDA(cudaFuncSetAttribute(jg_linesum_kernel<true, NO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
+        IRS_CUDA(cudaFuncSetAttribute(jg_linesum_kernel<false, NO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
+        if (lm) jg_linesum_kernel<true, NO><<<g2, kJgWarps * 32, sm, st>>>(d_segs, d_sn, d_sw, d_pl, go, n_nu, cut_g, d_out); \
+        else jg_linesum_kernel<false, NO><<<g2, kJgWarps * 32, sm, st>>>(d_segs, d_sn, d_sw, d_pl, go, n_nu, cut_g, d_out); \
+    } while (0)
             switch (n_out) {
                 case 3: IRS_JG(3); break;
                 case 5: IRS_JG(5); break;
@@ -496,12 +506,15 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
             d_D, n_nu, (int)n_state, d_kern, n_taps, ig.dnu_hi, to_dev(ig.g), to_dev(ch), o.with_ils, d_RB,
             sp.observable, d_K);
         check_launch(ctx);
-        Kf.resize((size_t)np * n_state * n_ch);
-        IRS_CUDA(cudaMemcpyAsync(Kf.data(), d_K, Kf.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+        if (!K_dev) {
+            Kf.resize((size_t)np * n_state * n_ch);
+            IRS_CUDA(cudaMemcpyAsync(Kf.data(), d_K, Kf.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+        }
         IRS_CUDA(cudaMemcpyAsync(y_h + (size_t)p0 * n_ch, d_RB + (sp.observable == 0 ? (size_t)np * n_ch : 0),
                                  (size_t)np * n_ch * sizeof(double), cudaMemcpyDeviceToHost, st));
         IRS_CUDA(cudaStreamSynchronize(st));
-        for (size_t k = 0; k < Kf.size(); ++k) K_h[(size_t)p0 * n_state * n_ch + k] = (double)Kf[k];
+        if (!K_dev)
+            for (size_t k = 0; k < Kf.size(); ++k) K_h[(size_t)p0 * n_state * n_ch + k] = (double)Kf[k];
     }
 }
 
@@ -582,6 +595,243 @@ static void forward_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, c
             ctx->prior.core_pairs += keep.core_pairs;
             ctx->n_h2d = h2d, ctx->n_d2h = d2h, ctx->n_launch = nl;
         }
+    }
+}
+
+// ------------------------------------------------------------ optimal estimation
+// unpack_state (state_vector.jl:380-403) into an irs_profile whose arrays live in T / vmr
+static void unpack_into(const irs_state_spec& sp, const double* x, const irs_profile& base, double eps_fixed,
+                        std::vector<double>& T, std::vector<double>& vmr, irs_profile& out) {
+    const int nl = base.n_lev;
+    out = base;
+    T.assign(base.temperature, base.temperature + nl);
+    vmr.assign(base.vmr, base.vmr + (size_t)base.n_species * nl);
+    int k = 0;
+    if (sp.include_temperature) {
+        for (int j = 0; j < nl; ++j) T[j] = x[k + j];
+        k += nl;
+    }
+    for (int r = 0; r < sp.n_retrieved; ++r) {
+        int q = -1;
+        for (int i = 0; i < base.n_species; ++i)
+            if (base.species[i] == sp.retrieved[r]) q = i;
+        IRS_REQUIRE(q >= 0, "base profile is missing a retrieved species");
+        for (int j = 0; j < nl; ++j) vmr[(size_t)q * nl + j] = sp.log_vmr ? std::exp(x[k + j]) : x[k + j];
+        k += nl;
+    }
+    out.temperature = T.data();
+    out.vmr = vmr.data();
+    out.T_sfc = sp.include_tsfc ? x[k++] : T[0];
+    out.eps_sfc = sp.include_emissivity ? x[k++] : eps_fixed;
+}
+
+// Profiles of the states x[list[i]] (arrays owned by the returned holder)
+struct StateProfiles {
+    std::vector<std::vector<double>> T, vmr;
+    std::vector<irs_profile> prof;
+};
+static void build_profiles(const irs_state_spec& sp, const std::vector<int>& list, const double* x, int n,
+                           const irs_profile* base, double eps_fixed, StateProfiles& h) {
+    h.T.assign(list.size(), {});
+    h.vmr.assign(list.size(), {});
+    h.prof.assign(list.size(), irs_profile{});
+    for (size_t i = 0; i < list.size(); ++i)
+        unpack_into(sp, x + (size_t)list[i] * n, base[list[i]], eps_fixed, h.T[i], h.vmr[i], h.prof[i]);
+}
+
+static void launch_oe_normal(irs_ctx* ctx, const int* d_list, int n_list, int n, int n_ch, const float* K,
+                             const double* w, const double* r, double* M, double* b) {
+    const size_t smem = (size_t)(2 * kOeTile * n + kOeTile) * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+        IRS_CUDA(cudaFuncSetAttribute(oe_normal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr = true;
+    }
+    const int grid = std::min(n_list, 148 * 4);
+    oe_normal_kernel<<<grid, kOeThreads, smem, ctx->stream>>>(d_list, n_list, n, n_ch, K, w, r, M, b);
+    check_launch(ctx);
+}
+
+static void launch_oe_solve(irs_ctx* ctx, const int* d_list, int n_list, int n, const double* M, const double* b,
+                            const double* Sa_inv, const double* x, const double* xa, const double* gamma, double* dx,
+                            double* d2, int* ok) {
+    const size_t smem = ((size_t)n * n + 4 * (size_t)n) * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+        IRS_CUDA(cudaFuncSetAttribute(oe_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr = true;
+    }
+    const int grid = std::min(n_list, 148);
+    oe_solve_kernel<<<grid, kOeThreads, smem, ctx->stream>>>(d_list, n_list, n, M, b, Sa_inv, x, xa, gamma, dx, d2, ok);
+    check_launch(ctx);
+}
+
+// optimal_estimation (optimal_estimation.jl:142-291) for a batch of scenes: every scene
+// runs its own Levenberg-Marquardt (or Gauss-Newton) iteration; each LM stage (normal
+// equations, damped solve, trial forward model, Jacobian at accepted states) is one
+// batched call over the scenes still iterating.
+static void oe_batch(irs_ctx* ctx, const irs_profile* base, int n_scene, const irs_sounder& s,
+                     const irs_fm_options& o_in, const irs_state_spec& sp, const double* y_obs, const double* se_inv,
+                     const double* xa, const double* Sa_inv, const double* x0, const irs_oe_params& prm,
+                     double* x_out, double* y_fit, double* M_out, int32_t* n_iter, int32_t* converged,
+                     double* cost_out) {
+    IRS_REQUIRE(n_scene >= 1 && base, "need at least one scene");
+    IRS_REQUIRE(prm.method == 0 || prm.method == 1, "method must be 0 (levenberg_marquardt) or 1 (gauss_newton)");
+    IRS_REQUIRE(prm.max_iter >= 1 && prm.max_linesearch >= 1, "max_iter and max_linesearch must be positive");
+    const int n = (int)state_size(sp, base[0].n_lev);
+    IRS_REQUIRE(n >= 1 && n <= kOeMaxState, "the state vector must have 1 to 127 elements on this path");
+    const int64_t n_ch = make_grid(s.nu_min, s.nu_max, s.dnu).n;
+    irs_fm_options o = o_in;
+    o.dptmn = 0.0;  // frozen line set for F as for K (optimal_estimation.jl:193-198)
+    const cudaStream_t st = ctx->stream;
+    const size_t S = (size_t)n_scene;
+    // device state
+    float* d_K = (float*)workspace(ctx, "oe_K", S * n * n_ch * sizeof(float));
+    float* d_Kt = (float*)workspace(ctx, "oe_Ktmp", S * n * n_ch * sizeof(float));
+    double* d_w = (double*)workspace(ctx, "oe_w", S * n_ch * sizeof(double));
+    double* d_r = (double*)workspace(ctx, "oe_r", S * n_ch * sizeof(double));
+    double* d_M = (double*)workspace(ctx, "oe_M", S * n * n * sizeof(double));
+    double* d_b = (double*)workspace(ctx, "oe_b", S * n * sizeof(double));
+    double* d_Sa = (double*)workspace(ctx, "oe_Sa", (size_t)n * n * sizeof(double));
+    double* d_x = (double*)workspace(ctx, "oe_x", S * n * sizeof(double));
+    double* d_xa = (double*)workspace(ctx, "oe_xa", S * n * sizeof(double));
+    double* d_g = (double*)workspace(ctx, "oe_gamma", S * sizeof(double));
+    double* d_dx = (double*)workspace(ctx, "oe_dx", S * n * sizeof(double));
+    double* d_d2 = (double*)workspace(ctx, "oe_d2", S * sizeof(double));
+    int* d_ok = (int*)workspace(ctx, "oe_ok", S * sizeof(int));
+    int* d_list = (int*)workspace(ctx, "oe_list", S * sizeof(int));
+    double* d_fm = (double*)workspace(ctx, "oe_fm", 2 * S * n_ch * sizeof(double));
+    IRS_CUDA(cudaMemcpyAsync(d_w, se_inv, S * n_ch * sizeof(double), cudaMemcpyHostToDevice, st));
+    IRS_CUDA(cudaMemcpyAsync(d_Sa, Sa_inv, (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice, st));
+    IRS_CUDA(cudaMemcpyAsync(d_xa, xa, S * n * sizeof(double), cudaMemcpyHostToDevice, st));
+
+    std::vector<double> x(x0, x0 + S * n), F(S * n_ch), J(S), gamma(S, prm.method == 1 ? 0.0 : prm.gamma0);
+    std::vector<int32_t> iters(S, 0), conv(S, 0);
+    auto cost = [&](int sc, const double* Fs, const double* xs) {
+        double c = 0.0;
+        const double* ys = y_obs + (size_t)sc * n_ch;
+        const double* ws = se_inv + (size_t)sc * n_ch;
+        for (int64_t i = 0; i < n_ch; ++i) {
+            const double r = ys[i] - Fs[i];
+            c += r * ws[i] * r;
+        }
+        std::vector<double> d(n);
+        for (int i = 0; i < n; ++i) d[i] = xs[i] - xa[(size_t)sc * n + i];
+        for (int i = 0; i < n; ++i) {
+            double v = 0.0;
+            for (int j = 0; j < n; ++j) v += Sa_inv[(size_t)i * n + j] * d[j];
+            c += d[i] * v;
+        }
+        return c;
+    };
+    // F and K at the states of `list` (K into the scene slots of d_K)
+    auto jac = [&](const std::vector<int>& list) {
+        if (list.empty()) return;
+        StateProfiles h;
+        build_profiles(sp, list, x.data(), n, base, prm.eps_fixed, h);
+        std::vector<double> y((size_t)list.size() * n_ch);
+        jacobian_device(ctx, h.prof.data(), (int)list.size(), s, o, sp, nullptr, y.data(), d_Kt);
+        for (size_t i = 0; i < list.size(); ++i) {
+            const int sc = list[i];
+            if (sc != (int)i || d_Kt != d_K)
+                IRS_CUDA(cudaMemcpyAsync(d_K + (size_t)sc * n * n_ch, d_Kt + i * n * n_ch, (size_t)n * n_ch * sizeof(float),
+                                         cudaMemcpyDeviceToDevice, st));
+            std::copy(y.begin() + i * n_ch, y.begin() + (i + 1) * n_ch, F.begin() + (size_t)sc * n_ch);
+        }
+    };
+    auto upload_resid = [&](const std::vector<int>& list) {
+        std::vector<double> r((size_t)n_ch);
+        for (int sc : list) {
+            for (int64_t i = 0; i < n_ch; ++i) r[i] = y_obs[(size_t)sc * n_ch + i] - F[(size_t)sc * n_ch + i];
+            IRS_CUDA(cudaMemcpyAsync(d_r + (size_t)sc * n_ch, r.data(), n_ch * sizeof(double), cudaMemcpyHostToDevice, st));
+            IRS_CUDA(cudaStreamSynchronize(st));
+        }
+    };
+
+    std::vector<int> all(S);
+    std::iota(all.begin(), all.end(), 0);
+    jac(all);
+    for (int sc = 0; sc < n_scene; ++sc) J[sc] = cost(sc, F.data() + (size_t)sc * n_ch, x.data() + (size_t)sc * n);
+    std::vector<int> active = all;
+    while (!active.empty()) {
+        for (int sc : active) iters[sc] += 1;
+        upload_resid(active);
+        IRS_CUDA(cudaMemcpyAsync(d_list, active.data(), active.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        launch_oe_normal(ctx, d_list, (int)active.size(), n, (int)n_ch, d_K, d_w, d_r, d_M, d_b);
+        std::vector<int> pending = active, accepted;
+        std::vector<double> d2n(S, 0.0);
+        for (int ls = 0; ls < prm.max_linesearch && !pending.empty(); ++ls) {
+            IRS_CUDA(cudaMemcpyAsync(d_x, x.data(), S * n * sizeof(double), cudaMemcpyHostToDevice, st));
+            IRS_CUDA(cudaMemcpyAsync(d_g, gamma.data(), S * sizeof(double), cudaMemcpyHostToDevice, st));
+            IRS_CUDA(cudaMemcpyAsync(d_list, pending.data(), pending.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+            launch_oe_solve(ctx, d_list, (int)pending.size(), n, d_M, d_b, d_Sa, d_x, d_xa, d_g, d_dx, d_d2, d_ok);
+            std::vector<double> dx(S * n), d2(S);
+            std::vector<int> okv(S);
+            IRS_CUDA(cudaMemcpyAsync(dx.data(), d_dx, S * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+            IRS_CUDA(cudaMemcpyAsync(d2.data(), d_d2, S * sizeof(double), cudaMemcpyDeviceToHost, st));
+            IRS_CUDA(cudaMemcpyAsync(okv.data(), d_ok, S * sizeof(int), cudaMemcpyDeviceToHost, st));
+            IRS_CUDA(cudaStreamSynchronize(st));
+            std::vector<double> xt(S * n);
+            std::vector<int> trial;
+            for (int sc : pending) {
+                if (!okv[sc]) continue;  // damped normal matrix not positive definite: no step
+                for (int i = 0; i < n; ++i) xt[(size_t)sc * n + i] = x[(size_t)sc * n + i] + dx[(size_t)sc * n + i];
+                trial.push_back(sc);
+            }
+            std::vector<double> Ft;
+            if (!trial.empty()) {
+                StateProfiles h;
+                build_profiles(sp, trial, xt.data(), n, base, prm.eps_fixed, h);
+                const size_t nt = trial.size();
+                IRS_REQUIRE(2 * nt * n_ch <= 2 * S * n_ch, "trial batch");
+                forward_device(ctx, h.prof.data(), (int)nt, s, o, d_fm, d_fm + nt * n_ch);
+                Ft.resize(nt * n_ch);
+                IRS_CUDA(cudaMemcpyAsync(Ft.data(), d_fm + (sp.observable == 0 ? nt * n_ch : 0), nt * n_ch * sizeof(double),
+                                         cudaMemcpyDeviceToHost, st));
+                IRS_CUDA(cudaStreamSynchronize(st));
+            }
+            std::vector<int> still;
+            size_t ti = 0;
+            for (int sc : pending) {
+                if (!okv[sc]) {
+                    if (prm.method == 0) { gamma[sc] *= prm.gamma_factor; still.push_back(sc); }
+                    continue;
+                }
+                const double* Fs = Ft.data() + (ti++) * n_ch;
+                const double Jt = cost(sc, Fs, xt.data() + (size_t)sc * n);
+                if (Jt < J[sc]) {
+                    d2n[sc] = d2[sc] / n;
+                    std::copy(xt.begin() + (size_t)sc * n, xt.begin() + (size_t)(sc + 1) * n, x.begin() + (size_t)sc * n);
+                    J[sc] = Jt;
+                    if (prm.method == 0) gamma[sc] = std::max(gamma[sc] / prm.gamma_factor, prm.gamma_min);
+                    accepted.push_back(sc);
+                } else if (prm.method == 0) {
+                    gamma[sc] *= prm.gamma_factor;
+                    still.push_back(sc);
+                }
+            }
+            pending.swap(still);
+        }
+        jac(accepted);  // F, K at the accepted states (optimal_estimation.jl:227-229)
+        std::vector<int> next;
+        for (int sc : accepted) {
+            if (d2n[sc] < prm.conv_factor) conv[sc] = 1;
+            else if (iters[sc] < prm.max_iter) next.push_back(sc);
+        }
+        active.swap(next);
+    }
+    // normal matrix at the solution for the diagnostics
+    upload_resid(all);
+    IRS_CUDA(cudaMemcpyAsync(d_list, all.data(), S * sizeof(int), cudaMemcpyHostToDevice, st));
+    launch_oe_normal(ctx, d_list, n_scene, n, (int)n_ch, d_K, d_w, d_r, d_M, d_b);
+    IRS_CUDA(cudaMemcpyAsync(M_out, d_M, S * n * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    IRS_CUDA(cudaStreamSynchronize(st));
+    std::copy(x.begin(), x.end(), x_out);
+    std::copy(F.begin(), F.end(), y_fit);
+    for (int sc = 0; sc < n_scene; ++sc) {
+        n_iter[sc] = iters[sc];
+        converged[sc] = conv[sc];
+        cost_out[sc] = J[sc];
     }
 }
 
@@ -867,6 +1117,20 @@ int irs_vjp_batch(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_
             for (int64_t c = 0; c < n_ch; ++c) acc += row[c] * d[c];
             dx[(size_t)p * n_state + x] = acc;
         }
+    IRS_API_END
+}
+
+int irs_oe_batch(irs_ctx* ctx, const irs_profile* base, int n_scene, const irs_sounder* s, const irs_fm_options* o,
+                 const irs_state_spec* spec, const double* y_obs, const double* se_inv, const double* xa,
+                 const double* Sa_inv, const double* x0, const irs_oe_params* prm, double* x_out, double* y_fit,
+                 double* M_out, int32_t* n_iter, int32_t* converged, double* cost) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && base && s && o && spec && y_obs && se_inv && xa && Sa_inv && x0 && prm && x_out && y_fit &&
+                    M_out && n_iter && converged && cost,
+                "invalid arguments");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    oe_batch(ctx, base, n_scene, *s, *o, *spec, y_obs, se_inv, xa, Sa_inv, x0, *prm, x_out, y_fit, M_out, n_iter,
+             converged, cost);
     IRS_API_END
 }
 

@@ -126,11 +126,6 @@ constexpr int kJgWarpPts = 32 * kJgQ;          // 128 points per warp
 constexpr int kJgWarps = 8;
 constexpr int kJgStrip = kJgWarps * kJgWarpPts;
 
-struct JgTile {
-    float4 u[32];   // uh, ul, class, dfar2
-    float4 q0[32], q1[32], q2[32], q3[32], q4[32];
-};
-
 // Per pair: the value and derivative terms of one line at offset d (grid units).
 // H-ped and its derivatives; x = d fx, y; c1 = P/cut^2, c0 = -2P with P = An Hc.
 // Far wing: H = y/(sqrt(pi)(x^2+y^2)); core: FP32 Faddeeva with w' = -2 z w + 2i/sqrt(pi).
@@ -182,11 +177,34 @@ __device__ __forceinline__ void jg_pair(float d, bool core, const float4& q0, co
     }
 }
 
+// Warp-private staging of one 32-line tile, compacted into the two line classes.
+// Fast lines (all 128 points of the warp inside the cutoff and outside the Faddeeva
+// core) carry closed-form coefficients of the far-wing terms in rho = 1/(d^2 + b2),
+// d the offset in grid units and b2 = (y/fx)^2:
+//   s  = a_s rho
+//   sT = aT1 rho + aT2 rho^2
+//   sp = ap1 rho + ap2 rho^2 + ap3 d rho^2        (sv likewise)
+//   D  = cD d rho,  DT = cT1 d rho + cT2 d rho^2,
+//   Dp = cp1 d rho + cp2 rho + cp3 rho^2 + cp4 d rho^2          (line mixing)
+// which follow from H = y/(sqrt(pi)(x^2+y^2)), its x and y derivatives and
+// x = d fx (x_T = d fx_T, x_p = -fx u_p); their pedestals are quadratics in the point
+// index summed over the tile.  Slow lines keep the general per-pair form (jg_pair).
+struct JgTile {
+    float4 fu[32];   // fast: uh, ul, b2, a_s
+    float4 fT[32];   // fast: aT1, aT2, ap1, ap2
+    float4 fp[32];   // fast: ap3, av1, av2, av3
+    float4 fL0[32];  // fast, line mixing: cD, cT1, cT2, cp1
+    float4 fL1[32];  // fast, line mixing: cp2, cp3, cp4, -
+    float4 su[32];   // slow: uh, ul, -, dfar2
+    float4 q0[32], q1[32], q2[32], q3[32], q4[32];  // slow: per-line primitives
+};
+
 template <bool LM>
 __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long long wb, float cut, int lane,
                            JgTile& T, float sum[4][kJgQ], float dsum[3][kJgQ]) {
     constexpr float kCentre = 0.5f * (kJgWarpPts - 1);
     constexpr float kHalf = 0.5f * kJgWarpPts + 0.5f;
+    constexpr float k = (float)kInvSqrtPi;
     const float cut2 = cut * cut, icut2 = 1.f / cut2;
     long long jlo = 0, jhi = 0;
     if (lane == 0) {
@@ -195,67 +213,191 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
     }
     jlo = __shfl_sync(kFull, jlo, 0);
     jhi = __shfl_sync(kFull, jhi, 0);
-    float comp[4][kJgQ], dcomp[3][kJgQ];
+    const float pl0 = (float)lane;
+    const unsigned lt = (1u << lane) - 1u;
+    // packed accumulators over point pairs (q = 2h, 2h + 1)
+    float2 S[kJgQ / 2], C[kJgQ / 2], ST[kJgQ / 2], SP[kJgQ / 2], SV[kJgQ / 2];
+    float2 SD[kJgQ / 2], CD[kJgQ / 2], SDT[kJgQ / 2], SDP[kJgQ / 2];
 #pragma unroll
-    for (int c = 0; c < 4; ++c)
+    for (int h = 0; h < kJgQ / 2; ++h) {
+        S[h] = C[h] = ST[h] = SP[h] = SV[h] = make_float2(0.f, 0.f);
+        SD[h] = CD[h] = SDT[h] = SDP[h] = make_float2(0.f, 0.f);
+    }
+    float2 offn[kJgQ / 2], offs[kJgQ / 2];  // natural (32q, 32(q+1)) and swapped offsets
 #pragma unroll
-        for (int q = 0; q < kJgQ; ++q) sum[c][q] = comp[c][q] = 0.f;
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int q = 0; q < kJgQ; ++q) dsum[c][q] = dcomp[c][q] = 0.f;
+    for (int h = 0; h < kJgQ / 2; ++h) {
+        offn[h] = make_float2(64.f * h, 64.f * h + 32.f);
+        offs[h] = make_float2(64.f * h + 32.f, 64.f * h);
+    }
     for (long long t0 = jlo; t0 < jhi; t0 += 32) {
         const int nt = (int)min(32LL, jhi - t0);
-        __syncwarp();
+        int cls = 0;
+        float uh = 0.f, ul = 0.f;
+        float4 a0, a1, a2, a3, a4;
+        // pedestal quadratic of a fast line: value at point i is A + B i + Cq i^2
+        float pA[4] = {0.f, 0.f, 0.f, 0.f}, pB[4] = {0.f, 0.f, 0.f, 0.f}, pC[4] = {0.f, 0.f, 0.f, 0.f};
         if (lane < nt) {
             const long long q = sg.off + t0 + lane;
             const double u = g.U[q] - (double)wb;
-            const float uh = (float)u;
-            const float4 q2 = g.q2[q];
+            uh = (float)u;
+            ul = (float)(u - (double)uh);
+            a0 = g.q0[q];
+            a1 = g.q1[q];
+            a2 = g.q2[q];
+            a3 = g.q3[q];
+            if (LM) a4 = g.q4[q];
             const float dist = fabsf(uh - kCentre);
-            float cls = 2.f;
-            if (dist > cut + kHalf) cls = 0.f;
-            else if (dist + kHalf <= cut && dist > q2.w + kHalf) cls = 1.f;
-            T.u[lane] = make_float4(uh, (float)(u - (double)uh), cls, q2.w * q2.w);
-            T.q0[lane] = g.q0[q];
-            T.q1[lane] = g.q1[q];
-            T.q2[lane] = q2;
-            T.q3[lane] = g.q3[q];
-            if (LM) T.q4[lane] = g.q4[q];
+            if (dist > cut + kHalf) cls = 0;
+            else if (dist + kHalf <= cut && dist > a2.w + kHalf) cls = 1;
+            else cls = 2;
+        }
+        const unsigned fm = __ballot_sync(kFull, cls == 1), sm = __ballot_sync(kFull, cls == 2);
+        __syncwarp();
+        if (cls == 1) {
+            const int pos = __popc(fm & lt);
+            const float An = a0.x, fx = a0.y, y = a0.z, Hc = a0.w;
+            const float AnT = a1.x, fxT = a1.y, yT = a1.z, HcT = a1.w;
+            const float yp = a2.x, up = a2.y, Hcp = a2.z, yv = a3.x, uv = a3.y, Hcv = a3.z;
+            const float gg = 1.f / (fx * fx), b2 = y * y * gg, Aky = An * k * y;
+            T.fu[pos] = make_float4(uh, ul, b2, Aky * gg);
+            const float r_fx = fxT / fx;
+            T.fT[pos] = make_float4(gg * k * (AnT * y + An * yT) - 2.f * Aky * r_fx * gg,
+                                    2.f * Aky * b2 * r_fx * gg - 2.f * An * k * yT * b2 * gg, An * k * yp * gg,
+                                    -2.f * An * k * yp * b2 * gg);
+            T.fp[pos] = make_float4(2.f * Aky * up * gg, An * k * yv * gg, -2.f * An * k * yv * b2 * gg,
+                                    2.f * Aky * uv * gg);
+            if (LM) {
+                const float Yw = a4.x, YwT = a4.y, Ywp = a4.z;
+                T.fL0[pos] = make_float4(Yw * k / fx, YwT * k / fx - Yw * k * gg * fxT,
+                                         2.f * Yw * k * gg * fxT * b2 - 2.f * Yw * k * y * fx * yT * gg * gg,
+                                         Ywp * k / fx);
+                T.fL1[pos] = make_float4(Yw * k * up / fx, -2.f * Yw * k * up * b2 / fx,
+                                         -2.f * Yw * k * y * fx * yp * gg * gg, 0.f);
+            }
+            // pedestals: -P0 pf, -PT pf, -An Hc pf_p - An Hc_p pf, ... with pf = 2 - (i - u)^2 / c^2
+            const float P[4] = {An * Hc, AnT * Hc + An * HcT, An * Hcp, An * Hcv};
+            const float e0 = 2.f - uh * uh * icut2, e1 = 2.f * uh * icut2;
+#pragma unroll
+            for (int o = 0; o < 4; ++o) {
+                pA[o] = -P[o] * e0;
+                pB[o] = -P[o] * e1;
+                pC[o] = P[o] * icut2;
+            }
+            const float shp = 2.f * An * Hc * icut2;  // pf_p = 2 (i - u) u_p / c^2
+            pA[2] += shp * up * uh;
+            pB[2] -= shp * up;
+            pA[3] += shp * uv * uh;
+            pB[3] -= shp * uv;
+        } else if (cls == 2) {
+            const int pos = __popc(sm & lt);
+            T.su[pos] = make_float4(uh, ul, 0.f, a2.w * a2.w);
+            T.q0[pos] = a0;
+            T.q1[pos] = a1;
+            T.q2[pos] = a2;
+            T.q3[pos] = a3;
+            if (LM) T.q4[pos] = a4;
+        }
+        float wA[4], wB[4], wC[4];
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            wA[o] = warp_sum(pA[o]);
+            wB[o] = warp_sum(pB[o]);
+            wC[o] = warp_sum(pC[o]);
         }
         __syncwarp();
-        float t[4][kJgQ], td[3][kJgQ];
+        const int nf = __popc(fm), ns = __popc(sm);
+        float2 TS[kJgQ / 2], TD[kJgQ / 2];  // tile partials of the value sums (Kahan-added below)
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
+        for (int h = 0; h < kJgQ / 2; ++h) TS[h] = TD[h] = make_float2(0.f, 0.f);
+        for (int kk = 0; kk < nf; ++kk) {
+            const float4 f0 = T.fu[kk], f1 = T.fT[kk], f2 = T.fp[kk];
+            const float d0 = (pl0 - f0.x) - f0.y;
+            const float2 d0s = make_float2(d0, d0), b2 = make_float2(f0.z, f0.z);
+            float4 l0, l1;
+            if (LM) {
+                l0 = T.fL0[kk];
+                l1 = T.fL1[kk];
+            }
 #pragma unroll
-            for (int q = 0; q < kJgQ; ++q) t[c][q] = 0.f;
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-            for (int q = 0; q < kJgQ; ++q) td[c][q] = 0.f;
-        for (int k = 0; k < nt; ++k) {
-            const float4 u = T.u[k];
-            if (u.z == 0.f) continue;
-            const float4 q0 = T.q0[k], q1 = T.q1[k], q2 = T.q2[k], q3 = T.q3[k];
-            const float4 q4 = LM ? T.q4[k] : make_float4(0.f, 0.f, 0.f, 0.f);
-            const bool fast = u.z == 1.f;
-#pragma unroll
-            for (int q = 0; q < kJgQ; ++q) {
-                const float d = (((float)lane + 32.f * q) - u.x) - u.y;
-                const float d2 = d * d;
-                if (!fast && d2 > cut2) continue;
-                jg_pair<LM>(d, !fast && d2 <= u.w, q0, q1, q2, q3, q4, icut2, t[0][q], t[1][q], t[2][q], t[3][q],
-                            td[0][q], td[1][q], td[2][q]);
+            for (int h = 0; h < kJgQ / 2; ++h) {
+                const float2 dsw = __fadd2_rn(d0s, offs[h]);      // (d[q+1], d[q])
+                const float2 dn = __fadd2_rn(d0s, offn[h]);       // (d[q], d[q+1])
+                const float2 es = __ffma2_rn(dsw, dsw, b2);       // (e[q+1], e[q])
+                const float R = rcp_fast(es.x * es.y);
+                const float2 rho = __fmul2_rn(es, make_float2(R, R));  // (1/e[q], 1/e[q+1])
+                const float2 rho2 = __fmul2_rn(rho, rho);
+                const float2 drho2 = __fmul2_rn(dn, rho2);
+                TS[h] = __ffma2_rn(make_float2(f0.w, f0.w), rho, TS[h]);
+                ST[h] = __ffma2_rn(make_float2(f1.x, f1.x), rho, ST[h]);
+                ST[h] = __ffma2_rn(make_float2(f1.y, f1.y), rho2, ST[h]);
+                SP[h] = __ffma2_rn(make_float2(f1.z, f1.z), rho, SP[h]);
+                SP[h] = __ffma2_rn(make_float2(f1.w, f1.w), rho2, SP[h]);
+                SP[h] = __ffma2_rn(make_float2(f2.x, f2.x), drho2, SP[h]);
+                SV[h] = __ffma2_rn(make_float2(f2.y, f2.y), rho, SV[h]);
+                SV[h] = __ffma2_rn(make_float2(f2.z, f2.z), rho2, SV[h]);
+                SV[h] = __ffma2_rn(make_float2(f2.w, f2.w), drho2, SV[h]);
+                if (LM) {
+                    const float2 drho = __fmul2_rn(dn, rho);
+                    TD[h] = __ffma2_rn(make_float2(l0.x, l0.x), drho, TD[h]);
+                    SDT[h] = __ffma2_rn(make_float2(l0.y, l0.y), drho, SDT[h]);
+                    SDT[h] = __ffma2_rn(make_float2(l0.z, l0.z), drho2, SDT[h]);
+                    SDP[h] = __ffma2_rn(make_float2(l0.w, l0.w), drho, SDP[h]);
+                    SDP[h] = __ffma2_rn(make_float2(l1.x, l1.x), rho, SDP[h]);
+                    SDP[h] = __ffma2_rn(make_float2(l1.y, l1.y), rho2, SDP[h]);
+                    SDP[h] = __ffma2_rn(make_float2(l1.z, l1.z), drho2, SDP[h]);
+                }
             }
         }
+        for (int kk = 0; kk < ns; ++kk) {
+            const float4 u = T.su[kk];
+            const float4 q0 = T.q0[kk], q1 = T.q1[kk], q2 = T.q2[kk], q3 = T.q3[kk];
+            const float4 q4 = LM ? T.q4[kk] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-        for (int q = 0; q < kJgQ; ++q) {
-#pragma unroll
-            for (int c = 0; c < 4; ++c) kahan_add(sum[c][q], comp[c][q], t[c][q]);
-            if (LM)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) kahan_add(dsum[c][q], dcomp[c][q], td[c][q]);
+            for (int q = 0; q < kJgQ; ++q) {
+                const float d = ((pl0 + 32.f * q) - u.x) - u.y;
+                const float d2 = d * d;
+                if (d2 > cut2) continue;
+                float s = 0.f, sT = 0.f, sp = 0.f, sv = 0.f, D = 0.f, DT = 0.f, Dp = 0.f;
+                jg_pair<LM>(d, d2 <= u.w, q0, q1, q2, q3, q4, icut2, s, sT, sp, sv, D, DT, Dp);
+                const int h = q >> 1;
+                if (q & 1) {
+                    TS[h].y += s; ST[h].y += sT; SP[h].y += sp; SV[h].y += sv;
+                    if (LM) { TD[h].y += D; SDT[h].y += DT; SDP[h].y += Dp; }
+                } else {
+                    TS[h].x += s; ST[h].x += sT; SP[h].x += sp; SV[h].x += sv;
+                    if (LM) { TD[h].x += D; SDT[h].x += DT; SDP[h].x += Dp; }
+                }
+            }
         }
+        // pedestal quadratics of the fast lines, then the compensated tile sums
+#pragma unroll
+        for (int h = 0; h < kJgQ / 2; ++h) {
+            const float i0 = pl0 + 64.f * h, i1 = i0 + 32.f;
+            TS[h].x += fmaf(i0, fmaf(i0, wC[0], wB[0]), wA[0]);
+            TS[h].y += fmaf(i1, fmaf(i1, wC[0], wB[0]), wA[0]);
+            ST[h].x += fmaf(i0, fmaf(i0, wC[1], wB[1]), wA[1]);
+            ST[h].y += fmaf(i1, fmaf(i1, wC[1], wB[1]), wA[1]);
+            SP[h].x += fmaf(i0, fmaf(i0, wC[2], wB[2]), wA[2]);
+            SP[h].y += fmaf(i1, fmaf(i1, wC[2], wB[2]), wA[2]);
+            SV[h].x += fmaf(i0, fmaf(i0, wC[3], wB[3]), wA[3]);
+            SV[h].y += fmaf(i1, fmaf(i1, wC[3], wB[3]), wA[3]);
+            kahan_add(S[h].x, C[h].x, TS[h].x);
+            kahan_add(S[h].y, C[h].y, TS[h].y);
+            if (LM) {
+                kahan_add(SD[h].x, CD[h].x, TD[h].x);
+                kahan_add(SD[h].y, CD[h].y, TD[h].y);
+            }
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < kJgQ / 2; ++h) {
+        sum[0][2 * h] = S[h].x; sum[0][2 * h + 1] = S[h].y;
+        sum[1][2 * h] = ST[h].x; sum[1][2 * h + 1] = ST[h].y;
+        sum[2][2 * h] = SP[h].x; sum[2][2 * h + 1] = SP[h].y;
+        sum[3][2 * h] = SV[h].x; sum[3][2 * h + 1] = SV[h].y;
+        dsum[0][2 * h] = SD[h].x; dsum[0][2 * h + 1] = SD[h].y;
+        dsum[1][2 * h] = SDT[h].x; dsum[1][2 * h + 1] = SDT[h].y;
+        dsum[2][2 * h] = SDP[h].x; dsum[2][2 * h + 1] = SDP[h].y;
     }
 }
 
@@ -264,21 +406,26 @@ struct SegW {
     float w[kJgMaxOut][4];
 };
 
+// dynamic shared memory of jg_linesum_kernel<*, NOUT>: the warps' tiles and their
+// per-point output accumulators
+constexpr size_t jg_smem_bytes(int nout) {
+    return sizeof(JgTile) * kJgWarps + sizeof(float) * kJgWarps * nout * kJgWarpPts;
+}
+
 template <bool ANY_LM, int NOUT>
-__global__ void __launch_bounds__(kJgWarps * 32) jg_linesum_kernel(
+__global__ void __launch_bounds__(kJgWarps * 32, 2) jg_linesum_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_n, const SegW* __restrict__ wts,
     const int2* __restrict__ pl_segs, JgOut g, long long n_nu, float cut_g, float* __restrict__ out) {
-    __shared__ JgTile tiles[kJgWarps];
+    extern __shared__ float4 jg_sh[];
+    JgTile* tiles = (JgTile*)jg_sh;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* acc = (float*)(tiles + kJgWarps) + (size_t)warp * NOUT * kJgWarpPts;  // [NOUT][128], warp-private
     const int pl = blockIdx.y;
     const long long wb = (long long)blockIdx.x * kJgStrip + (long long)warp * kJgWarpPts;
     if (wb >= n_nu) return;
-    constexpr int n_out = NOUT;
-    float acc[NOUT][kJgQ];
-#pragma unroll
     for (int o = 0; o < NOUT; ++o)
 #pragma unroll
-        for (int q = 0; q < kJgQ; ++q) acc[o][q] = 0.f;
+        for (int q = 0; q < kJgQ; ++q) acc[o * kJgWarpPts + 32 * q + lane] = 0.f;
     const int2 rng = pl_segs[pl];
     for (int si = rng.x; si < rng.x + rng.y; ++si) {
         const SegDev sg = segs[si];
@@ -290,6 +437,7 @@ __global__ void __launch_bounds__(kJgWarps * 32) jg_linesum_kernel(
         else
             jg_segment<false>(sg, nl, g, wb, cut_g, lane, tiles[warp], s, ds);
         // clamps (voigt.jl:276, line_mixing.jl:1368, cross_section_jacobian.jl:107-113, :312-319)
+        const SegW& W = wts[si];
 #pragma unroll
         for (int q = 0; q < kJgQ; ++q) {
             float v = s[0][q], vT = s[1][q], vp = s[2][q], vv = s[3][q];
@@ -300,19 +448,16 @@ __global__ void __launch_bounds__(kJgWarps * 32) jg_linesum_kernel(
                 vp += ds[2][q];
                 if (!(v > 0.f)) v = vT = vp = 0.f;
             }
-            const SegW& W = wts[si];
-#pragma unroll
             for (int o = 0; o < NOUT; ++o)
-                acc[o][q] += W.w[o][0] * v + W.w[o][1] * vT + W.w[o][2] * vp + W.w[o][3] * vv;
+                acc[o * kJgWarpPts + 32 * q + lane] += W.w[o][0] * v + W.w[o][1] * vT + W.w[o][2] * vp + W.w[o][3] * vv;
         }
     }
-    float* base = out + (size_t)pl * n_out * n_nu;
-#pragma unroll
+    float* base = out + (size_t)pl * NOUT * n_nu;
     for (int o = 0; o < NOUT; ++o)
 #pragma unroll
         for (int q = 0; q < kJgQ; ++q) {
             const long long i = wb + 32 * q + lane;
-            if (i < n_nu) base[(size_t)o * n_nu + i] = acc[o][q];
+            if (i < n_nu) base[(size_t)o * n_nu + i] = acc[o * kJgWarpPts + 32 * q + lane];
         }
 }
 

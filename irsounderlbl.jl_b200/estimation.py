@@ -513,3 +513,267 @@ def forward_model_rrule(prof, linelists, spec: StateVectorSpec, *, sounder=None,
 
     pullback(np.zeros(n_ch))
     return cache["y"], pullback
+
+
+# ------------------------------------------------------------------ a-priori and noise
+def _corr(kernel: str, r):
+    """sa_builder.jl:28-32"""
+    if kernel == "exponential":
+        return np.exp(-r)
+    if kernel == "matern32":
+        return (1.0 + np.sqrt(3.0) * r) * np.exp(-np.sqrt(3.0) * r)
+    if kernel == "matern52":
+        return (1.0 + np.sqrt(5.0) * r + 5.0 * r * r / 3.0) * np.exp(-np.sqrt(5.0) * r)
+    return np.exp(-0.5 * r * r)
+
+
+def _resolve_sigma(sig, n, name):
+    if np.isscalar(sig):
+        if not sig > 0:
+            raise IRSError(f"{name} must be positive")
+        return np.full(n, float(sig))
+    v = np.asarray(sig, dtype=np.float64)
+    if len(v) != n:
+        raise IRSError(f"{name} must be a scalar or length n_levels={n}; got {len(v)}")
+    if not np.all(v > 0):
+        raise IRSError(f"{name} entries must all be positive")
+    return v
+
+
+def build_sa(spec: StateVectorSpec, base_prof, sigma_T=2.0, L_T=1.0, sigma_vmr=0.5, L_vmr=1.0, sigma_col=0.2,
+             sigma_tsfc=2.0, sigma_emis=0.02, kernel="matern52", jitter=0.0) -> np.ndarray:
+    """build_sa (sa_builder.jl:101-153): block a-priori covariance correlated in log-pressure.
+    sigma_vmr / L_vmr / sigma_col may be dicts keyed by species."""
+    if kernel not in ("matern52", "matern32", "exponential", "sqexp"):
+        raise IRSError(f"kernel must be :matern52, :matern32, :exponential, or :sqexp; got :{kernel}")
+    p = np.asarray(base_prof.pressure, dtype=np.float64)
+    if len(p) != spec.n_levels:
+        raise IRSError(f"base_prof has {len(p)} levels, spec expects {spec.n_levels}")
+    if not np.all(p > 0):
+        raise IRSError("pressures must be positive for log-pressure correlation")
+    if jitter < 0:
+        raise IRSError("jitter must be ≥ 0")
+    logp = np.log(p)
+    dist = np.abs(logp[:, None] - logp[None, :])
+    Sa = np.zeros((spec.n, spec.n))
+
+    def per_species(v, s, what):
+        if isinstance(v, dict):
+            if s not in v:
+                raise IRSError(f"{what} has no entry for {SPECIES_NAME.get(s, s)}")
+            return v[s]
+        return v
+
+    if spec.include_temperature:
+        sg = _resolve_sigma(sigma_T, spec.n_levels, "σ_T")
+        r = spec.temp_range
+        Sa[r.start:r.stop, r.start:r.stop] = np.outer(sg, sg) * _corr(kernel, dist / float(L_T))
+    for b in spec.vmr_blocks:
+        sl = slice(b.range.start, b.range.stop)
+        if b.basis is None:
+            sg = _resolve_sigma(per_species(sigma_vmr, b.species, "σ_vmr"), spec.n_levels, "σ_vmr")
+            L = float(per_species(L_vmr, b.species, "L_vmr"))
+            if not L > 0:
+                raise IRSError("L_vmr must be positive")
+            Sa[sl, sl] = np.outer(sg, sg) * _corr(kernel, dist / L)
+        else:
+            sc = _resolve_sigma(per_species(sigma_col, b.species, "σ_col"), b.m, "σ_col")
+            Sa[sl, sl] = np.diag(sc ** 2)
+    if spec.include_tsfc:
+        Sa[spec.tsfc_index, spec.tsfc_index] = float(sigma_tsfc) ** 2
+    if spec.include_emissivity:
+        Sa[spec.emis_index, spec.emis_index] = float(sigma_emis) ** 2
+    if jitter > 0:
+        Sa[np.diag_indices(spec.n)] *= 1.0 + jitter
+    return Sa
+
+
+def _dB_dT(nu, T):
+    """planck.jl:67-71 (host copy for covariance set-up)."""
+    c1, c2 = 1.191042953e-5, 1.4387769
+    x = c2 * nu / T
+    ex = np.exp(x)
+    return c1 * c2 * nu ** 4 * ex / (T * T * (ex - 1.0) ** 2)
+
+
+def scene_nedt(nu, Tb_scene, nedt_280K=0.25, T_ref=280.0) -> np.ndarray:
+    """scene_nedt (covariance.jl:106-117): NEdT at the scene BT from the NEdT at T_ref."""
+    nu = np.asarray(nu, dtype=np.float64)
+    Tb = np.asarray(Tb_scene, dtype=np.float64)
+    if Tb.shape != nu.shape:
+        raise IRSError(f"Tb_scene must match length(ν)={len(nu)}; got {len(Tb)}")
+    n0 = np.broadcast_to(np.asarray(nedt_280K, dtype=np.float64), nu.shape)
+    return n0 * _dB_dT(nu, float(T_ref)) / _dB_dT(nu, Tb)
+
+
+def exclude_channels(nu, *ranges) -> np.ndarray:
+    """exclude_channels (optimal_estimation.jl): keep-mask dropping channels inside any (lo, hi)."""
+    nu = np.asarray(nu, dtype=np.float64)
+    keep = np.ones(len(nu), bool)
+    for lo, hi in ranges:
+        keep &= ~((nu >= lo) & (nu <= hi))
+    return keep
+
+
+# ------------------------------------------------------------------ optimal estimation
+@dataclass
+class RetrievalResult:
+    """RetrievalResult (optimal_estimation.jl:53-72)."""
+    x: np.ndarray
+    spec: StateVectorSpec
+    converged: bool
+    n_iter: int
+    cost: float
+    S_hat: np.ndarray
+    A: np.ndarray
+    G: Optional[np.ndarray]
+    K: Optional[np.ndarray]
+    dof: float
+    dfn: float
+    H: float
+    S_noise: Optional[np.ndarray]
+    S_smoothing: np.ndarray
+    chi2: float
+    y_fit: np.ndarray
+    nu: np.ndarray
+    channel_mask: np.ndarray
+
+
+def _se_inverse(Se, n_ch, keep):
+    Se = np.asarray(Se, dtype=np.float64)
+    if Se.ndim == 2:
+        if Se.shape != (n_ch, n_ch):
+            raise IRSError(f"Se must be n_y×n_y with n_y = {n_ch}")
+        if np.any(Se - np.diag(np.diag(Se))):
+            raise IRSError("a dense Se is not supported on this path: pass its diagonal")
+        Se = np.diag(Se)
+    if Se.shape != (n_ch,):
+        raise IRSError(f"Se must have {n_ch} variances")
+    if np.any(Se[keep] <= 0):
+        raise IRSError("Se variances must be positive")
+    w = np.zeros(n_ch)
+    w[keep] = 1.0 / Se[keep]
+    return w, Se
+
+
+def optimal_estimation_batch(ys, spec: StateVectorSpec, base_profs, linelists, *, xa, Sa, Se, x0=None,
+                             channel_mask=None, method="levenberg_marquardt", max_iter=15, max_linesearch=8,
+                             gamma0=1.0, gamma_factor=3.0, gamma_min=1e-4, conv_factor=1e-1, observable="bt",
+                             eps_fixed=1.0, fm_kwargs=None, sounder=None, geoms=None, backend=None,
+                             line_mixing=None):
+    """optimal_estimation (optimal_estimation.jl:142-291) for a batch of scenes on the GPU.
+
+    ys [n_scene, n_ch]; xa [n_scene, n] (or [n]); Sa [n, n] shared; Se per scene:
+    [n_scene, n_ch] variances (or one [n_ch] vector).  Returns dict(x, y_fit, M, n_iter,
+    converged, cost, nu)."""
+    from . import (IASIInstrument, _prepare, _ProfileBatch, default_context, fm_options, nadir_geometry,
+                   sounder_grid)
+    if method not in ("levenberg_marquardt", "gauss_newton"):
+        raise IRSError(f"method must be :levenberg_marquardt or :gauss_newton, got :{method}")
+    _check_observable(observable)
+    if any(b.basis is not None for b in spec.vmr_blocks):
+        raise IRSError("reduced VMR blocks are not supported by the batched retrieval")
+    ctx = backend or default_context()
+    sounder = sounder or IASIInstrument()
+    nu = sounder_grid(sounder)
+    n_ch, n = len(nu), spec.n
+    ys = np.ascontiguousarray(np.atleast_2d(ys), dtype=np.float64)
+    S = len(ys)
+    if ys.shape[1] != n_ch:
+        raise IRSError(f"y has {ys.shape[1]} channels, the sounder {n_ch}")
+    xa = np.ascontiguousarray(np.broadcast_to(np.asarray(xa, dtype=np.float64), (S, n)))
+    x0 = xa.copy() if x0 is None else np.ascontiguousarray(np.broadcast_to(np.asarray(x0, np.float64), (S, n)))
+    Sa = np.asarray(Sa, dtype=np.float64)
+    if Sa.shape != (n, n):
+        raise IRSError(f"Sa must be {n}×{n}")
+    keep = np.ones(n_ch, bool) if channel_mask is None else np.asarray(channel_mask, bool)
+    if len(keep) != n_ch:
+        raise IRSError(f"channel_mask length {len(keep)} ≠ length(y) {n_ch}")
+    if not keep.any():
+        raise IRSError("channel_mask excludes every channel")
+    Se = np.asarray(Se, dtype=np.float64)
+    Se_rows = np.broadcast_to(Se, (S, n_ch)) if Se.ndim == 1 or (Se.ndim == 2 and Se.shape == (S, n_ch)) else None
+    if Se_rows is None:
+        raise IRSError("Se must be [n_ch] or [n_scene, n_ch] variances")
+    w = np.ascontiguousarray(np.stack([_se_inverse(Se_rows[k], n_ch, keep)[0] for k in range(S)]))
+    Sa_inv = np.ascontiguousarray(np.linalg.inv(Sa))
+    base_profs = list(base_profs) if isinstance(base_profs, (list, tuple)) else [base_profs] * S
+    geoms = geoms or [nadir_geometry()] * S
+    kw = dict(fm_kwargs or {})
+    kw.pop("dptmn", None)
+    prec = kw.pop("precision", "mixed")
+    _prepare(ctx, linelists, line_mixing)
+    o = fm_options(line_mixing=line_mixing, dptmn=0.0, precision=prec, **kw)
+    batch = _ProfileBatch(base_profs, [None] * S, [g.mu for g in geoms], [eps_fixed] * S)
+    cs, keep_ref = _c_spec(spec, spec.log_vmr, True, observable)
+    prm = _lib.OEParams()
+    prm.max_iter, prm.max_linesearch = int(max_iter), int(max_linesearch)
+    prm.method = 0 if method == "levenberg_marquardt" else 1
+    prm.gamma0, prm.gamma_factor, prm.gamma_min = float(gamma0), float(gamma_factor), float(gamma_min)
+    prm.conv_factor, prm.eps_fixed = float(conv_factor), float(eps_fixed)
+    s = sounder.c_struct()
+    x = np.empty((S, n))
+    y_fit = np.empty((S, n_ch))
+    M = np.empty((S, n, n))
+    n_iter = np.empty(S, np.int32)
+    conv = np.empty(S, np.int32)
+    cost = np.empty(S)
+    I32 = C.POINTER(C.c_int32)
+    check(ctx.lib.irs_oe_batch(ctx.h, batch.arr, S, C.byref(s), C.byref(o), C.byref(cs), dptr(ys), dptr(w), dptr(xa),
+                               dptr(Sa_inv), dptr(x0), C.byref(prm), dptr(x), dptr(y_fit), dptr(M),
+                               n_iter.ctypes.data_as(I32), conv.ctypes.data_as(I32), dptr(cost)))
+    return dict(x=x, y_fit=y_fit, M=M, n_iter=n_iter, converged=conv.astype(bool), cost=cost, nu=nu, w=w,
+                Sa_inv=Sa_inv, keep=keep)
+
+
+def oe_diagnostics(M, Sa, Sa_inv=None):
+    """Rodgers diagnostics from M = K^T Se^-1 K (optimal_estimation.jl:257-282):
+    (S_hat, A, dof, H, S_smoothing)."""
+    Sa_inv = np.linalg.inv(Sa) if Sa_inv is None else Sa_inv
+    S_hat = np.linalg.inv(Sa_inv + M)
+    A = S_hat @ M
+    dof = float(np.trace(A))
+    n = len(A)
+    _, ld = np.linalg.slogdet(np.eye(n) - A)
+    H = -0.5 * ld / np.log(2.0)
+    ImA = np.eye(n) - A
+    return S_hat, A, dof, float(H), ImA @ Sa @ ImA.T
+
+
+def optimal_estimation(y, spec: StateVectorSpec, base_prof, linelists, *, xa, Sa, Se, channel_mask=None, x0=None,
+                       method="levenberg_marquardt", max_iter=15, max_linesearch=8, gamma0=1.0, gamma_factor=3.0,
+                       gamma_min=1e-4, conv_factor=1e-1, observable="bt", eps_fixed=1.0, fm_kwargs=None,
+                       sounder=None, geom=None, backend=None, line_mixing=None, verbose=False) -> RetrievalResult:
+    """optimal_estimation (optimal_estimation.jl:142-291) -> RetrievalResult, one scene."""
+    from . import nadir_geometry
+    r = optimal_estimation_batch(np.atleast_2d(y), spec, [base_prof], linelists, xa=np.asarray(xa)[None],
+                                 Sa=Sa, Se=np.diag(Se) if np.ndim(Se) == 2 else Se, x0=None if x0 is None else
+                                 np.asarray(x0)[None], channel_mask=channel_mask, method=method, max_iter=max_iter,
+                                 max_linesearch=max_linesearch, gamma0=gamma0, gamma_factor=gamma_factor,
+                                 gamma_min=gamma_min, conv_factor=conv_factor, observable=observable,
+                                 eps_fixed=eps_fixed, fm_kwargs=fm_kwargs, sounder=sounder,
+                                 geoms=[geom or nadir_geometry()], backend=backend, line_mixing=line_mixing)
+    x = r["x"][0]
+    M = r["M"][0]
+    keep = r["keep"]
+    S_hat, A, dof, H, S_smooth = oe_diagnostics(M, np.asarray(Sa, np.float64), r["Sa_inv"])
+    # K at the solution (full channel grid) for the gain matrix and the noise budget
+    prof, Ts, es = unpack_state(spec, x, base_prof)
+    kw = dict(fm_kwargs or {})
+    kw.pop("dptmn", None)
+    kw.pop("precision", None)
+    jac = analytic_jacobian(prof, linelists, spec, sounder=sounder, geom=geom, T_sfc=Ts,
+                            eps_sfc=es if spec.include_emissivity else eps_fixed, observable=observable,
+                            backend=backend, line_mixing=line_mixing, **kw)
+    wk = r["w"][0][keep]
+    Kk = jac.K[keep]
+    G = S_hat @ (Kk * wk[:, None]).T
+    se_k = 1.0 / wk
+    S_noise = (G * se_k[None, :]) @ G.T
+    resid = (np.atleast_2d(y)[0] - r["y_fit"][0])[keep]
+    chi2 = float(np.sum(resid * wk * resid))
+    m = int(keep.sum())
+    return RetrievalResult(x=x, spec=spec, converged=bool(r["converged"][0]), n_iter=int(r["n_iter"][0]),
+                           cost=float(r["cost"][0]), S_hat=S_hat, A=A, G=G, K=jac.K, dof=dof, dfn=m - dof, H=H,
+                           S_noise=S_noise, S_smoothing=S_smooth, chi2=chi2, y_fit=r["y_fit"][0], nu=r["nu"],
+                           channel_mask=keep)

@@ -1,0 +1,190 @@
+"""MLP surrogate of forward_model: profile + scan angle -> channel brightness temperatures.
+
+No counterpart in the reference.  The network (n_in -> n_layers x n_hidden GELU ->
+n_out) runs on the tcgen05 tensor cores through ``libirs_b200.so`` (BF16 weights and
+activations, FP32 accumulation, FP32 master weights and Adam); it is trained only on
+spectra of the GPU line-by-line path, which is also its fallback for inputs whose
+out-of-distribution score exceeds the threshold and the judge of its error on a
+held-out share of every batch.
+
+Input features (152 for 50 levels): T [n_lev], log VMR H2O [n_lev], log VMR O3
+[n_lev], T_sfc, scan angle (degrees).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import IRSError, check, dptr, fptr
+
+VMR_FLOOR = 1e-30
+
+
+def surrogate_features(profiles, scan_angles, T_sfcs=None) -> np.ndarray:
+    """[n, 3 n_lev + 2] float32 features of the profiles (T, log H2O, log O3, T_sfc, angle)."""
+    n = len(profiles)
+    T_sfcs = T_sfcs if T_sfcs is not None else [None] * n
+    rows = []
+    for p, a, ts in zip(profiles, scan_angles, T_sfcs):
+        T = np.asarray(p.temperature, dtype=np.float64)
+        h = np.log(np.maximum(np.asarray(p.vmr[1], dtype=np.float64), VMR_FLOOR))
+        o = np.log(np.maximum(np.asarray(p.vmr[3], dtype=np.float64), VMR_FLOOR))
+        rows.append(np.concatenate([T, h, o, [T[0] if ts is None else ts, float(a)]]))
+    return np.ascontiguousarray(np.array(rows, dtype=np.float32))
+
+
+class Surrogate:
+    """One MLP on one GPU context (irs_surrogate_* of the C ABI)."""
+
+    def __init__(self, ctx=None, n_in: int = 152, n_hidden: int = 1024, n_layers: int = 4, n_out: int = 8461,
+                 seed: int = 1003):
+        from . import default_context
+        self.ctx = ctx or default_context()
+        self.lib = self.ctx.lib
+        self.n_in, self.n_hidden, self.n_layers, self.n_out = n_in, n_hidden, n_layers, n_out
+        h = C.c_void_p()
+        check(self.lib.irs_surrogate_create(self.ctx.h, n_in, n_hidden, n_layers, n_out, seed, C.byref(h)))
+        self.h = h
+        self.ood_threshold = np.inf
+        self.x_mean = np.zeros(n_in, np.float32)
+        self.x_sd = np.ones(n_in, np.float32)
+        self.y_mean = np.zeros(n_out, np.float32)
+        self.y_sd = np.ones(n_out, np.float32)
+
+    # -------------------------------------------------------------- parameters
+    def param_count(self) -> int:
+        n = C.c_int64()
+        check(self.lib.irs_surrogate_param_count(self.h, C.byref(n)))
+        return n.value
+
+    def get_params(self) -> np.ndarray:
+        p = np.empty(self.param_count(), np.float32)
+        check(self.lib.irs_surrogate_get_params(self.h, fptr(p)))
+        return p
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.shape != (self.param_count(),):
+            raise IRSError(f"parameter vector has shape {p.shape}, expected ({self.param_count()},)")
+        check(self.lib.irs_surrogate_set_params(self.h, fptr(p)))
+
+    def layer_shapes(self):
+        dims = [self.n_in] + [self.n_hidden] * self.n_layers + [self.n_out]
+        return [(dims[l + 1], dims[l]) for l in range(len(dims) - 1)]
+
+    def unflatten(self, p: np.ndarray):
+        """[(W, b)] per layer from the flat parameter vector."""
+        out, k = [], 0
+        for o, i in self.layer_shapes():
+            W = p[k:k + o * i].reshape(o, i)
+            k += o * i
+            b = p[k:k + o]
+            k += o
+            out.append((W, b))
+        return out
+
+    # -------------------------------------------------------------- scaling / OOD
+    def fit_scaling(self, X: np.ndarray, Y: np.ndarray, ood_quantile: float = 0.999, ood_margin: float = 2.0):
+        """Input/output standardisation, the whitening matrix of the scaled inputs and
+        the OOD threshold (ood_margin x the ood_quantile of the training scores)."""
+        X = np.asarray(X, dtype=np.float64)
+        Y = np.asarray(Y, dtype=np.float64)
+        self.x_mean = X.mean(0).astype(np.float32)
+        self.x_sd = np.maximum(X.std(0), 1e-6 * np.maximum(np.abs(X).max(0), 1.0)).astype(np.float32)
+        self.y_mean = Y.mean(0).astype(np.float32)
+        self.y_sd = np.maximum(Y.std(0), 1e-3).astype(np.float32)
+        check(self.lib.irs_surrogate_set_scaling(self.h, fptr(self.x_mean), fptr(self.x_sd), fptr(self.y_mean),
+                                                 fptr(self.y_sd)))
+        Z = (X - self.x_mean) / self.x_sd
+        cov = np.cov(Z, rowvar=False) + 1e-9 * np.eye(self.n_in)
+        w, V = np.linalg.eigh(cov)
+        w = np.maximum(w, 1e-4 * w.max())
+        W = np.ascontiguousarray((V / np.sqrt(w)) @ V.T, dtype=np.float32)
+        check(self.lib.irs_surrogate_set_whitening(self.h, fptr(W)))
+        _, s = self.predict(X.astype(np.float32))
+        self.ood_threshold = float(ood_margin * np.quantile(s, ood_quantile))
+        return self.ood_threshold
+
+    # -------------------------------------------------------------- training
+    def train(self, X: np.ndarray, Y: np.ndarray, epochs: int = 10, batch: int = 256, lr: float = 1e-3,
+              seed: int = 1003) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        self._check(X, Y)
+        losses = np.zeros(epochs)
+        check(self.lib.irs_surrogate_train(self.h, fptr(X), fptr(Y), len(X), batch, epochs, lr, seed, dptr(losses)))
+        return losses
+
+    def gradients(self, X: np.ndarray, Y: np.ndarray):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        self._check(X, Y)
+        g = np.empty(self.param_count(), np.float32)
+        loss = C.c_double()
+        check(self.lib.irs_surrogate_gradients(self.h, fptr(X), fptr(Y), len(X), fptr(g), C.byref(loss)))
+        return g, loss.value
+
+    def _check(self, X, Y=None):
+        if X.ndim != 2 or X.shape[1] != self.n_in:
+            raise IRSError(f"inputs have shape {X.shape}, expected (n, {self.n_in})")
+        if Y is not None and (Y.shape != (len(X), self.n_out)):
+            raise IRSError(f"targets have shape {Y.shape}, expected ({len(X)}, {self.n_out})")
+
+    # -------------------------------------------------------------- inference
+    def predict(self, X: np.ndarray):
+        """(BT [n, n_out] float32, OOD score [n])."""
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        self._check(X)
+        out = np.empty((len(X), self.n_out), np.float32)
+        ood = np.empty(len(X), np.float32)
+        check(self.lib.irs_surrogate_infer(self.h, fptr(X), len(X), fptr(out), fptr(ood)))
+        return out, ood
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.irs_surrogate_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def surrogate_forward_batch(sur: Surrogate, profiles: Sequence, scan_angles, linelists, *, sounder=None,
+                            T_sfcs=None, holdout: float = 0.01, seed: int = 0, backend=None, **lbl_kw):
+    """Brightness temperatures of a batch from the surrogate, with the line-by-line path
+    as fallback for OOD inputs and as judge on a held-out share.
+
+    Returns dict(BT [n, n_ch], lbl_mask [n] (rows computed by LBL), ood [n],
+    holdout_index, holdout_rms, holdout_max)."""
+    from . import ViewingGeometry, forward_model_batch, scan_angle_to_local_zenith
+    X = surrogate_features(profiles, scan_angles, T_sfcs)
+    BT, ood = sur.predict(X)
+    BT = BT.astype(np.float64)
+    n = len(profiles)
+    fall = ood > sur.ood_threshold
+    rng = np.random.Generator(np.random.PCG64(seed))
+    n_hold = int(np.ceil(holdout * n)) if holdout > 0 else 0
+    cand = np.flatnonzero(~fall)
+    hold = rng.choice(cand, size=min(n_hold, len(cand)), replace=False) if n_hold else np.zeros(0, int)
+    need = np.union1d(np.flatnonzero(fall), hold).astype(int)
+    res = dict(ood=ood, lbl_mask=fall, holdout_index=hold, holdout_rms=None, holdout_max=None)
+    if len(need):
+        geoms = [ViewingGeometry(scan_angle_to_local_zenith(float(scan_angles[i]))) for i in need]
+        T_need = [None if T_sfcs is None else T_sfcs[i] for i in need]
+        _, _, BT_lbl = forward_model_batch([profiles[i] for i in need], linelists, sounder=sounder, geoms=geoms,
+                                           T_sfcs=T_need, backend=backend, **lbl_kw)
+        pos = {int(i): k for k, i in enumerate(need)}
+        if len(hold):
+            d = np.stack([BT[i] - BT_lbl[pos[int(i)]] for i in hold])
+            res["holdout_rms"] = float(np.sqrt(np.mean(d ** 2)))
+            res["holdout_max"] = float(np.max(np.abs(d)))
+        for i in np.flatnonzero(fall):
+            BT[i] = BT_lbl[pos[int(i)]]
+    res["BT"] = BT
+    return res

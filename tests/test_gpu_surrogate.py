@@ -1,0 +1,139 @@
+"""The tensor-core GEMM and the MLP surrogate (irs_gemm_bf16, irs_surrogate_*).
+
+* GEMM: BF16 inputs, FP32 accumulation, against numpy FP32 products of the same
+  BF16 values (relative 1e-4 of the output scale: only the summation order differs).
+* Gradients: against the numpy oracle of the same network (oracle/mlp_oracle.py) with
+  the GPU's BF16 roundings replayed (relative Frobenius error 1e-2 per parameter block:
+  FP32 vs FP64 sums can move a BF16 rounding by one unit).
+* Training and OOD on a smooth synthetic map, then the surrogate trained on spectra of
+  the GPU line-by-line path: its held-out error against LBL, what it gains over the
+  climatological mean (the estimate without it), and the LBL fallback for OOD inputs.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_package
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pkg():
+    return load_package()
+
+
+@pytest.fixture(scope="module")
+def ctx(pkg):
+    c = pkg.B200Context()
+    yield c
+    c.close()
+
+
+def to_bf16_bits(x):
+    a = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    return (((a + 0x7FFF + ((a >> 16) & 1)) >> 16)).astype(np.uint16)
+
+
+def from_bf16_bits(b):
+    return (b.astype(np.uint32) << 16).view(np.float32)
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 256, 64), (300, 520, 200), (1, 7, 5), (1024, 1024, 1024),
+                                   (512, 8461, 1024), (8461, 192, 256)])
+def test_gemm_bf16(pkg, ctx, M, N, K):
+    import ctypes as C
+    rng = np.random.default_rng(M + N + K)
+    A = to_bf16_bits(rng.standard_normal((M, K)))
+    B = to_bf16_bits(rng.standard_normal((N, K)))
+    out = np.empty((M, N), np.float32)
+    pkg._lib.check(ctx.lib.irs_gemm_bf16(ctx.h, A.ctypes.data_as(C.c_void_p), B.ctypes.data_as(C.c_void_p), M, N, K,
+                                         pkg._lib.fptr(out)))
+    ref = from_bf16_bits(A).astype(np.float64) @ from_bf16_bits(B).astype(np.float64).T
+    assert np.max(np.abs(out - ref)) <= 1e-4 * max(1.0, np.sqrt(K)) + 1e-5 * np.max(np.abs(ref))
+
+
+def test_surrogate_gradients_vs_oracle(pkg, ctx):
+    import mlp_oracle as mo
+    n_in, hid, nl, n_out = 152, 64, 2, 100
+    s = pkg.Surrogate(ctx, n_in=n_in, n_hidden=hid, n_layers=nl, n_out=n_out, seed=11)
+    rng = np.random.default_rng(3)
+    X = rng.normal(0, 1, (96, n_in)).astype(np.float32)
+    Y = rng.normal(0, 1, (96, n_out)).astype(np.float32)
+    p = s.get_params()
+    p = p + rng.normal(0, 0.05, p.shape).astype(np.float32)  # non-zero biases too
+    s.set_params(p)
+    assert np.array_equal(s.get_params(), p)
+    g, loss = s.gradients(X, Y)
+    dims = [n_in] + [hid] * nl + [n_out]
+    z = np.zeros
+    lo, go, _ = mo.forward_backward(p, dims, X, Y, z(n_in), np.ones(n_in), z(n_out), np.ones(n_out), bf16=True)
+    assert abs(loss - lo) <= 1e-3 * lo
+    k = 0
+    for o, i in [(dims[l + 1], dims[l]) for l in range(len(dims) - 1)]:
+        for size in (o * i, o):
+            a, b = g[k:k + size].astype(np.float64), go[k:k + size]
+            assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(b), (k, size)
+            k += size
+    s.close()
+
+
+def test_training_and_ood(pkg, ctx):
+    rng = np.random.default_rng(5)
+    n_in, n_out = 152, 300
+    A = rng.normal(0, 1 / np.sqrt(8), (8, 16))
+    Bm = rng.normal(0, 1, (16, n_out))
+
+    def f(X):  # a smooth map of 8 of the inputs
+        return (np.tanh(X[:, :8] @ A) @ Bm * 3.0 + 250.0).astype(np.float32)
+
+    X = rng.normal(0, 1, (4096, n_in)).astype(np.float32)
+    Y = f(X)
+    s = pkg.Surrogate(ctx, n_in=n_in, n_hidden=256, n_layers=3, n_out=n_out, seed=1)
+    thr = s.fit_scaling(X, Y)
+    losses = s.train(X, Y, epochs=120, batch=256, lr=2e-3, seed=2)
+    assert losses[-1] < 0.1 * losses[0]
+    Xt = rng.normal(0, 1, (512, n_in)).astype(np.float32)
+    P, ood = s.predict(Xt)
+    rms = np.sqrt(np.mean((P - f(Xt)) ** 2))
+    assert rms < 0.25 * np.std(f(Xt))
+    assert np.mean(ood > thr) < 0.01
+    Xo = Xt[:16] + 12.0
+    _, ood_o = s.predict(Xo)
+    assert np.all(ood_o > thr)
+    s.close()
+
+
+def test_surrogate_on_lbl_spectra(pkg, ctx):
+    """Trained only on spectra of the GPU LBL path (5,000-line CO2 list + MT-CKD
+    continua, 221 channels); judged by LBL on held-out profiles."""
+    lists = pkg.synthetic.lists_5k_co2()
+    snd = pkg.Sounder.make(645.0, 700.0, 0.25, opd_max=2.0, fwhm_gauss=0.5)
+    kw = dict(precision="mixed", internal_dnu=0.0025, apply_continuum=True, continua=("h2o", "co2"))
+
+    def lbl(profs, ang):
+        geoms = [pkg.ViewingGeometry(pkg.scan_angle_to_local_zenith(a)) for a in ang]
+        return pkg.forward_model_batch(profs, lists, sounder=snd, geoms=geoms, backend=ctx, **kw)[2]
+
+    profs, ang = pkg.synthetic.perturbed_profiles(1024 + 128, seed=2024)
+    BT = lbl(profs, ang)
+    X = pkg.surrogate_features(profs, ang)
+    tr, te = slice(0, 1024), slice(1024, None)
+    s = pkg.Surrogate(ctx, n_in=X.shape[1], n_hidden=512, n_layers=3, n_out=BT.shape[1], seed=3)
+    s.fit_scaling(X[tr], BT[tr])
+    losses = s.train(X[tr], BT[tr].astype(np.float32), epochs=150, batch=128, lr=1e-3, seed=4)
+    assert losses[-1] < 0.02 * losses[0]
+    P, ood = s.predict(X[te])
+    rms = float(np.sqrt(np.mean((P - BT[te]) ** 2)))
+    clim = float(np.sqrt(np.mean((BT[tr].mean(0) - BT[te]) ** 2)))  # the estimate without the network
+    print(f"surrogate held-out BT RMS {rms:.3f} K vs climatology {clim:.3f} K")
+    assert rms < 0.2 * clim
+    # OOD fallback: a profile 40 K warmer is computed by LBL, exactly
+    hot = pkg.AtmosphericProfile(profs[1030].pressure, profs[1030].temperature + 40.0, profs[1030].altitude,
+                                 profs[1030].vmr)
+    batch = [profs[1024], hot, profs[1025]]
+    res = pkg.surrogate_forward_batch(s, batch, [ang[1024], 10.0, ang[1025]], lists, sounder=snd, holdout=0.5,
+                                      seed=1, backend=ctx, **kw)
+    assert res["lbl_mask"].tolist() == [False, True, False]
+    assert np.array_equal(res["BT"][1], lbl([hot], [10.0])[0])
+    assert res["holdout_rms"] is not None and res["holdout_rms"] < 0.2 * clim
+    s.close()
