@@ -30,6 +30,8 @@ import sys
 import time
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parent
 N_PROF = 6
 FAR_PAIR_FLOPS = 10     # d (2), d^2, d^2+b^2, rcp, pedestal FMA (2), value FMA (2), accumulate
@@ -182,6 +184,108 @@ def reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def bench_extras(pkg, ctx, lists, snd, torch, stream):
+    """Surrogate inference, analytic Jacobian and batched optimal estimation, each on a
+    bounded workload of its configuration (stated in its `config`)."""
+    out = {}
+    peaks, src = _peaks()
+    # ---- MLP surrogate: 152 -> 4 x 1024 GELU -> 8461, batches of 4096, BF16 tcgen05
+    n_in, n_hid, n_lay, n_out, B = 152, 1024, 4, 8461, 4096
+    sur = pkg.Surrogate(ctx, n_in=n_in, n_hidden=n_hid, n_layers=n_lay, n_out=n_out, seed=1003)
+    X = torch.randn((B, n_in), device="cuda", dtype=torch.float32)
+    Y = torch.empty((B, n_out), device="cuda", dtype=torch.float32)
+    ood = torch.empty((B,), device="cuda", dtype=torch.float32)
+
+    def infer():
+        pkg.check(ctx.lib.irs_surrogate_infer_device(sur.h, C.c_void_p(X.data_ptr()), B, C.c_void_p(Y.data_ptr()),
+                                                     C.c_void_p(ood.data_ptr()), C.c_void_p(stream.cuda_stream)))
+
+    for _ in range(3):
+        infer()
+    torch.cuda.synchronize()
+    reps = 20
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        infer()
+    b.record(stream)
+    torch.cuda.synchronize()
+    t = a.elapsed_time(b) / reps / 1e3
+    flop = 2.0 * B * (n_in * n_hid + (n_lay - 1) * n_hid * n_hid + n_hid * n_out)
+    Xh = np.random.default_rng(0).standard_normal((B, n_in)).astype(np.float32)
+    sur.predict(Xh)
+    t0 = time.perf_counter()
+    for _ in range(5):
+        sur.predict(Xh)
+    te = (time.perf_counter() - t0) / 5
+    out["surrogate"] = {
+        "metric": "IASI spectra/s (MLP surrogate inference, batches of 4096)", "value": B / t, "unit": "spectra/s",
+        "ms_per_batch": t * 1e3, "dtype": "bf16 weights/activations, fp32 accumulation (tcgen05)",
+        "config": {"workload": "mlp-152-4x1024-8461", "batch": B, "weights": "seeded random (throughput only)"},
+        "roofline": {"bound": "tensor", "achieved": flop / t / 1e12, "peak": peaks["bf16_tflops"],
+                     "unit": "TFLOP/s", "frac": flop / t / 1e12 / peaks["bf16_tflops"],
+                     "peak_source": f"{src} bf16_tflops", "flop_per_batch": flop},
+        "e2e": {"value": B / te, "unit": "spectra/s", "h2d_bytes_per_step": Xh.nbytes,
+                "d2h_bytes_per_step": B * n_out * 4 + B * 4},
+    }
+    sur.close()
+    # ---- analytic Jacobian: 400k lines + VP_Y on CO2, state T + log H2O + log O3 + T_sfc
+    profs, ang = pkg.synthetic.perturbed_profiles(4, seed=1002)
+    geoms = [pkg.ViewingGeometry(pkg.scan_angle_to_local_zenith(x)) for x in ang]
+    lm = pkg.VPYLineMixing(pkg.synthetic.vpy_y0(len(lists[2])))
+    spec = pkg.StateVectorSpec(50, [pkg.H2O, pkg.O3], include_emissivity=False)
+    kw = _workload_kw()
+    kw.pop("dptmn")
+    pkg.analytic_jacobian_batch(profs[:1], lists, spec, sounder=snd, geoms=geoms[:1], backend=ctx,
+                                line_mixing=lm, **kw)
+    t0 = time.perf_counter()
+    pkg.analytic_jacobian_batch(profs, lists, spec, sounder=snd, geoms=geoms, backend=ctx, line_mixing=lm, **kw)
+    tj = time.perf_counter() - t0
+    out["jacobian"] = {
+        "metric": "IASI Jacobians/s (analytic, state T + log H2O + log O3 + T_sfc = 151, with VP_Y)",
+        "value": len(profs) / tj, "unit": "jacobians/s", "timing": "host wall clock around the C-ABI call, "
+        "host buffers (K is 8461 x 151 FP64 per profile)",
+        "config": {"workload": "iasi-400k-lm", "profiles": len(profs), "n_state": spec.n, "channels": 8461}}
+    # ---- batched optimal estimation: 5,000-line CO2 list, state T + log H2O + T_sfc = 101
+    l5 = pkg.synthetic.lists_5k_co2()
+    s5 = pkg.Sounder.make(645.0, 700.0, 0.25, opd_max=2.0, fwhm_gauss=0.5)
+    kw5 = dict(internal_dnu=0.0025, apply_continuum=True, continua=("h2o", "co2"))
+    n_sc = 64
+    truth, _ = pkg.synthetic.perturbed_profiles(n_sc, seed=1004)
+    base = pkg.afgl_atmosphere("us_standard")
+    spec5 = pkg.StateVectorSpec(50, [pkg.H2O], include_emissivity=False)
+    xa = pkg.pack_state(spec5, base)
+    L3 = 3.0 * float(np.median(np.abs(np.diff(np.log(base.pressure)))))  # 3-level correlation in ln p
+    Sa = pkg.build_sa(spec5, base, sigma_T=0.5, L_T=L3, sigma_vmr=0.3, L_vmr=L3)
+    scenes = [pkg.AtmosphericProfile(base.pressure, p.temperature, base.altitude, {**base.vmr, 1: p.vmr[1]})
+              for p in truth]  # on the US-standard pressure grid
+    nu5, _, bt5 = pkg.forward_model_batch(scenes, l5, sounder=s5, backend=ctx, dptmn=0.0, **kw5)
+    rng = np.random.default_rng(1004)
+    se = np.stack([pkg.scene_nedt(nu5, b, nedt_280K=0.2) ** 2 for b in bt5])
+    y = bt5 + np.sqrt(se) * rng.standard_normal(bt5.shape)
+    t0 = time.perf_counter()
+    r = pkg.optimal_estimation_batch(y, spec5, [base] * n_sc, l5, xa=xa, Sa=Sa, Se=se, sounder=s5, backend=ctx,
+                                     fm_kwargs=kw5)
+    to = time.perf_counter() - t0
+    out["optimal_estimation"] = {
+        "metric": "retrieved scenes/s (batched LM optimal estimation, GPU forward + Jacobian + FP64 Cholesky)",
+        "value": n_sc / to, "unit": "scenes/s", "converged": int(r["converged"].sum()), "scenes": n_sc,
+        "iterations": {"mean": float(r["n_iter"].mean()), "max": int(r["n_iter"].max()),
+                       "min": int(r["n_iter"].min())},
+        "config": {"workload": "oe-5k-co2", "lines": 5000, "channels": len(nu5), "n_state": spec5.n,
+                   "prior": "build_sa matern52, sigma_T 0.5 K, sigma_logH2O 0.3, L = 3 x median |d ln p|",
+                   "noise": "diagonal Se from scene_nedt(0.2 K at 280 K)", "first_guess": "a priori (US standard)",
+                   "scenes": "perturbed-AFGL sampler (seed 1004) on the US-standard pressure grid"}}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -190,6 +294,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the surrogate, Jacobian and optimal-estimation measurements")
     ap.add_argument("--profile-case", action="store_true",
                     help="run a small case of the line-sum kernels for ncu: the 400k-line list, one "
                          "profile, 645-1000 cm^-1, mixed then plain FP64, twice each")
@@ -355,6 +461,11 @@ def main():
                "sample": f"FP64 oracle, one AFGL profile, channels {c0}..{c0 + n_ch - 1} ({n_pts} of "
                          f"{n_full} internal grid points), scaled by grid points"}
 
+    extras = {}
+    if world == 1 and not args.no_extras:
+        extras = bench_extras(pkg, ctx, lists, snd, torch, stream)
+        pkg._prepare(ctx, lists, None)
+
     # consistency check of this run: mixed vs FP64 BT on the last batch
     step_device(om)
     torch.cuda.synchronize()
@@ -392,6 +503,7 @@ def main():
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": clocks,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:

@@ -392,4 +392,4 @@ from .estimation import (ColumnScale, FullProfile, Jacobian, PartialColumns, Sta
                          finite_difference_jacobian, forward_model_rrule, pack_state, partial_column_basis,
                          state_labels, unpack_state, vmr_range, build_sa, scene_nedt, exclude_channels,
                          RetrievalResult, optimal_estimation, optimal_estimation_batch, oe_diagnostics)
-from .surrogate import Surrogate, surrogate_features, surrogate_forward_batch  # noqa: E402,F401
+from .surrogate import Surrogate, surrogate_features, surrogate_first_guess, surrogate_forward_batch  # noqa: E402,F401,E501

@@ -188,3 +188,51 @@ def surrogate_forward_batch(sur: Surrogate, profiles: Sequence, scan_angles, lin
             BT[i] = BT_lbl[pos[int(i)]]
     res["BT"] = BT
     return res
+
+
+def surrogate_first_guess(sur: Surrogate, ys, spec, base_profs, scan_angles, *, xa, Sa, Se, n_iter: int = 4,
+                          step: float = 1e-2):
+    """First guesses of a batched retrieval from the surrogate: Gauss-Newton MAP steps
+    (Rodgers 2000, eq. 5.9) with F and K both from the network (K by central
+    differences of batched inferences, 2 n_state + 1 samples per scene).  The state is
+    the full-profile [T][log VMR H2O / O3][T_sfc] layout of StateVectorSpec.
+
+    Returns x0 [n_scene, n_state]."""
+    from .estimation import unpack_state
+    ys = np.atleast_2d(np.asarray(ys, dtype=np.float64))
+    S, n = len(ys), spec.n
+    xa = np.broadcast_to(np.asarray(xa, dtype=np.float64), (S, n))
+    Se = np.broadcast_to(np.asarray(Se, dtype=np.float64), ys.shape)
+    w = 1.0 / Se
+    Sa_inv = np.linalg.inv(Sa)
+    base_profs = list(base_profs) if isinstance(base_profs, (list, tuple)) else [base_profs] * S
+    x = xa.copy()
+
+    def feats(xs, idx):
+        rows = []
+        for x_, i in zip(xs, idx):
+            p, Ts, _ = unpack_state(spec, x_, base_profs[i])
+            rows.append((p, Ts, scan_angles[i]))
+        return surrogate_features([r[0] for r in rows], [r[2] for r in rows], [r[1] for r in rows])
+
+    for _ in range(n_iter):
+        pert, idx = [], []
+        for s_ in range(S):
+            pert.append(x[s_])
+            idx.append(s_)
+            for j in range(n):
+                for sg in (1.0, -1.0):
+                    xp = x[s_].copy()
+                    xp[j] += sg * step
+                    pert.append(xp)
+                    idx.append(s_)
+        F, _ = sur.predict(feats(pert, idx))
+        F = F.astype(np.float64).reshape(S, 2 * n + 1, -1)
+        for s_ in range(S):
+            F0 = F[s_, 0]
+            K = ((F[s_, 1::2] - F[s_, 2::2]) / (2 * step)).T  # [n_ch, n]
+            KtW = K.T * w[s_]
+            H = Sa_inv + KtW @ K
+            g = KtW @ (ys[s_] - F0 + K @ (x[s_] - xa[s_]))
+            x[s_] = xa[s_] + np.linalg.solve(H, g)
+    return x

@@ -136,4 +136,38 @@ def test_surrogate_on_lbl_spectra(pkg, ctx):
     assert res["lbl_mask"].tolist() == [False, True, False]
     assert np.array_equal(res["BT"][1], lbl([hot], [10.0])[0])
     assert res["holdout_rms"] is not None and res["holdout_rms"] < 0.2 * clim
+    # What the network gains a retrieval: optimal estimation of T + log H2O + T_sfc from
+    # the surrogate's first guess against the same retrieval started at the a priori
+    base = pkg.afgl_atmosphere("us_standard")
+    spec = pkg.StateVectorSpec(50, [pkg.H2O], include_emissivity=False)
+    xa = pkg.pack_state(spec, base)
+    Sa = pkg.build_sa(spec, base, sigma_T=3.0, L_T=1.0, sigma_vmr=0.3)
+    rng = np.random.default_rng(77)
+    n_sc = 6
+    xt = xa + (np.linalg.cholesky(Sa) @ rng.standard_normal((spec.n, n_sc))).T
+    truth = [pkg.unpack_state(spec, x, base) for x in xt]
+    ang_sc = rng.uniform(0.0, 48.0, n_sc)
+    geoms = [pkg.ViewingGeometry(pkg.scan_angle_to_local_zenith(a)) for a in ang_sc]
+    _, _, bt = pkg.forward_model_batch([t[0] for t in truth], lists, sounder=snd, geoms=geoms,
+                                       T_sfcs=[t[1] for t in truth], backend=ctx, **kw)
+    se = np.full(bt.shape[1], 0.2 ** 2)
+    y = bt + 0.2 * rng.standard_normal(bt.shape)
+    x0 = pkg.surrogate_first_guess(s, y, spec, [base] * n_sc, ang_sc, xa=xa, Sa=Sa, Se=se)
+
+    def cost(xs):
+        profs_x = [pkg.unpack_state(spec, x, base) for x in xs]
+        F = pkg.forward_model_batch([p[0] for p in profs_x], lists, sounder=snd, geoms=geoms,
+                                    T_sfcs=[p[1] for p in profs_x], backend=ctx, dptmn=0.0, **kw)[2]
+        Si = np.linalg.inv(Sa)
+        return np.array([np.sum((y[k] - F[k]) ** 2 / se) + (xs[k] - xa) @ Si @ (xs[k] - xa) for k in range(n_sc)])
+
+    j_prior, j_first = cost(np.tile(xa, (n_sc, 1))), cost(x0)
+    okw = dict(sounder=snd, geoms=geoms, backend=ctx, fm_kwargs={k: v for k, v in kw.items() if k != "precision"})
+    r_prior = pkg.optimal_estimation_batch(y, spec, [base] * n_sc, lists, xa=xa, Sa=Sa, Se=se, **okw)
+    r_first = pkg.optimal_estimation_batch(y, spec, [base] * n_sc, lists, xa=xa, Sa=Sa, Se=se, x0=x0, **okw)
+    print(f"OE cost at start: a priori {np.median(j_prior):.1f}, surrogate first guess {np.median(j_first):.1f}; "
+          f"LBL iterations {r_prior['n_iter'].sum()} -> {r_first['n_iter'].sum()}")
+    assert np.median(j_first) < 0.5 * np.median(j_prior)
+    assert r_first["n_iter"].sum() <= r_prior["n_iter"].sum()
+    assert r_first["converged"].all()
     s.close()
