@@ -37,7 +37,10 @@ extern "C" {
 
 /* arithmetic of the line sum */
 #define IRS_FP64          0   /* FP64 everywhere: the plain GPU kernel                  */
-#define IRS_MIXED         1   /* FP32 Faddeeva + Kahan-compensated FP32 line sum        */
+#define IRS_MIXED         1   /* FP32 Faddeeva + Kahan-compensated FP32 line sum; the far
+                                 wings of lines >= 640 grid points from a 256-point block
+                                 are summed at 8 Chebyshev nodes and interpolated        */
+#define IRS_MIXED_DIRECT  2   /* as IRS_MIXED with every (point, line) pair evaluated   */
 
 /* HITRANLine, src/HITRAN/linelist.jl:20-31 (isbits, 56 bytes): a Julia
  * Vector{HITRANLine} is passed as pointer(ll.lines) without a copy. */
@@ -71,7 +74,7 @@ typedef struct {
  * continua: bit mask 1 :h2o, 2 :co2, 4 :co2_cia, 8 :n2, 16 :o2 (CIA tables are
  *   not bundled and contribute zeros, as the reference does without them)
  * method: VoigtMethod of the line sum (forward_model uses FullFaddeeva)
- * precision: IRS_FP64 or IRS_MIXED */
+ * precision: IRS_FP64, IRS_MIXED or IRS_MIXED_DIRECT */
 typedef struct {
     double  internal_dnu;      /* <= 0: use high_res_factor (or 4) */
     int32_t high_res_factor;   /* > 0 overrides internal_dnu       */
@@ -110,6 +113,8 @@ typedef struct {
     double h2d_bytes;          /* host->device bytes copied by the call */
     double d2h_bytes;          /* device->host bytes copied by the call */
     double launches;           /* kernels launched by the call */
+    double evaluated_pairs;    /* pair evaluations the line-sum kernel issued (IRS_MIXED:
+                                  near lines x block points + far lines x nodes) */
 } irs_stage_times;
 
 typedef struct irs_ctx irs_ctx;

@@ -24,7 +24,7 @@ from typing import Dict, Iterable, Optional, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import (IRS_FP64, IRS_MIXED, LINE_DTYPE, FMOptions, IRSError, Profile, StageTimes,
+from ._lib import (IRS_FP64, IRS_MIXED, IRS_MIXED_DIRECT, LINE_DTYPE, FMOptions, IRSError, Profile, StageTimes,
                    check, dptr)
 
 DATA = Path(__file__).resolve().parent / "data"
@@ -56,7 +56,7 @@ class GasSpecies(IntEnum):
 H2O, CO2, O3, N2O, CO, CH4 = (GasSpecies.H2O, GasSpecies.CO2, GasSpecies.O3, GasSpecies.N2O,
                               GasSpecies.CO, GasSpecies.CH4)
 
-PRECISION = {"fp64": IRS_FP64, "mixed": IRS_MIXED}
+PRECISION = {"fp64": IRS_FP64, "mixed": IRS_MIXED, "mixed_direct": IRS_MIXED_DIRECT}
 APODIZATION = {"gaussian": 0, "norton_beer_weak": 1, "norton_beer_medium": 2, "norton_beer_strong": 3}
 CONTINUA = {"h2o": 1, "co2": 2, "co2_cia": 4, "n2": 8, "o2": 16}
 

@@ -14,7 +14,7 @@ HERE = Path(__file__).resolve().parent
 SO = HERE / "libirs_b200.so"
 
 IRS_WEIDEMAN, IRS_PSEUDOVOIGT, IRS_FULLFADDEEVA = 1, 2, 3
-IRS_FP64, IRS_MIXED = 0, 1
+IRS_FP64, IRS_MIXED, IRS_MIXED_DIRECT = 0, 1, 2
 
 # HITRANLine isbits layout (src/HITRAN/linelist.jl:20-31), 56 bytes
 LINE_DTYPE = np.dtype({
@@ -64,7 +64,7 @@ class StageTimes(C.Structure):
     _fields_ = [("line_params_ms", C.c_double), ("line_sum_ms", C.c_double),
                 ("rte_ms", C.c_double), ("ils_ms", C.c_double), ("total_ms", C.c_double),
                 ("pairs", C.c_double), ("core_pairs", C.c_double), ("h2d_bytes", C.c_double),
-                ("d2h_bytes", C.c_double), ("launches", C.c_double)]
+                ("d2h_bytes", C.c_double), ("launches", C.c_double), ("evaluated_pairs", C.c_double)]
 
 
 # every symbol the header declares, with its ctypes signature

@@ -101,7 +101,8 @@ static void check_launch(irs_ctx* ctx) {
 
 static void validate_options(const irs_fm_options& o) {
     IRS_REQUIRE(o.method >= 1 && o.method <= 3, "method must be 1 (Weideman), 2 (PseudoVoigt) or 3 (FullFaddeeva)");
-    IRS_REQUIRE(o.precision == IRS_FP64 || o.precision == IRS_MIXED, "precision must be IRS_FP64 or IRS_MIXED");
+    IRS_REQUIRE(o.precision == IRS_FP64 || o.precision == IRS_MIXED || o.precision == IRS_MIXED_DIRECT,
+                "precision must be IRS_FP64, IRS_MIXED or IRS_MIXED_DIRECT");
     IRS_REQUIRE(o.cutoff > 0.0, "cutoff must be positive");
     IRS_REQUIRE(o.apodization >= 0 && o.apodization <= 3, "unknown apodization");
     IRS_REQUIRE(o.T_method == 0 || o.T_method == 1, "T_method must be :logp_at_pcg or :mass_weighted");
@@ -158,10 +159,10 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
     int2* d_pl = upload(ctx, "pl_segs", pl.pl_segs);
     int* d_count = (int*)workspace(ctx, "seg_count", sizeof(int) * std::max(nseg, 1));
     IRS_CUDA(cudaMemsetAsync(d_count, 0, sizeof(int) * std::max(nseg, 1), st));
-    unsigned long long* d_pairs = (unsigned long long*)workspace(ctx, "pair_counts", 16);
-    IRS_CUDA(cudaMemsetAsync(d_pairs, 0, 16, st));
+    unsigned long long* d_pairs = (unsigned long long*)workspace(ctx, "pair_counts", 24);
+    IRS_CUDA(cudaMemsetAsync(d_pairs, 0, 24, st));
 
-    const int mixed = o.precision == IRS_MIXED;
+    const int mixed = o.precision != IRS_FP64;
     const size_t tau_elem = mixed ? sizeof(float) : sizeof(double);
     void* d_tau = workspace(ctx, "tau", (size_t)pl.n_prof * pl.L * n_nu * tau_elem);
     IRS_CUDA(cudaMemsetAsync(d_tau, 0, (size_t)pl.n_prof * pl.L * n_nu * tau_elem, st));
@@ -212,14 +213,15 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
     } else {
         dim3 g2((unsigned)((n_nu + kMxStrip - 1) / kMxStrip), npl);
         const float cut_g = (float)(o.cutoff / dnu_g);
-        if (o.method == 1)
-            linesum_mixed_kernel<1, false><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau);
-        else if (o.method == 2)
-            linesum_mixed_kernel<2, false><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau);
-        else if (o.line_mixing)
-            linesum_mixed_kernel<3, true><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau);
-        else
-            linesum_mixed_kernel<3, false><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau);
+        unsigned long long* d_eval = d_pairs + 2;
+#define IRS_MX(M, LMX, F) \
+    linesum_mixed_kernel<M, LMX, F><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau, d_eval)
+        const bool far = o.precision == IRS_MIXED;
+        if (o.method == 1) { if (far) IRS_MX(1, false, true); else IRS_MX(1, false, false); }
+        else if (o.method == 2) IRS_MX(2, false, false);
+        else if (o.line_mixing) { if (far) IRS_MX(3, true, true); else IRS_MX(3, true, false); }
+        else { if (far) IRS_MX(3, false, true); else IRS_MX(3, false, false); }
+#undef IRS_MX
     }
     check_launch(ctx);
     return d_tau;
@@ -274,7 +276,7 @@ static void forward_pass(irs_ctx* ctx, const irs_profile* profs, int n_prof, con
     {  // size every workspace up front so no (synchronising) reallocation falls inside a timed stage
         int64_t slots = 0, max_list = 0;
         for (auto& g : pl.segs) { slots += ctx->lists[g.list].n; max_list = std::max<int64_t>(max_list, ctx->lists[g.list].n); }
-        const bool mixed = o.precision == IRS_MIXED;
+        const bool mixed = o.precision != IRS_FP64;
         const int nseg = std::max<int>((int)pl.segs.size(), 1);
         workspace(ctx, "tau", (size_t)n_prof * L * n_nu * (mixed ? sizeof(float) : sizeof(double)));
         workspace(ctx, "I", (size_t)n_prof * n_nu * sizeof(double));
@@ -306,7 +308,7 @@ static void forward_pass(irs_ctx* ctx, const irs_profile* profs, int n_prof, con
         if ((o.continua & 2) && ctx->n_co2 > 1) cd.mask |= 2;
     }
     dim3 g3((unsigned)((n_nu + 255) / 256), n_prof);
-    if (o.precision == IRS_MIXED)
+    if (o.precision != IRS_FP64)
         rte_kernel<float><<<g3, 256, 0, st>>>((const float*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
     else
         rte_kernel<double><<<g3, 256, 0, st>>>((const double*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
@@ -530,11 +532,12 @@ static void collect_times(irs_ctx* ctx) {
     ctx->last.rte_ms = c + ctx->prior.rte_ms;
     ctx->last.ils_ms = d + ctx->prior.ils_ms;
     ctx->last.total_ms = a + b + c + d + ctx->prior.total_ms;
-    unsigned long long pc[2] = {0, 0};
+    unsigned long long pc[3] = {0, 0, 0};
     DevBuf& pb = ctx->work["pair_counts"];
-    if (pb.p) IRS_CUDA(cudaMemcpy(pc, pb.p, 16, cudaMemcpyDeviceToHost));
+    if (pb.p) IRS_CUDA(cudaMemcpy(pc, pb.p, 24, cudaMemcpyDeviceToHost));
     ctx->last.pairs = (double)pc[0] + ctx->prior.pairs;
     ctx->last.core_pairs = (double)pc[1] + ctx->prior.core_pairs;
+    ctx->last.evaluated_pairs = (double)(pc[2] ? pc[2] : pc[0]) + ctx->prior.evaluated_pairs;
     ctx->last.h2d_bytes = ctx->n_h2d;
     ctx->last.d2h_bytes = ctx->n_d2h;
     ctx->last.launches = ctx->n_launch;
@@ -574,7 +577,7 @@ static void forward_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, c
     IRS_REQUIRE(L >= 1, "a profile needs at least two levels");
     int64_t total_lines = 0;
     for (auto& l : ctx->lists) total_lines += l.n;
-    const bool mixed = o.precision == IRS_MIXED;
+    const bool mixed = o.precision != IRS_FP64;
     const size_t per_prof = (size_t)L * total_lines * (mixed ? 65 : 49) + (size_t)L * ig.g.n * (mixed ? 4 : 8) +
                             (size_t)ig.g.n * 8;
     const int chunk = profiles_per_pass(ctx, n_prof, L, per_prof);
@@ -593,6 +596,7 @@ static void forward_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, c
             ctx->prior.total_ms += keep.total_ms;
             ctx->prior.pairs += keep.pairs;
             ctx->prior.core_pairs += keep.core_pairs;
+            ctx->prior.evaluated_pairs += keep.evaluated_pairs;
             ctx->n_h2d = h2d, ctx->n_d2h = d2h, ctx->n_launch = nl;
         }
     }
@@ -1000,7 +1004,7 @@ int irs_cross_sections(irs_ctx* ctx, int species, const double* grid, int64_t n_
     validate_options(o);
     upload_tables(ctx);
     double dnu_g = n_nu > 1 ? (grid[n_nu - 1] - grid[0]) / double(n_nu - 1) : 1.0;
-    if (precision == IRS_MIXED) {
+    if (precision != IRS_FP64) {
         IRS_REQUIRE(n_nu > 1 && dnu_g > 0, "the mixed kernel needs a uniform increasing grid");
         for (int64_t i = 0; i < n_nu; ++i)
             IRS_REQUIRE(std::fabs(grid[i] - (grid[0] + double(i) * dnu_g)) <= 1e-9 * std::max(1.0, std::fabs(grid[i])),
@@ -1020,7 +1024,7 @@ int irs_cross_sections(irs_ctx* ctx, int species, const double* grid, int64_t n_
     IRS_CUDA(cudaMemcpyAsync(d_grid, grid, n_nu * sizeof(double), cudaMemcpyHostToDevice, st));
     void* d_tau = run_linesum(ctx, pl, d_grid, n_nu, grid[0], dnu_g, o, 1);
     IRS_CUDA(cudaEventRecord(ctx->ev[2], st));
-    if (precision == IRS_MIXED) {
+    if (precision != IRS_FP64) {
         std::vector<float> tmp(n_nu);
         IRS_CUDA(cudaMemcpyAsync(tmp.data(), d_tau, n_nu * sizeof(float), cudaMemcpyDeviceToHost, st));
         IRS_CUDA(cudaStreamSynchronize(st));

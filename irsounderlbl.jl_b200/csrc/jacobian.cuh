@@ -199,9 +199,32 @@ struct JgTile {
     float4 q0[32], q1[32], q2[32], q3[32], q4[32];  // slow: per-line primitives
 };
 
+// Far field of the Jacobian sums: as in the forward line sum, the fast lines whose
+// centres lie kJgFarDist or more points from the centre of the warp's 128-point block
+// are summed at the 8 Chebyshev nodes of the block (all seven sums: s, s_T, s_p, s_v
+// and the three dispersive ones) and interpolated; kJgFarDist / 64 = 5 gives the same
+// 1.6e-7 bound on one line's interpolation error as the forward kernel's 640 / 128.
+constexpr float kJgFarDist = 320.f;
+constexpr int kJgFarNodes = 8;
+struct JgFarTable {
+    float L[kJgFarNodes][kJgWarpPts];
+};
+__device__ __forceinline__ double jg_far_node(int k) {
+    return 63.5 + 63.5 * cos((2 * k + 1) * 3.14159265358979323846 / (2 * kJgFarNodes));
+}
+__device__ __forceinline__ void jg_far_table_init(JgFarTable& F) {
+    for (int idx = threadIdx.x; idx < kJgFarNodes * kJgWarpPts; idx += blockDim.x) {
+        const int kk = idx / kJgWarpPts, i = idx % kJgWarpPts;
+        double v = 1.0;
+        for (int j = 0; j < kJgFarNodes; ++j)
+            if (j != kk) v *= ((double)i - jg_far_node(j)) / (jg_far_node(kk) - jg_far_node(j));
+        F.L[kk][i] = (float)v;
+    }
+}
+
 template <bool LM>
 __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long long wb, float cut, int lane,
-                           JgTile& T, float sum[4][kJgQ], float dsum[3][kJgQ]) {
+                           JgTile& T, const JgFarTable& FT, float xn, float sum[4][kJgQ], float dsum[3][kJgQ]) {
     constexpr float kCentre = 0.5f * (kJgWarpPts - 1);
     constexpr float kHalf = 0.5f * kJgWarpPts + 0.5f;
     constexpr float k = (float)kInvSqrtPi;
@@ -229,6 +252,8 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
         offn[h] = make_float2(64.f * h, 64.f * h + 32.f);
         offs[h] = make_float2(64.f * h + 32.f, 64.f * h);
     }
+    // far-field node sums: lane l accumulates node l % 8 over every fourth far line
+    float fS = 0.f, fC = 0.f, fT_ = 0.f, fP = 0.f, fV = 0.f, fD = 0.f, fDC = 0.f, fDT = 0.f, fDP = 0.f;
     for (long long t0 = jlo; t0 < jhi; t0 += 32) {
         const int nt = (int)min(32LL, jhi - t0);
         int cls = 0;
@@ -248,13 +273,14 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
             if (LM) a4 = g.q4[q];
             const float dist = fabsf(uh - kCentre);
             if (dist > cut + kHalf) cls = 0;
-            else if (dist + kHalf <= cut && dist > a2.w + kHalf) cls = 1;
+            else if (dist + kHalf <= cut && dist > a2.w + kHalf) cls = dist >= kJgFarDist ? 3 : 1;
             else cls = 2;
         }
         const unsigned fm = __ballot_sync(kFull, cls == 1), sm = __ballot_sync(kFull, cls == 2);
+        const unsigned xm = __ballot_sync(kFull, cls == 3);
         __syncwarp();
-        if (cls == 1) {
-            const int pos = __popc(fm & lt);
+        if (cls == 1 || cls == 3) {  // fast lines first, far lines after them
+            const int pos = cls == 1 ? __popc(fm & lt) : __popc(fm) + __popc(xm & lt);
             const float An = a0.x, fx = a0.y, y = a0.z, Hc = a0.w;
             const float AnT = a1.x, fxT = a1.y, yT = a1.z, HcT = a1.w;
             const float yp = a2.x, up = a2.y, Hcp = a2.z, yv = a3.x, uv = a3.y, Hcv = a3.z;
@@ -305,7 +331,29 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
             wC[o] = warp_sum(pC[o]);
         }
         __syncwarp();
-        const int nf = __popc(fm), ns = __popc(sm);
+        const int nf = __popc(fm), ns = __popc(sm), nx = __popc(xm);
+        {
+            float ts = 0.f, td = 0.f;
+            for (int kk = nf + (lane >> 3); kk < nf + nx; kk += 4) {
+                const float4 f0 = T.fu[kk], f1 = T.fT[kk], f2 = T.fp[kk];
+                const float d = (xn - f0.x) - f0.y;
+                const float rho = rcp_fast(fmaf(d, d, f0.z));
+                const float rho2 = rho * rho, drho2 = d * rho2;
+                ts = fmaf(f0.w, rho, ts);
+                fT_ = fmaf(f1.x, rho, fmaf(f1.y, rho2, fT_));
+                fP = fmaf(f1.z, rho, fmaf(f1.w, rho2, fmaf(f2.x, drho2, fP)));
+                fV = fmaf(f2.y, rho, fmaf(f2.z, rho2, fmaf(f2.w, drho2, fV)));
+                if (LM) {
+                    const float4 l0 = T.fL0[kk], l1 = T.fL1[kk];
+                    const float drho = d * rho;
+                    td = fmaf(l0.x, drho, td);
+                    fDT = fmaf(l0.y, drho, fmaf(l0.z, drho2, fDT));
+                    fDP = fmaf(l0.w, drho, fmaf(l1.x, rho, fmaf(l1.y, rho2, fmaf(l1.z, drho2, fDP))));
+                }
+            }
+            kahan_add(fS, fC, ts);
+            if (LM) kahan_add(fD, fDC, td);
+        }
         float2 TS[kJgQ / 2], TD[kJgQ / 2];  // tile partials of the value sums (Kahan-added below)
 #pragma unroll
         for (int h = 0; h < kJgQ / 2; ++h) TS[h] = TD[h] = make_float2(0.f, 0.f);
@@ -389,6 +437,47 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
             }
         }
     }
+    {  // node totals (4 lanes per node), then the interpolants at this lane's points
+        float v[7] = {fS, fT_, fP, fV, fD, fDT, fDP};
+#pragma unroll
+        for (int c = 0; c < 7; ++c) {
+            if (!LM && c >= 4) continue;
+            v[c] += __shfl_xor_sync(kFull, v[c], 8);
+            v[c] += __shfl_xor_sync(kFull, v[c], 16);
+        }
+        float it[7][kJgQ];
+#pragma unroll
+        for (int c = 0; c < 7; ++c)
+#pragma unroll
+            for (int q = 0; q < kJgQ; ++q) it[c][q] = 0.f;
+#pragma unroll
+        for (int kk = 0; kk < kJgFarNodes; ++kk) {
+            float w[kJgQ];
+#pragma unroll
+            for (int q = 0; q < kJgQ; ++q) w[q] = FT.L[kk][32 * q + lane];
+#pragma unroll
+            for (int c = 0; c < 7; ++c) {
+                if (!LM && c >= 4) continue;
+                const float n = __shfl_sync(kFull, v[c], kk);
+#pragma unroll
+                for (int q = 0; q < kJgQ; ++q) it[c][q] = fmaf(n, w[q], it[c][q]);
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < kJgQ / 2; ++h) {
+            kahan_add(S[h].x, C[h].x, it[0][2 * h]);
+            kahan_add(S[h].y, C[h].y, it[0][2 * h + 1]);
+            ST[h].x += it[1][2 * h]; ST[h].y += it[1][2 * h + 1];
+            SP[h].x += it[2][2 * h]; SP[h].y += it[2][2 * h + 1];
+            SV[h].x += it[3][2 * h]; SV[h].y += it[3][2 * h + 1];
+            if (LM) {
+                kahan_add(SD[h].x, CD[h].x, it[4][2 * h]);
+                kahan_add(SD[h].y, CD[h].y, it[4][2 * h + 1]);
+                SDT[h].x += it[5][2 * h]; SDT[h].y += it[5][2 * h + 1];
+                SDP[h].x += it[6][2 * h]; SDP[h].y += it[6][2 * h + 1];
+            }
+        }
+    }
 #pragma unroll
     for (int h = 0; h < kJgQ / 2; ++h) {
         sum[0][2 * h] = S[h].x; sum[0][2 * h + 1] = S[h].y;
@@ -409,7 +498,7 @@ struct SegW {
 // dynamic shared memory of jg_linesum_kernel<*, NOUT>: the warps' tiles and their
 // per-point output accumulators
 constexpr size_t jg_smem_bytes(int nout) {
-    return sizeof(JgTile) * kJgWarps + sizeof(float) * kJgWarps * nout * kJgWarpPts;
+    return sizeof(JgTile) * kJgWarps + sizeof(float) * kJgWarps * nout * kJgWarpPts + sizeof(JgFarTable);
 }
 
 template <bool ANY_LM, int NOUT>
@@ -418,11 +507,15 @@ __global__ void __launch_bounds__(kJgWarps * 32, 2) jg_linesum_kernel(
     const int2* __restrict__ pl_segs, JgOut g, long long n_nu, float cut_g, float* __restrict__ out) {
     extern __shared__ float4 jg_sh[];
     JgTile* tiles = (JgTile*)jg_sh;
+    JgFarTable& ftab = *(JgFarTable*)((float*)(tiles + kJgWarps) + (size_t)kJgWarps * NOUT * kJgWarpPts);
+    jg_far_table_init(ftab);
+    __syncthreads();  // the only block-wide barrier: before any warp leaves
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float* acc = (float*)(tiles + kJgWarps) + (size_t)warp * NOUT * kJgWarpPts;  // [NOUT][128], warp-private
     const int pl = blockIdx.y;
     const long long wb = (long long)blockIdx.x * kJgStrip + (long long)warp * kJgWarpPts;
     if (wb >= n_nu) return;
+    const float xn = (float)jg_far_node(lane & (kJgFarNodes - 1));
     for (int o = 0; o < NOUT; ++o)
 #pragma unroll
         for (int q = 0; q < kJgQ; ++q) acc[o * kJgWarpPts + 32 * q + lane] = 0.f;
@@ -433,9 +526,9 @@ __global__ void __launch_bounds__(kJgWarps * 32, 2) jg_linesum_kernel(
         const long long nl = seg_n[si];
         const bool lm = ANY_LM && (sg.flags & SEG_LM);
         if (lm)
-            jg_segment<true>(sg, nl, g, wb, cut_g, lane, tiles[warp], s, ds);
+            jg_segment<true>(sg, nl, g, wb, cut_g, lane, tiles[warp], ftab, xn, s, ds);
         else
-            jg_segment<false>(sg, nl, g, wb, cut_g, lane, tiles[warp], s, ds);
+            jg_segment<false>(sg, nl, g, wb, cut_g, lane, tiles[warp], ftab, xn, s, ds);
         // clamps (voigt.jl:276, line_mixing.jl:1368, cross_section_jacobian.jl:107-113, :312-319)
         const SegW& W = wts[si];
 #pragma unroll

@@ -146,7 +146,37 @@ struct WarpTile {
     float4 sp[32];  // slow lines: c1, c0, dfar2, An           (PV: kPV, gPV, -, -)
     float4 sq[32];  // slow lines: fx, y, g, Yw
     float fg[32];   // fast lines: g (dispersive line mixing)
+    float4 ff[32];  // far lines: uh, ul, b2, a
+    float ffg[32];  // far lines: g
 };
+
+// Far field.  A fast line whose centre lies kFarDist or more points from the centre
+// of a warp's 256-point block contributes a function of the point index that is
+// analytic well beyond the block (its poles sit at complex distance >= kFarDist - 128
+// from it), so its far-wing sum over all such lines is evaluated at the 8 Chebyshev
+// nodes of the block and interpolated to the 256 points with the fixed Lagrange
+// weights L_k(i): 8 pairs per line instead of 256.  The interpolation error of one
+// line's term is at most 1.6e-7 of its largest value on the block (degree 7, nodes
+// on [0, 255], distance 640); pedestals stay exact (quadratic sums), as do the
+// near lines, the Faddeeva cores and the cutoff edges.
+constexpr float kFarDist = 640.f;
+constexpr int kFarNodes = 8;
+struct FarTable {
+    float L[kFarNodes][kMxWarpPts];  // L_k(i), i = 0..255
+};
+__device__ __forceinline__ double far_node(int k) {
+    return 127.5 + 127.5 * cos((2 * k + 1) * 3.14159265358979323846 / (2 * kFarNodes));
+}
+// whole block, before any early exit
+__device__ __forceinline__ void far_table_init(FarTable& F) {
+    for (int idx = threadIdx.x; idx < kFarNodes * kMxWarpPts; idx += blockDim.x) {
+        const int k = idx / kMxWarpPts, i = idx % kMxWarpPts;
+        double v = 1.0;
+        for (int j = 0; j < kFarNodes; ++j)
+            if (j != k) v *= ((double)i - far_node(j)) / (far_node(k) - far_node(j));
+        F.L[k][i] = (float)v;
+    }
+}
 
 // window [jlo, jhi) of the lines that can reach this warp's points [wb, wb + 255]
 __device__ __forceinline__ void warp_window(const LpOutMixed& lp, const SegDev& sg, long long cnt,
@@ -173,9 +203,10 @@ __device__ __forceinline__ void fast_pair(float2 d0s, float2 offs, float2 b2, fl
     acc = __ffma2_rn(a, r, acc);
 }
 
-template <int METHOD, bool LM>
+template <int METHOD, bool LM, bool FAR>
 __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, const LpOutMixed& lp, long long wb,
-                                             float cut, float cut2, int lane, WarpTile& T, float* tsum) {
+                                             float cut, float cut2, int lane, WarpTile& T, const FarTable& FT,
+                                             float xn, float* tsum, unsigned long long& work) {
     constexpr float kCentre = 0.5f * (kMxWarpPts - 1);
     constexpr float kHalf = 0.5f * kMxWarpPts + 0.5f;
     long long jlo, jhi;
@@ -188,10 +219,12 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
     float sum[kMxQ], comp[kMxQ], sumD[kMxQ], compD[kMxQ];
 #pragma unroll
     for (int q = 0; q < kMxQ; ++q) sum[q] = comp[q] = sumD[q] = compD[q] = 0.f;
+    // far-field node sums: lane l accumulates node l % 8 over every fourth far line
+    float farS = 0.f, farC = 0.f, farDS = 0.f, farDC = 0.f;
     const unsigned lt = (1u << lane) - 1u;
     for (long long t0 = jlo; t0 < jhi; t0 += 32) {
         const int nt = (int)min(32LL, jhi - t0);
-        float pa = 0.f, pb = 0.f, pc = 0.f;  // this line's pedestal quadratic (fast lines)
+        float pa = 0.f, pb = 0.f, pc = 0.f;  // this line's pedestal quadratic (fast and far lines)
         int cls = 0;
         float4 a0, a1, a2;
         float uh = 0.f, ul = 0.f;
@@ -205,7 +238,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             const float dist = fabsf(uh - kCentre);
             if (dist > cut + kHalf) cls = 0;
             else if (dist + kHalf <= cut && dist > a2.z + kHalf) {
-                cls = 1;
+                cls = (FAR && dist >= kFarDist) ? 3 : 1;
                 // sum over points p of c1 (p - u)^2 + c0 = p^2 c1 - 2 p c1 u + (c1 u^2 + c0)
                 pa = a0.z;
                 pb = a0.z * uh;
@@ -216,11 +249,16 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             }
         }
         const unsigned fm = __ballot_sync(kFull, cls == 1), sm = __ballot_sync(kFull, cls == 2);
+        const unsigned xm = FAR ? __ballot_sync(kFull, cls == 3) : 0u;
         __syncwarp();
         if (cls == 1) {
             const int pos = __popc(fm & lt);
             T.fu[pos] = make_float4(uh, ul, a0.x, a0.y);
             if (LM) T.fg[pos] = a2.x;
+        } else if (FAR && cls == 3) {
+            const int pos = __popc(xm & lt);
+            T.ff[pos] = make_float4(uh, ul, a0.x, a0.y);
+            if (LM) T.ffg[pos] = a2.x;
         } else if (cls == 2) {
             const int pos = __popc(sm & lt);
             T.su[pos] = make_float4(uh, ul, a0.x, a0.y);
@@ -230,6 +268,22 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
         const float A = warp_sum(pa), B = warp_sum(pb), Cc = warp_sum(pc);
         __syncwarp();
         const int nf = __popc(fm), ns = __popc(sm);
+        if (FAR) {
+            const int nx = __popc(xm);
+            if (lane == 0) work += (unsigned long long)(nf + ns) * kMxWarpPts + (unsigned long long)nx * kFarNodes;
+            float ft = 0.f, fd = 0.f;
+            for (int k = lane >> 3; k < nx; k += 4) {
+                const float4 f = T.ff[k];
+                const float d = (xn - f.x) - f.y;
+                const float r = rcp_fast(fmaf(d, d, f.z));
+                ft = fmaf(f.w, r, ft);
+                if (LM) fd = fmaf(T.ffg[k] * d, r, fd);
+            }
+            kahan_add(farS, farC, ft);
+            if (LM) kahan_add(farDS, farDC, fd);
+        } else if (lane == 0) {
+            work += (unsigned long long)(nf + ns) * kMxWarpPts;
+        }
         float2 acc2[kMxQ / 2];
         float tdsp[kMxQ];
 #pragma unroll
@@ -294,6 +348,32 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             if (LM) kahan_add(sumD[q], compD[q], tdsp[q]);
         }
     }
+    if (FAR) {  // node totals (4 lanes per node), then the interpolant at this lane's points
+        farS += __shfl_xor_sync(kFull, farS, 8);
+        farS += __shfl_xor_sync(kFull, farS, 16);
+        if (LM) {
+            farDS += __shfl_xor_sync(kFull, farDS, 8);
+            farDS += __shfl_xor_sync(kFull, farDS, 16);
+        }
+        float Fn[kFarNodes], Dn[kFarNodes];
+#pragma unroll
+        for (int k = 0; k < kFarNodes; ++k) {
+            Fn[k] = __shfl_sync(kFull, farS, k);
+            Dn[k] = LM ? __shfl_sync(kFull, farDS, k) : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < kMxQ; ++q) {
+            float v = 0.f, vd = 0.f;
+#pragma unroll
+            for (int k = 0; k < kFarNodes; ++k) {
+                const float w = FT.L[k][32 * q + lane];
+                v = fmaf(Fn[k], w, v);
+                if (LM) vd = fmaf(Dn[k], w, vd);
+            }
+            kahan_add(sum[q], comp[q], v);
+            if (LM) kahan_add(sumD[q], compD[q], vd);
+        }
+    }
 #pragma unroll
     for (int q = 0; q < kMxQ; ++q) {
         float sig = fmaxf(sum[q], 0.f);
@@ -351,15 +431,22 @@ __device__ __forceinline__ void warp_segment_pv(const SegDev& sg, long long cnt,
     for (int q = 0; q < kMxQ; ++q) tsum[q] += fmaxf(sum[q], 0.f);
 }
 
-template <int METHOD, bool ANY_LM>
+template <int METHOD, bool ANY_LM, bool FAR>
 __global__ void __launch_bounds__(kMxThreads, ANY_LM ? 2 : 3) linesum_mixed_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const int2* __restrict__ pl_segs,
-    LpOutMixed lp, long long n_nu, float cut_g, float* __restrict__ tau) {
+    LpOutMixed lp, long long n_nu, float cut_g, float* __restrict__ tau, unsigned long long* __restrict__ evald) {
     __shared__ WarpTile tiles[kMxWarps];
+    __shared__ FarTable ftab;
+    if (FAR) {
+        far_table_init(ftab);
+        __syncthreads();
+    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int pl = blockIdx.y;
     const long long wb = (long long)blockIdx.x * kMxStrip + (long long)warp * kMxWarpPts;
     if (wb >= n_nu) return;  // no block-wide barriers below: whole warps may leave
+    const float xn = FAR ? (float)far_node(lane & (kFarNodes - 1)) : 0.f;
+    unsigned long long work = 0;
     const float cut2 = cut_g * cut_g;
     WarpTile& T = tiles[warp];
     float tsum[kMxQ];
@@ -372,10 +459,11 @@ __global__ void __launch_bounds__(kMxThreads, ANY_LM ? 2 : 3) linesum_mixed_kern
         if (METHOD == 2)
             warp_segment_pv(sg, cnt, lp, wb, cut_g, cut2, lane, T, tsum);
         else if (ANY_LM && (sg.flags & 2))
-            warp_segment<METHOD, true>(sg, cnt, lp, wb, cut_g, cut2, lane, T, tsum);
+            warp_segment<METHOD, true, FAR>(sg, cnt, lp, wb, cut_g, cut2, lane, T, ftab, xn, tsum, work);
         else
-            warp_segment<METHOD, false>(sg, cnt, lp, wb, cut_g, cut2, lane, T, tsum);
+            warp_segment<METHOD, false, FAR>(sg, cnt, lp, wb, cut_g, cut2, lane, T, ftab, xn, tsum, work);
     }
+    if (evald && lane == 0 && work) atomicAdd(evald, work);
     float* out = tau + (size_t)pl * n_nu;
 #pragma unroll
     for (int q = 0; q < kMxQ; ++q) {

@@ -69,12 +69,13 @@ def test_cross_sections_5k(pkg, ctx, oracle, T, p):
     ref = oracle.voigt_xsec(ll.lines, grid, T, p)
     f64 = pkg.compute_voigt_cross_sections(grid, ll, T, p, backend=ctx)
     assert np.max(np.abs(f64 - ref)) <= 1e-12 * ref.max()
-    mx = pkg.compute_voigt_cross_sections(grid, ll, T, p, backend=ctx, precision="mixed")
-    # FP32 parameters and an FP32 Faddeeva accurate to ~4e-7 of each line's peak:
-    # ~1e-6 relative near the cores, ~1e-5 of the peak everywhere
-    m = ref > 1e-2 * ref.max()
-    assert np.max(np.abs(mx[m] - ref[m]) / ref[m]) < 2e-4
-    assert np.max(np.abs(mx - ref)) < 2e-5 * ref.max()
+    for prec in ("mixed", "mixed_direct"):
+        mx = pkg.compute_voigt_cross_sections(grid, ll, T, p, backend=ctx, precision=prec)
+        # FP32 parameters and an FP32 Faddeeva accurate to ~4e-7 of each line's peak:
+        # ~1e-6 relative near the cores, ~1e-5 of the peak everywhere
+        m = ref > 1e-2 * ref.max()
+        assert np.max(np.abs(mx[m] - ref[m]) / ref[m]) < 2e-4, prec
+        assert np.max(np.abs(mx - ref)) < 2e-5 * ref.max(), prec
 
 
 def test_cross_sections_mixed_weideman_pv(pkg, ctx, oracle, orc_mod, golden):
@@ -99,7 +100,7 @@ def _run(pkg, ctx, oracle, orc_mod, prof, lists, snd, channels=None, y0=None, ge
                                y0=None if y0 is None else {2: y0})
     lm = pkg.VPYLineMixing(y0) if y0 is not None else None
     out = {}
-    for prec in ("fp64", "mixed"):
+    for prec in ("fp64", "mixed", "mixed_direct"):
         _, R, BT = pkg.forward_model(prof, lists, sounder=snd, geom=geom, T_sfc=T_sfc, eps_sfc=eps,
                                      backend=ctx, precision=prec, line_mixing=lm,
                                      method=pkg.VoigtMethod[method], **kw)
@@ -114,9 +115,10 @@ def _check(ref, out, fp64_tol=1e-6, rms=0.01, mx=0.05):
     R, BT = out["fp64"]
     assert np.max(np.abs(BT - BT0)) < fp64_tol
     assert np.max(np.abs(R - R0) / np.abs(R0)) < 1e-9
-    Rm, BTm = out["mixed"]
-    d = BTm - BT0
-    assert np.sqrt(np.mean(d * d)) <= rms and np.max(np.abs(d)) <= mx
+    for prec in ("mixed", "mixed_direct"):
+        Rm, BTm = out[prec]
+        d = BTm - BT0
+        assert np.sqrt(np.mean(d * d)) <= rms and np.max(np.abs(d)) <= mx, prec
 
 
 def test_forward_5k_co2(pkg, ctx, oracle, orc_mod):
@@ -236,3 +238,22 @@ def test_iasi_400k_mixed_vs_fp64_full_spectrum(pkg, ctx, iasi_lists):
     assert BT64.shape == (8461,) and np.all(np.isfinite(BT64)) and np.all(BT64 > 150)
     d = BTm - BT64
     assert np.sqrt(np.mean(d * d)) <= 0.01 and np.max(np.abs(d)) <= 0.05
+
+
+def test_iasi_400k_far_field_vs_direct(pkg, ctx, iasi_lists):
+    """The far-field interpolation (IRS_MIXED) against the direct FP32 sum
+    (IRS_MIXED_DIRECT) over the whole IASI spectrum, with line mixing on CO2: BT
+    within 1e-3 K (the interpolation error is ~1e-7 of each far line's term), while
+    the line-sum kernel evaluates a fraction of the pairs."""
+    prof = pkg.afgl_atmosphere("tropical")
+    lm = pkg.VPYLineMixing(pkg.synthetic.vpy_y0(len(iasi_lists[2])))
+    out = {}
+    for prec in ("mixed_direct", "mixed"):
+        _, _, out[prec] = pkg.forward_model(prof, iasi_lists, backend=ctx, internal_dnu=0.0025, precision=prec,
+                                            line_mixing=lm)
+        st = ctx.stage_times()
+        if prec == "mixed":
+            print("pairs", st.pairs, "evaluated", st.evaluated_pairs)
+            assert st.evaluated_pairs < 0.3 * st.pairs
+    d = out["mixed"] - out["mixed_direct"]
+    assert np.max(np.abs(d)) < 1e-3
