@@ -184,6 +184,23 @@ def reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def reduce_max(dist, x: float, device: str) -> float:
+    """Max of a per-rank scalar over the process group (the timing rule for N > 1);
+    `dist` None means one process."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def weak_scaling_value(world: int, profiles_per_rank: int, ms_per_step: float) -> float:
+    """Whole-job spectra/s: every rank runs its own profiles (no data-path collective),
+    the step time is the max over ranks."""
+    return world * profiles_per_rank / (ms_per_step / 1e3)
+
+
 def _peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -359,11 +376,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(dist, x, "cuda")
 
     pkg = _package()
     ctx = pkg.B200Context(local)
@@ -405,7 +418,7 @@ def main():
         torch.cuda.synchronize()
     barrier()
     ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
-    value = world * N_PROF / (ms / 1e3)
+    value = weak_scaling_value(world, N_PROF, ms)
 
     # per-stage device times (library events on its launching stream), averaged
     acc = {"line_params_ms": 0.0, "line_sum_ms": 0.0, "rte_ms": 0.0, "ils_ms": 0.0}

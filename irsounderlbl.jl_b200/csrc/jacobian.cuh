@@ -229,13 +229,9 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
     constexpr float kHalf = 0.5f * kJgWarpPts + 0.5f;
     constexpr float k = (float)kInvSqrtPi;
     const float cut2 = cut * cut, icut2 = 1.f / cut2;
-    long long jlo = 0, jhi = 0;
-    if (lane == 0) {
-        jlo = lower_bound0(g.V + sg.off, (double)wb - cut - sg.margin_g, cnt);
-        jhi = lower_bound0(g.V + sg.off, (double)(wb + kJgWarpPts - 1) + cut + sg.margin_g + 1e-9, cnt);
-    }
-    jlo = __shfl_sync(kFull, jlo, 0);
-    jhi = __shfl_sync(kFull, jhi, 0);
+    const long long jlo = warp_lower_bound(g.V + sg.off, (double)wb - cut - sg.margin_g, cnt, lane);
+    const long long jhi =
+        warp_lower_bound(g.V + sg.off, (double)(wb + kJgWarpPts - 1) + cut + sg.margin_g + 1e-9, cnt, lane);
     const float pl0 = (float)lane;
     const unsigned lt = (1u << lane) - 1u;
     // packed accumulators over point pairs (q = 2h, 2h + 1)
@@ -254,6 +250,10 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
     }
     // far-field node sums: lane l accumulates node l % 8 over every fourth far line
     float fS = 0.f, fC = 0.f, fT_ = 0.f, fP = 0.f, fV = 0.f, fD = 0.f, fDC = 0.f, fDT = 0.f, fDP = 0.f;
+    // pedestal quadratics of this lane's fast and far lines (the value sum compensated),
+    // reduced over the warp once per segment
+    float QA[4] = {0.f, 0.f, 0.f, 0.f}, QB[4] = {0.f, 0.f, 0.f, 0.f}, QC[4] = {0.f, 0.f, 0.f, 0.f};
+    float QAc = 0.f, QBc = 0.f, QCc = 0.f;
     for (long long t0 = jlo; t0 < jhi; t0 += 32) {
         const int nt = (int)min(32LL, jhi - t0);
         int cls = 0;
@@ -323,12 +323,14 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
             T.q3[pos] = a3;
             if (LM) T.q4[pos] = a4;
         }
-        float wA[4], wB[4], wC[4];
+        kahan_add(QA[0], QAc, pA[0]);
+        kahan_add(QB[0], QBc, pB[0]);
+        kahan_add(QC[0], QCc, pC[0]);
 #pragma unroll
-        for (int o = 0; o < 4; ++o) {
-            wA[o] = warp_sum(pA[o]);
-            wB[o] = warp_sum(pB[o]);
-            wC[o] = warp_sum(pC[o]);
+        for (int o = 1; o < 4; ++o) {
+            QA[o] += pA[o];
+            QB[o] += pB[o];
+            QC[o] += pC[o];
         }
         __syncwarp();
         const int nf = __popc(fm), ns = __popc(sm), nx = __popc(xm);
@@ -354,6 +356,7 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
             kahan_add(fS, fC, ts);
             if (LM) kahan_add(fD, fDC, td);
         }
+        if (nf + ns == 0) continue;  // warp-uniform: nothing per point in this tile
         float2 TS[kJgQ / 2], TD[kJgQ / 2];  // tile partials of the value sums (Kahan-added below)
 #pragma unroll
         for (int h = 0; h < kJgQ / 2; ++h) TS[h] = TD[h] = make_float2(0.f, 0.f);
@@ -417,24 +420,39 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
                 }
             }
         }
-        // pedestal quadratics of the fast lines, then the compensated tile sums
+        // the compensated tile sums
 #pragma unroll
         for (int h = 0; h < kJgQ / 2; ++h) {
-            const float i0 = pl0 + 64.f * h, i1 = i0 + 32.f;
-            TS[h].x += fmaf(i0, fmaf(i0, wC[0], wB[0]), wA[0]);
-            TS[h].y += fmaf(i1, fmaf(i1, wC[0], wB[0]), wA[0]);
-            ST[h].x += fmaf(i0, fmaf(i0, wC[1], wB[1]), wA[1]);
-            ST[h].y += fmaf(i1, fmaf(i1, wC[1], wB[1]), wA[1]);
-            SP[h].x += fmaf(i0, fmaf(i0, wC[2], wB[2]), wA[2]);
-            SP[h].y += fmaf(i1, fmaf(i1, wC[2], wB[2]), wA[2]);
-            SV[h].x += fmaf(i0, fmaf(i0, wC[3], wB[3]), wA[3]);
-            SV[h].y += fmaf(i1, fmaf(i1, wC[3], wB[3]), wA[3]);
             kahan_add(S[h].x, C[h].x, TS[h].x);
             kahan_add(S[h].y, C[h].y, TS[h].y);
             if (LM) {
                 kahan_add(SD[h].x, CD[h].x, TD[h].x);
                 kahan_add(SD[h].y, CD[h].y, TD[h].y);
             }
+        }
+    }
+    {  // pedestals of the fast and far lines
+        float wA[4], wB[4], wC[4];
+        wA[0] = warp_sum(QA[0] - QAc);
+        wB[0] = warp_sum(QB[0] - QBc);
+        wC[0] = warp_sum(QC[0] - QCc);
+#pragma unroll
+        for (int o = 1; o < 4; ++o) {
+            wA[o] = warp_sum(QA[o]);
+            wB[o] = warp_sum(QB[o]);
+            wC[o] = warp_sum(QC[o]);
+        }
+#pragma unroll
+        for (int h = 0; h < kJgQ / 2; ++h) {
+            const float i0 = pl0 + 64.f * h, i1 = i0 + 32.f;
+            kahan_add(S[h].x, C[h].x, fmaf(i0, fmaf(i0, wC[0], wB[0]), wA[0]));
+            kahan_add(S[h].y, C[h].y, fmaf(i1, fmaf(i1, wC[0], wB[0]), wA[0]));
+            ST[h].x += fmaf(i0, fmaf(i0, wC[1], wB[1]), wA[1]);
+            ST[h].y += fmaf(i1, fmaf(i1, wC[1], wB[1]), wA[1]);
+            SP[h].x += fmaf(i0, fmaf(i0, wC[2], wB[2]), wA[2]);
+            SP[h].y += fmaf(i1, fmaf(i1, wC[2], wB[2]), wA[2]);
+            SV[h].x += fmaf(i0, fmaf(i0, wC[3], wB[3]), wA[3]);
+            SV[h].y += fmaf(i1, fmaf(i1, wC[3], wB[3]), wA[3]);
         }
     }
     {  // node totals (4 lanes per node), then the interpolants at this lane's points

@@ -148,6 +148,8 @@ struct WarpTile {
     float fg[32];   // fast lines: g (dispersive line mixing)
     float4 ff[32];  // far lines: uh, ul, b2, a
     float ffg[32];  // far lines: g
+    float4 eu[32];  // cutoff-edge lines (far field only): uh, ul, b2, a
+    float4 ep[32];  // cutoff-edge lines: c1, c0, g, -
 };
 
 // Far field.  A fast line whose centre lies kFarDist or more points from the centre
@@ -178,17 +180,32 @@ __device__ __forceinline__ void far_table_init(FarTable& F) {
     }
 }
 
+// First index i in [0, n) with a[i] >= v (n if none), found by the whole warp: each
+// round probes 32 evenly spaced positions and keeps the interval between the last
+// probe below v and the first one at or above it (32-ary search: 4 dependent loads
+// for 66 k lines instead of 17).  All lanes return the same value.
+__device__ __forceinline__ long long warp_lower_bound(const double* a, double v, long long n, int lane) {
+    long long lo = 0, hi = n;  // the answer lies in [lo, hi]
+    while (hi - lo > 32) {
+        const long long step = (hi - lo + 31) / 32;
+        const long long p = min(lo + (long long)(lane + 1) * step - 1, hi - 1);
+        const unsigned below = __ballot_sync(kFull, a[p] < v);  // a prefix of the lanes
+        const int c = __popc(below);
+        const long long nlo = lo + (long long)c * step;
+        hi = min(hi, lo + (long long)(c + 1) * step);
+        lo = min(nlo, hi);
+    }
+    const long long p = lo + lane;
+    const unsigned below = __ballot_sync(kFull, p < hi && a[p] < v);
+    return lo + __popc(below);
+}
+
 // window [jlo, jhi) of the lines that can reach this warp's points [wb, wb + 255]
 __device__ __forceinline__ void warp_window(const LpOutMixed& lp, const SegDev& sg, long long cnt,
                                             long long wb, float cut, int lane, long long& jlo, long long& jhi) {
-    long long a = 0, b = 0;
-    if (lane == 0) {
-        const double* V = lp.V + sg.off;
-        a = lower_bound0(V, (double)wb - cut - sg.margin_g, cnt);
-        b = lower_bound0(V, (double)(wb + kMxWarpPts - 1) + cut + sg.margin_g + 1e-9, cnt);
-    }
-    jlo = __shfl_sync(kFull, a, 0);
-    jhi = __shfl_sync(kFull, b, 0);
+    const double* V = lp.V + sg.off;
+    jlo = warp_lower_bound(V, (double)wb - cut - sg.margin_g, cnt, lane);
+    jhi = warp_lower_bound(V, (double)(wb + kMxWarpPts - 1) + cut + sg.margin_g + 1e-9, cnt, lane);
 }
 
 // Fast line, two points q and q+1 with packed FP32x2 arithmetic.  The squared
@@ -221,6 +238,10 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
     for (int q = 0; q < kMxQ; ++q) sum[q] = comp[q] = sumD[q] = compD[q] = 0.f;
     // far-field node sums: lane l accumulates node l % 8 over every fourth far line
     float farS = 0.f, farC = 0.f, farDS = 0.f, farDC = 0.f;
+    // with the far field, each lane accumulates its own lines' pedestal quadratics
+    // (compensated) and the warp reduces them once per segment, so tiles holding only
+    // far lines need no per-point work
+    float PA = 0.f, PAc = 0.f, PB = 0.f, PBc = 0.f, PC = 0.f, PCc = 0.f;
     const unsigned lt = (1u << lane) - 1u;
     for (long long t0 = jlo; t0 < jhi; t0 += 32) {
         const int nt = (int)min(32LL, jhi - t0);
@@ -237,7 +258,9 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             a2 = lp.p2[q];
             const float dist = fabsf(uh - kCentre);
             if (dist > cut + kHalf) cls = 0;
-            else if (dist + kHalf <= cut && dist > a2.z + kHalf) {
+            else if (FAR && dist + kHalf > cut && dist > a2.z + kHalf) {
+                cls = 4;  // far wing at every point, the cutoff falls among the points
+            } else if (dist + kHalf <= cut && dist > a2.z + kHalf) {
                 cls = (FAR && dist >= kFarDist) ? 3 : 1;
                 // sum over points p of c1 (p - u)^2 + c0 = p^2 c1 - 2 p c1 u + (c1 u^2 + c0)
                 pa = a0.z;
@@ -250,6 +273,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
         }
         const unsigned fm = __ballot_sync(kFull, cls == 1), sm = __ballot_sync(kFull, cls == 2);
         const unsigned xm = FAR ? __ballot_sync(kFull, cls == 3) : 0u;
+        const unsigned em = FAR ? __ballot_sync(kFull, cls == 4) : 0u;
         __syncwarp();
         if (cls == 1) {
             const int pos = __popc(fm & lt);
@@ -259,18 +283,32 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             const int pos = __popc(xm & lt);
             T.ff[pos] = make_float4(uh, ul, a0.x, a0.y);
             if (LM) T.ffg[pos] = a2.x;
+        } else if (FAR && cls == 4) {
+            const int pos = __popc(em & lt);
+            T.eu[pos] = make_float4(uh, ul, a0.x, a0.y);
+            T.ep[pos] = make_float4(a0.z, a0.w, a2.x, 0.f);
         } else if (cls == 2) {
             const int pos = __popc(sm & lt);
             T.su[pos] = make_float4(uh, ul, a0.x, a0.y);
             T.sp[pos] = make_float4(a0.z, a0.w, a1.x, a1.y);
             T.sq[pos] = make_float4(a1.z, a1.w, a2.x, a2.y);
         }
-        const float A = warp_sum(pa), B = warp_sum(pb), Cc = warp_sum(pc);
+        float A = 0.f, B = 0.f, Cc = 0.f;
+        if (FAR) {
+            kahan_add(PA, PAc, pa);
+            kahan_add(PB, PBc, pb);
+            kahan_add(PC, PCc, pc);
+        } else {
+            A = warp_sum(pa);
+            B = warp_sum(pb);
+            Cc = warp_sum(pc);
+        }
         __syncwarp();
-        const int nf = __popc(fm), ns = __popc(sm);
+        const int nf = __popc(fm), ns = __popc(sm), ne = FAR ? __popc(em) : 0;
         if (FAR) {
             const int nx = __popc(xm);
-            if (lane == 0) work += (unsigned long long)(nf + ns) * kMxWarpPts + (unsigned long long)nx * kFarNodes;
+            if (lane == 0)
+                work += (unsigned long long)(nf + ns + ne) * kMxWarpPts + (unsigned long long)nx * kFarNodes;
             float ft = 0.f, fd = 0.f;
             for (int k = lane >> 3; k < nx; k += 4) {
                 const float4 f = T.ff[k];
@@ -284,6 +322,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
         } else if (lane == 0) {
             work += (unsigned long long)(nf + ns) * kMxWarpPts;
         }
+        if (FAR && nf + ns + ne == 0) continue;  // warp-uniform: nothing per point in this tile
         float2 acc2[kMxQ / 2];
         float tdsp[kMxQ];
 #pragma unroll
@@ -302,6 +341,30 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
                 for (int q = 0; q < kMxQ; ++q) {
                     const float d = d0 + 32.f * q;
                     tdsp[q] = fmaf(g * d, rcp_fast(fmaf(d, d, f.z)), tdsp[q]);
+                }
+            }
+        }
+        // cutoff-edge lines: the far-wing value and the pedestal at every point, masked
+        // to the points inside the cutoff (packed, branch-free)
+        for (int k = 0; k < ne; ++k) {
+            const float4 f = T.eu[k], e = T.ep[k];
+            const float d0 = (pl0 - f.x) - f.y;
+            const float2 d0s = make_float2(d0, d0), b2 = make_float2(f.z, f.z), a = make_float2(f.w, f.w);
+            const float2 c1 = make_float2(e.x, e.x), c0 = make_float2(e.y, e.y);
+#pragma unroll
+            for (int h = 0; h < kMxQ / 2; ++h) {
+                const float2 dsw = __fadd2_rn(d0s, offs[h]);            // (d[q+1], d[q])
+                const float2 es = __ffma2_rn(dsw, dsw, b2);             // (e[q+1], e[q])
+                const float R = rcp_fast(es.x * es.y);
+                const float2 r = __fmul2_rn(es, make_float2(R, R));     // (1/e[q], 1/e[q+1])
+                const float2 dn = make_float2(dsw.y, dsw.x);
+                const float2 dn2 = __fmul2_rn(dn, dn);
+                const float2 v = __ffma2_rn(a, r, __ffma2_rn(c1, dn2, c0));
+                acc2[h].x += dn2.x <= cut2 ? v.x : 0.f;
+                acc2[h].y += dn2.y <= cut2 ? v.y : 0.f;
+                if (LM) {
+                    tdsp[2 * h] += dn2.x <= cut2 ? e.z * dn.x * r.x : 0.f;
+                    tdsp[2 * h + 1] += dn2.y <= cut2 ? e.z * dn.y * r.y : 0.f;
                 }
             }
         }
@@ -344,7 +407,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
 #pragma unroll
         for (int q = 0; q < kMxQ; ++q) {
             const float pp = pl0 + 32.f * q;
-            kahan_add(sum[q], comp[q], tacc[q] + fmaf(pp, fmaf(pp, A, -2.f * B), Cc));
+            kahan_add(sum[q], comp[q], FAR ? tacc[q] : tacc[q] + fmaf(pp, fmaf(pp, A, -2.f * B), Cc));
             if (LM) kahan_add(sumD[q], compD[q], tdsp[q]);
         }
     }
@@ -361,9 +424,11 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             Fn[k] = __shfl_sync(kFull, farS, k);
             Dn[k] = LM ? __shfl_sync(kFull, farDS, k) : 0.f;
         }
+        const float A = warp_sum(PA - PAc), B = warp_sum(PB - PBc), Cc = warp_sum(PC - PCc);
 #pragma unroll
         for (int q = 0; q < kMxQ; ++q) {
-            float v = 0.f, vd = 0.f;
+            const float pp = pl0 + 32.f * q;
+            float v = fmaf(pp, fmaf(pp, A, -2.f * B), Cc), vd = 0.f;
 #pragma unroll
             for (int k = 0; k < kFarNodes; ++k) {
                 const float w = FT.L[k][32 * q + lane];
