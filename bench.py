@@ -320,8 +320,23 @@ def main():
                     help="run a small case of the Jacobian kernels for ncu: the 400k-line list with VP_Y "
                          "line mixing on CO2, two perturbed profiles, 645-1000 cm^-1, state T + log H2O + "
                          "log O3 + T_sfc, twice")
+    ap.add_argument("--profile-surrogate", action="store_true",
+                    help="run the MLP surrogate (152 -> 4 x 1024 -> 8461) on three batches of 4096 for ncu")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.profile_surrogate:
+        pkg = _package()
+        ctx = pkg.B200Context(0)
+        sur = pkg.Surrogate(ctx, n_in=152, n_hidden=1024, n_layers=4, n_out=8461, seed=1003)
+        X = np.random.default_rng(0).standard_normal((4096, 152)).astype(np.float32)
+        for _ in range(3):
+            t0 = time.perf_counter()
+            Y, ood = sur.predict(X)
+            print(json.dumps({"batch": 4096, "wall_s": time.perf_counter() - t0,
+                              "finite": bool(np.isfinite(Y).all())}), flush=True)
+        sur.close()
+        ctx.close()
+        return
     if args.profile_jacobian:
         pkg = _package()
         ctx = pkg.B200Context(0)

@@ -55,22 +55,26 @@ static CUtensorMap make_map(const void* ptr, int64_t rows, int64_t cols, int64_t
     return m;
 }
 
+constexpr int kTBN = 128;  // 128 x 128 tiles, two CTAs per SM
+
 template <int EPI>
 static void gemm(cudaStream_t st, const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int M, int N, int K,
                  umma::EpiArgs ep) {
+    using Cfg = umma::TileCfg<kTBN>;
     static bool attr = false;
     if (!attr) {
-        IRS_CUDA(cudaFuncSetAttribute(umma::umma_gemm_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)umma::kSmemBytes));
+        IRS_CUDA(cudaFuncSetAttribute(umma::umma_gemm_kernel<EPI, kTBN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)Cfg::kSmemBytes));
         attr = true;
     }
-    IRS_REQUIRE(M >= 1 && N >= 1 && K >= 1 && ep.ldc % 8 == 0, "GEMM sizes");
+    const bool f32_out = EPI == umma::EPI_F32 || EPI == umma::EPI_BIAS_F32;
+    IRS_REQUIRE(M >= 1 && N >= 1 && K >= 1 && ep.ldc >= N && (f32_out || ep.ldc % 8 == 0), "GEMM sizes");
     const CUtensorMap ta = make_map(A, M, K, lda, umma::BM);
-    const CUtensorMap tb = make_map(B, N, K, ldb, umma::BN);
+    const CUtensorMap tb = make_map(B, N, K, ldb, kTBN);
     ep.M = M;
     ep.N = N;
-    const dim3 grid((unsigned)((N + umma::BN - 1) / umma::BN), (unsigned)((M + umma::BM - 1) / umma::BM));
-    umma::umma_gemm_kernel<EPI><<<grid, umma::kThreads, umma::kSmemBytes, st>>>(ta, tb, K, ep);
+    const dim3 grid((unsigned)((N + kTBN - 1) / kTBN), (unsigned)((M + umma::BM - 1) / umma::BM));
+    umma::umma_gemm_kernel<EPI, kTBN><<<grid, umma::kThreads, Cfg::kSmemBytes, st>>>(ta, tb, K, ep);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) throw Error{IRS_E_CUDA, std::string("GEMM launch: ") + cudaGetErrorString(e)};
 }
@@ -169,26 +173,23 @@ __global__ void to_bf16_kernel(const float* __restrict__ w, int64_t n, bf16* __r
     if (i < n) o[i] = __float2bfloat16_rn(w[i]);
 }
 
-// BT[b][k] = y * sd + mean for k < n_out
-__global__ void unscale_kernel(const float* __restrict__ Y, int ldy, int n_out, int B, const float* __restrict__ ymean,
-                               const float* __restrict__ ysd, float* __restrict__ out) {
-    const int b = blockIdx.y;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= B || k >= n_out) return;
-    out[(size_t)b * n_out + k] = Y[(size_t)b * ldy + k] * ysd[k] + ymean[k];
-}
-
 // OOD score: |W (x - mean) / sd|^2 / n_in with W the whitening matrix of the scaled
-// training inputs (one warp per sample)
+// training inputs, stored transposed (WT[j][i] = W[i][j]) so that lanes read
+// consecutive rows; one warp per sample, its scaled input staged in shared memory
 __global__ void ood_kernel(const float* __restrict__ x, int n_in, int B, const float* __restrict__ mean,
-                           const float* __restrict__ sd, const float* __restrict__ W, float* __restrict__ score) {
-    const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+                           const float* __restrict__ sd, const float* __restrict__ WT, float* __restrict__ score) {
+    extern __shared__ float xs_all[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.x * (blockDim.x >> 5) + warp;
+    float* xs = xs_all + (size_t)warp * n_in;
+    if (b < B)
+        for (int j = lane; j < n_in; j += 32) xs[j] = (x[(size_t)b * n_in + j] - mean[j]) / sd[j];
+    __syncwarp();
     if (b >= B) return;
-    const float* xr = x + (size_t)b * n_in;
     float acc = 0.f;
     for (int i = lane; i < n_in; i += 32) {
         float s = 0.f;
-        for (int j = 0; j < n_in; ++j) s = fmaf(W[(size_t)i * n_in + j], (xr[j] - mean[j]) / sd[j], s);
+        for (int j = 0; j < n_in; ++j) s = fmaf(WT[(size_t)j * n_in + i], xs[j], s);
         acc = fmaf(s, s, acc);
     }
     for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -286,8 +287,9 @@ static void refresh_bf16(irs_surrogate* s) {
     IRS_CUDA(cudaGetLastError());
 }
 
-// forward pass of B rows already in act[0]; Y = scaled outputs
-static void forward(irs_surrogate* s, int B) {
+// forward pass of B rows already in act[0]; Y = scaled outputs, or with yout the
+// unscaled outputs y' y_sd + y_mean written straight to yout [B][ldy] (n_out columns)
+static void forward(irs_surrogate* s, int B, float* yout = nullptr, int ldy = 0) {
     const cudaStream_t st = s->stream;
     for (int l = 0; l < s->nl; ++l) {
         umma::EpiArgs ep{};
@@ -298,6 +300,12 @@ static void forward(irs_surrogate* s, int B) {
             ep.Z = s->z[l];
             ep.ldc = s->pout[l];
             gemm<umma::EPI_GELU_FWD>(st, s->act[l], s->pin[l], s->wb + s->woff[l], s->pin[l], B, s->pout[l], s->pin[l], ep);
+        } else if (yout) {
+            ep.Cf = yout;
+            ep.ldc = ldy;
+            ep.scale = s->ysd;
+            ep.shift = s->ymean;
+            gemm<umma::EPI_BIAS_F32>(st, s->act[l], s->pin[l], s->wb + s->woff[l], s->pin[l], B, s->n_out, s->pin[l], ep);
         } else {
             ep.Cf = s->Y;
             ep.ldc = s->pout[l];
@@ -498,7 +506,10 @@ int irs_surrogate_set_whitening(irs_surrogate* s, const float* W) {
     SG_BEGIN
     IRS_REQUIRE(s && W, "invalid arguments");
     IRS_CUDA(cudaSetDevice(s->device));
-    IRS_CUDA(cudaMemcpy(s->white, W, (size_t)s->n_in * s->n_in * sizeof(float), cudaMemcpyHostToDevice));
+    std::vector<float> wt((size_t)s->n_in * s->n_in);  // stored transposed for the OOD kernel
+    for (int i = 0; i < s->n_in; ++i)
+        for (int j = 0; j < s->n_in; ++j) wt[(size_t)j * s->n_in + i] = W[(size_t)i * s->n_in + j];
+    IRS_CUDA(cudaMemcpy(s->white, wt.data(), wt.size() * sizeof(float), cudaMemcpyHostToDevice));
     SG_END
 }
 
@@ -573,12 +584,10 @@ static void infer_device(irs_surrogate* s, const float* dX, int64_t n, float* dO
         const int nb = (int)std::min<int64_t>(B, n - b0);
         prep_input_kernel<<<nb, 256, 0, st>>>(dX + b0 * s->n_in, nullptr, s->n_in, s->pin[0], nb, s->xmean, s->xsd,
                                               s->act[0]);
-        forward(s, nb);
-        unscale_kernel<<<dim3((s->n_out + 255) / 256, nb), 256, 0, st>>>(s->Y, s->pout[s->nl - 1], s->n_out, nb,
-                                                                         s->ymean, s->ysd, dOut + b0 * s->n_out);
+        forward(s, nb, dOut + b0 * s->n_out, s->n_out);
         if (dOod)
-            ood_kernel<<<(nb * 32 + 255) / 256, 256, 0, st>>>(dX + b0 * s->n_in, s->n_in, nb, s->xmean, s->xsd,
-                                                              s->white, dOod + b0);
+            ood_kernel<<<(nb + 7) / 8, 256, 8 * s->n_in * sizeof(float), st>>>(dX + b0 * s->n_in, s->n_in, nb,
+                                                                               s->xmean, s->xsd, s->white, dOod + b0);
     }
     IRS_CUDA(cudaGetLastError());
 }

@@ -22,11 +22,18 @@
 namespace irs {
 namespace umma {
 
-constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
+// Tile shapes: BM x TBN x BK with TBN = 256 (4 stages, one CTA per SM) or TBN = 128
+// (3 stages, 97 KB of shared memory and 128 TMEM columns, two CTAs per SM so that one
+// CTA's epilogue overlaps the other's main loop).
+constexpr int BM = 128, BK = 64;
 constexpr int kThreads = 128;
 constexpr uint32_t kTileA = BM * BK * 2;  // 16 KB
-constexpr uint32_t kTileB = BN * BK * 2;  // 32 KB
-constexpr size_t kSmemBytes = STAGES * (kTileA + kTileB) + 1024 + 256;
+template <int TBN> struct TileCfg {
+    static constexpr int STAGES = TBN == 256 ? 4 : 3;
+    static constexpr uint32_t kTileB = TBN * BK * 2;
+    static constexpr size_t kSmemBytes = STAGES * (kTileA + kTileB) + 1024 + 256;
+    static constexpr int kMinBlocks = TBN == 256 ? 1 : 2;
+};
 constexpr uint32_t kMaxSpin = 1u << 22;
 
 enum Epilogue : int {
@@ -42,6 +49,8 @@ struct EpiArgs {
     __nv_bfloat16* Z;          // BF16 pre-activation output (GELU_FWD)
     const __nv_bfloat16* Zin;  // BF16 pre-activation input (GELU_BWD)
     const float* bias;
+    const float* scale;        // EPI_BIAS_F32, nullable: Cf = (acc + bias) * scale[n] + shift[n]
+    const float* shift;
     int ldc;                   // leading dimension of every output / Zin (elements)
     int M, N;
     int* err;
@@ -87,15 +96,20 @@ __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
     d |= (uint64_t)2 << 61;              // SWIZZLE_128B
     return d;
 }
-// kind::f16 instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = BN
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+// kind::f16 instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = TBN
+template <int TBN>
+struct IdescBf16 {
+    static constexpr uint32_t value =
+        (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TBN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+};
 
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate));
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
@@ -118,10 +132,14 @@ __device__ __forceinline__ float gelu_grad(float z) {
     return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
 }
 
-template <int EPI>
-__global__ void __launch_bounds__(kThreads, 1)
+template <int EPI, int TBN>
+__global__ void __launch_bounds__(kThreads, TileCfg<TBN>::kMinBlocks)
     umma_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int K,
                      EpiArgs ep) {
+    constexpr int BN = TBN;
+    constexpr int STAGES = TileCfg<TBN>::STAGES;
+    constexpr uint32_t kTileB = TileCfg<TBN>::kTileB;
+    constexpr uint32_t kIdesc = IdescBf16<TBN>::value;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint8_t* sA = smem;
@@ -181,7 +199,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t a0 = smem_u32(sA + s * kTileA), b0 = smem_u32(sB + s * kTileB);
 #pragma unroll
             for (int k = 0; k < BK / 16; ++k)
-                umma_bf16(tmem, sdesc_sw128(a0 + 32u * k), sdesc_sw128(b0 + 32u * k), (kt | k) != 0 ? 1u : 0u);
+                umma_bf16(tmem, sdesc_sw128(a0 + 32u * k), sdesc_sw128(b0 + 32u * k), kIdesc, (kt | k) != 0 ? 1u : 0u);
             umma_commit(&empty[s]);
         }
         umma_commit(done);  // arrives once every MMA issued above has completed
@@ -206,10 +224,13 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                 for (int i = 0; i < 16; ++i) {
                     float x = v[i];
-                    if (EPI == EPI_BIAS_F32 && (full16 || nb + i < ep.N)) x += ep.bias[nb + i];
+                    if (EPI == EPI_BIAS_F32 && (full16 || nb + i < ep.N)) {
+                        x += ep.bias[nb + i];
+                        if (ep.scale) x = fmaf(x, ep.scale[nb + i], ep.shift[nb + i]);
+                    }
                     v[i] = x;
                 }
-                if (full16) {
+                if (full16 && (ep.ldc & 3) == 0) {
                     float4* dst = (float4*)(ep.Cf + rowoff + nb);
 #pragma unroll
                     for (int i = 0; i < 4; ++i) dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
