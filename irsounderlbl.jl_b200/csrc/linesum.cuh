@@ -150,7 +150,22 @@ struct WarpTile {
     float ffg[32];  // far lines: g
     float4 eu[32];  // cutoff-edge lines (far field only): uh, ul, b2, a
     float4 ep[32];  // cutoff-edge lines: c1, c0, g, -
+    // mid lines (far field only) share su/sp/sq with the slow lines, from the top
+    // down (position 31 - k): su = (uh, ul, b2, a), sp = (c1, c0, fx, y),
+    // sq = (An, g, Yw, dfar2)
 };
+
+// Faddeeva w(z) for |x| + y >= 15 by the two-level Laplace continued fraction of
+// faddeeva32 (w = i/sqrt(pi) / (z - 1/2 / (z - 1/z))), written out in real arithmetic
+// with three MUFU reciprocals; returns (Re w, Im w)
+__device__ __forceinline__ float2 faddeeva_cf2(float x, float y, float y2) {
+    const float iz = rcp_fast(fmaf(x, x, y2));                 // 1/|z|^2
+    const float q1x = fmaf(-x, iz, x), q1y = fmaf(y, iz, y);   // z - 1/z
+    const float i1 = 0.5f * rcp_fast(fmaf(q1x, q1x, q1y * q1y));
+    const float qx = fmaf(-q1x, i1, x), qy = fmaf(q1y, i1, y); // z - (1/2)/(z - 1/z)
+    const float iq = (float)kInvSqrtPi * rcp_fast(fmaf(qx, qx, qy * qy));
+    return make_float2(qy * iq, qx * iq);
+}
 
 // Far field.  A fast line whose centre lies kFarDist or more points from the centre
 // of a warp's 256-point block contributes a function of the point index that is
@@ -269,11 +284,16 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             } else {
                 cls = 2;
                 a1 = lp.p1[q];
+                // mid: inside the cutoff, and |x| + y >= 15 at every point (the continued
+                // fraction of faddeeva32 or the far wing, no Weideman/CF4 region)
+                if (FAR && METHOD == 3 && dist + kHalf <= cut && fmaxf(dist - kHalf, 0.f) * a1.z + a1.w >= 15.05f)
+                    cls = 5;
             }
         }
         const unsigned fm = __ballot_sync(kFull, cls == 1), sm = __ballot_sync(kFull, cls == 2);
         const unsigned xm = FAR ? __ballot_sync(kFull, cls == 3) : 0u;
         const unsigned em = FAR ? __ballot_sync(kFull, cls == 4) : 0u;
+        const unsigned mm = FAR ? __ballot_sync(kFull, cls == 5) : 0u;
         __syncwarp();
         if (cls == 1) {
             const int pos = __popc(fm & lt);
@@ -287,6 +307,11 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             const int pos = __popc(em & lt);
             T.eu[pos] = make_float4(uh, ul, a0.x, a0.y);
             T.ep[pos] = make_float4(a0.z, a0.w, a2.x, 0.f);
+        } else if (FAR && cls == 5) {
+            const int pos = 31 - __popc(mm & lt);
+            T.su[pos] = make_float4(uh, ul, a0.x, a0.y);
+            T.sp[pos] = make_float4(a0.z, a0.w, a1.z, a1.w);
+            T.sq[pos] = make_float4(a1.y, a2.x, a2.y, a1.x);
         } else if (cls == 2) {
             const int pos = __popc(sm & lt);
             T.su[pos] = make_float4(uh, ul, a0.x, a0.y);
@@ -304,11 +329,11 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             Cc = warp_sum(pc);
         }
         __syncwarp();
-        const int nf = __popc(fm), ns = __popc(sm), ne = FAR ? __popc(em) : 0;
+        const int nf = __popc(fm), ns = __popc(sm), ne = FAR ? __popc(em) : 0, nm = FAR ? __popc(mm) : 0;
         if (FAR) {
             const int nx = __popc(xm);
             if (lane == 0)
-                work += (unsigned long long)(nf + ns + ne) * kMxWarpPts + (unsigned long long)nx * kFarNodes;
+                work += (unsigned long long)(nf + ns + ne + nm) * kMxWarpPts + (unsigned long long)nx * kFarNodes;
             float ft = 0.f, fd = 0.f;
             for (int k = lane >> 3; k < nx; k += 4) {
                 const float4 f = T.ff[k];
@@ -322,7 +347,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
         } else if (lane == 0) {
             work += (unsigned long long)(nf + ns) * kMxWarpPts;
         }
-        if (FAR && nf + ns + ne == 0) continue;  // warp-uniform: nothing per point in this tile
+        if (FAR && nf + ns + ne + nm == 0) continue;  // warp-uniform: nothing per point in this tile
         float2 acc2[kMxQ / 2];
         float tdsp[kMxQ];
 #pragma unroll
@@ -373,6 +398,30 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
         for (int h = 0; h < kMxQ / 2; ++h) {
             tacc[2 * h] = acc2[h].x;
             tacc[2 * h + 1] = acc2[h].y;
+        }
+        // mid lines: the far wing where |x| > x_far, else the continued fraction; the
+        // warp takes the continued fraction only for the 32-point rows that need it
+        for (int k = 0; k < nm; ++k) {
+            const float4 u = T.su[31 - k], pm = T.sp[31 - k], qm = T.sq[31 - k];
+            const float y2 = pm.w * pm.w;
+#pragma unroll
+            for (int q = 0; q < kMxQ; ++q) {
+                const float d = ((pl0 + 32.f * q) - u.x) - u.y;
+                const float d2 = d * d;
+                const float ped = fmaf(pm.x, d2, pm.y);
+                const float r = rcp_fast(d2 + u.z);
+                float v = fmaf(u.w, r, ped), vd = qm.y * d * r;
+                const bool core = d2 <= qm.w;
+                if (__any_sync(kFull, core)) {
+                    const float2 w = faddeeva_cf2(d * pm.z, pm.w, y2);
+                    if (core) {
+                        v = fmaf(qm.x, w.x, ped);
+                        vd = qm.z * w.y;
+                    }
+                }
+                tacc[q] += v;
+                if (LM) tdsp[q] += vd;
+            }
         }
         for (int k = 0; k < ns; ++k) {
             const float4 u = T.su[k];

@@ -187,10 +187,17 @@ __global__ void ood_kernel(const float* __restrict__ x, int n_in, int B, const f
     __syncwarp();
     if (b >= B) return;
     float acc = 0.f;
-    for (int i = lane; i < n_in; i += 32) {
-        float s = 0.f;
-        for (int j = 0; j < n_in; ++j) s = fmaf(WT[(size_t)j * n_in + i], xs[j], s);
-        acc = fmaf(s, s, acc);
+    for (int i0 = lane; i0 < n_in; i0 += 32 * 4) {  // four rows per pass: independent FMA chains
+        float s[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int j = 0; j < n_in; ++j) {
+            const float xj = xs[j];
+            const float* w = WT + (size_t)j * n_in;
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if (i0 + 32 * r < n_in) s[r] = fmaf(w[i0 + 32 * r], xj, s[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc = fmaf(s[r], s[r], acc);
     }
     for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) score[b] = acc / (float)n_in;

@@ -216,8 +216,32 @@ __global__ void __launch_bounds__(kThreads, TileCfg<TBN>::kMinBlocks)
             if (n0 + c0 >= ep.N) break;  // warp-uniform
             float v[16];
             tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-            if (!row_ok) continue;
             const int nb = n0 + c0;
+            if ((EPI == EPI_F32 || EPI == EPI_BIAS_F32) && (ep.ldc & 3) != 0) {
+                // rows not 16-byte aligned: stage the warp's 32 x 16 chunk in shared memory
+                // (the operand ring is idle now) and write each row's 64 bytes contiguously,
+                // two rows per store instruction
+                float* stg = (float*)smem + warp * (32 * 17);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    float x = v[i];
+                    if (EPI == EPI_BIAS_F32 && nb + i < ep.N) {
+                        x += ep.bias[nb + i];
+                        if (ep.scale) x = fmaf(x, ep.scale[nb + i], ep.shift[nb + i]);
+                    }
+                    stg[lane * 17 + i] = x;
+                }
+                __syncwarp();
+                const int col = lane & 15, half = lane >> 4;
+#pragma unroll 4
+                for (int rr = 0; rr < 32; rr += 2) {
+                    const int r = rr + half, mr = m0 + warp * 32 + r;
+                    if (mr < ep.M && nb + col < ep.N) ep.Cf[(size_t)mr * ep.ldc + nb + col] = stg[r * 17 + col];
+                }
+                __syncwarp();
+                continue;
+            }
+            if (!row_ok) continue;
             const size_t rowoff = (size_t)m * ep.ldc;
             const bool full16 = nb + 16 <= ep.N;
             if (EPI == EPI_F32 || EPI == EPI_BIAS_F32) {

@@ -54,7 +54,7 @@ def test_gemm_bf16(pkg, ctx, M, N, K):
 
 def test_surrogate_gradients_vs_oracle(pkg, ctx):
     import mlp_oracle as mo
-    n_in, hid, nl, n_out = 152, 64, 2, 100
+    n_in, hid, nl, n_out = 152, 64, 2, 101  # 101 outputs: rows of the output not 16-byte aligned
     s = pkg.Surrogate(ctx, n_in=n_in, n_hidden=hid, n_layers=nl, n_out=n_out, seed=11)
     rng = np.random.default_rng(3)
     X = rng.normal(0, 1, (96, n_in)).astype(np.float32)
@@ -66,8 +66,10 @@ def test_surrogate_gradients_vs_oracle(pkg, ctx):
     g, loss = s.gradients(X, Y)
     dims = [n_in] + [hid] * nl + [n_out]
     z = np.zeros
-    lo, go, _ = mo.forward_backward(p, dims, X, Y, z(n_in), np.ones(n_in), z(n_out), np.ones(n_out), bf16=True)
+    lo, go, out = mo.forward_backward(p, dims, X, Y, z(n_in), np.ones(n_in), z(n_out), np.ones(n_out), bf16=True)
     assert abs(loss - lo) <= 1e-3 * lo
+    P, _ = s.predict(X)  # inference writes the unscaled outputs straight from the GEMM epilogue
+    assert np.max(np.abs(P - out)) <= 5e-3 * np.max(np.abs(out))
     k = 0
     for o, i in [(dims[l + 1], dims[l]) for l in range(len(dims) - 1)]:
         for size in (o * i, o):
