@@ -268,7 +268,8 @@ int irs_surrogate_set_scaling(irs_surrogate* s, const float* x_mean, const float
                               const float* y_sd);
 /* OOD score of a sample = |W x'|^2 / n_in with W [n_in][n_in] the whitening matrix */
 int irs_surrogate_set_whitening(irs_surrogate* s, const float* W);
-/* epochs of Adam on 0.5 mean((y' - t')^2) over full mini-batches of a shuffled set */
+/* epochs of Adam on 0.5 mean((y' - t')^2) over full mini-batches of a shuffled set, the
+ * learning rate following a cosine schedule from lr down to lr / 100 */
 int irs_surrogate_train(irs_surrogate* s, const float* X, const float* Y, int64_t n, int batch, int epochs,
                         float lr, uint64_t seed, double* loss_per_epoch);
 /* loss and its gradient (same layout as the parameters) on one batch, no update */

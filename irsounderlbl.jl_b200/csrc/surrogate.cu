@@ -173,36 +173,6 @@ __global__ void to_bf16_kernel(const float* __restrict__ w, int64_t n, bf16* __r
     if (i < n) o[i] = __float2bfloat16_rn(w[i]);
 }
 
-// OOD score: |W (x - mean) / sd|^2 / n_in with W the whitening matrix of the scaled
-// training inputs, stored transposed (WT[j][i] = W[i][j]) so that lanes read
-// consecutive rows; one warp per sample, its scaled input staged in shared memory
-__global__ void ood_kernel(const float* __restrict__ x, int n_in, int B, const float* __restrict__ mean,
-                           const float* __restrict__ sd, const float* __restrict__ WT, float* __restrict__ score) {
-    extern __shared__ float xs_all[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = blockIdx.x * (blockDim.x >> 5) + warp;
-    float* xs = xs_all + (size_t)warp * n_in;
-    if (b < B)
-        for (int j = lane; j < n_in; j += 32) xs[j] = (x[(size_t)b * n_in + j] - mean[j]) / sd[j];
-    __syncwarp();
-    if (b >= B) return;
-    float acc = 0.f;
-    for (int i0 = lane; i0 < n_in; i0 += 32 * 4) {  // four rows per pass: independent FMA chains
-        float s[4] = {0.f, 0.f, 0.f, 0.f};
-        for (int j = 0; j < n_in; ++j) {
-            const float xj = xs[j];
-            const float* w = WT + (size_t)j * n_in;
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-                if (i0 + 32 * r < n_in) s[r] = fmaf(w[i0 + 32 * r], xj, s[r]);
-        }
-#pragma unroll
-        for (int r = 0; r < 4; ++r) acc = fmaf(s[r], s[r], acc);
-    }
-    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) score[b] = acc / (float)n_in;
-}
-
 inline int64_t pad64(int64_t n) { return (n + 63) / 64 * 64; }
 
 }  // namespace sg
@@ -222,7 +192,8 @@ struct irs_surrogate {
     int64_t n_par = 0;
     float *w = nullptr, *m = nullptr, *v = nullptr, *g = nullptr;
     bf16 *wb = nullptr, *wt = nullptr;  // BF16 weights [pout][pin] and transposes [pin][pout] (same offsets)
-    float *xmean = nullptr, *xsd = nullptr, *ymean = nullptr, *ysd = nullptr, *white = nullptr;
+    float *xmean = nullptr, *xsd = nullptr, *ymean = nullptr, *ysd = nullptr;
+    bf16* white_b = nullptr;  // whitening matrix, BF16 [n_in][pin0], for the tensor-core OOD score
     int* err = nullptr;
     double* loss = nullptr;
     int64_t t_step = 0;
@@ -367,6 +338,19 @@ static void backward(irs_surrogate* s, int B, const float* t, const int* idx) {
     }                                                \
     return IRS_OK;
 
+static void upload_white_bf16(irs_surrogate* s, const float* W) {
+    const int ld = s->pin[0];
+    std::vector<uint16_t> h((size_t)s->n_in * ld, 0);
+    for (int i = 0; i < s->n_in; ++i)
+        for (int j = 0; j < s->n_in; ++j) {
+            uint32_t u;
+            std::memcpy(&u, &W[(size_t)i * s->n_in + j], 4);
+            h[(size_t)i * ld + j] = (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);  // round to nearest even
+        }
+    if (!s->white_b) s->white_b = (bf16*)dmalloc(h.size() * sizeof(bf16));
+    IRS_CUDA(cudaMemcpy(s->white_b, h.data(), h.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+}
+
 extern "C" {
 
 int irs_surrogate_create(irs_ctx* ctx, int n_in, int n_hidden, int n_layers, int n_out, uint64_t seed,
@@ -415,14 +399,13 @@ int irs_surrogate_create(irs_ctx* ctx, int n_in, int n_hidden, int n_layers, int
     s->xsd = (float*)dmalloc(n_in * sizeof(float));
     s->ymean = (float*)dmalloc(n_out * sizeof(float));
     s->ysd = (float*)dmalloc(n_out * sizeof(float));
-    s->white = (float*)dmalloc((size_t)n_in * n_in * sizeof(float));
     IRS_CUDA(cudaMemcpy(s->xmean, zeros.data(), n_in * sizeof(float), cudaMemcpyHostToDevice));
     IRS_CUDA(cudaMemcpy(s->xsd, ones.data(), n_in * sizeof(float), cudaMemcpyHostToDevice));
     IRS_CUDA(cudaMemcpy(s->ymean, zeros.data(), n_out * sizeof(float), cudaMemcpyHostToDevice));
     IRS_CUDA(cudaMemcpy(s->ysd, ones.data(), n_out * sizeof(float), cudaMemcpyHostToDevice));
     std::vector<float> eye((size_t)n_in * n_in, 0.f);
     for (int i = 0; i < n_in; ++i) eye[(size_t)i * n_in + i] = 1.f;
-    IRS_CUDA(cudaMemcpy(s->white, eye.data(), eye.size() * sizeof(float), cudaMemcpyHostToDevice));
+    upload_white_bf16(s.get(), eye.data());
     refresh_bf16(s.get());
     IRS_CUDA(cudaStreamSynchronize(s->stream));
     *out = s.release();
@@ -436,7 +419,7 @@ int irs_surrogate_destroy(irs_surrogate* s) {
     cudaStreamSynchronize(s->stream);
     for (auto p : s->act) cudaFree(p);
     for (auto p : s->z) cudaFree(p);
-    void* bufs[] = {s->w, s->m, s->v, s->g, s->wb, s->wt, s->xmean, s->xsd, s->ymean, s->ysd, s->white, s->err,
+    void* bufs[] = {s->w, s->m, s->v, s->g, s->wb, s->wt, s->xmean, s->xsd, s->ymean, s->ysd, s->white_b, s->err,
                     s->loss, s->Y, s->dY, s->dZa, s->dZb, s->T1, s->T2, s->dx, s->dt, s->didx, s->dout_buf, s->dood};
     for (void* p : bufs)
         if (p) cudaFree(p);
@@ -513,10 +496,7 @@ int irs_surrogate_set_whitening(irs_surrogate* s, const float* W) {
     SG_BEGIN
     IRS_REQUIRE(s && W, "invalid arguments");
     IRS_CUDA(cudaSetDevice(s->device));
-    std::vector<float> wt((size_t)s->n_in * s->n_in);  // stored transposed for the OOD kernel
-    for (int i = 0; i < s->n_in; ++i)
-        for (int j = 0; j < s->n_in; ++j) wt[(size_t)j * s->n_in + i] = W[(size_t)i * s->n_in + j];
-    IRS_CUDA(cudaMemcpy(s->white, wt.data(), wt.size() * sizeof(float), cudaMemcpyHostToDevice));
+    upload_white_bf16(s, W);
     SG_END
 }
 
@@ -537,6 +517,11 @@ int irs_surrogate_train(irs_surrogate* s, const float* X, const float* Yt, int64
     std::vector<int> perm((size_t)n);
     std::mt19937_64 rng(seed);
     for (int ep = 0; ep < epochs; ++ep) {
+        // cosine learning-rate schedule from lr down to lr / 100 over the epochs
+        const float lr_min = 0.01f * lr;
+        const float lr_ep = epochs > 1 ? lr_min + 0.5f * (lr - lr_min) *
+                                                      (1.f + std::cos(3.14159265f * (float)ep / (float)(epochs - 1)))
+                                       : lr;
         std::iota(perm.begin(), perm.end(), 0);
         std::shuffle(perm.begin(), perm.end(), rng);
         IRS_CUDA(cudaMemcpyAsync(s->didx, perm.data(), perm.size() * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -550,8 +535,8 @@ int irs_surrogate_train(irs_surrogate* s, const float* X, const float* Yt, int64
             s->t_step += 1;
             const float b1 = 0.9f, b2 = 0.999f;
             const float c1 = 1.f - std::pow(b1, (float)s->t_step), c2 = 1.f - std::pow(b2, (float)s->t_step);
-            adam_kernel<<<(unsigned)((s->n_par + 255) / 256), 256, 0, st>>>(s->w, s->m, s->v, s->g, s->n_par, lr, b1,
-                                                                             b2, 1e-8f, c1, c2);
+            adam_kernel<<<(unsigned)((s->n_par + 255) / 256), 256, 0, st>>>(s->w, s->m, s->v, s->g, s->n_par, lr_ep,
+                                                                             b1, b2, 1e-8f, c1, c2);
             refresh_bf16(s);
         }
         double l = 0.0;
@@ -591,10 +576,15 @@ static void infer_device(irs_surrogate* s, const float* dX, int64_t n, float* dO
         const int nb = (int)std::min<int64_t>(B, n - b0);
         prep_input_kernel<<<nb, 256, 0, st>>>(dX + b0 * s->n_in, nullptr, s->n_in, s->pin[0], nb, s->xmean, s->xsd,
                                               s->act[0]);
+        if (dOod) {  // |W x'|^2 / n_in on the tensor cores from the BF16 scaled inputs
+            IRS_CUDA(cudaMemsetAsync(dOod + b0, 0, (size_t)nb * sizeof(float), st));
+            umma::EpiArgs eo{};
+            eo.Cf = dOod + b0;
+            eo.ldc = s->n_in;
+            eo.err = s->err;
+            gemm<umma::EPI_SUMSQ>(st, s->act[0], s->pin[0], s->white_b, s->pin[0], nb, s->n_in, s->pin[0], eo);
+        }
         forward(s, nb, dOut + b0 * s->n_out, s->n_out);
-        if (dOod)
-            ood_kernel<<<(nb + 7) / 8, 256, 8 * s->n_in * sizeof(float), st>>>(dX + b0 * s->n_in, s->n_in, nb,
-                                                                               s->xmean, s->xsd, s->white, dOod + b0);
     }
     IRS_CUDA(cudaGetLastError());
 }

@@ -41,6 +41,7 @@ enum Epilogue : int {
     EPI_BIAS_F32 = 1,   // Cf[m][n] = acc + bias[n]
     EPI_GELU_FWD = 2,   // Z[m][n] = acc + bias[n] (bf16), Cb[m][n] = gelu(Z) (bf16)
     EPI_GELU_BWD = 3,   // Cb[m][n] = acc * gelu'(Zin[m][n]) (bf16)
+    EPI_SUMSQ = 4,      // Cf[m] += sum_n acc^2 / N (Cf zeroed by the caller)
 };
 
 struct EpiArgs {
@@ -217,6 +218,14 @@ __global__ void __launch_bounds__(kThreads, TileCfg<TBN>::kMinBlocks)
             float v[16];
             tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
             const int nb = n0 + c0;
+            if (EPI == EPI_SUMSQ) {
+                float ss = 0.f;
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    if (nb + i < ep.N) ss = fmaf(v[i], v[i], ss);
+                if (row_ok) atomicAdd(ep.Cf + m, ss / (float)ep.N);
+                continue;
+            }
             if ((EPI == EPI_F32 || EPI == EPI_BIAS_F32) && (ep.ldc & 3) != 0) {
                 // rows not 16-byte aligned: stage the warp's 32 x 16 chunk in shared memory
                 // (the operand ring is idle now) and write each row's 64 bytes contiguously,
