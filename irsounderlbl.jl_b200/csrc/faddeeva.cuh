@@ -154,6 +154,33 @@ static __device__ __noinline__ float2 faddeeva32(float x, float y) {
     return make_float2(t1.x + t2.x, t1.y + t2.y);
 }
 
+// 1/x by the MUFU approximation (about 1 ulp); x > 0 and finite where it is used
+__device__ __forceinline__ float rcp_approx32(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// Faddeeva w(z) for |x| + y >= 15 by the two-level Laplace continued fraction of
+// faddeeva32 (w = i/sqrt(pi) / (z - 1/2 / (z - 1/z))), written out in real arithmetic
+// with three MUFU reciprocals; returns (Re w, Im w)
+__device__ __forceinline__ float2 faddeeva_cf2(float x, float y, float y2) {
+    const float iz = rcp_approx32(fmaf(x, x, y2));                 // 1/|z|^2
+    const float q1x = fmaf(-x, iz, x), q1y = fmaf(y, iz, y);   // z - 1/z
+    const float i1 = 0.5f * rcp_approx32(fmaf(q1x, q1x, q1y * q1y));
+    const float qx = fmaf(-q1x, i1, x), qy = fmaf(q1y, i1, y); // z - (1/2)/(z - 1/z)
+    const float iq = (float)kInvSqrtPi * rcp_approx32(fmaf(qx, qx, qy * qy));
+    return make_float2(qy * iq, qx * iq);
+}
+
+
+// faddeeva32 with its |x| + y >= 15 branch (the two-level continued fraction) inlined
+// in real arithmetic; the CF4 and Weideman regions go through the shared routine
+__device__ __forceinline__ float2 faddeeva32_fast(float x, float y) {
+    if (fabsf(x) + y >= 15.0f) return faddeeva_cf2(x, y, y * y);
+    return faddeeva32(x, y);
+}
+
 // voigt.jl:105-117 (Float32 Weideman-24, IEEE division as Julia's Float32 `/`)
 static __device__ __noinline__ float weideman24_32(float x, float y) {
     float A = 0.0f, B = 0.0f;

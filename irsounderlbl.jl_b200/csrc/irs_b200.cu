@@ -176,6 +176,11 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
     LpConfig cfg;
     cfg.cutoff = o.cutoff; cfg.x_far = o.x_far; cfg.dptmn = o.dptmn;
     cfg.grid0 = grid0; cfg.dnu_g = dnu_g; cfg.method = o.method; cfg.n_nu = n_nu;
+    {  // shifted centres within the grid plus its cutoff margins: |U| < 2^24 u_gran
+        const double reach = (double)n_nu + 2.0 * o.cutoff / dnu_g + 64.0;
+        cfg.u_gran = 1.0 / 16.0;
+        while (reach >= 16777216.0 * cfg.u_gran) cfg.u_gran *= 2.0;
+    }
     const TipsDev tp = tips_dev(ctx);
     dim3 g1(n_chunks, nseg);
     lp_keep_kernel<<<g1, kLpThreads, 0, st>>>(d_segs, d_lists, tp, cfg, d_keep, d_chunk, n_chunks);
@@ -192,7 +197,7 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
     } else {
         char* base = (char*)workspace(ctx, "lpmx", S * (8 + 8 + 16 + 16 + 16));
         om.V = (double*)base;
-        om.U = (double*)(base + S * 8);
+        om.U = (float2*)(base + S * 8);
         om.p0 = (float4*)(base + S * 16);
         om.p1 = (float4*)(base + S * 32);
         om.p2 = (float4*)(base + S * 48);
@@ -465,7 +470,7 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
         IRS_CUDA(cudaMemsetAsync(d_out, 0, (size_t)np * L * n_out * n_nu * sizeof(float), st));
         if (nseg > 0) {
             LpConfig cfg;
-            cfg.cutoff = o.cutoff; cfg.x_far = o.x_far; cfg.dptmn = 0.0; cfg.grid0 = ig.g.at(0);
+            cfg.cutoff = o.cutoff; cfg.x_far = o.x_far; cfg.dptmn = 0.0; cfg.grid0 = ig.g.at(0); cfg.u_gran = 1.0 / 16.0;
             cfg.dnu_g = ig.dnu_hi; cfg.method = o.method; cfg.n_nu = n_nu;
             jg_params_kernel<<<dim3((unsigned)((max_list + 255) / 256), nseg), 256, 0, st>>>(d_segs, d_lists, tips_dev(ctx), cfg, go);
             check_launch(ctx);

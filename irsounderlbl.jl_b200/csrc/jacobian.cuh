@@ -139,7 +139,7 @@ __device__ __forceinline__ void jg_pair(float d, bool core, const float4& q0, co
     const float xp = -fx * q2.y, xv = -fx * q3.y;
     float H, Hx, Hy, Lw = 0.f, Lx = 0.f, Ly = 0.f;
     if (core) {
-        const float2 w = faddeeva32(x, y);
+        const float2 w = faddeeva32_fast(x, y);
         H = w.x;
         Hx = -2.f * x * w.x + 2.f * y * w.y;
         Hy = 2.f * (x * w.y + y * w.x) - 2.f * (float)kInvSqrtPi;

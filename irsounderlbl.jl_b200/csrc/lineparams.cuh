@@ -43,6 +43,7 @@ struct LpConfig {
     double cutoff, x_far, dptmn;
     double grid0, dnu_g;  // grid start and spacing (mixed parameters are in grid units)
     long long n_nu;       // grid points (for the pair counts)
+    double u_gran;        // granularity of the FP32 high part of the shifted centres (mixed)
     int method;           // 1 Weideman, 2 PseudoVoigt, 3 FullFaddeeva
 };
 
@@ -77,9 +78,9 @@ __device__ __forceinline__ LinePhys line_phys(const ListDev& L, long long j, con
     const double n_air = L.nair[j];
     const double n_self = mol == 1 ? 0.95 : (mol == 2 ? 0.75 : n_air);        // broadening.jl:17-20
     const double d_self = mol == 1 ? 0.002 : (mol == 2 ? -0.003 : 0.0);        // :21-24
-    const double tr = 296.0 / T;
+    const double ln_tr = log(296.0 / T);  // (296/T)^n as exp(n ln(296/T)): one exp per exponent
     LinePhys o;
-    o.gl = pow(tr, n_air) * L.gair[j] * (1.0 - vs) * p + pow(tr, n_self) * L.gself[j] * vs * p;
+    o.gl = exp(n_air * ln_tr) * L.gair[j] * (1.0 - vs) * p + exp(n_self * ln_tr) * L.gself[j] * vs * p;
     o.gd = nu * 3.58126e-7 * sqrt(T / mol_mass(mol));
     const int ti = L.tips[j];
     const double Qr = ti >= 0 ? tips_lookup(tp, ti, 296.0) / tips_lookup(tp, ti, T) : 296.0 / T;
@@ -129,10 +130,19 @@ struct LpOutF64 {
     double *nu0, *f, *y, *Sn, *Hc, *YSn;
 };
 struct LpOutMixed {
-    double *V, *U;
+    double* V;   // unshifted centre, grid units (the sorted key of the window searches)
+    float2* U;   // shifted centre, grid units, as hi + lo: hi = (float)U, lo = (float)(U - hi)
     float4 *p0, *p1;
     float4* p2;
 };
+// U as hi + lo with hi a multiple of the power of two g (LpConfig::u_gran, chosen so
+// that |U| < 2^24 g over the grid and its cutoff margin): for an integer grid index w,
+// hi - w is then a multiple of g below 2^24 g in magnitude, exact in FP32, so the
+// kernels get U - w as (hi - w) + lo without FP64 arithmetic (|lo| <= g/2)
+__device__ __forceinline__ float2 split_hi_lo(double u, double g) {
+    const double h = rint(u / g) * g;
+    return make_float2((float)h, (float)(u - h));
+}
 
 // Pass B: compacted parameters.  PREC 0 -> FP64 arrays, 1 -> mixed arrays.
 template <int PREC>
@@ -222,7 +232,7 @@ __global__ void __launch_bounds__(kLpThreads) lp_write_kernel(
                     const double dg = cfg.dnu_g, co = sg.coef;
                     const double gVg = gV / dg;
                     om.V[slot] = (L.nu[j] - cfg.grid0) / dg;
-                    om.U[slot] = (ph.nu0s - cfg.grid0) / dg;
+                    om.U[slot] = split_hi_lo((ph.nu0s - cfg.grid0) / dg, cfg.u_gran);
                     const double P = basev * co;
                     om.p0[slot] = make_float4((float)(gVg * gVg), (float)(ph.S * co * eta * gVg / (M_PI * dg)),
                                               (float)(P * (dg / c) * (dg / c)), (float)(-2.0 * P));
@@ -245,7 +255,7 @@ __global__ void __launch_bounds__(kLpThreads) lp_write_kernel(
                     const double P = An * Hc;         // pedestal scale
                     const double Yw = YSn * co;
                     om.V[slot] = (L.nu[j] - cfg.grid0) / dg;
-                    om.U[slot] = (ph.nu0s - cfg.grid0) / dg;
+                    om.U[slot] = split_hi_lo((ph.nu0s - cfg.grid0) / dg, cfg.u_gran);
                     // b^2 floored at 1e-12 grid units^2 (gamma_L ~ 1e-9 cm^-1) so the far-wing
                     // denominators stay normal in FP32 even at p -> 0
                     const double b2 = fmax((y / fx) * (y / fx), 1e-12);

@@ -155,17 +155,6 @@ struct WarpTile {
     // sq = (An, g, Yw, dfar2)
 };
 
-// Faddeeva w(z) for |x| + y >= 15 by the two-level Laplace continued fraction of
-// faddeeva32 (w = i/sqrt(pi) / (z - 1/2 / (z - 1/z))), written out in real arithmetic
-// with three MUFU reciprocals; returns (Re w, Im w)
-__device__ __forceinline__ float2 faddeeva_cf2(float x, float y, float y2) {
-    const float iz = rcp_fast(fmaf(x, x, y2));                 // 1/|z|^2
-    const float q1x = fmaf(-x, iz, x), q1y = fmaf(y, iz, y);   // z - 1/z
-    const float i1 = 0.5f * rcp_fast(fmaf(q1x, q1x, q1y * q1y));
-    const float qx = fmaf(-q1x, i1, x), qy = fmaf(q1y, i1, y); // z - (1/2)/(z - 1/z)
-    const float iq = (float)kInvSqrtPi * rcp_fast(fmaf(qx, qx, qy * qy));
-    return make_float2(qy * iq, qx * iq);
-}
 
 // Far field.  A fast line whose centre lies kFarDist or more points from the centre
 // of a warp's 256-point block contributes a function of the point index that is
@@ -266,9 +255,9 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
         float uh = 0.f, ul = 0.f;
         if (lane < nt) {
             const long long q = sg.off + t0 + lane;
-            const double u = lp.U[q] - (double)wb;
-            uh = (float)u;
-            ul = (float)(u - (double)uh);
+            const float2 uf = lp.U[q];
+            uh = uf.x - (float)wb;  // exact: see split_hi_lo
+            ul = uf.y;
             a0 = lp.p0[q];
             a2 = lp.p2[q];
             const float dist = fabsf(uh - kCentre);
@@ -440,7 +429,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
                         v = fmaf(p.w, weideman24_32(x, w.y), ped);
                         vd = 0.f;
                     } else {
-                        const float2 fw = faddeeva32(x, w.y);
+                        const float2 fw = faddeeva32_fast(x, w.y);
                         v = fmaf(p.w, fw.x, ped);
                         vd = w.w * fw.y;
                     }
@@ -513,11 +502,11 @@ __device__ __forceinline__ void warp_segment_pv(const SegDev& sg, long long cnt,
         __syncwarp();
         if (lane < nt) {
             const long long q = sg.off + t0 + lane;
-            const double u = lp.U[q] - (double)wb;
-            const float uh = (float)u;
+            const float2 uf = lp.U[q];
+            const float uh = uf.x - (float)wb;  // exact: see split_hi_lo
             const float dist = fabsf(uh - kCentre);
             const float cls = dist > cut + kHalf ? 0.f : (dist + kHalf <= cut ? 1.f : 2.f);
-            T.fu[lane] = make_float4(uh, (float)(u - (double)uh), 0.f, cls);
+            T.fu[lane] = make_float4(uh, uf.y, 0.f, cls);
             T.su[lane] = lp.p0[q];
             T.sp[lane] = lp.p1[q];
         }
