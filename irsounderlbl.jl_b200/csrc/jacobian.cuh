@@ -274,13 +274,14 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
             const float dist = fabsf(uh - kCentre);
             if (dist > cut + kHalf) cls = 0;
             else if (dist + kHalf <= cut && dist > a2.w + kHalf) cls = dist >= kJgFarDist ? 3 : 1;
+            else if (dist > a2.w + kHalf) cls = 4;  // far wing everywhere, the cutoff falls among the points
             else cls = 2;
         }
         const unsigned fm = __ballot_sync(kFull, cls == 1), sm = __ballot_sync(kFull, cls == 2);
-        const unsigned xm = __ballot_sync(kFull, cls == 3);
+        const unsigned xm = __ballot_sync(kFull, cls == 3), em = __ballot_sync(kFull, cls == 4);
         __syncwarp();
-        if (cls == 1 || cls == 3) {  // fast lines first, far lines after them
-            const int pos = cls == 1 ? __popc(fm & lt) : __popc(fm) + __popc(xm & lt);
+        if (cls == 1 || cls == 3 || cls == 4) {  // fast lines first, far lines after them, edge lines from the top
+            const int pos = cls == 1 ? __popc(fm & lt) : (cls == 3 ? __popc(fm) + __popc(xm & lt) : 31 - __popc(em & lt));
             const float An = a0.x, fx = a0.y, y = a0.z, Hc = a0.w;
             const float AnT = a1.x, fxT = a1.y, yT = a1.z, HcT = a1.w;
             const float yp = a2.x, up = a2.y, Hcp = a2.z, yv = a3.x, uv = a3.y, Hcv = a3.z;
@@ -302,18 +303,23 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
             }
             // pedestals: -P0 pf, -PT pf, -An Hc pf_p - An Hc_p pf, ... with pf = 2 - (i - u)^2 / c^2
             const float P[4] = {An * Hc, AnT * Hc + An * HcT, An * Hcp, An * Hcv};
-            const float e0 = 2.f - uh * uh * icut2, e1 = 2.f * uh * icut2;
+            if (cls == 4) {  // edge lines: pedestals per point (masked by the cutoff), in the slow arrays' top
+                T.q0[pos] = make_float4(P[0], P[1], P[2], P[3]);
+                T.q1[pos] = make_float4(2.f * up * icut2 * P[0], 2.f * uv * icut2 * P[0], 0.f, 0.f);
+            } else {
+                const float e0 = 2.f - uh * uh * icut2, e1 = 2.f * uh * icut2;
 #pragma unroll
-            for (int o = 0; o < 4; ++o) {
-                pA[o] = -P[o] * e0;
-                pB[o] = -P[o] * e1;
-                pC[o] = P[o] * icut2;
+                for (int o = 0; o < 4; ++o) {
+                    pA[o] = -P[o] * e0;
+                    pB[o] = -P[o] * e1;
+                    pC[o] = P[o] * icut2;
             }
-            const float shp = 2.f * An * Hc * icut2;  // pf_p = 2 (i - u) u_p / c^2
-            pA[2] += shp * up * uh;
-            pB[2] -= shp * up;
-            pA[3] += shp * uv * uh;
-            pB[3] -= shp * uv;
+                const float shp = 2.f * An * Hc * icut2;  // pf_p = 2 (i - u) u_p / c^2
+                pA[2] += shp * up * uh;
+                pB[2] -= shp * up;
+                pA[3] += shp * uv * uh;
+                pB[3] -= shp * uv;
+            }
         } else if (cls == 2) {
             const int pos = __popc(sm & lt);
             T.su[pos] = make_float4(uh, ul, 0.f, a2.w * a2.w);
@@ -333,7 +339,7 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
             QC[o] += pC[o];
         }
         __syncwarp();
-        const int nf = __popc(fm), ns = __popc(sm), nx = __popc(xm);
+        const int nf = __popc(fm), ns = __popc(sm), nx = __popc(xm), ne = __popc(em);
         {
             float ts = 0.f, td = 0.f;
             for (int kk = nf + (lane >> 3); kk < nf + nx; kk += 4) {
@@ -356,7 +362,7 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
             kahan_add(fS, fC, ts);
             if (LM) kahan_add(fD, fDC, td);
         }
-        if (nf + ns == 0) continue;  // warp-uniform: nothing per point in this tile
+        if (nf + ns + ne == 0) continue;  // warp-uniform: nothing per point in this tile
         float2 TS[kJgQ / 2], TD[kJgQ / 2];  // tile partials of the value sums (Kahan-added below)
 #pragma unroll
         for (int h = 0; h < kJgQ / 2; ++h) TS[h] = TD[h] = make_float2(0.f, 0.f);
@@ -396,6 +402,44 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
                     SDP[h] = __ffma2_rn(make_float2(l1.x, l1.x), rho, SDP[h]);
                     SDP[h] = __ffma2_rn(make_float2(l1.y, l1.y), rho2, SDP[h]);
                     SDP[h] = __ffma2_rn(make_float2(l1.z, l1.z), drho2, SDP[h]);
+                }
+            }
+        }
+        // cutoff-edge lines: the far-wing coefficients and the per-point pedestals,
+        // masked to the points inside the cutoff
+        for (int e = 0; e < ne; ++e) {
+            const int kk = 31 - e;
+            const float4 f0 = T.fu[kk], f1 = T.fT[kk], f2 = T.fp[kk], P = T.q0[kk], c = T.q1[kk];
+            float4 l0, l1;
+            if (LM) {
+                l0 = T.fL0[kk];
+                l1 = T.fL1[kk];
+            }
+            const float d0 = (pl0 - f0.x) - f0.y;
+#pragma unroll
+            for (int q = 0; q < kJgQ; ++q) {
+                const float d = d0 + 32.f * q, d2 = d * d;
+                if (d2 > cut2) continue;
+                const float rho = rcp_fast(d2 + f0.z), rho2 = rho * rho, drho2 = d * rho2;
+                const float pf = fmaf(-d2, icut2, 2.f);
+                const float vs = fmaf(f0.w, rho, -P.x * pf);
+                const float vT = fmaf(f1.x, rho, fmaf(f1.y, rho2, -P.y * pf));
+                const float vp = fmaf(f1.z, rho, fmaf(f1.w, rho2, fmaf(f2.x, drho2, -fmaf(c.x, d, P.z * pf))));
+                const float vv = fmaf(f2.y, rho, fmaf(f2.z, rho2, fmaf(f2.w, drho2, -fmaf(c.y, d, P.w * pf))));
+                const int h = q >> 1;
+                float vD = 0.f, vDT = 0.f, vDP = 0.f;
+                if (LM) {
+                    const float drho = d * rho;
+                    vD = l0.x * drho;
+                    vDT = fmaf(l0.y, drho, l0.z * drho2);
+                    vDP = fmaf(l0.w, drho, fmaf(l1.x, rho, fmaf(l1.y, rho2, l1.z * drho2)));
+                }
+                if (q & 1) {
+                    TS[h].y += vs; ST[h].y += vT; SP[h].y += vp; SV[h].y += vv;
+                    if (LM) { TD[h].y += vD; SDT[h].y += vDT; SDP[h].y += vDP; }
+                } else {
+                    TS[h].x += vs; ST[h].x += vT; SP[h].x += vp; SV[h].x += vv;
+                    if (LM) { TD[h].x += vD; SDT[h].x += vDT; SDP[h].x += vDP; }
                 }
             }
         }

@@ -55,26 +55,37 @@ static CUtensorMap make_map(const void* ptr, int64_t rows, int64_t cols, int64_t
     return m;
 }
 
-constexpr int kTBN = 128;  // 128 x 128 tiles, two CTAs per SM
+// 128 x 128 tiles (two CTAs per SM) by default; 128 x 256 tiles (half the B-operand
+// traffic per FLOP, one CTA per SM) for wide outputs, where there are tiles enough to
+// fill the GPU several times over
+template <int EPI, int TBN>
+static void gemm_tbn(cudaStream_t st, const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int M, int N, int K,
+                     umma::EpiArgs ep) {
+    using Cfg = umma::TileCfg<TBN>;
+    static bool attr = false;
+    if (!attr) {
+        IRS_CUDA(cudaFuncSetAttribute(umma::umma_gemm_kernel<EPI, TBN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)Cfg::kSmemBytes));
+        attr = true;
+    }
+    const CUtensorMap ta = make_map(A, M, K, lda, umma::BM);
+    const CUtensorMap tb = make_map(B, N, K, ldb, TBN);
+    ep.M = M;
+    ep.N = N;
+    const dim3 grid((unsigned)((N + TBN - 1) / TBN), (unsigned)((M + umma::BM - 1) / umma::BM));
+    umma::umma_gemm_kernel<EPI, TBN><<<grid, umma::kThreads, Cfg::kSmemBytes, st>>>(ta, tb, K, ep);
+}
 
 template <int EPI>
 static void gemm(cudaStream_t st, const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int M, int N, int K,
                  umma::EpiArgs ep) {
-    using Cfg = umma::TileCfg<kTBN>;
-    static bool attr = false;
-    if (!attr) {
-        IRS_CUDA(cudaFuncSetAttribute(umma::umma_gemm_kernel<EPI, kTBN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)Cfg::kSmemBytes));
-        attr = true;
-    }
     const bool f32_out = EPI == umma::EPI_F32 || EPI == umma::EPI_BIAS_F32;
     IRS_REQUIRE(M >= 1 && N >= 1 && K >= 1 && ep.ldc >= N && (f32_out || ep.ldc % 8 == 0), "GEMM sizes");
-    const CUtensorMap ta = make_map(A, M, K, lda, umma::BM);
-    const CUtensorMap tb = make_map(B, N, K, ldb, kTBN);
-    ep.M = M;
-    ep.N = N;
-    const dim3 grid((unsigned)((N + kTBN - 1) / kTBN), (unsigned)((M + umma::BM - 1) / umma::BM));
-    umma::umma_gemm_kernel<EPI, kTBN><<<grid, umma::kThreads, Cfg::kSmemBytes, st>>>(ta, tb, K, ep);
+    const long long tiles256 = (long long)((N + 255) / 256) * ((M + umma::BM - 1) / umma::BM);
+    if (N >= 4096 && tiles256 >= 4 * 148)
+        gemm_tbn<EPI, 256>(st, A, lda, B, ldb, M, N, K, ep);
+    else
+        gemm_tbn<EPI, 128>(st, A, lda, B, ldb, M, N, K, ep);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) throw Error{IRS_E_CUDA, std::string("GEMM launch: ") + cudaGetErrorString(e)};
 }

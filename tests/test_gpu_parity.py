@@ -89,6 +89,27 @@ def test_cross_sections_mixed_weideman_pv(pkg, ctx, oracle, orc_mod, golden):
         assert np.max(np.abs(got - ref)) <= tol * ref.max(), method
 
 
+@pytest.mark.parametrize("method", ["Weideman", "FullFaddeeva"])
+def test_cross_sections_5k_far_field(pkg, ctx, oracle, method):
+    """The 5,000-line list on its 34,801-point grid, where most lines reach a block only
+    through the interpolated far field, the mid and cutoff-edge classes: mixed (far
+    field) and mixed_direct against the FP64 oracle, for both Voigt evaluators that have
+    a far-wing switch."""
+    ll = pkg.synthetic.lists_5k_co2()[2]
+    grid = np.array([(251600 + i) / 400 for i in range(34801)])
+    for T, p in ((296.0, 1.0), (220.0, 0.05)):
+        ref = oracle.voigt_xsec(ll.lines, grid, T, p, method=method)
+        m = ref > 1e-2 * ref.max()
+        for prec in ("mixed", "mixed_direct"):
+            got = pkg.compute_voigt_cross_sections(grid, ll, T, p, backend=ctx, precision=prec,
+                                                   method=pkg.VoigtMethod[method])
+            if method == "FullFaddeeva":
+                assert np.max(np.abs(got[m] - ref[m]) / ref[m]) < 2e-4, (method, prec, T)
+                assert np.max(np.abs(got - ref)) < 2e-5 * ref.max(), (method, prec, T)
+            else:  # FP32 Weideman-24, as the golden-fixture test
+                assert np.max(np.abs(got - ref)) < 5e-5 * ref.max(), (method, prec, T)
+
+
 # ------------------------------------------------------------ forward model
 def _run(pkg, ctx, oracle, orc_mod, prof, lists, snd, channels=None, y0=None, geom=None, T_sfc=None,
          eps=1.0, method="FullFaddeeva", **kw):
