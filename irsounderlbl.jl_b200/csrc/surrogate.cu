@@ -55,9 +55,10 @@ static CUtensorMap make_map(const void* ptr, int64_t rows, int64_t cols, int64_t
     return m;
 }
 
-// 128 x 128 tiles (two CTAs per SM) by default; 128 x 256 tiles (half the B-operand
-// traffic per FLOP, one CTA per SM) for wide outputs, where there are tiles enough to
-// fill the GPU several times over
+// 128 x 128 tiles (two CTAs per SM, so one CTA's epilogue runs under the other's main
+// loop).  The 128 x 256 variant (one CTA per SM, half the B-operand traffic per FLOP)
+// measured slower on the 1024 -> 8461 output layer (261 vs 189 us per 4096 batch):
+// without a second CTA its epilogue is exposed.
 template <int EPI, int TBN>
 static void gemm_tbn(cudaStream_t st, const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int M, int N, int K,
                      umma::EpiArgs ep) {
@@ -81,11 +82,7 @@ static void gemm(cudaStream_t st, const bf16* A, int64_t lda, const bf16* B, int
                  umma::EpiArgs ep) {
     const bool f32_out = EPI == umma::EPI_F32 || EPI == umma::EPI_BIAS_F32;
     IRS_REQUIRE(M >= 1 && N >= 1 && K >= 1 && ep.ldc >= N && (f32_out || ep.ldc % 8 == 0), "GEMM sizes");
-    const long long tiles256 = (long long)((N + 255) / 256) * ((M + umma::BM - 1) / umma::BM);
-    if (N >= 4096 && tiles256 >= 4 * 148)
-        gemm_tbn<EPI, 256>(st, A, lda, B, ldb, M, N, K, ep);
-    else
-        gemm_tbn<EPI, 128>(st, A, lda, B, ldb, M, N, K, ep);
+    gemm_tbn<EPI, 128>(st, A, lda, B, ldb, M, N, K, ep);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) throw Error{IRS_E_CUDA, std::string("GEMM launch: ") + cudaGetErrorString(e)};
 }

@@ -39,7 +39,7 @@ def from_bf16_bits(b):
 
 
 @pytest.mark.parametrize("M,N,K", [(128, 256, 64), (300, 520, 200), (1, 7, 5), (1024, 1024, 1024),
-                                   (512, 8461, 1024), (8461, 192, 256), (4096, 8461, 192)])  # last: 128x256 tiles
+                                   (512, 8461, 1024), (8461, 192, 256), (4096, 8461, 192)])
 def test_gemm_bf16(pkg, ctx, M, N, K):
     import ctypes as C
     rng = np.random.default_rng(M + N + K)
