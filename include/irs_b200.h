@@ -70,7 +70,9 @@ typedef struct {
  * T_method: 0 :logp_at_pcg, 1 :mass_weighted (layers.jl:133)
  * source_function: 0 :cim, 1 :toon (schwarzschild.jl:130)
  * line_mixing: 0 nothing, 1 VPYLineMixing with per-line Y(T) = y0 (296/T)^0.75
- *   (the y0 uploaded with the CO2 list; line_mixing.jl:1351-1369)
+ *   (the y0 uploaded with the CO2 list; line_mixing.jl:1351-1369),
+ *   2 VPYLineMixing(relmat) and 3 VPWLineMixing(relmat) on the relaxation-matrix
+ *   data of irs_upload_relmat (line_mixing.jl:208-241, 1093-1154, 1303-1369)
  * continua: bit mask 1 :h2o, 2 :co2, 4 :co2_cia, 8 :n2, 16 :o2 (CIA tables are
  *   not bundled and contribute zeros, as the reference does without them)
  * method: VoigtMethod of the line sum (forward_model uses FullFaddeeva)
@@ -226,6 +228,83 @@ int irs_oe_batch(irs_ctx* ctx, const irs_profile* base, int n_scene, const irs_s
                  const double* se_inv, const double* xa, const double* Sa_inv, const double* x0,
                  const irs_oe_params* prm, double* x_out, double* y_fit, double* M_out,
                  int32_t* n_iter, int32_t* converged, double* cost);
+
+/* ------------------------------------------------------------------------------
+ * Relaxation-matrix line mixing (src/CrossSections/line_mixing.jl).
+ * ------------------------------------------------------------------------------ */
+#define IRS_LM_NONE        0
+#define IRS_LM_PER_LINE_Y  1   /* VP_Y with per-line y0 on the HITRAN list          */
+#define IRS_LM_RELMAT_VPY  2   /* VPYLineMixing(relmat): first-order Y from W(T)    */
+#define IRS_LM_RELMAT_VPW  3   /* VPWLineMixing(relmat): whitelisted bands by their
+                                  eigenmodes, the other bands by VP_Y              */
+
+/* RelmatLine (line_mixing.jl:35-47); Julia's isbits layout, 72 bytes, so a band's
+ * Vector{RelmatLine} is passed as pointer(band.lines). */
+typedef struct {
+    int8_t  isot;
+    double  nu;          /* line centre, cm^-1                 */
+    int16_t ji;          /* initial J                          */
+    int8_t  branch;      /* -1 P, 0 Q, +1 R                    */
+    double  gv_air;      /* air HWHM at 296 K, cm^-1/atm       */
+    float   n_air;
+    float   shift;       /* pressure shift, cm^-1/atm          */
+    double  e_lower;
+    double  dipo0, popu_t0, dipo_t;
+} irs_relmat_line;
+
+/* RelmatBand (line_mixing.jl:72-82).  whitelisted: the band's name is in
+ * VPWLineMixing.whitelist (default_vpw_whitelist, line_mixing.jl:813-849, is host
+ * logic of the caller). */
+typedef struct {
+    const irs_relmat_line* lines;
+    int64_t n_lines;
+    double  nu_min, nu_max;
+    int32_t li, lf, isot, molecule;
+    int32_t whitelisted, _pad;
+} irs_relmat_band;
+
+/* One entry of a W0B0Table (line_mixing.jl:92-102, read by _load_wtfit :434-472):
+ * the table of key (lli, llf) = (min(li,lf), max(li,lf)), branch pair sub = 3 t_i +
+ * t_ip with t = 0 P, 1 Q, 2 R (pp, pq, ..., rr), J pair (ji, jip), W(T) = exp(w0r)
+ * (T/T0)^b0r.  A later entry with the same key overwrites an earlier one. */
+typedef struct {
+    int32_t lli, llf, sub, ji, jip, _pad;
+    double  w0r, b0r;
+} irs_wtfit_entry;
+
+/* HITRANRelmatData (line_mixing.jl:106-118) of `species` with the LM object's
+ * min_band_strength: the context keeps a copy and builds each band's
+ * temperature-independent coupling table (_build_coupling, :530-578) once.
+ * n_bands = 0 removes it. */
+int irs_upload_relmat(irs_ctx* ctx, int species, const irs_relmat_band* bands, int n_bands,
+                      const irs_wtfit_entry* wtfit, int64_t n_wtfit, double min_band_strength);
+
+/* Host-side building blocks (no device work; usable without a GPU).  q_ratio is
+ * Q(296 K)/Q(T) of the band's isotopologue.  W is [n][n] row-major, W[i*n + j] the
+ * reference's W[i, j]. */
+int irs_relmat_w_matrix(const irs_relmat_band* band, const irs_wtfit_entry* wtfit, int64_t n_wtfit,
+                        double T, double q_ratio, double* W, double* popu);      /* :607-700 */
+int irs_relmat_y(const irs_relmat_band* band, const irs_wtfit_entry* wtfit, int64_t n_wtfit,
+                 double T, double q_ratio, double* Y);                          /* :712-738 */
+/* band_modes (:892-955): poles and amplitudes as interleaved (re, im) pairs
+ * [2 n_lines]; n_kept of them are written. */
+int irs_band_modes(const irs_relmat_band* band, const irs_wtfit_entry* wtfit, int64_t n_wtfit,
+                   double T, double p_atm, double q_ratio, double keep_threshold,
+                   double* poles, double* amps, double* f, int64_t* n_kept);
+
+/* compute_vpw_band_xsec(ν_grid, modes; cutoff, x_far) (:972-1020) on the device:
+ * grid[n_nu] sorted, poles/amps interleaved (re, im) [2 n_poles]. */
+int irs_vpw_band_xsec(irs_ctx* ctx, const double* grid, int64_t n_nu, const double* poles,
+                      const double* amps, int64_t n_poles, double f, double cutoff, double x_far,
+                      double* sigma);
+
+/* The line-mixing perturbation of the uploaded relmat at (T, p_atm) on grid[n_nu]:
+ * mode IRS_LM_RELMAT_VPY is compute_lm_dispersive_correction (:1303-1337), mode
+ * IRS_LM_RELMAT_VPW is _vpw_perturbation (:1120-1154).  isotope_mask: bit k keeps
+ * isotopologue k (0 keeps all), the reference's `isotopes` filter. */
+int irs_lm_perturbation(irs_ctx* ctx, int mode, const double* grid, int64_t n_nu, double T,
+                        double p_atm, double cutoff, double x_far, double keep_threshold,
+                        uint32_t isotope_mask, double* dsigma);
 
 /* Wait for the context's work; fill per-stage times of the last forward call. */
 int irs_synchronize(irs_ctx* ctx);

@@ -7,7 +7,9 @@ error behaviour as the Julia package) over the C ABI of ``libirs_b200.so``:
     forward_model                  src/Sensor/sounder.jl:233-360
     Sounder / IASIInstrument ...   src/Sensor/sounder.jl:33-128
     ViewingGeometry, scan angles   src/Sensor/geometry.jl:18-101
-    VoigtMethod, VPYLineMixing     voigt.jl:32-36, line_mixing.jl:144-149
+    VoigtMethod                    voigt.jl:32-36
+    VPYLineMixing, VPWLineMixing,  line_mixing.jl (relmat.py: data types, readers,
+    relmat operators                W(T), Y(T), eigenmodes, pole sums)
 
 Every computation runs in the CUDA library; nothing here evaluates physics
 beyond argument marshalling and the scalar geometry helpers.
@@ -161,16 +163,6 @@ def scan_angle_to_local_zenith(scan_angle: float, h_sat_km: float = 817.0,
     return math.degrees(math.asin(s))
 
 
-@dataclass
-class VPYLineMixing:
-    """First-order (Rosenkranz) line mixing on the CO2 list (line_mixing.jl:144-149).
-
-    The reference derives Y(T) from the HITRAN2020 relaxation matrix, which is not
-    redistributable; here each CO2 line carries y0 and Y(T) = y0 (296/T)^0.75
-    (per atm), aligned with the CO2 HITRANLinelist order."""
-    y0: np.ndarray
-
-
 # ------------------------------------------------------------------ context
 def _read_tips(path=DATA / "tips2024_q.csv"):
     out = {}
@@ -200,6 +192,7 @@ class B200Context:
         self.h = h
         self.device = device
         self._lists: Dict[int, tuple] = {}
+        self._relmat_key = None
         if load_tables:
             self.load_tables()
 
@@ -227,6 +220,19 @@ class B200Context:
         check(self.lib.irs_upload_linelist(self.h, int(species), lines.ctypes.data, len(lines),
                                            dptr(yy) if yy is not None else None))
         self._lists[int(species)] = (key, ll, y0)
+
+    def upload_relmat(self, data, whitelist=frozenset(), min_band_strength: float = 0.0, bands=None):
+        """Hand HITRANRelmatData (optionally a subset of its bands) to the library."""
+        bands = data.bands if bands is None else bands
+        key = (id(data), tuple(id(b) for b in bands), frozenset(whitelist), float(min_band_strength))
+        if self._relmat_key == key:
+            return
+        from .relmat import _CRelmat
+        c = _CRelmat(bands, data.wtfit, set(whitelist))
+        check(self.lib.irs_upload_relmat(self.h, int(data.species), c.bands, c.n_bands, c.wt, c.n_wt,
+                                         float(min_band_strength)))
+        self._relmat_key = key
+        self._relmat_ref = (data, bands)
 
     def stage_times(self) -> StageTimes:
         t = StageTimes()
@@ -295,7 +301,7 @@ def fm_options(internal_dnu=0.001, high_res_factor=None, cutoff=25.0, lm_cutoff=
     o.continua = sum(CONTINUA[c] for c in continua)
     o.with_ils = int(bool(with_ils))
     o.apodization = APODIZATION[apodization]
-    o.line_mixing = int(line_mixing is not None)
+    o.line_mixing = 0 if line_mixing is None else int(line_mixing.mode)
     o.T_method = 0 if T_method == "logp_at_pcg" else 1
     o.source_function = 0 if source_function == "cim" else 1
     o.method = int(method)
@@ -342,6 +348,9 @@ def _prepare(ctx, linelists, line_mixing):
     for sp, ll in linelists.items():
         y0 = line_mixing.y0 if (line_mixing is not None and int(sp) == 2) else None
         ctx.upload_linelist(int(sp), ll, y0)
+    if line_mixing is not None and line_mixing.y0 is None:  # relaxation-matrix data
+        wl = line_mixing.whitelist if line_mixing.mode == _lib.IRS_LM_RELMAT_VPW else set()
+        ctx.upload_relmat(line_mixing.data, wl, line_mixing.min_band_strength)
     # species uploaded earlier but absent from this call must not contribute
     for sp in list(ctx._lists):
         if sp not in {int(s) for s in linelists}:
@@ -392,4 +401,10 @@ from .estimation import (ColumnScale, FullProfile, Jacobian, PartialColumns, Sta
                          finite_difference_jacobian, forward_model_rrule, pack_state, partial_column_basis,
                          state_labels, unpack_state, vmr_range, build_sa, scene_nedt, exclude_channels,
                          RetrievalResult, optimal_estimation, optimal_estimation_batch, oe_diagnostics)
+from .relmat import (BandModes, HITRANRelmatData, RelmatBand, VPWLineMixing, VPYLineMixing,  # noqa: E402,F401
+                     W0B0Table, band_eff_strength, band_modes, build_w_matrix, calc_w_and_y,
+                     compute_lm_dispersive_correction, compute_voigt_lm_cross_sections,
+                     compute_voigt_vpw_cross_sections, compute_vpw_band_perturbation, compute_vpw_band_xsec,
+                     default_vpw_whitelist, load_hitran_relmat, load_wtfit, parse_bandinfo, parse_sfile,
+                     relmat_lines, vpw_perturbation)
 from .surrogate import Surrogate, surrogate_features, surrogate_first_guess, surrogate_forward_batch  # noqa: E402,F401,E501

@@ -15,6 +15,13 @@ SO = HERE / "libirs_b200.so"
 
 IRS_WEIDEMAN, IRS_PSEUDOVOIGT, IRS_FULLFADDEEVA = 1, 2, 3
 IRS_FP64, IRS_MIXED, IRS_MIXED_DIRECT = 0, 1, 2
+IRS_LM_NONE, IRS_LM_PER_LINE_Y, IRS_LM_RELMAT_VPY, IRS_LM_RELMAT_VPW = 0, 1, 2, 3
+
+# RelmatLine isbits layout (src/CrossSections/line_mixing.jl:35-47), 72 bytes
+RELMAT_LINE_DTYPE = np.dtype([("isot", "i1"), ("nu", "f8"), ("ji", "i2"), ("branch", "i1"), ("gv_air", "f8"),
+                              ("n_air", "f4"), ("shift", "f4"), ("e_lower", "f8"), ("dipo0", "f8"),
+                              ("popu_t0", "f8"), ("dipo_t", "f8")], align=True)
+assert RELMAT_LINE_DTYPE.itemsize == 72
 
 # HITRANLine isbits layout (src/HITRAN/linelist.jl:20-31), 56 bytes
 LINE_DTYPE = np.dtype({
@@ -71,6 +78,17 @@ class StageTimes(C.Structure):
 _P = C.c_void_p
 _PD = C.POINTER(C.c_double)
 _PF = C.POINTER(C.c_float)
+class RelmatBandC(C.Structure):  # irs_relmat_band
+    _fields_ = [("lines", C.c_void_p), ("n_lines", C.c_int64), ("nu_min", C.c_double), ("nu_max", C.c_double),
+                ("li", C.c_int32), ("lf", C.c_int32), ("isot", C.c_int32), ("molecule", C.c_int32),
+                ("whitelisted", C.c_int32), ("_pad", C.c_int32)]
+
+
+class WtfitEntryC(C.Structure):  # irs_wtfit_entry
+    _fields_ = [("lli", C.c_int32), ("llf", C.c_int32), ("sub", C.c_int32), ("ji", C.c_int32),
+                ("jip", C.c_int32), ("_pad", C.c_int32), ("w0r", C.c_double), ("b0r", C.c_double)]
+
+
 SIGNATURES = {
     "irs_abi_version": ([], C.c_int),
     "irs_last_error": ([], C.c_char_p),
@@ -113,6 +131,18 @@ SIGNATURES = {
     "irs_surrogate_infer": ([_P, _PF, C.c_int64, _PF, _PF], C.c_int),
     "irs_surrogate_infer_device": ([_P, _P, C.c_int64, _P, _P, _P], C.c_int),
     "irs_gemm_bf16": ([_P, _P, _P, C.c_int, C.c_int, C.c_int, _PF], C.c_int),
+    "irs_upload_relmat": ([_P, C.c_int, C.POINTER(RelmatBandC), C.c_int, C.POINTER(WtfitEntryC), C.c_int64,
+                           C.c_double], C.c_int),
+    "irs_relmat_w_matrix": ([C.POINTER(RelmatBandC), C.POINTER(WtfitEntryC), C.c_int64, C.c_double, C.c_double,
+                             _PD, _PD], C.c_int),
+    "irs_relmat_y": ([C.POINTER(RelmatBandC), C.POINTER(WtfitEntryC), C.c_int64, C.c_double, C.c_double, _PD],
+                     C.c_int),
+    "irs_band_modes": ([C.POINTER(RelmatBandC), C.POINTER(WtfitEntryC), C.c_int64, C.c_double, C.c_double,
+                        C.c_double, C.c_double, _PD, _PD, _PD, C.POINTER(C.c_int64)], C.c_int),
+    "irs_vpw_band_xsec": ([_P, _PD, C.c_int64, _PD, _PD, C.c_int64, C.c_double, C.c_double, C.c_double, _PD],
+                          C.c_int),
+    "irs_lm_perturbation": ([_P, C.c_int, _PD, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double,
+                             C.c_double, C.c_uint32, _PD], C.c_int),
     "irs_grid_size": ([C.POINTER(Sounder), C.POINTER(FMOptions), C.POINTER(C.c_int64),
                        C.POINTER(C.c_int64)], C.c_int),
 }

@@ -15,12 +15,14 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 SO = HERE / "libirs_b200.so"
 SOURCES = [HERE / "csrc" / "irs_b200.cu", HERE / "csrc" / "noalloc.cu", HERE / "csrc" / "surrogate.cu",
-           HERE / "csrc" / "irs_host.cpp"]
+           HERE / "csrc" / "irs_host.cpp", HERE / "csrc" / "relmat.cpp"]
 DEPS = SOURCES + sorted((HERE / "csrc").glob("*.cuh")) + sorted((HERE / "csrc").glob("*.h")) + \
     [HERE.parent / "include" / "irs_b200.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+# -fcx-limited-range: host complex products and quotients by the textbook formulas (the
+# eigensolver of relmat.cpp; its values are finite and moderate) instead of libgcc calls.
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-         "-Xcompiler", "-fPIC", "-shared"]
+         "-Xcompiler", "-fPIC", "-Xcompiler", "-fcx-limited-range", "-shared"]
 
 
 def up_to_date() -> bool:

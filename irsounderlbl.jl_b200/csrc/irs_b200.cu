@@ -15,6 +15,11 @@
 #include "rte_ils.cuh"
 #include "jacobian.cuh"
 #include "oe.cuh"
+#include "lm_pert.cuh"
+#include <atomic>
+#include <exception>
+#include <mutex>
+#include <thread>
 
 namespace irs {
 const char* last_error();
@@ -107,10 +112,13 @@ static void validate_options(const irs_fm_options& o) {
     IRS_REQUIRE(o.apodization >= 0 && o.apodization <= 3, "unknown apodization");
     IRS_REQUIRE(o.T_method == 0 || o.T_method == 1, "T_method must be :logp_at_pcg or :mass_weighted");
     IRS_REQUIRE(o.source_function == 0 || o.source_function == 1, "source_function must be :cim or :toon");
-    IRS_REQUIRE(o.line_mixing == 0 || o.line_mixing == 1, "line_mixing must be 0 or 1 (VP_Y)");
-    if (o.line_mixing) {
-        IRS_REQUIRE(o.lm_cutoff == o.cutoff, "lm_cutoff must equal cutoff on this path");
+    IRS_REQUIRE(o.line_mixing >= IRS_LM_NONE && o.line_mixing <= IRS_LM_RELMAT_VPW,
+                "line_mixing must be 0 (none), 1 (per-line Y), 2 (VPYLineMixing) or 3 (VPWLineMixing)");
+    if (o.line_mixing == IRS_LM_PER_LINE_Y)
+        IRS_REQUIRE(o.lm_cutoff == o.cutoff, "lm_cutoff must equal cutoff with per-line Y");
+    if (o.line_mixing != IRS_LM_NONE) {
         IRS_REQUIRE(o.method == IRS_FULLFADDEEVA, "line mixing evaluates the Voigt part with FullFaddeeva");
+        IRS_REQUIRE(o.lm_cutoff > 0.0, "lm_cutoff must be positive");
     }
 }
 
@@ -138,7 +146,8 @@ static std::vector<ListDev> list_descs(irs_ctx* ctx) {
 // Runs the line-parameter passes and the line sum for the plan; returns the
 // device tau buffer ([n_prof * L][n_nu], FP32 for mixed or FP64 for plain).
 static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n_nu, double grid0,
-                         double dnu_g, const irs_fm_options& o, int ev_mid) {
+                         double dnu_g, const irs_fm_options& o, int ev_mid, const double* d_pert = nullptr,
+                         long long pstride = 0) {
     cudaStream_t st = ctx->stream;
     const int nseg = (int)pl.segs.size();
     std::vector<SegDev> sd(std::max(nseg, 1));
@@ -210,22 +219,23 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
     if (!mixed) {
         dim3 g2((unsigned)((n_nu + 255) / 256), npl);
         if (o.method == 1)
-            linesum_f64_kernel<1><<<g2, 256, 0, st>>>(d_segs, d_count, d_pl, o64, d_grid, n_nu, o.cutoff, o.x_far, (double*)d_tau);
+            linesum_f64_kernel<1><<<g2, 256, 0, st>>>(d_segs, d_count, d_pl, o64, d_grid, n_nu, o.cutoff, o.x_far, (double*)d_tau, d_pert, pstride);
         else if (o.method == 2)
-            linesum_f64_kernel<2><<<g2, 256, 0, st>>>(d_segs, d_count, d_pl, o64, d_grid, n_nu, o.cutoff, o.x_far, (double*)d_tau);
+            linesum_f64_kernel<2><<<g2, 256, 0, st>>>(d_segs, d_count, d_pl, o64, d_grid, n_nu, o.cutoff, o.x_far, (double*)d_tau, d_pert, pstride);
         else
-            linesum_f64_kernel<3><<<g2, 256, 0, st>>>(d_segs, d_count, d_pl, o64, d_grid, n_nu, o.cutoff, o.x_far, (double*)d_tau);
+            linesum_f64_kernel<3><<<g2, 256, 0, st>>>(d_segs, d_count, d_pl, o64, d_grid, n_nu, o.cutoff, o.x_far, (double*)d_tau, d_pert, pstride);
     } else {
         dim3 g2((unsigned)((n_nu + kMxStrip - 1) / kMxStrip), npl);
         const float cut_g = (float)(o.cutoff / dnu_g);
         unsigned long long* d_eval = d_pairs + 2;
-#define IRS_MX(M, LMX, F) \
-    linesum_mixed_kernel<M, LMX, F><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau, d_eval)
+#define IRS_MX(M, LMX, F, P) \
+    linesum_mixed_kernel<M, LMX, F, P><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau, d_eval, d_pert, pstride)
         const bool far = o.precision == IRS_MIXED;
-        if (o.method == 1) { if (far) IRS_MX(1, false, true); else IRS_MX(1, false, false); }
-        else if (o.method == 2) IRS_MX(2, false, false);
-        else if (o.line_mixing) { if (far) IRS_MX(3, true, true); else IRS_MX(3, true, false); }
-        else { if (far) IRS_MX(3, false, true); else IRS_MX(3, false, false); }
+        if (o.method == 1) { if (far) IRS_MX(1, false, true, false); else IRS_MX(1, false, false, false); }
+        else if (o.method == 2) IRS_MX(2, false, false, false);
+        else if (o.line_mixing == IRS_LM_PER_LINE_Y) { if (far) IRS_MX(3, true, true, false); else IRS_MX(3, true, false, false); }
+        else if (d_pert) { if (far) IRS_MX(3, false, true, true); else IRS_MX(3, false, false, true); }
+        else { if (far) IRS_MX(3, false, true, false); else IRS_MX(3, false, false, false); }
 #undef IRS_MX
     }
     check_launch(ctx);
@@ -244,6 +254,85 @@ static void ensure_ils(irs_ctx* ctx, double dnu, double opd, double fwhm, int ap
     check_launch(ctx);
     std::memcpy(ctx->ils_key, key, sizeof key);
     ctx->ils_n = n;
+}
+
+// Runs f(0..n-1) on the host's cores.
+template <class F>
+static void parallel_for(int n, F&& f) {
+    const int nt = std::max(1, std::min<int>(n, (int)std::thread::hardware_concurrency()));
+    if (nt <= 1) {
+        for (int i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::atomic<int> next(0);
+    std::exception_ptr err;
+    std::mutex mu;
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+        th.emplace_back([&] {
+            for (int i; (i = next++) < n;) {
+                try {
+                    f(i);
+                } catch (...) {
+                    std::lock_guard<std::mutex> g(mu);
+                    if (!err) err = std::current_exception();
+                }
+            }
+        });
+    for (auto& t : th) t.join();
+    if (err) std::rethrow_exception(err);
+}
+
+// Relaxation-matrix line mixing (line_mixing = 2, 3): the poles of the LM species'
+// perturbation for every (profile, layer) where it is present, at that layer's
+// Curtis-Godson T and p of the species (sounder.jl:283-305), built on the host cores.
+struct RelmatPlan {
+    std::vector<LmPole> poles;
+    std::vector<long long> off;  // per (profile, layer): poles[off[k], off[k+1])
+};
+static_assert(sizeof(LmPole) == sizeof(LmPoleDev), "pole layouts differ");
+
+static bool relmat_plan(irs_ctx* ctx, Plan& pl, const irs_fm_options& o, RelmatPlan& rp) {
+    if (o.line_mixing != IRS_LM_RELMAT_VPY && o.line_mixing != IRS_LM_RELMAT_VPW) return false;
+    const RelmatHost& R = ctx->relmat;
+    IRS_REQUIRE(R.species != 0, "line_mixing 2 and 3 need the relaxation-matrix data (irs_upload_relmat)");
+    int li = -1;
+    for (size_t i = 0; i < ctx->lists.size(); ++i)
+        if (ctx->lists[i].species == R.species && ctx->lists[i].n > 0) li = (int)i;
+    if (li < 0) return false;  // the LM species has no line list in this call
+    const uint32_t iso_mask = ctx->lists[li].iso_mask;
+    const int npl = pl.n_prof * pl.L;
+    std::vector<int> seg_of(npl, -1);
+    for (size_t i = 0; i < pl.segs.size(); ++i)
+        if (pl.segs[i].list == li) {
+            pl.segs[i].flags |= SEG_RELMAT;
+            seg_of[pl.segs[i].prof * pl.L + pl.segs[i].layer] = (int)i;
+        }
+    std::vector<std::vector<LmPole>> per(npl);
+    parallel_for(npl, [&](int k) {
+        if (seg_of[k] < 0) return;
+        const Segment& g = pl.segs[seg_of[k]];
+        lm_poles(R, ctx->tables, o.line_mixing, iso_mask, g.T, g.p_atm, 1e-4, per[k]);  // keep_threshold 1e-4 (:1123)
+    });
+    rp.off.assign(npl + 1, 0);
+    for (int k = 0; k < npl; ++k) rp.off[k + 1] = rp.off[k] + (long long)per[k].size();
+    rp.poles.resize(rp.off[npl]);
+    for (int k = 0; k < npl; ++k) std::copy(per[k].begin(), per[k].end(), rp.poles.begin() + rp.off[k]);
+    return true;
+}
+
+// The perturbation rows [(profile, layer)][pstride] on the device grid.
+static const double* relmat_launch(irs_ctx* ctx, const RelmatPlan& rp, const double* d_grid, int64_t n_nu,
+                                   double cutoff, double x_far, long long& pstride) {
+    const int npl = (int)rp.off.size() - 1;
+    pstride = ((n_nu + kMxStrip - 1) / kMxStrip) * kMxStrip;
+    const LmPoleDev* d_p = (const LmPoleDev*)upload(ctx, "lm_poles", rp.poles);
+    const long long* d_off = upload(ctx, "lm_off", rp.off);
+    double* d_out = (double*)workspace(ctx, "lm_pert", (size_t)npl * pstride * sizeof(double));
+    dim3 g((unsigned)((pstride + 255) / 256), npl);
+    lm_pert_kernel<<<g, 256, 0, ctx->stream>>>(d_p, d_off, d_grid, n_nu, pstride, cutoff, x_far, d_out);
+    check_launch(ctx);
+    return d_out;
 }
 
 static void forward_pass(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder& s,
@@ -295,12 +384,22 @@ static void forward_pass(irs_ctx* ctx, const irs_profile* profs, int n_prof, con
         workspace(ctx, "lrt", std::max<size_t>(lrt.size(), 1) * sizeof(LayerRT));
         workspace(ctx, "prt", std::max<size_t>(prt.size(), 1) * sizeof(ProfileRT));
     }
+    RelmatPlan rp;
+    const bool relmat = relmat_plan(ctx, pl, o, rp);
+    if (relmat) {
+        const long long ps = ((n_nu + kMxStrip - 1) / kMxStrip) * kMxStrip;
+        workspace(ctx, "lm_pert", (size_t)n_prof * L * ps * sizeof(double));
+        workspace(ctx, "lm_poles", std::max<size_t>(rp.poles.size(), 1) * sizeof(LmPole));
+        workspace(ctx, "lm_off", rp.off.size() * sizeof(long long));
+    }
     IRS_CUDA(cudaEventRecord(ctx->ev[0], st));
     double* d_grid = (double*)workspace(ctx, "grid", n_nu * sizeof(double));
     grid_values_kernel<<<(unsigned)((n_nu + 255) / 256), 256, 0, st>>>(to_dev(ig.g), d_grid);
     check_launch(ctx);
     if (o.with_ils) ensure_ils(ctx, ig.dnu_hi, s.opd_max, s.fwhm_gauss, o.apodization);
-    void* d_tau = run_linesum(ctx, pl, d_grid, n_nu, ig.g.at(0), ig.dnu_hi, o, 1);
+    long long pstride = 0;
+    const double* d_pert = relmat ? relmat_launch(ctx, rp, d_grid, n_nu, o.lm_cutoff, o.x_far, pstride) : nullptr;
+    void* d_tau = run_linesum(ctx, pl, d_grid, n_nu, ig.g.at(0), ig.dnu_hi, o, 1, d_pert, pstride);
     IRS_CUDA(cudaEventRecord(ctx->ev[2], st));
     LayerRT* d_lrt = upload(ctx, "lrt", lrt);
     ProfileRT* d_prt = upload(ctx, "prt", prt);
@@ -349,6 +448,8 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
     o.dptmn = 0.0;               // frozen line set (vmr_jacobian.jl:188-201)
     o.precision = IRS_MIXED;
     validate_options(o);
+    IRS_REQUIRE(o.line_mixing <= IRS_LM_PER_LINE_Y,
+                "the analytic Jacobian supports line_mixing 0 or 1; use finite differences with relmat line mixing");
     upload_tables(ctx);
     cudaStream_t st = ctx->stream;
     const InternalGrid ig = internal_grid(s, o);
@@ -945,6 +1046,7 @@ int irs_upload_linelist(irs_ctx* ctx, int species, const irs_line* lines, int64_
     std::vector<double> h((size_t)n * 8);
     std::vector<int> tips(n);
     double max_shift = 0.0;
+    uint32_t iso_mask = 0;
     const double d_self = species == 1 ? 0.002 : (species == 2 ? -0.003 : 0.0);
     for (int64_t k = 0; k < n; ++k) {
         const irs_line& l = lines[ord[k]];
@@ -959,6 +1061,8 @@ int irs_upload_linelist(irs_ctx* ctx, int species, const irs_line* lines, int64_
         h[7 * n + k] = y0 ? y0[ord[k]] : 0.0;
         auto it = ctx->tips_index.find({(int)l.mol_id, (int)l.iso_id});
         tips[k] = it == ctx->tips_index.end() ? -1 : it->second;
+        const int iso = l.iso_id == 0 ? 10 : (int)l.iso_id;
+        if (iso >= 0 && iso < 32) iso_mask |= 1u << iso;
         max_shift = std::max(max_shift, std::fabs((double)l.pressure_shift) + std::fabs(d_self));
     }
     // replace an existing list of this species
@@ -973,6 +1077,7 @@ int irs_upload_linelist(irs_ctx* ctx, int species, const irs_line* lines, int64_
     d.n = n;
     d.has_y0 = y0 != nullptr;
     d.max_abs_shift = max_shift;
+    d.iso_mask = iso_mask;
     const size_t bytes = (size_t)std::max<int64_t>(n, 1) * (8 * sizeof(double) + sizeof(int));
     char* base = nullptr;
     if (cudaMalloc((void**)&base, bytes) != cudaSuccess) {
@@ -1073,6 +1178,64 @@ int irs_forward_model_batch(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
     ctx->n_d2h += 2.0 * n * sizeof(double);
     IRS_CUDA(cudaStreamSynchronize(ctx->stream));
     collect_times(ctx);
+    IRS_API_END
+}
+
+int irs_upload_relmat(irs_ctx* ctx, int species, const irs_relmat_band* bands, int n_bands,
+                      const irs_wtfit_entry* wtfit, int64_t n_wtfit, double min_band_strength) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && n_bands >= 0 && (n_bands == 0 || bands) && n_wtfit >= 0 && (n_wtfit == 0 || wtfit),
+                "invalid relmat arguments");
+    RelmatHost R;
+    if (n_bands > 0) {
+        IRS_REQUIRE(species > 0, "relmat species must be a HITRAN molecule id");
+        R.species = species;
+        R.min_band_strength = min_band_strength;
+        for (int b = 0; b < n_bands; ++b) R.bands.push_back(make_band(bands[b], wtfit, n_wtfit));
+    }
+    ctx->relmat = std::move(R);
+    IRS_API_END
+}
+
+int irs_vpw_band_xsec(irs_ctx* ctx, const double* grid, int64_t n_nu, const double* poles, const double* amps,
+                      int64_t n_poles, double f, double cutoff, double x_far, double* sigma) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && grid && sigma && n_nu >= 1 && n_poles >= 0 && (n_poles == 0 || (poles && amps)),
+                "invalid arguments");
+    IRS_REQUIRE(cutoff > 0.0, "cutoff must be positive");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    RelmatPlan rp;
+    const double pre = f * kInvSqrtPi;
+    for (int64_t k = 0; k < n_poles; ++k)  // compute_vpw_band_xsec, line_mixing.jl:972-1020
+        rp.poles.push_back({poles[2 * k], f, poles[2 * k + 1] * f, amps[2 * k] * pre, amps[2 * k + 1] * pre, 0, 0});
+    std::stable_sort(rp.poles.begin(), rp.poles.end(), [](const LmPole& a, const LmPole& b) { return a.c < b.c; });
+    rp.off = {0, (long long)rp.poles.size()};
+    double* d_grid = (double*)workspace(ctx, "lm_grid", n_nu * sizeof(double));
+    IRS_CUDA(cudaMemcpyAsync(d_grid, grid, n_nu * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    long long ps = 0;
+    const double* d_out = relmat_launch(ctx, rp, d_grid, n_nu, cutoff, x_far, ps);
+    IRS_CUDA(cudaMemcpyAsync(sigma, d_out, n_nu * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    IRS_CUDA(cudaStreamSynchronize(ctx->stream));
+    IRS_API_END
+}
+
+int irs_lm_perturbation(irs_ctx* ctx, int mode, const double* grid, int64_t n_nu, double T, double p_atm,
+                        double cutoff, double x_far, double keep_threshold, uint32_t isotope_mask, double* dsigma) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && grid && dsigma && n_nu >= 1, "invalid arguments");
+    IRS_REQUIRE(mode == IRS_LM_RELMAT_VPY || mode == IRS_LM_RELMAT_VPW, "mode must be IRS_LM_RELMAT_VPY or _VPW");
+    IRS_REQUIRE(T > 0.0 && p_atm >= 0.0 && cutoff > 0.0, "T must be positive, p_atm non-negative, cutoff positive");
+    IRS_REQUIRE(ctx->relmat.species != 0, "no relaxation-matrix data uploaded (irs_upload_relmat)");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    RelmatPlan rp;
+    lm_poles(ctx->relmat, ctx->tables, mode, isotope_mask, T, p_atm, keep_threshold, rp.poles);
+    rp.off = {0, (long long)rp.poles.size()};
+    double* d_grid = (double*)workspace(ctx, "lm_grid", n_nu * sizeof(double));
+    IRS_CUDA(cudaMemcpyAsync(d_grid, grid, n_nu * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    long long ps = 0;
+    const double* d_out = relmat_launch(ctx, rp, d_grid, n_nu, cutoff, x_far, ps);
+    IRS_CUDA(cudaMemcpyAsync(dsigma, d_out, n_nu * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    IRS_CUDA(cudaStreamSynchronize(ctx->stream));
     IRS_API_END
 }
 

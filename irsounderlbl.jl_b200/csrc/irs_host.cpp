@@ -173,8 +173,10 @@ void layer_setup(const irs_profile& P, int pi, const irs_fm_options& o,
             s.vmr_self = sp == 1 ? vmr : 0.0;
             s.coef = vmr * dp * 2.1209e22;
             s.list = (int)li;
-            const bool lm_co2 = sp == 2 && o.line_mixing == 1;
-            s.flags = (o.dptmn > 0.0 && !lm_co2 ? SEG_DPTMIN : 0) | (lm_co2 ? SEG_LM : 0);
+            // sounder.jl:294-300: DPTMIN is skipped for CO2 under any line-mixing model
+            const bool lm_co2 = sp == 2 && o.line_mixing != IRS_LM_NONE;
+            s.flags = (o.dptmn > 0.0 && !lm_co2 ? SEG_DPTMIN : 0) |
+                      (lm_co2 && o.line_mixing == IRS_LM_PER_LINE_Y ? SEG_LM : 0);
             s.margin_g = list_max_shift[li] * s.p_atm / dnu_grid + 2.0;
             s.prof = pi;
             s.layer = k;

@@ -60,10 +60,12 @@ struct Segment {
     double margin_g;  // window margin (grid units) covering the pressure shifts
     int64_t out_off;  // first slot of this segment in the per-line parameter arrays
     int32_t list;     // line-list index in the context
-    int32_t flags;    // SEG_DPTMIN | SEG_LM
+    int32_t flags;    // SEG_DPTMIN | SEG_LM | SEG_RELMAT
     int32_t prof, layer;
 };
-enum { SEG_DPTMIN = 1, SEG_LM = 2 };
+// SEG_LM: per-line Y dispersive sum fused into the line sum; SEG_RELMAT: the
+// relaxation-matrix perturbation of this (profile, layer) is added before the clamp.
+enum { SEG_DPTMIN = 1, SEG_LM = 2, SEG_RELMAT = 4 };
 
 // Per (profile, layer) inputs of the fused RTE/continuum kernel.
 struct LayerRT {
@@ -94,6 +96,7 @@ struct DevLineList {
     int64_t n = 0;
     double max_abs_shift = 0;  // max |delta_air| + |delta_self| (cm^-1/atm)
     bool has_y0 = false;
+    uint32_t iso_mask = 0;     // isotopologues present, iso 0 counted as 10 (line_mixing.jl:202-203)
     // SoA, sorted by wavenumber
     double *nu = nullptr, *S296 = nullptr, *E = nullptr, *gair = nullptr, *gself = nullptr,
            *nair = nullptr, *delta = nullptr, *y0 = nullptr;
@@ -119,9 +122,38 @@ struct LineParamsMixed {  // FP32 kernel, grid units relative to the grid start
 
 struct Tables {
     std::map<std::pair<int, int>, std::pair<int, std::vector<double>>> tips;  // (tmin, q)
+    double q_value(int mol, int iso, double T) const;  // partition.jl:8-24
     std::vector<double> h2o_nu, h2o_cs, h2o_cf, h2o_te;
     std::vector<double> co2_nu, co2_s, co2_tdep;  // S already multiplied by xfac
 };
+
+// ---------------------------------------------- relaxation-matrix line mixing
+// One band of HITRANRelmatData with its temperature-independent coupling pairs
+// (BandCoupling, line_mixing.jl:65-70: CSR over the outer line i).
+struct RelmatBandHost {
+    std::vector<irs_relmat_line> lines;
+    int li = 0, lf = 0, isot = 0, molecule = 2;
+    bool whitelisted = false, has_wtfit = false;
+    double nu_min = 0, nu_max = 0, eff_strength = 0;
+    std::vector<int> row_ptr, col;
+    std::vector<double> w0r, b0r;
+};
+struct RelmatHost {
+    int species = 0;  // 0: no relmat uploaded
+    double min_band_strength = 0;
+    std::vector<RelmatBandHost> bands;
+};
+// A line-mixing pole: centre (cm^-1), Doppler factor f, y = Im(pole) f and the
+// amplitudes (already times f/sqrt(pi)) of Re w and Im w; window 0 takes the pole
+// where |nu - c| <= cutoff (VP_W), 1 where nu - cutoff <= c <= nu + cutoff (VP_Y).
+struct LmPole {
+    double c, f, y, ar, ai;
+    int window, pad;
+};
+RelmatBandHost make_band(const irs_relmat_band& b, const irs_wtfit_entry* wt, int64_t n_wt);
+// Poles of the whole LM perturbation at (T, p_atm), sorted by centre.
+void lm_poles(const RelmatHost& R, const Tables& tabs, int mode, uint32_t iso_mask, double T,
+              double p_atm, double keep_threshold, std::vector<LmPole>& out);
 
 }  // namespace irs
 
@@ -141,6 +173,7 @@ struct irs_ctx {
     double *d_h2o = nullptr, *d_co2 = nullptr;  // packed tables
     int n_h2o = 0, n_co2 = 0;
     std::vector<irs::DevLineList> lists;
+    irs::RelmatHost relmat;
     std::map<std::string, irs::DevBuf> work;  // named growable workspaces
     irs_stage_times last{};
     irs_stage_times prior{};  // stage times of the earlier passes of a multi-pass batch

@@ -44,7 +44,7 @@ template <int METHOD>
 __global__ void __launch_bounds__(256) linesum_f64_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const int2* __restrict__ pl_segs,
     LpOutF64 lp, const double* __restrict__ grid, long long n_nu, double cutoff, double x_far,
-    double* __restrict__ tau) {
+    double* __restrict__ tau, const double* __restrict__ pert, long long pstride) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int pl = blockIdx.y;
     if (i >= n_nu) return;
@@ -86,6 +86,7 @@ __global__ void __launch_bounds__(256) linesum_f64_kernel(
         }
         double sig = fmax(acc, 0.0);
         if (lm) sig = fmax(sig + accD, 0.0);
+        if (pert && (sg.flags & 4)) sig = fmax(sig + pert[(size_t)pl * pstride + i], 0.0);  // relmat LM
         tsum += sig * sg.coef;
     }
     tau[(size_t)pl * n_nu + i] = tsum;
@@ -227,7 +228,8 @@ __device__ __forceinline__ void fast_pair(float2 d0s, float2 offs, float2 b2, fl
 template <int METHOD, bool LM, bool FAR>
 __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, const LpOutMixed& lp, long long wb,
                                              float cut, float cut2, int lane, WarpTile& T, const FarTable& FT,
-                                             float xn, float* tsum, unsigned long long& work) {
+                                             float xn, float* tsum, unsigned long long& work,
+                                             const double* __restrict__ prow) {
     constexpr float kCentre = 0.5f * (kMxWarpPts - 1);
     constexpr float kHalf = 0.5f * kMxWarpPts + 0.5f;
     long long jlo, jhi;
@@ -477,10 +479,13 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             if (LM) kahan_add(sumD[q], compD[q], vd);
         }
     }
+    const bool rel = prow && (sg.flags & 4);  // relmat line mixing: sigma = max(sigma_V + d_sigma, 0)
+    const float rc = (float)sg.coef;
 #pragma unroll
     for (int q = 0; q < kMxQ; ++q) {
         float sig = fmaxf(sum[q], 0.f);
         if (LM) sig = fmaxf(sig + sumD[q], 0.f);
+        if (rel) sig = fmaxf(sig + rc * (float)prow[wb + 32 * q + lane], 0.f);
         tsum[q] += sig;
     }
 }
@@ -534,10 +539,14 @@ __device__ __forceinline__ void warp_segment_pv(const SegDev& sg, long long cnt,
     for (int q = 0; q < kMxQ; ++q) tsum[q] += fmaxf(sum[q], 0.f);
 }
 
-template <int METHOD, bool ANY_LM, bool FAR>
+// PERT: segments flagged SEG_RELMAT add the relaxation-matrix perturbation rows
+// pert[(profile, layer)][pstride] before their clamp (a separate instantiation, so the
+// kernels without it are unchanged).
+template <int METHOD, bool ANY_LM, bool FAR, bool PERT = false>
 __global__ void __launch_bounds__(kMxThreads, ANY_LM ? 2 : 3) linesum_mixed_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const int2* __restrict__ pl_segs,
-    LpOutMixed lp, long long n_nu, float cut_g, float* __restrict__ tau, unsigned long long* __restrict__ evald) {
+    LpOutMixed lp, long long n_nu, float cut_g, float* __restrict__ tau, unsigned long long* __restrict__ evald,
+    const double* __restrict__ pert, long long pstride) {
     __shared__ WarpTile tiles[kMxWarps];
     __shared__ FarTable ftab;
     if (FAR) {
@@ -562,9 +571,10 @@ __global__ void __launch_bounds__(kMxThreads, ANY_LM ? 2 : 3) linesum_mixed_kern
         if (METHOD == 2)
             warp_segment_pv(sg, cnt, lp, wb, cut_g, cut2, lane, T, tsum);
         else if (ANY_LM && (sg.flags & 2))
-            warp_segment<METHOD, true, FAR>(sg, cnt, lp, wb, cut_g, cut2, lane, T, ftab, xn, tsum, work);
+            warp_segment<METHOD, true, FAR>(sg, cnt, lp, wb, cut_g, cut2, lane, T, ftab, xn, tsum, work, nullptr);
         else
-            warp_segment<METHOD, false, FAR>(sg, cnt, lp, wb, cut_g, cut2, lane, T, ftab, xn, tsum, work);
+            warp_segment<METHOD, false, FAR>(sg, cnt, lp, wb, cut_g, cut2, lane, T, ftab, xn, tsum, work,
+                                             PERT ? pert + (size_t)pl * pstride : nullptr);
     }
     if (evald && lane == 0 && work) atomicAdd(evald, work);
     float* out = tau + (size_t)pl * n_nu;

@@ -98,3 +98,56 @@ def perturbed_profiles(n: int, seed: int = 1002):
         out.append(AtmosphericProfile(b.pressure.copy(), T, b.altitude.copy(), vmr))
         scans.append(g.uniform(0.0, 48.0))
     return out, np.array(scans)
+
+
+def synthetic_relmat(n_bands: int = 6, j_max: int = 60, seed: int = 1003, nu_lo: float = 650.0,
+                     nu_hi: float = 760.0, molecule: int = 2):
+    """CO2-like relaxation-matrix data (HITRANRelmatData) for the VP_Y/VP_W paths.
+
+    Band b: isotopologue 1 (2 for b % 3 == 2), l_i = b % 3, l_f = l_i + (b + 1) % 2;
+    centre ~ U(nu_lo + 30, nu_hi - 30).  P and R branches at 2B spacing (B = 0.39 cm^-1),
+    plus a Q branch packed near the centre (nu_c - 8e-4 J(J+1)) when l_i != l_f; even J
+    only for isotopologue 1.  Lower-state populations (2J+1) exp(-c2 B J(J+1)/296)/527,
+    band strengths 10^U(-20, -18), DipoT = Dipo0 from S = Dipo^2 PopuT0 nu stim;
+    gamma_air = 0.075 - 3e-4 J (>= 0.05), n_air 0.72, shift -0.0025 cm^-1/atm.  Each
+    (l_i, l_f) W0B0 table couples every branch pair and J pair with
+    exp(W0) = 0.025 exp(-|J - J'|/8) cm^-1/atm and B0 = 0.75."""
+    from .relmat import HITRANRelmatData, RelmatBand, W0B0Table, relmat_lines
+    g = np.random.Generator(np.random.PCG64(seed))
+    c2, B = 1.4388, 0.39
+    bands, tables = [], {}
+    for b in range(n_bands):
+        isot = 2 if b % 3 == 2 else 1
+        li = b % 3
+        lf = li + (b + 1) % 2
+        nu_c = g.uniform(nu_lo + 30.0, nu_hi - 30.0)
+        s_band = 10.0 ** g.uniform(-20.0, -18.0)
+        js = list(range(0, j_max + 1, 2 if isot == 1 else 1))
+        rows = []
+        for br in ((-1, 0, 1) if li != lf else (-1, 1)):
+            for J in js:
+                if br != 1 and J == 0:
+                    continue
+                nu = (nu_c - 2 * B * J if br == -1 else (nu_c + 2 * B * (J + 1) if br == 1 else nu_c - 8e-4 * J * (J + 1)))
+                nu += g.uniform(-0.01, 0.01)
+                E = B * J * (J + 1)
+                pop = (2 * J + 1) * np.exp(-c2 * E / 296.0) / 527.0
+                stim = 1.0 - np.exp(-c2 * nu / 296.0)
+                dip = np.sqrt(s_band * pop / (pop * nu * stim))
+                gam = max(0.075 - 3e-4 * J, 0.05) + g.uniform(-0.002, 0.002)
+                rows.append((isot, nu, J, br, gam, 0.72, -0.0025, E, dip, pop, dip))
+        rows.sort(key=lambda r: r[1])
+        L = relmat_lines(rows)
+        bands.append(RelmatBand(f"SB{b:02d}", li, lf, isot, float(L["nu"].min()), float(L["nu"].max()), L,
+                                molecule))
+        key = (min(li, lf), max(li, lf))
+        if key not in tables:
+            t = W0B0Table()
+            for sub in ("pp", "pq", "pr", "qp", "qq", "qr", "rp", "rq", "rr"):
+                d = t.get(sub)
+                for J in range(0, j_max + 2):
+                    for Jp in range(0, J + 1):
+                        d[(J, Jp)] = (float(np.log(0.025 * np.exp(-(J - Jp) / 8.0))), 0.75)
+                        d[(Jp, J)] = d[(J, Jp)]
+            tables[key] = t
+    return HITRANRelmatData(bands, tables, molecule)

@@ -922,6 +922,17 @@ int orc_rte(const double* grid, int64_t n_nu, int L, const double* tau, const do
 }
 
 // sounder.jl:233-360
+static orc_lm_cb g_lm_cb = nullptr;
+static void* g_lm_user = nullptr;
+static int g_lm_species = 0;
+
+int orc_set_lm_callback(int species, orc_lm_cb cb, void* user) {
+    g_lm_cb = cb;
+    g_lm_user = user;
+    g_lm_species = species;
+    return 0;
+}
+
 int orc_forward_model(int n_lev, const double* p_lev, const double* T_lev, int nps,
                       const int* psp, const double* pvmr, int n_lists, const int* lsp,
                       const int64_t* loff, const orc_line* lines, const double* y0,
@@ -993,11 +1004,14 @@ int orc_forward_model(int n_lev, const double* p_lev, const double* T_lev, int n
             const double coef = vmr * dp[k] * NAIR_PER_VMR;
             const orc_line* ll = lines + loff[li];
             const long nL = (long)(loff[li + 1] - loff[li]);
+            // sounder.jl:294-300: DPTMIN is skipped for CO2 under any line-mixing model
             const bool lm_co2 = sp == 2 && o->line_mixing == 1;
+            const bool no_dpt = sp == 2 && o->line_mixing != 0;
+            const bool relmat = (o->line_mixing == 2 || o->line_mixing == 3) && g_lm_cb && sp == g_lm_species;
             std::vector<orc_line> kept;
             const orc_line* use = ll;
             long nuse = nL;
-            if (o->dptmn > 0.0 && !lm_co2) {
+            if (o->dptmn > 0.0 && !no_dpt) {
                 std::vector<uint8_t> keep(nL);
                 reject_weak(ll, nL, Tcg, p_atm, coef, vs, o->dptmn, keep.data());
                 for (long j = 0; j < nL; ++j) if (keep[j]) kept.push_back(ll[j]);
@@ -1010,6 +1024,10 @@ int orc_forward_model(int n_lev, const double* p_lev, const double* T_lev, int n
                     lm_dispersive(use, nuse, y0 + loff[li], grid.data(), nw, Tcg, p_atm, o->lm_cutoff, o->x_far, ds.data());
                     for (long i = 0; i < nw; ++i) sig[i] = std::max(sig[i] + ds[i], 0.0);
                 }
+            } else if (relmat) {  // compute_voigt_{lm,vpw}_cross_sections, line_mixing.jl:1093-1110, 1351-1369
+                voigt_xsec(use, nuse, grid.data(), nw, Tcg, p_atm, 0.0, o->cutoff, 3, o->x_far, sig.data());
+                if (g_lm_cb(g_lm_user, Tcg, p_atm, grid.data(), nw, ds.data()) != 0) return fail("line-mixing callback failed");
+                for (long i = 0; i < nw; ++i) sig[i] = std::max(sig[i] + ds[i], 0.0);
             } else if (nuse > 0) {
                 voigt_xsec(use, nuse, grid.data(), nw, Tcg, p_atm, vs, o->cutoff, o->method, o->x_far, sig.data());
             } else {

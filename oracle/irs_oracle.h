@@ -120,6 +120,14 @@ int orc_forward_model(int n_lev, const double* p_lev, const double* T_lev,
                       int64_t ch_begin, int64_t ch_end,
                       double* R_out, double* BT_out, double* tau_out, int64_t* n_nu_window);
 
+/* Relaxation-matrix line mixing (line_mixing 2 VPYLineMixing, 3 VPWLineMixing,
+ * line_mixing.jl:208-241): the perturbation of `species` at a layer's (T, p_atm) on the
+ * window grid comes from `cb` (the numpy restatement in lm_oracle.py); the species'
+ * cross section is then max(sigma_Voigt + dsigma, 0).  cb = NULL clears it. */
+typedef int (*orc_lm_cb)(void* user, double T, double p_atm, const double* grid, int64_t n_nu,
+                         double* dsigma);
+int orc_set_lm_callback(int species, orc_lm_cb cb, void* user);
+
 int orc_num_threads(void);
 const char* orc_last_error(void);
 

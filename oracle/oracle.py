@@ -61,7 +61,7 @@ def fm_options(internal_dnu=0.001, high_res_factor=0, cutoff=25.0, lm_cutoff=Non
     o.continua = sum(CONTINUA[c] for c in continua)
     o.with_ils = int(bool(with_ils))
     o.apodization = APODIZATION[apodization]
-    o.line_mixing = int(bool(line_mixing))
+    o.line_mixing = int(line_mixing)  # 0 none, 1 per-line y0, 2 VP_Y relmat, 3 VP_W relmat
     o.T_method = {"logp_at_pcg": 0, "mass_weighted": 1}[T_method]
     o.source_function = {"cim": 0, "toon": 1}[source_function]
     o.method = METHOD[method]
@@ -98,6 +98,11 @@ def read_tips(path=DATA / "tips2024_q.csv"):
 def read_csv_cols(path):
     rows = [l.strip().split(",") for l in open(path).readlines()[1:] if l.strip()]
     return np.array(rows, dtype=np.float64).T.copy()
+
+
+# int (*)(void* user, double T, double p_atm, const double* grid, int64_t n, double* dsigma)
+LM_CALLBACK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_double), C.c_int64,
+                          C.POINTER(C.c_double))
 
 
 def _lines(a):
@@ -165,6 +170,7 @@ class Oracle:
                                             C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.POINTER(Sounder), C.POINTER(FMOptions), i32, C.c_void_p,
                                             i32, i32, i32, i32, i32, i32, i64, i64, pd, pd]
+        L.orc_set_lm_callback.argtypes = [i32, LM_CALLBACK, C.c_void_p]
         L.orc_last_error.restype = C.c_char_p
         if load_tables:
             self.load_tables()
@@ -261,11 +267,29 @@ class Oracle:
         return vals, dhi.value
 
     def forward_model(self, profile, linelists, snd: Sounder, opt: FMOptions, channels=None,
-                      y0=None, return_tau=False):
+                      y0=None, return_tau=False, lm=None):
         """forward_model (src/Sensor/sounder.jl:233-360) on channels [c0, c1).
 
         profile: dict(p=[n_lev], T=[n_lev], vmr={mol: [n_lev]}); linelists: {mol: lines};
-        y0: {mol: per-line VP_Y coefficient} (line mixing on the CO2 list)."""
+        y0: {mol: per-line VP_Y coefficient} (line mixing on the CO2 list);
+        lm: (species, fn) with fn(T, p_atm, grid) -> the relmat line-mixing perturbation
+        (opt.line_mixing 2 or 3)."""
+        if lm is not None:
+            species, fn = lm
+
+            def cb(user, T, p_atm, g, n, out):
+                try:
+                    grid = np.ctypeslib.as_array(g, shape=(n,)).copy()
+                    np.ctypeslib.as_array(out, shape=(n,))[:] = fn(T, p_atm, grid)
+                    return 0
+                except Exception:  # reported as a failed call
+                    return -1
+            ccb = LM_CALLBACK(cb)
+            self.lib.orc_set_lm_callback(int(species), ccb, None)
+            try:
+                return self.forward_model(profile, linelists, snd, opt, channels, y0, return_tau)
+            finally:
+                self.lib.orc_set_lm_callback(0, LM_CALLBACK(), None)
         p = np.ascontiguousarray(profile["p"], dtype=np.float64)
         T = np.ascontiguousarray(profile["T"], dtype=np.float64)
         psp = np.array(sorted(profile["vmr"]), dtype=np.int32)
