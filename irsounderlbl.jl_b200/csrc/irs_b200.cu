@@ -286,13 +286,19 @@ static void parallel_for(int n, F&& f) {
 // Relaxation-matrix line mixing (line_mixing = 2, 3): the poles of the LM species'
 // perturbation for every (profile, layer) where it is present, at that layer's
 // Curtis-Godson T and p of the species (sounder.jl:283-305), built on the host cores.
+// With jac, three pole sets per (profile, layer), amplitudes times the column amount:
+// the perturbation and its central differences in T (h = 0.02 K) and p (h = 1e-4 p),
+// the pairs of evaluations folded into one set with amplitudes +-1/(2h)
+// (cross_section_jacobian.jl:252-319).
 struct RelmatPlan {
     std::vector<LmPole> poles;
-    std::vector<long long> off;  // per (profile, layer): poles[off[k], off[k+1])
+    std::vector<long long> off;  // per row (profile, layer[, variant]): poles[off[k], off[k+1])
 };
 static_assert(sizeof(LmPole) == sizeof(LmPoleDev), "pole layouts differ");
+constexpr long long kPertAlign = 8192;  // rows padded to whole line-sum strips of either kernel
+static_assert(kPertAlign % kMxStrip == 0 && kPertAlign % kJgStrip == 0, "perturbation row padding");
 
-static bool relmat_plan(irs_ctx* ctx, Plan& pl, const irs_fm_options& o, RelmatPlan& rp) {
+static bool relmat_plan(irs_ctx* ctx, Plan& pl, const irs_fm_options& o, RelmatPlan& rp, bool jac = false) {
     if (o.line_mixing != IRS_LM_RELMAT_VPY && o.line_mixing != IRS_LM_RELMAT_VPW) return false;
     const RelmatHost& R = ctx->relmat;
     IRS_REQUIRE(R.species != 0, "line_mixing 2 and 3 need the relaxation-matrix data (irs_upload_relmat)");
@@ -308,24 +314,43 @@ static bool relmat_plan(irs_ctx* ctx, Plan& pl, const irs_fm_options& o, RelmatP
             pl.segs[i].flags |= SEG_RELMAT;
             seg_of[pl.segs[i].prof * pl.L + pl.segs[i].layer] = (int)i;
         }
-    std::vector<std::vector<LmPole>> per(npl);
-    parallel_for(npl, [&](int k) {
-        if (seg_of[k] < 0) return;
-        const Segment& g = pl.segs[seg_of[k]];
-        lm_poles(R, ctx->tables, o.line_mixing, iso_mask, g.T, g.p_atm, 1e-4, per[k]);  // keep_threshold 1e-4 (:1123)
+    const int nv = jac ? 3 : 1;
+    std::vector<std::vector<LmPole>> per((size_t)npl * nv);
+    parallel_for(npl * nv, [&](int k) {
+        const int v = k % nv;
+        if (seg_of[k / nv] < 0) return;
+        const Segment& g = pl.segs[seg_of[k / nv]];
+        const double T = g.T, p = g.p_atm;
+        std::vector<LmPole>& out = per[k];
+        if (!jac) {  // keep_threshold 1e-4 (line_mixing.jl:1123)
+            lm_poles(R, ctx->tables, o.line_mixing, iso_mask, T, p, 1e-4, out);
+            return;
+        }
+        auto add = [&](double Tv, double pv, double scale) {
+            std::vector<LmPole> q;
+            lm_poles(R, ctx->tables, o.line_mixing, iso_mask, Tv, pv, 1e-4, q);
+            for (LmPole& e : q) { e.ar *= scale; e.ai *= scale; }
+            out.insert(out.end(), q.begin(), q.end());
+        };
+        const double hT = 0.02, hp = std::max(p, 1e-6) * 1e-4;
+        if (v == 0) add(T, p, g.coef);
+        if (v == 1) { add(T + hT, p, g.coef / (2 * hT)); add(T - hT, p, -g.coef / (2 * hT)); }
+        if (v == 2) { add(T, p + hp, g.coef / (2 * hp)); add(T, p - hp, -g.coef / (2 * hp)); }
+        std::stable_sort(out.begin(), out.end(), [](const LmPole& a, const LmPole& c) { return a.c < c.c; });
     });
-    rp.off.assign(npl + 1, 0);
-    for (int k = 0; k < npl; ++k) rp.off[k + 1] = rp.off[k] + (long long)per[k].size();
-    rp.poles.resize(rp.off[npl]);
-    for (int k = 0; k < npl; ++k) std::copy(per[k].begin(), per[k].end(), rp.poles.begin() + rp.off[k]);
+    const size_t rows = per.size();
+    rp.off.assign(rows + 1, 0);
+    for (size_t k = 0; k < rows; ++k) rp.off[k + 1] = rp.off[k] + (long long)per[k].size();
+    rp.poles.resize(rp.off[rows]);
+    for (size_t k = 0; k < rows; ++k) std::copy(per[k].begin(), per[k].end(), rp.poles.begin() + rp.off[k]);
     return true;
 }
 
-// The perturbation rows [(profile, layer)][pstride] on the device grid.
+// The perturbation rows [row][pstride] on the device grid.
 static const double* relmat_launch(irs_ctx* ctx, const RelmatPlan& rp, const double* d_grid, int64_t n_nu,
                                    double cutoff, double x_far, long long& pstride) {
     const int npl = (int)rp.off.size() - 1;
-    pstride = ((n_nu + kMxStrip - 1) / kMxStrip) * kMxStrip;
+    pstride = ((n_nu + kPertAlign - 1) / kPertAlign) * kPertAlign;
     const LmPoleDev* d_p = (const LmPoleDev*)upload(ctx, "lm_poles", rp.poles);
     const long long* d_off = upload(ctx, "lm_off", rp.off);
     double* d_out = (double*)workspace(ctx, "lm_pert", (size_t)npl * pstride * sizeof(double));
@@ -387,7 +412,7 @@ static void forward_pass(irs_ctx* ctx, const irs_profile* profs, int n_prof, con
     RelmatPlan rp;
     const bool relmat = relmat_plan(ctx, pl, o, rp);
     if (relmat) {
-        const long long ps = ((n_nu + kMxStrip - 1) / kMxStrip) * kMxStrip;
+        const long long ps = ((n_nu + kPertAlign - 1) / kPertAlign) * kPertAlign;
         workspace(ctx, "lm_pert", (size_t)n_prof * L * ps * sizeof(double));
         workspace(ctx, "lm_poles", std::max<size_t>(rp.poles.size(), 1) * sizeof(LmPole));
         workspace(ctx, "lm_off", rp.off.size() * sizeof(long long));
@@ -448,8 +473,6 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
     o.dptmn = 0.0;               // frozen line set (vmr_jacobian.jl:188-201)
     o.precision = IRS_MIXED;
     validate_options(o);
-    IRS_REQUIRE(o.line_mixing <= IRS_LM_PER_LINE_Y,
-                "the analytic Jacobian supports line_mixing 0 or 1; use finite differences with relmat line mixing");
     upload_tables(ctx);
     cudaStream_t st = ctx->stream;
     const InternalGrid ig = internal_grid(s, o);
@@ -525,6 +548,8 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
         }
         pl.n_prof = np;
         pl.L = L;
+        RelmatPlan rp;  // sets SEG_RELMAT on the LM species' segments
+        const bool relmat = relmat_plan(ctx, pl, o, rp, true);
         pl.pl_segs.assign((size_t)np * L, make_int2(0, 0));
         std::vector<SegDev> sd(std::max<size_t>(pl.segs.size(), 1));
         std::vector<SegW> sw(std::max<size_t>(pl.segs.size(), 1));
@@ -569,6 +594,8 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
         JgProfile* d_jp = upload(ctx, "jg_prof", jp);
         double* d_vlev = upload(ctx, "jg_vlev", vlev);
         IRS_CUDA(cudaMemsetAsync(d_out, 0, (size_t)np * L * n_out * n_nu * sizeof(float), st));
+        long long pstride = 0;
+        const double* d_pert = relmat ? relmat_launch(ctx, rp, d_grid, n_nu, o.lm_cutoff, o.x_far, pstride) : nullptr;
         if (nseg > 0) {
             LpConfig cfg;
             cfg.cutoff = o.cutoff; cfg.x_far = o.x_far; cfg.dptmn = 0.0; cfg.grid0 = ig.g.at(0); cfg.u_gran = 1.0 / 16.0;
@@ -583,8 +610,8 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
         const size_t sm = jg_smem_bytes(NO);                                                                \
         IRS_CUDA(cudaFuncSetAttribute(jg_linesum_kernel<true, NO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
         IRS_CUDA(cudaFuncSetAttribute(jg_linesum_kernel<false, NO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
-        if (lm) jg_linesum_kernel<true, NO><<<g2, kJgWarps * 32, sm, st>>>(d_segs, d_sn, d_sw, d_pl, go, n_nu, cut_g, d_out); \
-        else jg_linesum_kernel<false, NO><<<g2, kJgWarps * 32, sm, st>>>(d_segs, d_sn, d_sw, d_pl, go, n_nu, cut_g, d_out); \
+        if (lm) jg_linesum_kernel<true, NO><<<g2, kJgWarps * 32, sm, st>>>(d_segs, d_sn, d_sw, d_pl, go, n_nu, cut_g, d_out, d_pert, pstride); \
+        else jg_linesum_kernel<false, NO><<<g2, kJgWarps * 32, sm, st>>>(d_segs, d_sn, d_sw, d_pl, go, n_nu, cut_g, d_out, d_pert, pstride); \
     } while (0)
             switch (n_out) {
                 case 3: IRS_JG(3); break;

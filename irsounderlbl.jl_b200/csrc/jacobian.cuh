@@ -566,7 +566,8 @@ constexpr size_t jg_smem_bytes(int nout) {
 template <bool ANY_LM, int NOUT>
 __global__ void __launch_bounds__(kJgWarps * 32, 2) jg_linesum_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_n, const SegW* __restrict__ wts,
-    const int2* __restrict__ pl_segs, JgOut g, long long n_nu, float cut_g, float* __restrict__ out) {
+    const int2* __restrict__ pl_segs, JgOut g, long long n_nu, float cut_g, float* __restrict__ out,
+    const double* __restrict__ pert, long long pstride) {
     extern __shared__ float4 jg_sh[];
     JgTile* tiles = (JgTile*)jg_sh;
     JgFarTable& ftab = *(JgFarTable*)((float*)(tiles + kJgWarps) + (size_t)kJgWarps * NOUT * kJgWarpPts);
@@ -593,6 +594,8 @@ __global__ void __launch_bounds__(kJgWarps * 32, 2) jg_linesum_kernel(
             jg_segment<false>(sg, nl, g, wb, cut_g, lane, tiles[warp], ftab, xn, s, ds);
         // clamps (voigt.jl:276, line_mixing.jl:1368, cross_section_jacobian.jl:107-113, :312-319)
         const SegW& W = wts[si];
+        // relaxation-matrix line mixing: rows (perturbation, d/dT, d/dp) x column amount
+        const double* prow = pert && (sg.flags & SEG_RELMAT) ? pert + (size_t)pl * 3 * pstride + wb + lane : nullptr;
 #pragma unroll
         for (int q = 0; q < kJgQ; ++q) {
             float v = s[0][q], vT = s[1][q], vp = s[2][q], vv = s[3][q];
@@ -601,6 +604,12 @@ __global__ void __launch_bounds__(kJgWarps * 32, 2) jg_linesum_kernel(
                 v += ds[0][q];
                 vT += ds[1][q];
                 vp += ds[2][q];
+                if (!(v > 0.f)) v = vT = vp = 0.f;
+            }
+            if (prow) {
+                v += (float)prow[32 * q];
+                vT += (float)prow[pstride + 32 * q];
+                vp += (float)prow[2 * pstride + 32 * q];
                 if (!(v > 0.f)) v = vT = vp = 0.f;
             }
             for (int o = 0; o < NOUT; ++o)

@@ -17,6 +17,7 @@
 //    into a Kahan-compensated FP32 accumulator per point.
 #pragma once
 #include "faddeeva.cuh"
+#include "irs_internal.h"
 #include "lineparams.cuh"
 
 namespace irs {
@@ -86,7 +87,7 @@ __global__ void __launch_bounds__(256) linesum_f64_kernel(
         }
         double sig = fmax(acc, 0.0);
         if (lm) sig = fmax(sig + accD, 0.0);
-        if (pert && (sg.flags & 4)) sig = fmax(sig + pert[(size_t)pl * pstride + i], 0.0);  // relmat LM
+        if (pert && (sg.flags & SEG_RELMAT)) sig = fmax(sig + pert[(size_t)pl * pstride + i], 0.0);
         tsum += sig * sg.coef;
     }
     tau[(size_t)pl * n_nu + i] = tsum;
@@ -479,7 +480,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             if (LM) kahan_add(sumD[q], compD[q], vd);
         }
     }
-    const bool rel = prow && (sg.flags & 4);  // relmat line mixing: sigma = max(sigma_V + d_sigma, 0)
+    const bool rel = prow && (sg.flags & SEG_RELMAT);  // relmat line mixing: sigma = max(sigma_V + d_sigma, 0)
     const float rc = (float)sg.coef;
 #pragma unroll
     for (int q = 0; q < kMxQ; ++q) {

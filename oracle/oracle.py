@@ -370,9 +370,10 @@ class Oracle:
 
     def fd_jacobian(self, profile, linelists, snd: Sounder, opt_kw: dict, retrieved=(),
                     include_T=True, include_tsfc=True, include_eps=True, T_sfc=None, eps_sfc=1.0,
-                    steps=None, observable="bt", channels=None, y0=None):
+                    steps=None, observable="bt", channels=None, y0=None, lm=None):
         """finite_difference_jacobian (src/Estimation/jacobian_fd.jl:111-165), central,
-        with dptmn = 0 unless opt_kw overrides it.  Log-VMR state for retrieved species."""
+        with dptmn = 0 unless opt_kw overrides it.  Log-VMR state for retrieved species;
+        lm as forward_model's (relmat line mixing)."""
         n_lev = len(profile["p"])
         base_T = np.asarray(profile["T"], dtype=np.float64)
         labels = []
@@ -413,7 +414,7 @@ class Oracle:
                 es = x[i]
             o = fm_options(T_sfc=Ts, eps_sfc=es, **kw)
             R, BT = self.forward_model(dict(p=profile["p"], T=T, vmr=vmr), linelists, snd, o,
-                                       channels=channels, y0=y0)
+                                       channels=channels, y0=y0, lm=lm)
             return BT if observable == "bt" else R
 
         y_0 = run(x0)

@@ -152,6 +152,58 @@ def test_forward_model_relmat(pkg, ctx, oracle, orc_mod, vpw):
     assert np.sqrt(np.mean((BTm - BT0) ** 2)) < 0.01 and np.max(np.abs(BTm - BT0)) < 0.05
 
 
+@pytest.mark.parametrize("vpw", [False, True])
+def test_jacobian_relmat_vs_fd(pkg, ctx, oracle, orc_mod, vpw):  # runtests.jl:1426-1478
+    """The analytic Jacobian with VPYLineMixing(relmat) / VPWLineMixing(relmat) against
+    central differences of the oracle forward model (whose perturbation comes from
+    lm_oracle), on the reference suite's coupled CO2 Q branch and 6-level profile."""
+    dipo = 1.7e-13
+    L = pkg.relmat_lines([(1, 700.40, 20, 0, 0.09, 0.75, -0.004, 250.0, dipo, 0.10, dipo),
+                          (1, 700.55, 18, 0, 0.09, 0.75, -0.004, 240.0, dipo, 0.09, dipo),
+                          (1, 701.30, 16, 0, 0.085, 0.75, -0.004, 300.0, 0.9 * dipo, 0.08, 0.9 * dipo)])
+    b = pkg.RelmatBand("CO2Q", 1, 1, 1, 700.4, 701.3, L)
+    wt = pkg.W0B0Table()
+    wt.qq[(20, 18)] = (math.log(0.035), 0.5)
+    wt.qq[(20, 16)] = (math.log(0.025), 0.5)
+    wt.qq[(18, 16)] = (math.log(0.030), 0.5)
+    relmat = pkg.HITRANRelmatData([b], {(1, 1): wt})
+    lines = np.zeros(4, dtype=orc_mod.LINE_DTYPE)
+    for k, (nu, S, E) in enumerate([(700.40, 2.0e-24, 250.0), (700.55, 1.8e-24, 240.0),
+                                    (700.95, 9.0e-25, 500.0), (701.30, 1.4e-24, 300.0)]):
+        lines[k] = (2, 1, nu, S, 1.0, 0.09, 0.08, E, 0.75, -0.004)
+    ll = {2: pkg.HITRANLinelist(lines)}
+    p = np.linspace(1000.0, 200.0, 6)
+    T = 288.0 + (225.0 - 288.0) * (1000.0 - p) / 800.0
+    prof = pkg.AtmosphericProfile(p, T, (1000.0 - p) / 66.0, {2: np.full(6, 4.0e-4)})
+    spec = pkg.StateVectorSpec(6, [pkg.CO2], include_temperature=True, include_tsfc=True,
+                               include_emissivity=True)
+    snd_kw = dict(nu_min=699.0, nu_max=703.0, dnu=0.5, opd_max=2.0, fwhm_gauss=0.5)
+    kw = dict(apply_continuum=False, with_ils=True, internal_dnu=0.005)
+    lm = pkg.VPWLineMixing(relmat, whitelist={"CO2Q"}) if vpw else pkg.VPYLineMixing(relmat)
+
+    def pert(Tl, pl, g):
+        if vpw:
+            return lo.vpw_perturbation(g, relmat.bands, relmat.wtfit, Tl, pl, {"CO2Q"}, isotopes={1})
+        return lo.lm_dispersive_correction(g, relmat.bands, relmat.wtfit, Tl, pl, isotopes={1})
+
+    steps = np.array([0.1] * 6 + [1e-3] * 6 + [0.1, 1e-3])
+    Kf, yf, _ = oracle.fd_jacobian(dict(p=p, T=T, vmr={2: np.full(6, 4.0e-4)}), {2: lines},
+                                   orc_mod.sounder(**snd_kw), dict(line_mixing=3 if vpw else 2, **kw),
+                                   retrieved=[2], T_sfc=290.0, eps_sfc=0.98, steps=steps, lm=(2, pert))
+    jac = pkg.analytic_jacobian(prof, ll, spec, sounder=pkg.Sounder.make(**snd_kw), T_sfc=290.0, eps_sfc=0.98,
+                                backend=ctx, line_mixing=lm, **kw)
+    rel = lambda c: np.max(np.abs(jac.K[:, c] - Kf[:, c])) / (np.max(np.abs(Kf[:, c])) + 1e-30)
+    assert np.max(np.abs(jac.y0 - yf)) < 0.01
+    assert rel(slice(6, 12)) < 1e-3     # CO2 column: FP32 line sum against FP64 differences
+    assert rel(slice(0, 6)) < 2e-3      # temperature
+    assert np.max(np.abs(jac.K[:, 12] - Kf[:, 12])) < 1e-3
+    assert np.max(np.abs(jac.K[:, 13] - Kf[:, 13])) < 1e-2
+    # and the line mixing is visible in the Jacobian
+    jn = pkg.analytic_jacobian(prof, ll, spec, sounder=pkg.Sounder.make(**snd_kw), T_sfc=290.0, eps_sfc=0.98,
+                               backend=ctx, **kw)
+    assert np.max(np.abs(jn.K[:, 6:12] - Kf[:, 6:12])) > 3 * np.max(np.abs(jac.K[:, 6:12] - Kf[:, 6:12]))
+
+
 def test_relmat_errors(pkg, ctx):
     c = pkg.B200Context()
     try:
@@ -162,10 +214,9 @@ def test_relmat_errors(pkg, ctx):
         with pytest.raises(pkg.IRSError):  # bad mode
             pkg._lib.check(c.lib.irs_lm_perturbation(c.h, 7, pkg.dptr(g), len(g), 250.0, 0.5, 25.0, 122.0, 1e-4,
                                                      0, pkg.dptr(np.empty(len(g)))))
-        with pytest.raises(pkg.IRSError):  # the analytic Jacobian does not take relmat line mixing
+        with pytest.raises(pkg.IRSError):  # relmat line mixing with another Voigt method
             relmat, lists, prof, snd = _fm_case(pkg)
-            spec = pkg.StateVectorSpec(len(prof.pressure), [pkg.CO2])
-            pkg.analytic_jacobian(prof, lists, spec, sounder=snd, backend=c, internal_dnu=0.01,
-                                  line_mixing=pkg.VPYLineMixing(relmat))
+            pkg.forward_model(prof, lists, sounder=snd, backend=c, internal_dnu=0.01,
+                              method=pkg.VoigtMethod.Weideman, line_mixing=pkg.VPYLineMixing(relmat))
     finally:
         c.close()
