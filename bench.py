@@ -270,6 +270,25 @@ def bench_extras(pkg, ctx, lists, snd, torch, stream):
         "value": len(profs) / tj, "unit": "jacobians/s", "timing": "host wall clock around the C-ABI call, "
         "host buffers (K is 8461 x 151 FP64 per profile)",
         "config": {"workload": "iasi-400k-lm", "profiles": len(profs), "n_state": spec.n, "channels": 8461}}
+    # ---- relaxation-matrix line mixing on the 400k-line IASI workload (6 AFGL profiles)
+    relmat = pkg.synthetic.synthetic_relmat(n_bands=6, j_max=60)
+    profs6 = [pkg.afgl_atmosphere(n) for n in pkg.synthetic.AFGL]
+    kw6 = _workload_kw()
+    for name, lmx in (("vpy_relmat", pkg.VPYLineMixing(relmat)), ("vpw_relmat", pkg.VPWLineMixing(relmat, n_top=5))):
+        pkg.forward_model_batch(profs6, lists, sounder=snd, backend=ctx, precision="mixed", line_mixing=lmx, **kw6)
+        t0 = time.perf_counter()
+        pkg.forward_model_batch(profs6, lists, sounder=snd, backend=ctx, precision="mixed", line_mixing=lmx, **kw6)
+        tl = time.perf_counter() - t0
+        st = ctx.stage_times()
+        out[name] = {
+            "metric": f"IASI spectra/s (forward_model, 400k lines, mixed, {type(lmx).__name__} on relaxation-matrix "
+                      "data)", "value": len(profs6) / tl, "unit": "spectra/s",
+            "timing": "host wall clock around the C-ABI call, host buffers",
+            "lm_host_ms": st.lm_host_ms, "lm_device_ms": st.lm_device_ms, "line_sum_ms": st.line_sum_ms,
+            "config": {"workload": "iasi-400k + synthetic relmat", "relmat_bands": len(relmat.bands),
+                       "relmat_lines": int(sum(len(b.lines) for b in relmat.bands)),
+                       "vpw_bands": sorted(getattr(lmx, "whitelist", set())),
+                       "host_threads": os.cpu_count()}}
     # ---- batched optimal estimation: 5,000-line CO2 list, state T + log H2O + T_sfc = 101
     l5 = pkg.synthetic.lists_5k_co2()
     s5 = pkg.Sounder.make(645.0, 700.0, 0.25, opd_max=2.0, fwhm_gauss=0.5)

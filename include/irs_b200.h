@@ -117,6 +117,9 @@ typedef struct {
     double launches;           /* kernels launched by the call */
     double evaluated_pairs;    /* pair evaluations the line-sum kernel issued (IRS_MIXED:
                                   near lines x block points + far lines x nodes) */
+    double lm_host_ms;         /* relaxation-matrix line mixing: host time building the poles
+                                  (W(T), Y(T), eigenmodes; line_mixing 2 and 3) */
+    double lm_device_ms;       /* its device pole sums (part of line_params_ms) */
 } irs_stage_times;
 
 typedef struct irs_ctx irs_ctx;

@@ -71,7 +71,8 @@ class StageTimes(C.Structure):
     _fields_ = [("line_params_ms", C.c_double), ("line_sum_ms", C.c_double),
                 ("rte_ms", C.c_double), ("ils_ms", C.c_double), ("total_ms", C.c_double),
                 ("pairs", C.c_double), ("core_pairs", C.c_double), ("h2d_bytes", C.c_double),
-                ("d2h_bytes", C.c_double), ("launches", C.c_double), ("evaluated_pairs", C.c_double)]
+                ("d2h_bytes", C.c_double), ("launches", C.c_double), ("evaluated_pairs", C.c_double),
+                ("lm_host_ms", C.c_double), ("lm_device_ms", C.c_double)]
 
 
 # every symbol the header declares, with its ctypes signature

@@ -17,6 +17,7 @@
 #include "oe.cuh"
 #include "lm_pert.cuh"
 #include <atomic>
+#include <chrono>
 #include <exception>
 #include <mutex>
 #include <thread>
@@ -410,7 +411,10 @@ static void forward_pass(irs_ctx* ctx, const irs_profile* profs, int n_prof, con
         workspace(ctx, "prt", std::max<size_t>(prt.size(), 1) * sizeof(ProfileRT));
     }
     RelmatPlan rp;
+    const auto h0 = std::chrono::steady_clock::now();
     const bool relmat = relmat_plan(ctx, pl, o, rp);
+    ctx->lm_host_pass = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
+    ctx->lm_ev = relmat;
     if (relmat) {
         const long long ps = ((n_nu + kPertAlign - 1) / kPertAlign) * kPertAlign;
         workspace(ctx, "lm_pert", (size_t)n_prof * L * ps * sizeof(double));
@@ -423,7 +427,12 @@ static void forward_pass(irs_ctx* ctx, const irs_profile* profs, int n_prof, con
     check_launch(ctx);
     if (o.with_ils) ensure_ils(ctx, ig.dnu_hi, s.opd_max, s.fwhm_gauss, o.apodization);
     long long pstride = 0;
-    const double* d_pert = relmat ? relmat_launch(ctx, rp, d_grid, n_nu, o.lm_cutoff, o.x_far, pstride) : nullptr;
+    const double* d_pert = nullptr;
+    if (relmat) {
+        IRS_CUDA(cudaEventRecord(ctx->ev[7], st));
+        d_pert = relmat_launch(ctx, rp, d_grid, n_nu, o.lm_cutoff, o.x_far, pstride);
+        IRS_CUDA(cudaEventRecord(ctx->ev[8], st));
+    }
     void* d_tau = run_linesum(ctx, pl, d_grid, n_nu, ig.g.at(0), ig.dnu_hi, o, 1, d_pert, pstride);
     IRS_CUDA(cudaEventRecord(ctx->ev[2], st));
     LayerRT* d_lrt = upload(ctx, "lrt", lrt);
@@ -674,6 +683,10 @@ static void collect_times(irs_ctx* ctx) {
     ctx->last.h2d_bytes = ctx->n_h2d;
     ctx->last.d2h_bytes = ctx->n_d2h;
     ctx->last.launches = ctx->n_launch;
+    float e = 0;
+    if (ctx->lm_ev) IRS_CUDA(cudaEventElapsedTime(&e, ctx->ev[7], ctx->ev[8]));
+    ctx->last.lm_device_ms = e + ctx->prior.lm_device_ms;
+    ctx->last.lm_host_ms = ctx->lm_host_pass + ctx->prior.lm_host_ms;
 }
 
 // Device bytes the library may use: what is free plus its own workspaces (reused or
@@ -703,6 +716,8 @@ static void forward_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, c
     IRS_REQUIRE(n_prof >= 1 && profs, "need at least one profile");
     validate_options(o);
     ctx->n_h2d = ctx->n_d2h = ctx->n_launch = 0;
+    ctx->lm_host_pass = 0;
+    ctx->lm_ev = false;
     ctx->prior = irs_stage_times{};
     const InternalGrid ig = internal_grid(s, o);
     const GridSpec ch = make_grid(s.nu_min, s.nu_max, s.dnu);
@@ -730,6 +745,8 @@ static void forward_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, c
             ctx->prior.pairs += keep.pairs;
             ctx->prior.core_pairs += keep.core_pairs;
             ctx->prior.evaluated_pairs += keep.evaluated_pairs;
+            ctx->prior.lm_host_ms += keep.lm_host_ms;
+            ctx->prior.lm_device_ms += keep.lm_device_ms;
             ctx->n_h2d = h2d, ctx->n_d2h = d2h, ctx->n_launch = nl;
         }
     }

@@ -160,7 +160,7 @@ void lm_poles(const RelmatHost& R, const Tables& tabs, int mode, uint32_t iso_ma
 struct irs_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev[8] = {};
+    cudaEvent_t ev[10] = {};
     irs::Tables tables;
     bool tips_dirty = true, cont_dirty = true;
     // device copies of tables
@@ -178,6 +178,8 @@ struct irs_ctx {
     irs_stage_times last{};
     irs_stage_times prior{};  // stage times of the earlier passes of a multi-pass batch
     double n_h2d = 0, n_d2h = 0, n_launch = 0;  // counters of the current call
+    double lm_host_pass = 0;  // host ms building relmat poles in the current pass
+    bool lm_ev = false;       // ev[7], ev[8] bracket the relmat pole sums of the current pass
     // cached ILS kernel
     double ils_key[4] = {-1, -1, -1, -1};
     int64_t ils_n = 0;

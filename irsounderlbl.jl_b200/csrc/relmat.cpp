@@ -139,10 +139,12 @@ void calc_y(const RelmatBandHost& b, double T, double q_ratio, std::vector<doubl
 inline double abs1(cd z) { return std::fabs(z.real()) + std::fabs(z.imag()); }
 
 // A (row-major n x n) -> upper Hessenberg H = Q^H A Q by Householder reflections.
-void hessenberg(int n, std::vector<cd>& A, std::vector<cd>& Q) {
-    Q.assign((size_t)n * n, cd(0.0));
-    for (int i = 0; i < n; ++i) Q[(size_t)i * n + i] = 1.0;
-    std::vector<cd> v(n);
+// Qt holds Q transposed (Qt[j*n + r] = Q[r][j]) so that every update below runs along
+// contiguous memory.
+void hessenberg(int n, std::vector<cd>& A, std::vector<cd>& Qt) {
+    Qt.assign((size_t)n * n, cd(0.0));
+    for (int i = 0; i < n; ++i) Qt[(size_t)i * n + i] = 1.0;
+    std::vector<cd> v(n), s(n);
     for (int k = 0; k + 2 < n; ++k) {
         const int m = n - k - 1;
         double xn2 = 0.0;
@@ -158,24 +160,36 @@ void hessenberg(int n, std::vector<cd>& A, std::vector<cd>& Q) {
         for (int i = 0; i < m; ++i) vn2 += std::norm(v[i]);
         if (vn2 == 0.0) continue;
         const double tau = 2.0 / vn2;
-        for (int j = k; j < n; ++j) {  // A := (I - tau v v^H) A
-            cd s = 0.0;
-            for (int i = 0; i < m; ++i) s += std::conj(v[i]) * A[(size_t)(k + 1 + i) * n + j];
-            s *= tau;
-            for (int i = 0; i < m; ++i) A[(size_t)(k + 1 + i) * n + j] -= v[i] * s;
+        // A := (I - tau v v^H) A on rows k+1.., columns k..: s = tau v^H A, then A -= v s
+        std::fill(s.begin() + k, s.end(), cd(0.0));
+        for (int i = 0; i < m; ++i) {
+            const cd cv = std::conj(v[i]) * tau;
+            const cd* row = &A[(size_t)(k + 1 + i) * n];
+            for (int j = k; j < n; ++j) s[j] += cv * row[j];
         }
-        for (int r = 0; r < n; ++r) {  // A := A (I - tau v v^H), Q := Q (I - tau v v^H)
-            cd s = 0.0, t = 0.0;
-            for (int i = 0; i < m; ++i) {
-                s += A[(size_t)r * n + k + 1 + i] * v[i];
-                t += Q[(size_t)r * n + k + 1 + i] * v[i];
-            }
-            s *= tau;
+        for (int i = 0; i < m; ++i) {
+            cd* row = &A[(size_t)(k + 1 + i) * n];
+            for (int j = k; j < n; ++j) row[j] -= v[i] * s[j];
+        }
+        // A := A (I - tau v v^H) on all rows, columns k+1..
+        for (int r = 0; r < n; ++r) {
+            cd* row = &A[(size_t)r * n + k + 1];
+            cd t = 0.0;
+            for (int i = 0; i < m; ++i) t += row[i] * v[i];
             t *= tau;
-            for (int i = 0; i < m; ++i) {
-                A[(size_t)r * n + k + 1 + i] -= s * std::conj(v[i]);
-                Q[(size_t)r * n + k + 1 + i] -= t * std::conj(v[i]);
-            }
+            for (int i = 0; i < m; ++i) row[i] -= t * std::conj(v[i]);
+        }
+        // Q := Q (I - tau v v^H), i.e. rows k+1.. of Qt: Qt -= conj(v) (tau v^T Qt)
+        std::fill(s.begin(), s.end(), cd(0.0));
+        for (int i = 0; i < m; ++i) {
+            const cd cv = v[i] * tau;
+            const cd* row = &Qt[(size_t)(k + 1 + i) * n];
+            for (int r = 0; r < n; ++r) s[r] += cv * row[r];
+        }
+        for (int i = 0; i < m; ++i) {
+            const cd cv = std::conj(v[i]);
+            cd* row = &Qt[(size_t)(k + 1 + i) * n];
+            for (int r = 0; r < n; ++r) row[r] -= cv * s[r];
         }
         A[(size_t)(k + 1) * n + k] = alpha;
         for (int i = 1; i < m; ++i) A[(size_t)(k + 1 + i) * n + k] = 0.0;
@@ -192,8 +206,8 @@ inline void givens(cd x, cd y, double& c, cd& s) {
     s = (x / ax) * std::conj(y) / nr;
 }
 
-// Hessenberg H -> upper triangular T = Z^H A Z (Z enters holding Q).
-bool schur(int n, std::vector<cd>& H, std::vector<cd>& Z) {
+// Hessenberg H -> upper triangular T = Z^H A Z; Zt (Z transposed) enters holding Q.
+bool schur(int n, std::vector<cd>& H, std::vector<cd>& Zt) {
     const double eps = DBL_EPSILON;
     double hnorm = 0.0;
     for (auto& h : H) hnorm = std::max(hnorm, abs1(h));
@@ -229,21 +243,27 @@ bool schur(int n, std::vector<cd>& H, std::vector<cd>& Z) {
             double c;
             cd s;
             givens(x, y, c, s);
+            const cd sc = std::conj(s);
+            cd* r0 = &H[(size_t)k * n];
+            cd* r1 = &H[(size_t)(k + 1) * n];
             for (int j = (k == l ? l : k - 1); j < n; ++j) {
-                const cd h1 = H[(size_t)k * n + j], h2 = H[(size_t)(k + 1) * n + j];
-                H[(size_t)k * n + j] = c * h1 + s * h2;
-                H[(size_t)(k + 1) * n + j] = -std::conj(s) * h1 + c * h2;
+                const cd h1 = r0[j], h2 = r1[j];
+                r0[j] = c * h1 + s * h2;
+                r1[j] = -sc * h1 + c * h2;
             }
             const int rmax = std::min(k + 2, hi);
             for (int r = 0; r <= rmax; ++r) {
-                const cd h1 = H[(size_t)r * n + k], h2 = H[(size_t)r * n + k + 1];
-                H[(size_t)r * n + k] = h1 * c + h2 * std::conj(s);
-                H[(size_t)r * n + k + 1] = -h1 * s + h2 * c;
+                cd* row = &H[(size_t)r * n + k];
+                const cd h1 = row[0], h2 = row[1];
+                row[0] = h1 * c + h2 * sc;
+                row[1] = -h1 * s + h2 * c;
             }
+            cd* z0 = &Zt[(size_t)k * n];
+            cd* z1 = &Zt[(size_t)(k + 1) * n];
             for (int r = 0; r < n; ++r) {
-                const cd z1 = Z[(size_t)r * n + k], z2 = Z[(size_t)r * n + k + 1];
-                Z[(size_t)r * n + k] = z1 * c + z2 * std::conj(s);
-                Z[(size_t)r * n + k + 1] = -z1 * s + z2 * c;
+                const cd a = z0[r], b = z1[r];
+                z0[r] = a * c + b * sc;
+                z1[r] = -a * s + b * c;
             }
             if (k > l) H[(size_t)(k + 1) * n + k - 1] = 0.0;
         }
@@ -253,37 +273,42 @@ bool schur(int n, std::vector<cd>& H, std::vector<cd>& Z) {
 
 // Eigen-decomposition of M: lam[k], X[i*n + k] (column k = eigenvector k).
 bool eig(int n, std::vector<cd> M, std::vector<cd>& lam, std::vector<cd>& X) {
-    std::vector<cd> Z;
-    hessenberg(n, M, Z);
-    if (!schur(n, M, Z)) return false;
+    std::vector<cd> Zt;
+    hessenberg(n, M, Zt);
+    if (!schur(n, M, Zt)) return false;
     lam.resize(n);
     for (int k = 0; k < n; ++k) lam[k] = M[(size_t)k * n + k];
     const double eps = DBL_EPSILON, small = DBL_MIN * (n / eps);
-    std::vector<cd> V((size_t)n * n, cd(0.0));
+    std::vector<cd> V((size_t)n * n, cd(0.0)), v(n);
     for (int k = n - 1; k >= 0; --k) {  // T v = lam_k v, v upper part of column k
-        V[(size_t)k * n + k] = 1.0;
+        v[k] = 1.0;
         const cd lk = lam[k];
         const double smin = std::max(eps * abs1(lk), small);
         for (int i = k - 1; i >= 0; --i) {
+            const cd* row = &M[(size_t)i * n];
             cd s = 0.0;
-            for (int j = i + 1; j <= k; ++j) s += M[(size_t)i * n + j] * V[(size_t)j * n + k];
-            cd d = M[(size_t)i * n + i] - lk;
+            for (int j = i + 1; j <= k; ++j) s += row[j] * v[j];
+            cd d = row[i] - lk;
             if (abs1(d) < smin) d = smin;
-            const cd v = -s / d;
-            V[(size_t)i * n + k] = v;
-            if (abs1(v) > 1e50) {  // rescale the column built so far
-                const double sc = 1.0 / abs1(v);
-                for (int q = i; q <= k; ++q) V[(size_t)q * n + k] *= sc;
+            v[i] = -s / d;
+            if (abs1(v[i]) > 1e50) {  // rescale the vector built so far
+                const double sc = 1.0 / abs1(v[i]);
+                for (int q = i; q <= k; ++q) v[q] *= sc;
             }
         }
+        for (int i = 0; i <= k; ++i) V[(size_t)i * n + k] = v[i];
     }
+    // X = Z V, row by row: X[i][:] = sum_j Z[i][j] V[j][:] (V upper triangular)
     X.assign((size_t)n * n, cd(0.0));
-    for (int i = 0; i < n; ++i)
-        for (int k = 0; k < n; ++k) {
-            cd s = 0.0;
-            for (int j = 0; j <= k; ++j) s += Z[(size_t)i * n + j] * V[(size_t)j * n + k];
-            X[(size_t)i * n + k] = s;
+    for (int j = 0; j < n; ++j) {
+        const cd* vr = &V[(size_t)j * n];
+        const cd* zc = &Zt[(size_t)j * n];  // column j of Z
+        for (int i = 0; i < n; ++i) {
+            const cd z = zc[i];
+            cd* xr = &X[(size_t)i * n];
+            for (int k = j; k < n; ++k) xr[k] += z * vr[k];
         }
+    }
     return true;
 }
 
