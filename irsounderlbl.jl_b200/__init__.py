@@ -401,6 +401,8 @@ from .estimation import (ColumnScale, FullProfile, Jacobian, PartialColumns, Sta
                          finite_difference_jacobian, forward_model_rrule, pack_state, partial_column_basis,
                          state_labels, unpack_state, vmr_range, build_sa, scene_nedt, exclude_channels,
                          RetrievalResult, optimal_estimation, optimal_estimation_batch, oe_diagnostics)
+from .hitran import (LINELIST_CACHE_VERSION, clear_linelist_cache, filter_linelist, linelist_cache_dir,  # noqa: E402,F401,E501
+                     load_hitran_par, load_linelist, parse_hitran_par, set_linelist_cache_dir)
 from .relmat import (BandModes, HITRANRelmatData, RelmatBand, VPWLineMixing, VPYLineMixing,  # noqa: E402,F401
                      W0B0Table, band_eff_strength, band_modes, build_w_matrix, calc_w_and_y,
                      compute_lm_dispersive_correction, compute_voigt_lm_cross_sections,
