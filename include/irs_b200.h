@@ -73,8 +73,8 @@ typedef struct {
  *   (the y0 uploaded with the CO2 list; line_mixing.jl:1351-1369),
  *   2 VPYLineMixing(relmat) and 3 VPWLineMixing(relmat) on the relaxation-matrix
  *   data of irs_upload_relmat (line_mixing.jl:208-241, 1093-1154, 1303-1369)
- * continua: bit mask 1 :h2o, 2 :co2, 4 :co2_cia, 8 :n2, 16 :o2 (CIA tables are
- *   not bundled and contribute zeros, as the reference does without them)
+ * continua: bit mask 1 :h2o, 2 :co2, 4 :co2_cia, 8 :n2, 16 :o2 (the CIA pairs use
+ *   the tables of irs_set_cia and contribute zeros without them, as the reference)
  * method: VoigtMethod of the line sum (forward_model uses FullFaddeeva)
  * precision: IRS_FP64, IRS_MIXED or IRS_MIXED_DIRECT */
 typedef struct {
@@ -141,6 +141,14 @@ int irs_set_continuum_h2o(irs_ctx* ctx, int n, const double* nu, const double* c
                           const double* cf, const double* texp);
 int irs_set_continuum_co2(irs_ctx* ctx, int n, const double* nu, const double* s,
                           const double* xfac, const double* tdep);
+
+/* HITRAN CIA table of one pair (replaces continuum.jl:104-165 reading data/cia/*.cia):
+ * pair 1 CO2-CO2, 2 N2-N2, 3 O2-O2; block b (file order) is at temperature T[b] with
+ * knots nu/sigma[off[b] .. off[b+1]) in increasing nu (cm^-1; cm^5/molecule^2, clamped
+ * at 0 as the reader does).  n_blocks = 0 removes the table; a missing table
+ * contributes zeros, as in the reference. */
+int irs_set_cia(irs_ctx* ctx, int pair, int n_blocks, const double* T, const int64_t* off,
+                const double* nu, const double* sigma);
 
 /* Upload the line list of one species (HITRANLinelist, linelist.jl:51-56; lines
  * sorted by wavenumber as HITRANLinelist guarantees -- unsorted input is sorted

@@ -221,6 +221,19 @@ class B200Context:
                                            dptr(yy) if yy is not None else None))
         self._lists[int(species)] = (key, ll, y0)
 
+    def set_cia(self, pair: int, blocks):
+        """A HITRAN CIA table (pair 1 CO2-CO2, 2 N2-N2, 3 O2-O2) as load_cia_table returns it;
+        None or [] removes it."""
+        blocks = blocks or []
+        T = np.array([b[0] for b in blocks], dtype=np.float64)
+        off = np.zeros(len(blocks) + 1, dtype=np.int64)
+        off[1:] = np.cumsum([len(b[1]) for b in blocks])
+        nu = np.ascontiguousarray(np.concatenate([b[1] for b in blocks]) if blocks else np.zeros(0), dtype=np.float64)
+        sg = np.ascontiguousarray(np.concatenate([b[2] for b in blocks]) if blocks else np.zeros(0), dtype=np.float64)
+        check(self.lib.irs_set_cia(self.h, int(pair), len(blocks), dptr(T) if len(T) else None,
+                                   off.ctypes.data_as(C.POINTER(C.c_int64)), dptr(nu) if len(nu) else None,
+                                   dptr(sg) if len(sg) else None))
+
     def upload_relmat(self, data, whitelist=frozenset(), min_band_strength: float = 0.0, bands=None):
         """Hand HITRANRelmatData (optionally a subset of its bands) to the library."""
         bands = data.bands if bands is None else bands
@@ -401,6 +414,7 @@ from .estimation import (ColumnScale, FullProfile, Jacobian, PartialColumns, Sta
                          finite_difference_jacobian, forward_model_rrule, pack_state, partial_column_basis,
                          state_labels, unpack_state, vmr_range, build_sa, scene_nedt, exclude_channels,
                          RetrievalResult, optimal_estimation, optimal_estimation_batch, oe_diagnostics)
+from .continuum import CIA_PAIRS, load_cia_table  # noqa: E402,F401
 from .hitran import (LINELIST_CACHE_VERSION, clear_linelist_cache, filter_linelist, linelist_cache_dir,  # noqa: E402,F401,E501
                      load_hitran_par, load_linelist, parse_hitran_par, set_linelist_cache_dir)
 from .relmat import (BandModes, HITRANRelmatData, RelmatBand, VPWLineMixing, VPYLineMixing,  # noqa: E402,F401

@@ -132,6 +132,7 @@ SIGNATURES = {
     "irs_surrogate_infer": ([_P, _PF, C.c_int64, _PF, _PF], C.c_int),
     "irs_surrogate_infer_device": ([_P, _P, C.c_int64, _P, _P, _P], C.c_int),
     "irs_gemm_bf16": ([_P, _P, _P, C.c_int, C.c_int, C.c_int, _PF], C.c_int),
+    "irs_set_cia": ([_P, C.c_int, C.c_int, _PD, C.POINTER(C.c_int64), _PD, _PD], C.c_int),
     "irs_upload_relmat": ([_P, C.c_int, C.POINTER(RelmatBandC), C.c_int, C.POINTER(WtfitEntryC), C.c_int64,
                            C.c_double], C.c_int),
     "irs_relmat_w_matrix": ([C.POINTER(RelmatBandC), C.POINTER(WtfitEntryC), C.c_int64, C.c_double, C.c_double,

@@ -86,8 +86,36 @@ void upload_tables(irs_ctx* ctx) {
         ctx->d_co2 = upload(ctx, "ckd_co2", c);
         ctx->n_h2o = (int)t.h2o_nu.size();
         ctx->n_co2 = (int)t.co2_nu.size();
+        // CIA blocks of the three tables in order: (T, nu_min, nu_max, first knot, count)
+        std::vector<double> blk, knu, ksg;
+        for (int q = 0; q < 3; ++q) {
+            ctx->cia_b0[q] = (int)(blk.size() / 5);
+            for (const Tables::CiaBlock& b : t.cia[q]) {
+                blk.insert(blk.end(), {b.T, b.nu.front(), b.nu.back(), (double)knu.size(), (double)b.nu.size()});
+                knu.insert(knu.end(), b.nu.begin(), b.nu.end());
+                ksg.insert(ksg.end(), b.sg.begin(), b.sg.end());
+            }
+        }
+        ctx->cia_b0[3] = (int)(blk.size() / 5);
+        ctx->d_cia_blk = upload(ctx, "cia_blk", blk);
+        ctx->d_cia_nu = upload(ctx, "cia_nu", knu);
+        ctx->d_cia_sg = upload(ctx, "cia_sg", ksg);
         ctx->cont_dirty = false;
     }
+}
+
+// continua of the call: MT-CKD H2O/CO2 and the CIA pairs whose tables are loaded
+// (a missing table contributes zeros, continuum.jl:190-194, 268-272)
+static ContDev cont_dev(irs_ctx* ctx, const irs_fm_options& o) {
+    ContDev cd;
+    cd.h2o = ctx->d_h2o; cd.co2 = ctx->d_co2; cd.n_h2o = ctx->n_h2o; cd.n_co2 = ctx->n_co2;
+    cd.mask = 0;
+    cd.cia.blk = ctx->d_cia_blk; cd.cia.nu = ctx->d_cia_nu; cd.cia.sg = ctx->d_cia_sg;
+    for (int q = 0; q < 4; ++q) cd.cia.b0[q] = ctx->cia_b0[q];
+    if (o.apply_continuum)
+        for (int q = 0; q < 3; ++q)
+            if ((o.continua & (4 << q)) && ctx->cia_b0[q + 1] > ctx->cia_b0[q]) cd.mask |= 4 << q;
+    return cd;
 }
 
 static TipsDev tips_dev(irs_ctx* ctx) {
@@ -438,9 +466,7 @@ static void forward_pass(irs_ctx* ctx, const irs_profile* profs, int n_prof, con
     LayerRT* d_lrt = upload(ctx, "lrt", lrt);
     ProfileRT* d_prt = upload(ctx, "prt", prt);
     double* d_I = (double*)workspace(ctx, "I", (size_t)n_prof * n_nu * sizeof(double));
-    ContDev cd;
-    cd.h2o = ctx->d_h2o; cd.co2 = ctx->d_co2; cd.n_h2o = ctx->n_h2o; cd.n_co2 = ctx->n_co2;
-    cd.mask = 0;
+    ContDev cd = cont_dev(ctx, o);
     if (o.apply_continuum) {
         if ((o.continua & 1) && ctx->n_h2o > 1) cd.mask |= 1;
         if ((o.continua & 2) && ctx->n_co2 > 1) cd.mask |= 2;
@@ -632,8 +658,7 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
 #undef IRS_JG
             check_launch(ctx);
         }
-        ContDev cd;
-        cd.h2o = ctx->d_h2o; cd.co2 = ctx->d_co2; cd.n_h2o = ctx->n_h2o; cd.n_co2 = ctx->n_co2; cd.mask = 0;
+        ContDev cd = cont_dev(ctx, o);
         if (o.apply_continuum) {
             if ((o.continua & 1) && ctx->n_h2o > 1) cd.mask |= 1;
             if ((o.continua & 2) && ctx->n_co2 > 1) cd.mask |= 2;
@@ -1074,6 +1099,27 @@ int irs_set_continuum_co2(irs_ctx* ctx, int n, const double* nu, const double* s
     t.co2_s.resize(n);
     for (int i = 0; i < n; ++i) t.co2_s[i] = s[i] * xf[i];  // continuum.jl:90
     t.co2_tdep.assign(td, td + n);
+    ctx->cont_dirty = true;
+    IRS_API_END
+}
+
+int irs_set_cia(irs_ctx* ctx, int pair, int n_blocks, const double* T, const int64_t* off, const double* nu,
+                const double* sigma) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && pair >= 1 && pair <= 3, "CIA pair must be 1 (CO2-CO2), 2 (N2-N2) or 3 (O2-O2)");
+    IRS_REQUIRE(n_blocks >= 0 && (n_blocks == 0 || (T && off && nu && sigma)), "invalid CIA table");
+    std::vector<Tables::CiaBlock> B;
+    for (int b = 0; b < n_blocks; ++b) {
+        IRS_REQUIRE(off[b + 1] >= off[b], "CIA block offsets must not decrease");
+        if (off[b + 1] == off[b]) continue;
+        Tables::CiaBlock c;
+        c.T = T[b];
+        c.nu.assign(nu + off[b], nu + off[b + 1]);
+        c.sg.assign(sigma + off[b], sigma + off[b + 1]);
+        for (size_t i = 1; i < c.nu.size(); ++i) IRS_REQUIRE(c.nu[i] > c.nu[i - 1], "CIA knots must increase");
+        B.push_back(std::move(c));
+    }
+    ctx->tables.cia[pair - 1] = std::move(B);
     ctx->cont_dirty = true;
     IRS_API_END
 }

@@ -125,6 +125,12 @@ struct Tables {
     double q_value(int mol, int iso, double T) const;  // partition.jl:8-24
     std::vector<double> h2o_nu, h2o_cs, h2o_cf, h2o_te;
     std::vector<double> co2_nu, co2_s, co2_tdep;  // S already multiplied by xfac
+    // HITRAN CIA tables (CO2-CO2, N2-N2, O2-O2): per block T, knots, sigma
+    struct CiaBlock {
+        double T;
+        std::vector<double> nu, sg;
+    };
+    std::vector<CiaBlock> cia[3];
 };
 
 // ---------------------------------------------- relaxation-matrix line mixing
@@ -171,6 +177,8 @@ struct irs_ctx {
     int tips_stride = 2;
     std::map<std::pair<int, int>, int> tips_index;
     double *d_h2o = nullptr, *d_co2 = nullptr;  // packed tables
+    double *d_cia_blk = nullptr, *d_cia_nu = nullptr, *d_cia_sg = nullptr;
+    int cia_b0[4] = {0, 0, 0, 0};
     int n_h2o = 0, n_co2 = 0;
     std::vector<irs::DevLineList> lists;
     irs::RelmatHost relmat;

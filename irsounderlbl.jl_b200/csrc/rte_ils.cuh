@@ -34,12 +34,103 @@ inline GridDev to_dev(const GridSpec& g) {
     return d;
 }
 
+// HITRAN CIA tables on the device (continuum.jl:104-160): tables t = 0 CO2-CO2,
+// 1 N2-N2, 2 O2-O2 hold blocks [b0[t], b0[t+1]) in file order, each described by
+// (T, nu_min, nu_max, first knot, knot count) with ascending knots nu/sg.
+struct CiaDev {
+    const double* blk;
+    const double* nu;
+    const double* sg;
+    int b0[4];
+};
+constexpr int kCiaMax = 16;  // applicable blocks of one table cached per grid point
+// The blocks that contain one grid point, their temperatures and sigma(nu), in file
+// order (the temperature bracket of each layer is then a scan of these).
+struct CiaPoint {
+    double T[3][kCiaMax], s[3][kCiaMax];
+    int n[3];
+};
+
 struct ContDev {
     const double* h2o;  // nu[n], cs[n], cf[n], te[n]
     const double* co2;  // nu[n], seff[n], tdep[n]
     int n_h2o, n_co2;
-    int mask;           // 1 h2o, 2 co2 (only when apply_continuum)
+    int mask;           // 1 h2o, 2 co2, 4 co2_cia, 8 n2, 16 o2 (only when apply_continuum)
+    CiaDev cia;
 };
+constexpr int kCiaMask = 4 | 8 | 16;
+
+// linear interpolation on the block's knots (Interpolations.jl linear_interpolation)
+__device__ __forceinline__ double cia_block_value(const CiaDev& c, int b, double nu) {
+    const double* d = c.blk + 5 * (size_t)b;
+    const double* x = c.nu + (long long)d[3];
+    const double* y = c.sg + (long long)d[3];
+    const int n = (int)d[4];
+    if (n == 1) return y[0];
+    int lo = 0, hi = n;  // upper_bound
+    while (lo < hi) { const int mid = (lo + hi) >> 1; if (x[mid] <= nu) lo = mid + 1; else hi = mid; }
+    const int i = min(max(lo - 1, 0), n - 2);
+    const double w = (nu - x[i]) / (x[i + 1] - x[i]);
+    return y[i] * (1.0 - w) + y[i + 1] * w;
+}
+__device__ __forceinline__ void cia_prepare(const CiaDev& c, int mask, double nu, CiaPoint& cp) {
+    for (int t = 0; t < 3; ++t) {
+        cp.n[t] = 0;
+        if (!(mask & (4 << t))) continue;
+        for (int b = c.b0[t]; b < c.b0[t + 1]; ++b) {
+            const double* d = c.blk + 5 * (size_t)b;
+            if (nu < d[1] || nu > d[2]) continue;
+            const int k = cp.n[t]++;
+            if (k < kCiaMax) {
+                cp.T[t][k] = d[0];
+                cp.s[t][k] = cia_block_value(c, b, nu);
+            }
+        }
+    }
+}
+// _cia_sigma (continuum.jl:333-362): the applicable blocks bracketing T (first in file
+// order among equal temperatures), linear in T, the nearest one outside the range
+__device__ __forceinline__ double cia_sigma_at(const CiaDev& c, const CiaPoint& cp, int t, double nu, double T) {
+    const int na = cp.n[t];
+    if (na == 0) return 0.0;
+    bool hl = false, hh = false;
+    double T_lo = 0, s_lo = 0, T_hi = 0, s_hi = 0;
+    auto take = [&](double bt, double s) {
+        if (bt <= T && (!hl || bt > T_lo)) { hl = true; T_lo = bt; s_lo = s; }
+        if (bt >= T && (!hh || bt < T_hi)) { hh = true; T_hi = bt; s_hi = s; }
+    };
+    if (na <= kCiaMax) {
+        for (int k = 0; k < na; ++k) take(cp.T[t][k], cp.s[t][k]);
+    } else {  // more applicable blocks than cached: scan the table
+        for (int b = c.b0[t]; b < c.b0[t + 1]; ++b) {
+            const double* d = c.blk + 5 * (size_t)b;
+            if (nu < d[1] || nu > d[2]) continue;
+            take(d[0], cia_block_value(c, b, nu));
+        }
+    }
+    if (!hl) return s_hi;
+    if (!hh) return s_lo;
+    if (T_lo == T_hi) return s_lo;
+    const double w = (T - T_lo) / (T_hi - T_lo);
+    return (1.0 - w) * s_lo + w * s_hi;
+}
+// co2_cia, n2_cia, o2_cia (continuum.jl:252-331) times dz: sigma x pair densities
+__device__ __forceinline__ double cia_tau(const ContDev& c, const CiaPoint& cp, double nu, double vh, double vc,
+                                          double p, double T, double dz) {
+    const double nair = p * 100.0 / (1.380649e-23 * T) * 1e-6;
+    const double vdry = 1.0 - vh;
+    double k = 0.0;
+    if (c.mask & 4) k += cia_sigma_at(c.cia, cp, 0, nu, T) * (vc * nair) * nair;
+    if (c.mask & 8) {
+        const double n2 = 0.78084 * vdry * nair;
+        k += cia_sigma_at(c.cia, cp, 1, nu, T) * n2 * n2;
+    }
+    if (c.mask & 16) {
+        const double o2 = 0.20946 * vdry * nair;
+        k += cia_sigma_at(c.cia, cp, 2, nu, T) * o2 * o2;
+    }
+    return k * dz;
+}
 
 __global__ void grid_values_kernel(GridDev g, double* out) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -89,8 +180,9 @@ __device__ __forceinline__ double lerp_val(const double* v, const Lerp& l) {
 template <typename TT>
 __device__ __forceinline__ double layer_tau(const TT* tau_l, long long i, double nu, const LayerRT& r,
                                             const ContDev& c, double Cs, double Cf, double te, double Se,
-                                            double td) {
+                                            double td, const CiaPoint& cp) {
     double t = (double)tau_l[i];
+    if (c.mask & kCiaMask) t += cia_tau(c, cp, nu, r.vmr_h2o, r.vmr_co2, r.p_mid, r.T_mid, r.dz_cm);
     if (c.mask) {
         const double T = r.T_mid, p = r.p_mid;
         const double rho = (p / 1013.0) * (296.0 / T);
@@ -132,6 +224,8 @@ __global__ void __launch_bounds__(256) rte_kernel(const TT* __restrict__ tau, co
         Se = lerp_val(cont.co2 + cont.n_co2, l);
         td = lerp_val(cont.co2 + 2 * cont.n_co2, l);
     }
+    CiaPoint cp;
+    if (cont.mask & kCiaMask) cia_prepare(cont.cia, cont.mask, nu, cp);
     const ProfileRT pr = prt[p];
     const LayerRT* lr = lrt + (size_t)p * L;
     const TT* tp = tau + (size_t)p * L * n_nu;
@@ -139,7 +233,7 @@ __global__ void __launch_bounds__(256) rte_kernel(const TT* __restrict__ tau, co
     double I_atm = 0.0;
     for (int k = L - 1; k >= 0; --k) {
         const LayerRT r = lr[k];
-        const double s = layer_tau(tp + (size_t)k * n_nu, i, nu, r, cont, Cs, Cf, te, Se, td) / pr.mu;
+        const double s = layer_tau(tp + (size_t)k * n_nu, i, nu, r, cont, Cs, Cf, te, Se, td, cp) / pr.mu;
         const double Tr_k = Tr_up * exp(-s);
         const double dT = Tr_up - Tr_k;
         if (src == 0) {
@@ -157,7 +251,7 @@ __global__ void __launch_bounds__(256) rte_kernel(const TT* __restrict__ tau, co
         double Id = 0.0, g = 1.0;
         for (int k = 0; k < L; ++k) {
             const LayerRT r = lr[k];
-            const double s = layer_tau(tp + (size_t)k * n_nu, i, nu, r, cont, Cs, Cf, te, Se, td) / pr.mu;
+            const double s = layer_tau(tp + (size_t)k * n_nu, i, nu, r, cont, Cs, Cf, te, Se, td, cp) / pr.mu;
             double em;
             if (src == 0) {
                 const double Ba = planck64(nu, r.T_ave), Bb = planck64(nu, r.T_bot);

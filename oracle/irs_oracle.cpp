@@ -474,6 +474,56 @@ void co2_continuum_add(const double* grid, long n, double vmr, double p, double 
     }
 }
 
+// HITRAN CIA tables (continuum.jl:104-160): blocks of (T, nu range, sigma(nu)),
+// nu ascending within a block, sigma clamped at 0 when loaded.
+struct CiaBlock {
+    double T, numin, numax;
+    std::vector<double> nu, sg;
+};
+std::vector<CiaBlock> g_cia[3];  // 0 CO2-CO2, 1 N2-N2, 2 O2-O2
+
+// linear interpolation inside a block (the block's own knots)
+double cia_block_value(const CiaBlock& b, double nu) {
+    const std::vector<double>& x = b.nu;
+    const long n = (long)x.size();
+    if (n == 1) return b.sg[0];
+    long i = (long)(std::upper_bound(x.begin(), x.end(), nu) - x.begin()) - 1;
+    i = std::max(0L, std::min(i, n - 2));
+    const double w = (nu - x[i]) / (x[i + 1] - x[i]);
+    return b.sg[i] * (1.0 - w) + b.sg[i + 1] * w;
+}
+// _cia_sigma (continuum.jl:333-362): blocks containing nu, T bracketed linearly,
+// the nearest block's value outside the bracketed range
+double cia_sigma(const std::vector<CiaBlock>& B, double nu, double T) {
+    double T_lo = -INFINITY, s_lo = 0.0, T_hi = INFINITY, s_hi = 0.0;
+    bool any = false;
+    for (const CiaBlock& b : B) {
+        if (nu < b.numin || nu > b.numax) continue;
+        any = true;
+        const double s = cia_block_value(b, nu);
+        if (b.T <= T && b.T > T_lo) { T_lo = b.T; s_lo = s; }
+        if (b.T >= T && b.T < T_hi) { T_hi = b.T; s_hi = s; }
+    }
+    if (!any) return 0.0;
+    if (!std::isfinite(T_lo)) return s_hi;
+    if (!std::isfinite(T_hi)) return s_lo;
+    if (T_lo == T_hi) return s_lo;
+    const double w = (T - T_lo) / (T_hi - T_lo);
+    return (1.0 - w) * s_lo + w * s_hi;
+}
+// co2_cia / n2_cia / o2_cia (continuum.jl:252-331): sigma * pair densities * dz
+void cia_add(const double* grid, long n, int continua, double vh, double vc, double p, double T, double dz,
+             double* tau) {
+    const double nair = p * 100.0 / (1.380649e-23 * T) * 1e-6;
+    const double vdry = 1.0 - vh;
+    const double nn[3] = {vc * nair * nair, (0.78084 * vdry * nair) * (0.78084 * vdry * nair),
+                          (0.20946 * vdry * nair) * (0.20946 * vdry * nair)};
+    for (int t = 0; t < 3; ++t) {
+        if (!(continua & (4 << t)) || g_cia[t].empty()) continue;
+        for (long i = 0; i < n; ++i) tau[i] += cia_sigma(g_cia[t], grid[i], T) * nn[t] * dz;
+    }
+}
+
 // ------------------------------------------------------------- solver
 double planck(double nu, double T) { return PLANCK_C1 * (nu * nu * nu) / std::expm1(PLANCK_C2 * nu / T); }
 double bt(double nu, double R) {
@@ -922,6 +972,23 @@ int orc_rte(const double* grid, int64_t n_nu, int L, const double* tau, const do
 }
 
 // sounder.jl:233-360
+int orc_set_cia(int pair, int n_blocks, const double* T, const int64_t* off, const double* nu, const double* sg) {
+    if (pair < 1 || pair > 3) return fail("CIA pair must be 1 (CO2-CO2), 2 (N2-N2) or 3 (O2-O2)");
+    std::vector<CiaBlock> B;
+    for (int b = 0; b < n_blocks; ++b) {
+        CiaBlock c;
+        c.T = T[b];
+        c.nu.assign(nu + off[b], nu + off[b + 1]);
+        c.sg.assign(sg + off[b], sg + off[b + 1]);
+        if (c.nu.empty()) continue;
+        c.numin = c.nu.front();
+        c.numax = c.nu.back();
+        B.push_back(std::move(c));
+    }
+    g_cia[pair - 1] = std::move(B);
+    return 0;
+}
+
 static orc_lm_cb g_lm_cb = nullptr;
 static void* g_lm_user = nullptr;
 static int g_lm_species = 0;
@@ -1051,8 +1118,9 @@ int orc_forward_model(int n_lev, const double* p_lev, const double* T_lev, int n
             const double dz = dp_to_dz_cm(dp[k], p_mid[k], T_mid[k]);
             if (o->continua & 1) h2o_continuum_add(grid.data(), nw, vh, p_mid[k], T_mid[k], dz, tk);
             if (o->continua & 2) co2_continuum_add(grid.data(), nw, vc, p_mid[k], T_mid[k], dz, tk);
-            // CIA tables (:co2_cia, :n2, :o2) are not bundled: they contribute zeros
-            // exactly as the reference does when the data is absent (continuum.jl:268-272).
+            // CIA (:co2_cia, :n2, :o2) from the tables of orc_set_cia; zeros without them,
+            // as the reference does when the data is absent (continuum.jl:268-272)
+            cia_add(grid.data(), nw, o->continua, vh, vc, p_mid[k], T_mid[k], dz, tk);
         }
     }
     if (tau_out) std::copy(tau.begin(), tau.end(), tau_out);
@@ -1212,6 +1280,7 @@ int orc_analytic_jacobian(int n_lev, const double* p_lev, const double* T_lev, i
         const double dz = dp_to_dz_cm(dp[k], p_mid[k], Tm);
         if (o->continua & 1) h2o_continuum_add(grid.data(), nw, vh, p_mid[k], Tm, dz, out.data());
         if (o->continua & 2) co2_continuum_add(grid.data(), nw, vc, p_mid[k], Tm, dz, out.data());
+        cia_add(grid.data(), nw, o->continua, vh, vc, p_mid[k], Tm, dz, out.data());
     };
     const bool cvh = o->apply_continuum && vmr_coupling && is_retr(1);
     const bool cvc = o->apply_continuum && vmr_coupling && is_retr(2);

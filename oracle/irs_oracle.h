@@ -128,6 +128,12 @@ typedef int (*orc_lm_cb)(void* user, double T, double p_atm, const double* grid,
                          double* dsigma);
 int orc_set_lm_callback(int species, orc_lm_cb cb, void* user);
 
+/* HITRAN CIA table of a pair (1 CO2-CO2, 2 N2-N2, 3 O2-O2; continuum.jl:104-160):
+ * n_blocks blocks, block b at temperature T[b] with knots nu/sg[off[b] .. off[b+1])
+ * in ascending nu, sigma already clamped at 0.  n_blocks = 0 removes it. */
+int orc_set_cia(int pair, int n_blocks, const double* T, const int64_t* off, const double* nu,
+                const double* sg);
+
 int orc_num_threads(void);
 const char* orc_last_error(void);
 

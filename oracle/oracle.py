@@ -171,9 +171,21 @@ class Oracle:
                                             C.POINTER(Sounder), C.POINTER(FMOptions), i32, C.c_void_p,
                                             i32, i32, i32, i32, i32, i32, i64, i64, pd, pd]
         L.orc_set_lm_callback.argtypes = [i32, LM_CALLBACK, C.c_void_p]
+        L.orc_set_cia.argtypes = [i32, i32, pd, C.c_void_p, pd, pd]
         L.orc_last_error.restype = C.c_char_p
         if load_tables:
             self.load_tables()
+
+    def set_cia(self, pair, blocks):
+        """CIA table of a pair (1 CO2-CO2, 2 N2-N2, 3 O2-O2): [(T, nu[], sigma[])], or None."""
+        blocks = blocks or []
+        T = np.array([b[0] for b in blocks], dtype=np.float64)
+        off = np.zeros(len(blocks) + 1, dtype=np.int64)
+        off[1:] = np.cumsum([len(b[1]) for b in blocks])
+        nu = np.ascontiguousarray(np.concatenate([b[1] for b in blocks]) if blocks else np.zeros(1))
+        sg = np.ascontiguousarray(np.concatenate([b[2] for b in blocks]) if blocks else np.zeros(1))
+        self._check(self.lib.orc_set_cia(pair, len(blocks), _dp(T if len(T) else np.zeros(1)), off.ctypes.data,
+                                         _dp(nu), _dp(sg)))
 
     # -- tables -------------------------------------------------------------
     def load_tables(self, h2o=True, co2=True):
