@@ -423,4 +423,9 @@ from .relmat import (BandModes, HITRANRelmatData, RelmatBand, VPWLineMixing, VPY
                      compute_voigt_vpw_cross_sections, compute_vpw_band_perturbation, compute_vpw_band_xsec,
                      default_vpw_whitelist, load_hitran_relmat, load_wtfit, parse_bandinfo, parse_sfile,
                      relmat_lines, vpw_perturbation)
+from .iasi_l1c import (IASIL1CGranule, brightness_temperature, cloud_fraction, measurement, nfov,  # noqa: E402,F401
+                       read_iasi_l1c, retrieve_granule, solar_reflection_angle)
+from .noise_covariance import (SounderNoiseCovariance, load_noise_covariance, measurement_covariance,  # noqa: E402,F401,E501
+                               read_iasi_ncm, subset_channels, to_bt)
+from .robust import RobustRetrievalResult, robust_estimation, robust_estimation_batch  # noqa: E402,F401
 from .surrogate import Surrogate, surrogate_features, surrogate_first_guess, surrogate_forward_batch  # noqa: E402,F401,E501
