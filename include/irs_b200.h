@@ -317,6 +317,19 @@ int irs_lm_perturbation(irs_ctx* ctx, int mode, const double* grid, int64_t n_nu
                         double p_atm, double cutoff, double x_far, double keep_threshold,
                         uint32_t isotope_mask, double* dsigma);
 
+/* irs_oe_batch with a banded measurement covariance instead of a diagonal one: the
+ * apodised Se of IASI L1C (apodized_measurement_covariance, covariance.jl:62-81) that
+ * optimal_estimation takes as a matrix (optimal_estimation.jl:166-176).  se_band is
+ * [n_scene][n_channels][bw+1] with se_band[s][i][k] = Se(i, i-k) (0 <= bw <= 32); keep
+ * [n_channels] (1 keep, 0 drop, as channel_mask) restricts Se to Se[keep, keep].  The
+ * library factors each scene's Se and retrieves on whitened residuals and Jacobians;
+ * M_out is K^T Se^-1 K on the kept channels.  Other arguments as irs_oe_batch. */
+int irs_oe_batch_banded(irs_ctx* ctx, const irs_profile* base, int n_scene, const irs_sounder* s,
+                        const irs_fm_options* o, const irs_state_spec* spec, const double* y_obs,
+                        const double* se_band, int bw, const uint8_t* keep, const double* xa,
+                        const double* Sa_inv, const double* x0, const irs_oe_params* prm, double* x_out,
+                        double* y_fit, double* M_out, int32_t* n_iter, int32_t* converged, double* cost);
+
 /* Wait for the context's work; fill per-stage times of the last forward call. */
 int irs_synchronize(irs_ctx* ctx);
 int irs_last_stage_times(irs_ctx* ctx, irs_stage_times* out);

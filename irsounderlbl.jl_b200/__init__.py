@@ -413,6 +413,7 @@ from .estimation import (ColumnScale, FullProfile, Jacobian, PartialColumns, Sta
                          analytic_jacobian, analytic_jacobian_batch, column, default_fd_steps, dfs_partition,
                          finite_difference_jacobian, forward_model_rrule, pack_state, partial_column_basis,
                          state_labels, unpack_state, vmr_range, build_sa, scene_nedt, exclude_channels,
+                         apodized_measurement_covariance, scene_measurement_covariance,
                          RetrievalResult, optimal_estimation, optimal_estimation_batch, oe_diagnostics)
 from .continuum import CIA_PAIRS, load_cia_table  # noqa: E402,F401
 from .hitran import (LINELIST_CACHE_VERSION, clear_linelist_cache, filter_linelist, linelist_cache_dir,  # noqa: E402,F401,E501

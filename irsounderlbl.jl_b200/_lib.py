@@ -132,6 +132,10 @@ SIGNATURES = {
     "irs_surrogate_infer": ([_P, _PF, C.c_int64, _PF, _PF], C.c_int),
     "irs_surrogate_infer_device": ([_P, _P, C.c_int64, _P, _P, _P], C.c_int),
     "irs_gemm_bf16": ([_P, _P, _P, C.c_int, C.c_int, C.c_int, _PF], C.c_int),
+    "irs_oe_batch_banded": ([_P, C.POINTER(Profile), C.c_int, C.POINTER(Sounder), C.POINTER(FMOptions),
+                             C.POINTER(StateSpec), _PD, _PD, C.c_int, C.POINTER(C.c_uint8), _PD, _PD, _PD,
+                             C.POINTER(OEParams), _PD, _PD, _PD, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _PD],
+                            C.c_int),
     "irs_set_cia": ([_P, C.c_int, C.c_int, _PD, C.POINTER(C.c_int64), _PD, _PD], C.c_int),
     "irs_upload_relmat": ([_P, C.c_int, C.POINTER(RelmatBandC), C.c_int, C.POINTER(WtfitEntryC), C.c_int64,
                            C.c_double], C.c_int),

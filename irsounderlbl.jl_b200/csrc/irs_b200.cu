@@ -849,11 +849,19 @@ static void launch_oe_solve(irs_ctx* ctx, const int* d_list, int n_list, int n, 
 // runs its own Levenberg-Marquardt (or Gauss-Newton) iteration; each LM stage (normal
 // equations, damped solve, trial forward model, Jacobian at accepted states) is one
 // batched call over the scenes still iterating.
+// A banded Se per scene (lower band se_band[sc][i][k] = Se(i, i-k), k = 0..bw) on the
+// channels with keep[i] != 0; null band: diagonal Se given as se_inv.
+struct SeBand {
+    const double* band = nullptr;
+    int bw = 0;
+    const uint8_t* keep = nullptr;
+};
+
 static void oe_batch(irs_ctx* ctx, const irs_profile* base, int n_scene, const irs_sounder& s,
                      const irs_fm_options& o_in, const irs_state_spec& sp, const double* y_obs, const double* se_inv,
                      const double* xa, const double* Sa_inv, const double* x0, const irs_oe_params& prm,
                      double* x_out, double* y_fit, double* M_out, int32_t* n_iter, int32_t* converged,
-                     double* cost_out) {
+                     double* cost_out, const SeBand& seb = SeBand()) {
     IRS_REQUIRE(n_scene >= 1 && base, "need at least one scene");
     IRS_REQUIRE(prm.method == 0 || prm.method == 1, "method must be 0 (levenberg_marquardt) or 1 (gauss_newton)");
     IRS_REQUIRE(prm.max_iter >= 1 && prm.max_linesearch >= 1, "max_iter and max_linesearch must be positive");
@@ -880,20 +888,73 @@ static void oe_batch(irs_ctx* ctx, const irs_profile* base, int n_scene, const i
     int* d_ok = (int*)workspace(ctx, "oe_ok", S * sizeof(int));
     int* d_list = (int*)workspace(ctx, "oe_list", S * sizeof(int));
     double* d_fm = (double*)workspace(ctx, "oe_fm", 2 * S * n_ch * sizeof(double));
+    // banded Se: Cholesky factors on the kept channels; the retrieval then runs on
+    // whitened residuals and Jacobians with unit weights (optimal_estimation.jl:166-176)
+    const bool banded = seb.band != nullptr;
+    std::vector<int> kidx;
+    std::vector<double> Lb, w_unit;
+    int* d_kidx = nullptr;
+    double* d_Lb = nullptr;
+    if (banded) {
+        IRS_REQUIRE(seb.bw >= 0 && seb.bw <= kOeMaxBand, "the Se band half-width must be 0..32");
+        for (int64_t i = 0; i < n_ch; ++i) if (seb.keep[i]) kidx.push_back((int)i);
+        IRS_REQUIRE(!kidx.empty(), "channel_mask keeps no channel");
+        const int nk = (int)kidx.size(), bw = seb.bw;
+        Lb.assign(S * nk * (bw + 1), 0.0);
+        for (size_t sc = 0; sc < S; ++sc) {  // banded Cholesky of Se[keep, keep]
+            const double* B = seb.band + sc * n_ch * (bw + 1);
+            double* L = Lb.data() + sc * nk * (bw + 1);
+            for (int i = 0; i < nk; ++i) {
+                for (int k = bw; k >= 0; --k) {
+                    const int j = i - k;
+                    if (j < 0) continue;
+                    const int lag = kidx[i] - kidx[j];
+                    double v = lag <= bw ? B[(size_t)kidx[i] * (bw + 1) + lag] : 0.0;
+                    for (int m = 1; m <= bw && j - m >= 0; ++m)
+                        if (k + m <= bw) v -= L[(size_t)i * (bw + 1) + k + m] * L[(size_t)j * (bw + 1) + m];
+                    if (k == 0) {
+                        IRS_REQUIRE(v > 0.0, "Se is not positive definite on the kept channels");
+                        L[(size_t)i * (bw + 1)] = std::sqrt(v);
+                    } else {
+                        L[(size_t)i * (bw + 1) + k] = v / L[(size_t)j * (bw + 1)];
+                    }
+                }
+            }
+        }
+        w_unit.assign(S * n_ch, 0.0);
+        for (size_t sc = 0; sc < S; ++sc) for (int i : kidx) w_unit[sc * n_ch + i] = 1.0;
+        se_inv = w_unit.data();
+        d_kidx = upload(ctx, "oe_kidx", kidx);
+        d_Lb = upload(ctx, "oe_Lband", Lb);
+    }
+    // residual y - F of one scene, whitened (L^-1 r on the kept channels) for a banded Se
+    auto residual = [&](int sc, const double* Fs, double* r) {
+        const double* ys = y_obs + (size_t)sc * n_ch;
+        for (int64_t i = 0; i < n_ch; ++i) r[i] = ys[i] - Fs[i];
+        if (!banded) return;
+        const int nk = (int)kidx.size(), bw = seb.bw;
+        const double* L = Lb.data() + (size_t)sc * nk * (bw + 1);
+        std::vector<double> z(nk);
+        for (int i = 0; i < nk; ++i) {
+            double v = r[kidx[i]];
+            for (int k = 1; k <= bw && k <= i; ++k) v -= L[(size_t)i * (bw + 1) + k] * z[i - k];
+            z[i] = v / L[(size_t)i * (bw + 1)];
+        }
+        std::fill(r, r + n_ch, 0.0);
+        for (int i = 0; i < nk; ++i) r[kidx[i]] = z[i];
+    };
     IRS_CUDA(cudaMemcpyAsync(d_w, se_inv, S * n_ch * sizeof(double), cudaMemcpyHostToDevice, st));
     IRS_CUDA(cudaMemcpyAsync(d_Sa, Sa_inv, (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice, st));
     IRS_CUDA(cudaMemcpyAsync(d_xa, xa, S * n * sizeof(double), cudaMemcpyHostToDevice, st));
 
     std::vector<double> x(x0, x0 + S * n), F(S * n_ch), J(S), gamma(S, prm.method == 1 ? 0.0 : prm.gamma0);
     std::vector<int32_t> iters(S, 0), conv(S, 0);
+    std::vector<double> rbuf(n_ch);
     auto cost = [&](int sc, const double* Fs, const double* xs) {
         double c = 0.0;
-        const double* ys = y_obs + (size_t)sc * n_ch;
         const double* ws = se_inv + (size_t)sc * n_ch;
-        for (int64_t i = 0; i < n_ch; ++i) {
-            const double r = ys[i] - Fs[i];
-            c += r * ws[i] * r;
-        }
+        residual(sc, Fs, rbuf.data());
+        for (int64_t i = 0; i < n_ch; ++i) c += rbuf[i] * ws[i] * rbuf[i];
         std::vector<double> d(n);
         for (int i = 0; i < n; ++i) d[i] = xs[i] - xa[(size_t)sc * n + i];
         for (int i = 0; i < n; ++i) {
@@ -917,11 +978,18 @@ static void oe_batch(irs_ctx* ctx, const irs_profile* base, int n_scene, const i
                                          cudaMemcpyDeviceToDevice, st));
             std::copy(y.begin() + i * n_ch, y.begin() + (i + 1) * n_ch, F.begin() + (size_t)sc * n_ch);
         }
+        if (banded) {  // K <- L^-1 K for these scenes
+            IRS_CUDA(cudaMemcpyAsync(d_list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+            const int nt = (int)list.size() * n;
+            oe_whiten_kernel<<<(nt + 127) / 128, 128, 0, st>>>(d_list, (int)list.size(), n, (int)n_ch, d_K, d_kidx,
+                                                               (int)kidx.size(), d_Lb, seb.bw);
+            check_launch(ctx);
+        }
     };
     auto upload_resid = [&](const std::vector<int>& list) {
         std::vector<double> r((size_t)n_ch);
         for (int sc : list) {
-            for (int64_t i = 0; i < n_ch; ++i) r[i] = y_obs[(size_t)sc * n_ch + i] - F[(size_t)sc * n_ch + i];
+            residual(sc, F.data() + (size_t)sc * n_ch, r.data());
             IRS_CUDA(cudaMemcpyAsync(d_r + (size_t)sc * n_ch, r.data(), n_ch * sizeof(double), cudaMemcpyHostToDevice, st));
             IRS_CUDA(cudaStreamSynchronize(st));
         }
@@ -1393,6 +1461,25 @@ int irs_oe_batch(irs_ctx* ctx, const irs_profile* base, int n_scene, const irs_s
     IRS_CUDA(cudaSetDevice(ctx->device));
     oe_batch(ctx, base, n_scene, *s, *o, *spec, y_obs, se_inv, xa, Sa_inv, x0, *prm, x_out, y_fit, M_out, n_iter,
              converged, cost);
+    IRS_API_END
+}
+
+int irs_oe_batch_banded(irs_ctx* ctx, const irs_profile* base, int n_scene, const irs_sounder* s,
+                        const irs_fm_options* o, const irs_state_spec* spec, const double* y_obs,
+                        const double* se_band, int bw, const uint8_t* keep, const double* xa, const double* Sa_inv,
+                        const double* x0, const irs_oe_params* prm, double* x_out, double* y_fit, double* M_out,
+                        int32_t* n_iter, int32_t* converged, double* cost) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && base && s && o && spec && y_obs && se_band && keep && xa && Sa_inv && x0 && prm && x_out &&
+                    y_fit && M_out && n_iter && converged && cost,
+                "invalid arguments");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    SeBand b;
+    b.band = se_band;
+    b.bw = bw;
+    b.keep = keep;
+    oe_batch(ctx, base, n_scene, *s, *o, *spec, y_obs, nullptr, xa, Sa_inv, x0, *prm, x_out, y_fit, M_out, n_iter,
+             converged, cost, b);
     IRS_API_END
 }
 

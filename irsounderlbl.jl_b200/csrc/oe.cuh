@@ -173,4 +173,28 @@ __global__ void __launch_bounds__(kOeThreads) oe_solve_kernel(const int* __restr
     }
 }
 
+// Whitening by a banded Cholesky factor of Se (apodised covariance, covariance.jl:62-81):
+// every row x of K for the scenes in `list` (over the kept channels kidx, in order)
+// becomes L^-1 x by forward substitution, L[i][k] = L(i, i-k) for k = 0..bw.  Then
+// K^T K = K^T Se^-1 K.  One thread per (scene, state row); the recurrence runs in FP64.
+constexpr int kOeMaxBand = 32;
+__global__ void __launch_bounds__(128) oe_whiten_kernel(const int* __restrict__ list, int n_list, int n,
+                                                        int n_ch, float* __restrict__ K, const int* __restrict__ kidx,
+                                                        int n_kept, const double* __restrict__ Lb, int bw) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_list * n) return;
+    const int s = list[t / n], row = t % n;
+    float* x = K + ((size_t)s * n + row) * n_ch;
+    const double* L = Lb + (size_t)s * n_kept * (bw + 1);
+    double z[kOeMaxBand + 1];  // the last bw values, ring-indexed
+    for (int i = 0; i < n_kept; ++i) {
+        const double* Li = L + (size_t)i * (bw + 1);
+        double v = (double)x[kidx[i]];
+        for (int k = 1; k <= bw && k <= i; ++k) v -= Li[k] * z[(i - k) % (kOeMaxBand + 1)];
+        v /= Li[0];
+        z[i % (kOeMaxBand + 1)] = v;
+        x[kidx[i]] = (float)v;
+    }
+}
+
 }  // namespace irs

@@ -596,6 +596,39 @@ def _dB_dT(nu, T):
     return c1 * c2 * nu ** 4 * ex / (T * T * (ex - 1.0) ** 2)
 
 
+def _ils_noise_autocorr(dnu_sample: float, fwhm_gauss: float, max_lag: int = 4) -> np.ndarray:
+    """_ils_noise_autocorr (covariance.jl:28-36): channel-lag correlation of the Gaussian
+    apodisation weights exp(-(k dnu)^2 / 2 s^2), s = fwhm / (2 sqrt(2 ln 2))."""
+    if fwhm_gauss <= 0.0:
+        return np.array([1.0] + [0.0] * max_lag)
+    s = fwhm_gauss / (2.0 * np.sqrt(2.0 * np.log(2.0)))
+    K = max_lag + 6
+    w = np.exp(-((np.arange(-K, K + 1) * dnu_sample) ** 2) / (2.0 * s * s))
+    R0 = float(np.sum(w * w))
+    return np.array([1.0] + [float(np.sum(w[:len(w) - k] * w[k:])) / R0 for k in range(1, max_lag + 1)])
+
+
+def apodized_measurement_covariance(nu, sigma, dnu_sample: float = 0.25, fwhm_gauss: float = 0.5,
+                                    max_lag: int = 4) -> np.ndarray:
+    """apodized_measurement_covariance (covariance.jl:63-81): Se[i, j] = s_i s_j rho(lag),
+    lag = round(|nu_i - nu_j| / dnu_sample) <= max_lag (banded for contiguous channels)."""
+    nu = np.asarray(nu, dtype=np.float64)
+    n = len(nu)
+    sv = np.full(n, float(sigma)) if np.ndim(sigma) == 0 else np.asarray(sigma, dtype=np.float64)
+    if len(sv) != n:
+        raise IRSError(f"σ must be a scalar or length(ν)={n}; got {len(sv)}")
+    rho = _ils_noise_autocorr(dnu_sample, fwhm_gauss, max_lag)
+    lag = np.rint(np.abs(nu[:, None] - nu[None, :]) / dnu_sample).astype(np.int64)
+    Se = np.where(lag <= max_lag, np.outer(sv, sv) * rho[np.minimum(lag, max_lag)], 0.0)
+    return Se
+
+
+def scene_measurement_covariance(nu, Tb_scene, nedt_280K=0.25, T_ref=280.0, **kw) -> np.ndarray:
+    """scene_measurement_covariance (covariance.jl:125-130): scene NEdT on the diagonal,
+    apodisation correlations off it."""
+    return apodized_measurement_covariance(nu, scene_nedt(nu, Tb_scene, nedt_280K, T_ref), **kw)
+
+
 def scene_nedt(nu, Tb_scene, nedt_280K=0.25, T_ref=280.0) -> np.ndarray:
     """scene_nedt (covariance.jl:106-117): NEdT at the scene BT from the NEdT at T_ref."""
     nu = np.asarray(nu, dtype=np.float64)
@@ -663,9 +696,12 @@ def optimal_estimation_batch(ys, spec: StateVectorSpec, base_profs, linelists, *
                              line_mixing=None):
     """optimal_estimation (optimal_estimation.jl:142-291) for a batch of scenes on the GPU.
 
-    ys [n_scene, n_ch]; xa [n_scene, n] (or [n]); Sa [n, n] shared; Se per scene:
-    [n_scene, n_ch] variances (or one [n_ch] vector).  Returns dict(x, y_fit, M, n_iter,
-    converged, cost, nu)."""
+    ys [n_scene, n_ch]; xa [n_scene, n] (or [n]); Sa [n, n] shared; Se: per-channel
+    variances [n_scene, n_ch] or [n_ch], or covariance matrices [n_scene, n_ch, n_ch] or
+    one [n_ch, n_ch] (a square 2-D Se is always a covariance).  A non-diagonal covariance
+    must be banded (half-width <= 32, as the apodised Se of apodized_measurement_covariance):
+    the library factors it and retrieves on whitened residuals and Jacobians.  Returns
+    dict(x, y_fit, M, n_iter, converged, cost, nu, ...)."""
     from . import (IASIInstrument, _prepare, _ProfileBatch, default_context, fm_options, nadir_geometry,
                    sounder_grid)
     if method not in ("levenberg_marquardt", "gauss_newton"):
@@ -692,10 +728,29 @@ def optimal_estimation_batch(ys, spec: StateVectorSpec, base_profs, linelists, *
     if not keep.any():
         raise IRSError("channel_mask excludes every channel")
     Se = np.asarray(Se, dtype=np.float64)
-    Se_rows = np.broadcast_to(Se, (S, n_ch)) if Se.ndim == 1 or (Se.ndim == 2 and Se.shape == (S, n_ch)) else None
-    if Se_rows is None:
-        raise IRSError("Se must be [n_ch] or [n_scene, n_ch] variances")
-    w = np.ascontiguousarray(np.stack([_se_inverse(Se_rows[k], n_ch, keep)[0] for k in range(S)]))
+    Se_mats = None
+    if Se.ndim == 3 or (Se.ndim == 2 and Se.shape == (n_ch, n_ch)):
+        Se_mats = np.broadcast_to(Se, (S, n_ch, n_ch)) if Se.ndim == 2 else Se
+        if Se_mats.shape != (S, n_ch, n_ch):
+            raise IRSError(f"Se must be n_y×n_y with n_y = {n_ch}, per scene or shared")
+        off = Se_mats - np.eye(n_ch)[None] * np.diagonal(Se_mats, axis1=1, axis2=2)[:, :, None]
+        if not np.any(off):
+            Se, Se_mats = np.diagonal(Se_mats, axis1=1, axis2=2), None
+    w = None
+    if Se_mats is None:
+        Se_rows = np.broadcast_to(Se, (S, n_ch)) if Se.ndim == 1 or (Se.ndim == 2 and Se.shape == (S, n_ch)) else None
+        if Se_rows is None:
+            raise IRSError("Se must be [n_ch] or [n_scene, n_ch] variances, or n_ch×n_ch covariances")
+        w = np.ascontiguousarray(np.stack([_se_inverse(Se_rows[k], n_ch, keep)[0] for k in range(S)]))
+    else:
+        ii, jj = np.nonzero(np.any(Se_mats != 0.0, axis=0))
+        bw = int(np.max(np.abs(ii - jj))) if len(ii) else 0
+        if bw > 32:
+            raise IRSError(f"a covariance Se of band half-width {bw} is not supported on the GPU path (at most 32)")
+        band = np.zeros((S, n_ch, bw + 1))
+        for k in range(bw + 1):
+            band[:, k:, k] = np.diagonal(Se_mats, offset=-k, axis1=1, axis2=2)
+        band = np.ascontiguousarray(band)
     Sa_inv = np.ascontiguousarray(np.linalg.inv(Sa))
     base_profs = list(base_profs) if isinstance(base_profs, (list, tuple)) else [base_profs] * S
     geoms = geoms or [nadir_geometry()] * S
@@ -719,11 +774,32 @@ def optimal_estimation_batch(ys, spec: StateVectorSpec, base_profs, linelists, *
     conv = np.empty(S, np.int32)
     cost = np.empty(S)
     I32 = C.POINTER(C.c_int32)
-    check(ctx.lib.irs_oe_batch(ctx.h, batch.arr, S, C.byref(s), C.byref(o), C.byref(cs), dptr(ys), dptr(w), dptr(xa),
-                               dptr(Sa_inv), dptr(x0), C.byref(prm), dptr(x), dptr(y_fit), dptr(M),
-                               n_iter.ctypes.data_as(I32), conv.ctypes.data_as(I32), dptr(cost)))
+    if w is not None:
+        check(ctx.lib.irs_oe_batch(ctx.h, batch.arr, S, C.byref(s), C.byref(o), C.byref(cs), dptr(ys), dptr(w),
+                                   dptr(xa), dptr(Sa_inv), dptr(x0), C.byref(prm), dptr(x), dptr(y_fit), dptr(M),
+                                   n_iter.ctypes.data_as(I32), conv.ctypes.data_as(I32), dptr(cost)))
+    else:
+        kp = np.ascontiguousarray(keep.astype(np.uint8))
+        check(ctx.lib.irs_oe_batch_banded(ctx.h, batch.arr, S, C.byref(s), C.byref(o), C.byref(cs), dptr(ys),
+                                          dptr(band), band.shape[2] - 1, kp.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                          dptr(xa), dptr(Sa_inv), dptr(x0), C.byref(prm), dptr(x), dptr(y_fit),
+                                          dptr(M), n_iter.ctypes.data_as(I32), conv.ctypes.data_as(I32),
+                                          dptr(cost)))
     return dict(x=x, y_fit=y_fit, M=M, n_iter=n_iter, converged=conv.astype(bool), cost=cost, nu=nu, w=w,
-                Sa_inv=Sa_inv, keep=keep)
+                Se=Se_mats, Sa_inv=Sa_inv, keep=keep)
+
+
+def _banded_solver(Se_k):
+    """x -> Se_k^-1 x through the banded Cholesky factor of Se_k (scipy.linalg)."""
+    from scipy.linalg import cho_solve_banded, cholesky_banded
+    n = len(Se_k)
+    ii, jj = np.nonzero(Se_k)
+    bw = int(np.max(np.abs(ii - jj))) if len(ii) else 0
+    ab = np.zeros((bw + 1, n))
+    for k in range(bw + 1):
+        ab[bw - k, k:] = np.diagonal(Se_k, offset=k)
+    c = cholesky_banded(ab)
+    return lambda x: cho_solve_banded((c, False), x)
 
 
 def oe_diagnostics(M, Sa, Sa_inv=None):
@@ -747,7 +823,7 @@ def optimal_estimation(y, spec: StateVectorSpec, base_prof, linelists, *, xa, Sa
     """optimal_estimation (optimal_estimation.jl:142-291) -> RetrievalResult, one scene."""
     from . import nadir_geometry
     r = optimal_estimation_batch(np.atleast_2d(y), spec, [base_prof], linelists, xa=np.asarray(xa)[None],
-                                 Sa=Sa, Se=np.diag(Se) if np.ndim(Se) == 2 else Se, x0=None if x0 is None else
+                                 Sa=Sa, Se=Se, x0=None if x0 is None else
                                  np.asarray(x0)[None], channel_mask=channel_mask, method=method, max_iter=max_iter,
                                  max_linesearch=max_linesearch, gamma0=gamma0, gamma_factor=gamma_factor,
                                  gamma_min=gamma_min, conv_factor=conv_factor, observable=observable,
@@ -765,13 +841,19 @@ def optimal_estimation(y, spec: StateVectorSpec, base_prof, linelists, *, xa, Sa
     jac = analytic_jacobian(prof, linelists, spec, sounder=sounder, geom=geom, T_sfc=Ts,
                             eps_sfc=es if spec.include_emissivity else eps_fixed, observable=observable,
                             backend=backend, line_mixing=line_mixing, **kw)
-    wk = r["w"][0][keep]
     Kk = jac.K[keep]
-    G = S_hat @ (Kk * wk[:, None]).T
-    se_k = 1.0 / wk
-    S_noise = (G * se_k[None, :]) @ G.T
     resid = (np.atleast_2d(y)[0] - r["y_fit"][0])[keep]
-    chi2 = float(np.sum(resid * wk * resid))
+    if r["w"] is not None:
+        wk = r["w"][0][keep]
+        G = S_hat @ (Kk * wk[:, None]).T
+        S_noise = (G * (1.0 / wk)[None, :]) @ G.T
+        chi2 = float(np.sum(resid * wk * resid))
+    else:  # banded covariance: Se^-1 by its banded Cholesky factor on the kept channels
+        Se_k = r["Se"][0][np.ix_(keep, keep)]
+        solve = _banded_solver(Se_k)
+        G = S_hat @ solve(Kk).T
+        S_noise = G @ Se_k @ G.T
+        chi2 = float(resid @ solve(resid))
     m = int(keep.sum())
     return RetrievalResult(x=x, spec=spec, converged=bool(r["converged"][0]), n_iter=int(r["n_iter"][0]),
                            cost=float(r["cost"][0]), S_hat=S_hat, A=A, G=G, K=jac.K, dof=dof, dfn=m - dof, H=H,

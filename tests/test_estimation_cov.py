@@ -37,3 +37,25 @@ def test_scene_nedt_and_mask(pkg):
     assert np.all(cold > 0.2) and cold[2] > cold[0]
     keep = pkg.exclude_channels(nu, (650.0, 800.0), (2300.0, 2500.0))
     assert keep.tolist() == [False, True, False]
+
+
+def test_apodized_measurement_covariance(pkg):  # runtests.jl:1614-1636
+    nu = 645.0 + 0.25 * np.arange(21)
+    Se = pkg.apodized_measurement_covariance(nu, 0.2)
+    assert np.array_equal(Se, Se.T) and np.all(np.linalg.eigvalsh(Se) > 0)
+    assert np.allclose(np.diag(Se), 0.04)
+    s2 = 0.04
+    assert abs(Se[0, 1] / s2 - 0.705) < 0.02 and abs(Se[0, 2] / s2 - 0.250) < 0.02
+    assert abs(Se[0, 3] / s2 - 0.044) < 0.01 and Se[0, 4] / s2 < 0.006 and Se[0, 5] == 0.0
+    Ssp = pkg.apodized_measurement_covariance([645.0, 647.0, 649.0], 0.2)
+    assert Ssp[0, 1] == 0.0 and Ssp[0, 2] == 0.0
+    sv = np.array([0.1, 0.2, 0.3, 0.4, 0.5, 0.6, 0.7])
+    Sv = pkg.apodized_measurement_covariance(645.0 + 0.25 * np.arange(7), sv)
+    assert np.allclose(np.diag(Sv), sv ** 2)
+    Sd = pkg.apodized_measurement_covariance(nu, 0.2, fwhm_gauss=0.0)
+    assert Sd[0, 1] == 0.0 and np.allclose(np.diag(Sd), 0.04)
+    nuv = 660.0 + 0.25 * np.arange(5)
+    Tb = np.full(5, 230.0)
+    S = pkg.scene_measurement_covariance(nuv, Tb, nedt_280K=0.25)
+    assert np.array_equal(S, S.T) and np.all(np.linalg.eigvalsh(S) > 0)
+    assert abs(np.sqrt(S[0, 0]) - pkg.scene_nedt(nuv, Tb, nedt_280K=0.25)[0]) <= 1e-12 * np.sqrt(S[0, 0])

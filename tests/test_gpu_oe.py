@@ -154,3 +154,32 @@ def test_closed_loop_5k_lines(pkg, ctx):
     print(f"A-weighted T error: prior {err_prior:.2f} K -> retrieved {err_post:.2f} K, dof {res.dof:.1f}")
     assert err_post < err_prior
     assert res.chi2 < 3.0 * int(res.channel_mask.sum())
+
+
+@pytest.mark.parametrize("masked", [False, True])
+def test_apodized_se_vs_oracle(pkg, ctx, oracle, orc_mod, masked):
+    """The retrieval with the apodised (banded, non-diagonal) Se of IASI L1C through the
+    banded entry point, against the oracle with the same full Se inverted on the kept
+    channels; and the cost is r^T Se^-1 r (not its diagonal part)."""
+    import oe_oracle
+    ll, llp, base, spec, xa, Sa, y, se, snd = setup(pkg, ctx, orc_mod, dT=3.0, dv=0.15)
+    nu = pkg.sounder_grid(snd)
+    Se = pkg.scene_measurement_covariance(nu, y, nedt_280K=0.2, dnu_sample=0.5)
+    keep = np.ones(len(y), bool)
+    if masked:
+        keep[[1, 6]] = False
+    res = pkg.optimal_estimation(y, spec, base, llp, xa=xa, Sa=Sa, Se=Se, channel_mask=keep, sounder=snd,
+                                 backend=ctx, fm_kwargs=KW)
+    fwd, fwd_jac = oracle_fns(pkg, oracle, orc_mod, spec, base, ll)
+    ro = oe_oracle.optimal_estimation(y, fwd, fwd_jac, xa, Sa, Se, keep=keep)
+    sd = np.sqrt(np.diag(res.S_hat))
+    assert res.converged and ro["converged"]
+    assert np.max(np.abs(res.x - ro["x"]) / sd) < 0.1
+    k = np.flatnonzero(keep)
+    W = np.linalg.inv(Se[np.ix_(k, k)])
+    r = (y - res.y_fit)[k]
+    assert abs(res.chi2 - r @ W @ r) <= 1e-8 * max(1.0, res.chi2)
+    # the diagonal of the same Se gives a different retrieval
+    rd = pkg.optimal_estimation(y, spec, base, llp, xa=xa, Sa=Sa, Se=np.diag(Se), channel_mask=keep, sounder=snd,
+                                backend=ctx, fm_kwargs=KW)
+    assert np.max(np.abs(rd.x - res.x) / sd) > 0.01
