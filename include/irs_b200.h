@@ -330,6 +330,32 @@ int irs_oe_batch_banded(irs_ctx* ctx, const irs_profile* base, int n_scene, cons
                         const double* Sa_inv, const double* x0, const irs_oe_params* prm, double* x_out,
                         double* y_fit, double* M_out, int32_t* n_iter, int32_t* converged, double* cost);
 
+/* ------------------------------------------------------------------------------
+ * Array-level operators on the device, for callers that use them outside
+ * forward_model.  Host arrays in and out, FP64.
+ * ------------------------------------------------------------------------------ */
+/* voigt_profile(ν, ν₀, γ_L, γ_D, method) over nu[n] (voigt.jl:177-200; method 1
+ * Weideman, 2 PseudoVoigt, 3 FullFaddeeva), cm. */
+int irs_voigt_profile(irs_ctx* ctx, const double* nu, int64_t n, double nu0, double gamma_l, double gamma_d,
+                      int method, double* out);
+/* w(x + iy) = erfcx(y - ix) for y >= 0 (faddeeva_voigt = Re w, voigt.jl:152-160). */
+int irs_faddeeva(irs_ctx* ctx, const double* x, const double* y, int64_t n, double* re, double* im);
+/* ils_kernel(Δν, opd_max, fwhm; apodization) (ils.jl:80-115): the area-normalised taps
+ * at k Δν, k = -n_half..n_half, n_taps = 2 ceil(16/Δν) + 1. */
+int irs_ils_kernel(irs_ctx* ctx, double dnu, double opd_max, double fwhm_gauss, int apodization, int64_t n_taps,
+                   double* kern);
+/* apply_ils(ν_grid, spectrum, ils_δν, ils_kernel) (ils.jl:131-153): out[i] = Δν sum_k
+ * spectrum[i + k - half] kern[k], zero outside the grid. */
+int irs_apply_ils(irs_ctx* ctx, const double* spectrum, int64_t n_nu, double dnu, const double* kern,
+                  int64_t n_taps, double* out);
+/* schwarzschild_rte(ν_grid, τ_layers, T_levels, T_sfc; μ, ε_sfc, source_function,
+ * T_ave) (schwarzschild.jl:130-274): tau is [n_layers][n_nu] (the Julia n_ν x n_layers
+ * matrix in memory order), T_lev [n_layers + 1] surface first; source_function 0 :cim
+ * (T_ave required), 1 :toon. */
+int irs_schwarzschild_rte(irs_ctx* ctx, const double* grid, int64_t n_nu, int n_layers, const double* tau,
+                          const double* T_lev, double T_sfc, double mu, double eps, int source_function,
+                          const double* T_ave, double* I);
+
 /* Wait for the context's work; fill per-stage times of the last forward call. */
 int irs_synchronize(irs_ctx* ctx);
 int irs_last_stage_times(irs_ctx* ctx, irs_stage_times* out);

@@ -428,5 +428,7 @@ from .iasi_l1c import (IASIL1CGranule, brightness_temperature, cloud_fraction, m
                        read_iasi_l1c, retrieve_granule, solar_reflection_angle)
 from .noise_covariance import (SounderNoiseCovariance, load_noise_covariance, measurement_covariance,  # noqa: E402,F401,E501
                                read_iasi_ncm, subset_channels, to_bt)
+from .operators import (apply_ils, dB_dT, faddeeva, faddeeva_voigt, ils_kernel, level_transmittances,  # noqa: E402,F401,E501
+                        planck_radiance, schwarzschild_rte, voigt_profile)
 from .robust import RobustRetrievalResult, robust_estimation, robust_estimation_batch  # noqa: E402,F401
 from .surrogate import Surrogate, surrogate_features, surrogate_first_guess, surrogate_forward_batch  # noqa: E402,F401,E501

@@ -136,6 +136,12 @@ SIGNATURES = {
                              C.POINTER(StateSpec), _PD, _PD, C.c_int, C.POINTER(C.c_uint8), _PD, _PD, _PD,
                              C.POINTER(OEParams), _PD, _PD, _PD, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _PD],
                             C.c_int),
+    "irs_voigt_profile": ([_P, _PD, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_int, _PD], C.c_int),
+    "irs_faddeeva": ([_P, _PD, _PD, C.c_int64, _PD, _PD], C.c_int),
+    "irs_ils_kernel": ([_P, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int64, _PD], C.c_int),
+    "irs_apply_ils": ([_P, _PD, C.c_int64, C.c_double, _PD, C.c_int64, _PD], C.c_int),
+    "irs_schwarzschild_rte": ([_P, _PD, C.c_int64, C.c_int, _PD, _PD, C.c_double, C.c_double, C.c_double, C.c_int,
+                               _PD, _PD], C.c_int),
     "irs_set_cia": ([_P, C.c_int, C.c_int, _PD, C.POINTER(C.c_int64), _PD, _PD], C.c_int),
     "irs_upload_relmat": ([_P, C.c_int, C.POINTER(RelmatBandC), C.c_int, C.POINTER(WtfitEntryC), C.c_int64,
                            C.c_double], C.c_int),

@@ -16,6 +16,7 @@
 #include "jacobian.cuh"
 #include "oe.cuh"
 #include "lm_pert.cuh"
+#include "operators.cuh"
 #include <atomic>
 #include <chrono>
 #include <exception>
@@ -1480,6 +1481,121 @@ int irs_oe_batch_banded(irs_ctx* ctx, const irs_profile* base, int n_scene, cons
     b.keep = keep;
     oe_batch(ctx, base, n_scene, *s, *o, *spec, y_obs, nullptr, xa, Sa_inv, x0, *prm, x_out, y_fit, M_out, n_iter,
              converged, cost, b);
+    IRS_API_END
+}
+
+// ------------------------------------------------------------ operators
+// device copies of caller arrays for the operator entry points (grown as needed)
+static double* dev_copy(irs_ctx* ctx, const std::string& name, const double* h, int64_t n) {
+    double* d = (double*)workspace(ctx, name, (size_t)std::max<int64_t>(n, 1) * sizeof(double));
+    if (n > 0) IRS_CUDA(cudaMemcpyAsync(d, h, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    return d;
+}
+static void to_host(irs_ctx* ctx, double* h, const double* d, int64_t n) {
+    if (n > 0) IRS_CUDA(cudaMemcpyAsync(h, d, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    IRS_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+int irs_voigt_profile(irs_ctx* ctx, const double* nu, int64_t n, double nu0, double gamma_l, double gamma_d,
+                      int method, double* out) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && nu && out && n >= 0, "invalid arguments");
+    IRS_REQUIRE(method >= 1 && method <= 3, "method must be 1 (Weideman), 2 (PseudoVoigt) or 3 (FullFaddeeva)");
+    IRS_REQUIRE(gamma_d > 0.0 && gamma_l >= 0.0, "gamma_D must be positive and gamma_L non-negative");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    if (n == 0) return IRS_OK;
+    double* d_in = dev_copy(ctx, "op_a", nu, n);
+    double* d_out = (double*)workspace(ctx, "op_out", (size_t)n * sizeof(double));
+    voigt_profile_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(d_in, n, nu0, gamma_l, gamma_d, method,
+                                                                              d_out);
+    check_launch(ctx);
+    to_host(ctx, out, d_out, n);
+    IRS_API_END
+}
+
+int irs_faddeeva(irs_ctx* ctx, const double* x, const double* y, int64_t n, double* re, double* im) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && x && y && re && im && n >= 0, "invalid arguments");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    if (n == 0) return IRS_OK;
+    for (int64_t i = 0; i < n; ++i) IRS_REQUIRE(y[i] >= 0.0, "w(x + iy) is evaluated for y >= 0");
+    double* d_x = dev_copy(ctx, "op_a", x, n);
+    double* d_y = dev_copy(ctx, "op_b", y, n);
+    double* d_o = (double*)workspace(ctx, "op_out", 2 * (size_t)n * sizeof(double));
+    faddeeva_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(d_x, d_y, n, d_o, d_o + n);
+    check_launch(ctx);
+    to_host(ctx, re, d_o, n);
+    to_host(ctx, im, d_o + n, n);
+    IRS_API_END
+}
+
+int irs_ils_kernel(irs_ctx* ctx, double dnu, double opd_max, double fwhm_gauss, int apodization, int64_t n_taps,
+                   double* kern) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && kern && dnu > 0.0 && opd_max > 0.0, "invalid arguments");
+    IRS_REQUIRE(apodization >= 0 && apodization <= 3, "unknown apodization");
+    const int64_t n_half = (int64_t)std::ceil(16.0 / dnu);
+    IRS_REQUIRE(n_taps == 2 * n_half + 1, "n_taps must be 2 ceil(16/dnu) + 1");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    double* d_k = (double*)workspace(ctx, "op_out", (size_t)n_taps * sizeof(double));
+    ils_taps_kernel<<<(unsigned)((n_taps + 127) / 128), 128, 0, ctx->stream>>>(dnu, opd_max, fwhm_gauss, apodization,
+                                                                               n_half, d_k);
+    check_launch(ctx);
+    ils_normalise_kernel<<<1, 1024, 0, ctx->stream>>>(d_k, n_taps, dnu);
+    check_launch(ctx);
+    to_host(ctx, kern, d_k, n_taps);
+    IRS_API_END
+}
+
+int irs_apply_ils(irs_ctx* ctx, const double* spectrum, int64_t n_nu, double dnu, const double* kern, int64_t n_taps,
+                  double* out) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && spectrum && kern && out && n_nu >= 0 && n_taps >= 1 && (n_taps % 2) == 1,
+                "invalid arguments (the kernel needs an odd number of taps)");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    if (n_nu == 0) return IRS_OK;
+    double* d_s = dev_copy(ctx, "op_a", spectrum, n_nu);
+    double* d_k = dev_copy(ctx, "op_b", kern, n_taps);
+    double* d_o = (double*)workspace(ctx, "op_out", (size_t)n_nu * sizeof(double));
+    apply_ils_kernel<<<(unsigned)((n_nu + kIlsThreads - 1) / kIlsThreads), kIlsThreads, 0, ctx->stream>>>(
+        d_s, n_nu, d_k, n_taps, dnu, d_o);
+    check_launch(ctx);
+    to_host(ctx, out, d_o, n_nu);
+    IRS_API_END
+}
+
+int irs_schwarzschild_rte(irs_ctx* ctx, const double* grid, int64_t n_nu, int n_layers, const double* tau,
+                          const double* T_lev, double T_sfc, double mu, double eps, int source_function,
+                          const double* T_ave, double* I) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && grid && tau && T_lev && I && n_nu >= 1 && n_layers >= 1, "invalid arguments");
+    IRS_REQUIRE(mu > 0.0 && mu <= 1.0, "μ must be in (0, 1]");
+    IRS_REQUIRE(source_function == 0 || source_function == 1, "source_function must be :toon or :cim");
+    IRS_REQUIRE(source_function == 1 || T_ave, ":cim source_function requires T_ave");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    std::vector<LayerRT> lrt(n_layers);
+    for (int k = 0; k < n_layers; ++k) {
+        LayerRT& r = lrt[k];
+        r = LayerRT{};
+        r.T_bot = T_lev[k];
+        r.T_top = T_lev[k + 1];
+        r.T_ave = T_ave ? T_ave[k] : 0.5 * (T_lev[k] + T_lev[k + 1]);
+    }
+    std::vector<ProfileRT> prt(1);
+    prt[0].T_sfc = T_sfc;
+    prt[0].mu = mu;
+    prt[0].eps = eps;
+    double* d_grid = dev_copy(ctx, "op_a", grid, n_nu);
+    double* d_tau = dev_copy(ctx, "op_b", tau, n_nu * n_layers);
+    LayerRT* d_lrt = upload(ctx, "op_lrt", lrt);
+    ProfileRT* d_prt = upload(ctx, "op_prt", prt);
+    double* d_I = (double*)workspace(ctx, "op_out", (size_t)n_nu * sizeof(double));
+    ContDev cd{};
+    cd.mask = 0;
+    rte_kernel<double><<<dim3((unsigned)((n_nu + 255) / 256), 1), 256, 0, ctx->stream>>>(
+        d_tau, d_lrt, d_prt, n_layers, d_grid, n_nu, source_function, cd, d_I);
+    check_launch(ctx);
+    to_host(ctx, I, d_I, n_nu);
     IRS_API_END
 }
 
