@@ -175,6 +175,12 @@ struct FarTable {
 __device__ __forceinline__ double far_node(int k) {
     return 127.5 + 127.5 * cos((2 * k + 1) * 3.14159265358979323846 / (2 * kFarNodes));
 }
+// the same nodes rounded to FP32, as literals for fully unrolled node loops
+__device__ __forceinline__ float far_node_f(int k) {
+    return k == 0 ? 2.525501251e+02f : k == 1 ? 2.335123749e+02f : k == 2 ? 1.983352051e+02f
+         : k == 3 ? 1.523740234e+02f : k == 4 ? 1.026259842e+02f : k == 5 ? 5.666479492e+01f
+         : k == 6 ? 2.148762512e+01f : 2.449876785e+00f;
+}
 // whole block, before any early exit
 __device__ __forceinline__ void far_table_init(FarTable& F) {
     for (int idx = threadIdx.x; idx < kFarNodes * kMxWarpPts; idx += blockDim.x) {
@@ -249,6 +255,11 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
     // (compensated) and the warp reduces them once per segment, so tiles holding only
     // far lines need no per-point work
     float PA = 0.f, PAc = 0.f, PB = 0.f, PBc = 0.f, PC = 0.f, PCc = 0.f;
+    // tiles whose lines are all far lines skip the staging: each lane evaluates its own
+    // line at the 8 nodes and accumulates them here (reduced across the warp once)
+    float fnode[kFarNodes];
+#pragma unroll
+    for (int k = 0; k < kFarNodes; ++k) fnode[k] = 0.f;
     const unsigned lt = (1u << lane) - 1u;
     for (long long t0 = jlo; t0 < jhi; t0 += 32) {
         const int nt = (int)min(32LL, jhi - t0);
@@ -281,6 +292,20 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
                 if (FAR && METHOD == 3 && dist + kHalf <= cut && fmaxf(dist - kHalf, 0.f) * a1.z + a1.w >= 15.05f)
                     cls = 5;
             }
+        }
+        if (FAR && !LM && __all_sync(kFull, cls == 3 || lane >= nt)) {
+            if (lane < nt) {
+#pragma unroll
+                for (int k = 0; k < kFarNodes; ++k) {
+                    const float d = (far_node_f(k) - uh) - ul;
+                    fnode[k] = fmaf(a0.y, rcp_fast(fmaf(d, d, a0.x)), fnode[k]);
+                }
+            }
+            kahan_add(PA, PAc, pa);
+            kahan_add(PB, PBc, pb);
+            kahan_add(PC, PCc, pc);
+            if (lane == 0) work += (unsigned long long)nt * kFarNodes;
+            continue;
         }
         const unsigned fm = __ballot_sync(kFull, cls == 1), sm = __ballot_sync(kFull, cls == 2);
         const unsigned xm = FAR ? __ballot_sync(kFull, cls == 3) : 0u;
@@ -463,6 +488,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
 #pragma unroll
         for (int k = 0; k < kFarNodes; ++k) {
             Fn[k] = __shfl_sync(kFull, farS, k);
+            if (!LM) Fn[k] += warp_sum(fnode[k]);
             Dn[k] = LM ? __shfl_sync(kFull, farDS, k) : 0.f;
         }
         const float A = warp_sum(PA - PAc), B = warp_sum(PB - PBc), Cc = warp_sum(PC - PCc);
