@@ -293,8 +293,8 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
                     cls = 5;
             }
         }
-        if (FAR && !LM && __all_sync(kFull, cls == 3 || lane >= nt)) {
-            if (lane < nt) {
+        if (FAR && !LM && __all_sync(kFull, cls == 3 || cls == 0)) {  // far lines and lines out of reach
+            if (cls == 3) {
 #pragma unroll
                 for (int k = 0; k < kFarNodes; ++k) {
                     const float d = (far_node_f(k) - uh) - ul;
@@ -304,7 +304,8 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             kahan_add(PA, PAc, pa);
             kahan_add(PB, PBc, pb);
             kahan_add(PC, PCc, pc);
-            if (lane == 0) work += (unsigned long long)nt * kFarNodes;
+            const unsigned nfar = __popc(__ballot_sync(kFull, cls == 3));
+            if (lane == 0) work += (unsigned long long)nfar * kFarNodes;
             continue;
         }
         const unsigned fm = __ballot_sync(kFull, cls == 1), sm = __ballot_sync(kFull, cls == 2);
