@@ -474,9 +474,15 @@ static void forward_pass(irs_ctx* ctx, const irs_profile* profs, int n_prof, con
     }
     dim3 g3((unsigned)((n_nu + 255) / 256), n_prof);
     if (o.precision != IRS_FP64)
-        rte_kernel<float><<<g3, 256, 0, st>>>((const float*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
+        if (cd.mask & kCiaMask)
+            rte_kernel<float, true><<<g3, 256, 0, st>>>((const float*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
+        else
+            rte_kernel<float><<<g3, 256, 0, st>>>((const float*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
     else
-        rte_kernel<double><<<g3, 256, 0, st>>>((const double*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
+        if (cd.mask & kCiaMask)
+            rte_kernel<double, true><<<g3, 256, 0, st>>>((const double*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
+        else
+            rte_kernel<double><<<g3, 256, 0, st>>>((const double*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
     check_launch(ctx);
     IRS_CUDA(cudaEventRecord(ctx->ev[3], st));
     const double* d_kern = o.with_ils ? (const double*)ctx->work["ils"].p : nullptr;
@@ -664,8 +670,12 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
             if ((o.continua & 1) && ctx->n_h2o > 1) cd.mask |= 1;
             if ((o.continua & 2) && ctx->n_co2 > 1) cd.mask |= 2;
         }
-        jg_rte_kernel<<<dim3((unsigned)((n_nu + 127) / 128), np), 128, 0, st>>>(
-            d_out, n_out, d_lrt, d_jl, d_prt, d_jp, d_vlev, L, d_grid, n_nu, o.source_function, cd, d_I, d_D);
+        if (cd.mask & kCiaMask)
+            jg_rte_kernel<true><<<dim3((unsigned)((n_nu + 127) / 128), np), 128, 0, st>>>(
+                d_out, n_out, d_lrt, d_jl, d_prt, d_jp, d_vlev, L, d_grid, n_nu, o.source_function, cd, d_I, d_D);
+        else
+            jg_rte_kernel<<<dim3((unsigned)((n_nu + 127) / 128), np), 128, 0, st>>>(
+                d_out, n_out, d_lrt, d_jl, d_prt, d_jp, d_vlev, L, d_grid, n_nu, o.source_function, cd, d_I, d_D);
         check_launch(ctx);
         const double* d_kern = o.with_ils ? (const double*)ctx->work["ils"].p : nullptr;
         const int64_t n_taps = o.with_ils ? ctx->ils_n : 0;

@@ -655,6 +655,7 @@ __device__ __forceinline__ double lit_corr_d(double s) {
 
 // continuum optical depth of one layer at (vh, vc, Tm), continuum.jl:183-250 and
 // the dz(Tm) of optical_depth.jl:123-130 (vmr_jacobian.jl:300-311)
+template <bool CIA>
 __device__ __forceinline__ double cont_tau(double nu, const LayerRT& r, double dp, const ContDev& c, double Cs,
                                           double Cf, double te, double Se, double td, double vh, double vc,
                                           double Tm, const CiaPoint& cp) {
@@ -674,7 +675,7 @@ __device__ __forceinline__ double cont_tau(double nu, const LayerRT& r, double d
         const double tc = td == 0.0 ? 1.0 : pow(Tm / 246.0, td);
         t += Se * tc * (1e-20 * n * rho) * rad * dz;
     }
-    if (c.mask & kCiaMask) t += cia_tau(c, cp, nu, vh, vc, p, Tm, dz);
+    if (CIA) t += cia_tau(c, cp, nu, vh, vc, p, Tm, dz);
     return t;
 }
 
@@ -683,6 +684,7 @@ __device__ __forceinline__ double cont_tau(double nu, const LayerRT& r, double d
 // schwarzschild_jacobian.jl:66-266 with the state chains of vmr_jacobian.jl:383-503.
 // Transmittances come from the FP64 cumulative optical depth: the top-of-layer
 // transmittance of layer m is exp(-(OD_total - OD_below_and_m)).
+template <bool CIA = false>
 __global__ void __launch_bounds__(128) jg_rte_kernel(
     const float* __restrict__ jl, int n_out, const LayerRT* __restrict__ lrt, const JgLayer* __restrict__ jlay,
     const ProfileRT* __restrict__ prt, const JgProfile* __restrict__ jprof, const double* __restrict__ vlev,
@@ -711,11 +713,11 @@ __global__ void __launch_bounds__(128) jg_rte_kernel(
         td = lerp_val(cont.co2 + 2 * cont.n_co2, l);
     }
     CiaPoint cp;
-    if (cont.mask & kCiaMask) cia_prepare(cont.cia, cont.mask, nu, cp);
+    if (CIA) cia_prepare(cont.cia, cont.mask, nu, cp);
     const double invmu = 1.0 / pr.mu, eps = pr.eps;
     auto layer_s = [&](int k) {
         double t = (double)out[((size_t)k * n_out) * n_nu + i];
-        if (cont.mask) t += cont_tau(nu, lr[k], jy[k].dp, cont, Cs, Cf, te, Se, td, lr[k].vmr_h2o, lr[k].vmr_co2, lr[k].T_mid, cp);
+        if (cont.mask) t += cont_tau<CIA>(nu, lr[k], jy[k].dp, cont, Cs, Cf, te, Se, td, lr[k].vmr_h2o, lr[k].vmr_co2, lr[k].T_mid, cp);
         return t * invmu;
     };
     auto emission_down = [&](int k, double s, double& em, double& dem) {  // schwarzschild_jacobian.jl:221-243
@@ -806,17 +808,17 @@ __global__ void __launch_bounds__(128) jg_rte_kernel(
         if (cont.mask) {
             const double vh = r.vmr_h2o, vc = r.vmr_co2, Tm = r.T_mid;
             if (jp.include_T)
-                cT = (cont_tau(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh, vc, Tm + 0.05, cp) -
-                      cont_tau(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh, vc, Tm - 0.05, cp)) / 0.1;
+                cT = (cont_tau<CIA>(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh, vc, Tm + 0.05, cp) -
+                      cont_tau<CIA>(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh, vc, Tm - 0.05, cp)) / 0.1;
             if (jp.retr_h2o >= 0) {
                 const double h = fmax(fabs(vh), 1e-30) * 1e-6;
-                cvh = (cont_tau(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh + h, vc, Tm, cp) -
-                       cont_tau(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh - h, vc, Tm, cp)) / (2 * h);
+                cvh = (cont_tau<CIA>(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh + h, vc, Tm, cp) -
+                       cont_tau<CIA>(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh - h, vc, Tm, cp)) / (2 * h);
             }
             if (jp.retr_co2 >= 0) {
                 const double h = fmax(fabs(vc), 1e-30) * 1e-6;
-                cvc = (cont_tau(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh, vc + h, Tm, cp) -
-                       cont_tau(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh, vc - h, Tm, cp)) / (2 * h);
+                cvc = (cont_tau<CIA>(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh, vc + h, Tm, cp) -
+                       cont_tau<CIA>(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh, vc - h, Tm, cp)) / (2 * h);
             }
         }
         if (jp.include_T) {

@@ -177,12 +177,12 @@ __device__ __forceinline__ double lerp_val(const double* v, const Lerp& l) {
     return v[l.i] * (1.0 - l.w) + v[l.i + 1] * l.w;
 }
 
-template <typename TT>
+template <bool CIA, typename TT>
 __device__ __forceinline__ double layer_tau(const TT* tau_l, long long i, double nu, const LayerRT& r,
                                             const ContDev& c, double Cs, double Cf, double te, double Se,
                                             double td, const CiaPoint& cp) {
     double t = (double)tau_l[i];
-    if (c.mask & kCiaMask) t += cia_tau(c, cp, nu, r.vmr_h2o, r.vmr_co2, r.p_mid, r.T_mid, r.dz_cm);
+    if (CIA) t += cia_tau(c, cp, nu, r.vmr_h2o, r.vmr_co2, r.p_mid, r.T_mid, r.dz_cm);
     if (c.mask) {
         const double T = r.T_mid, p = r.p_mid;
         const double rho = (p / 1013.0) * (296.0 / T);
@@ -203,7 +203,9 @@ __device__ __forceinline__ double layer_tau(const TT* tau_l, long long i, double
     return t;
 }
 
-template <typename TT>
+// CIA: a CIA table is in use (a separate instantiation keeps the per-point CIA cache
+// out of the common kernel)
+template <typename TT, bool CIA = false>
 __global__ void __launch_bounds__(256) rte_kernel(const TT* __restrict__ tau, const LayerRT* __restrict__ lrt,
                                                   const ProfileRT* __restrict__ prt, int L,
                                                   const double* __restrict__ grid, long long n_nu, int src,
@@ -225,7 +227,7 @@ __global__ void __launch_bounds__(256) rte_kernel(const TT* __restrict__ tau, co
         td = lerp_val(cont.co2 + 2 * cont.n_co2, l);
     }
     CiaPoint cp;
-    if (cont.mask & kCiaMask) cia_prepare(cont.cia, cont.mask, nu, cp);
+    if (CIA) cia_prepare(cont.cia, cont.mask, nu, cp);
     const ProfileRT pr = prt[p];
     const LayerRT* lr = lrt + (size_t)p * L;
     const TT* tp = tau + (size_t)p * L * n_nu;
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(256) rte_kernel(const TT* __restrict__ tau, co
     double I_atm = 0.0;
     for (int k = L - 1; k >= 0; --k) {
         const LayerRT r = lr[k];
-        const double s = layer_tau(tp + (size_t)k * n_nu, i, nu, r, cont, Cs, Cf, te, Se, td, cp) / pr.mu;
+        const double s = layer_tau<CIA>(tp + (size_t)k * n_nu, i, nu, r, cont, Cs, Cf, te, Se, td, cp) / pr.mu;
         const double Tr_k = Tr_up * exp(-s);
         const double dT = Tr_up - Tr_k;
         if (src == 0) {
@@ -251,7 +253,7 @@ __global__ void __launch_bounds__(256) rte_kernel(const TT* __restrict__ tau, co
         double Id = 0.0, g = 1.0;
         for (int k = 0; k < L; ++k) {
             const LayerRT r = lr[k];
-            const double s = layer_tau(tp + (size_t)k * n_nu, i, nu, r, cont, Cs, Cf, te, Se, td, cp) / pr.mu;
+            const double s = layer_tau<CIA>(tp + (size_t)k * n_nu, i, nu, r, cont, Cs, Cf, te, Se, td, cp) / pr.mu;
             double em;
             if (src == 0) {
                 const double Ba = planck64(nu, r.T_ave), Bb = planck64(nu, r.T_bot);
