@@ -176,7 +176,7 @@ static std::vector<ListDev> list_descs(irs_ctx* ctx) {
 // Runs the line-parameter passes and the line sum for the plan; returns the
 // device tau buffer ([n_prof * L][n_nu], FP32 for mixed or FP64 for plain).
 static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n_nu, double grid0,
-                         double dnu_g, const irs_fm_options& o, int ev_mid, const double* d_pert = nullptr,
+                         double dnu_g, const irs_fm_options& o, int ev_mid, double* d_pert = nullptr,
                          long long pstride = 0) {
     cudaStream_t st = ctx->stream;
     const int nseg = (int)pl.segs.size();
@@ -323,12 +323,15 @@ static void parallel_for(int n, F&& f) {
 struct RelmatPlan {
     std::vector<LmPole> poles;
     std::vector<long long> off;  // per row (profile, layer[, variant]): poles[off[k], off[k+1])
+    std::vector<int> seg_of;     // per (profile, layer): the LM species' segment, or -1
+    uint32_t iso_mask = 0;
 };
 static_assert(sizeof(LmPole) == sizeof(LmPoleDev), "pole layouts differ");
 constexpr long long kPertAlign = 8192;  // rows padded to whole line-sum strips of either kernel
 static_assert(kPertAlign % kMxStrip == 0 && kPertAlign % kJgStrip == 0, "perturbation row padding");
 
-static bool relmat_plan(irs_ctx* ctx, Plan& pl, const irs_fm_options& o, RelmatPlan& rp, bool jac = false) {
+// Flags the LM species' segments SEG_RELMAT; false when relmat line mixing is off.
+static bool relmat_prepare(irs_ctx* ctx, Plan& pl, const irs_fm_options& o, RelmatPlan& rp) {
     if (o.line_mixing != IRS_LM_RELMAT_VPY && o.line_mixing != IRS_LM_RELMAT_VPW) return false;
     const RelmatHost& R = ctx->relmat;
     IRS_REQUIRE(R.species != 0, "line_mixing 2 and 3 need the relaxation-matrix data (irs_upload_relmat)");
@@ -336,14 +339,22 @@ static bool relmat_plan(irs_ctx* ctx, Plan& pl, const irs_fm_options& o, RelmatP
     for (size_t i = 0; i < ctx->lists.size(); ++i)
         if (ctx->lists[i].species == R.species && ctx->lists[i].n > 0) li = (int)i;
     if (li < 0) return false;  // the LM species has no line list in this call
-    const uint32_t iso_mask = ctx->lists[li].iso_mask;
-    const int npl = pl.n_prof * pl.L;
-    std::vector<int> seg_of(npl, -1);
+    rp.iso_mask = ctx->lists[li].iso_mask;
+    rp.seg_of.assign((size_t)pl.n_prof * pl.L, -1);
     for (size_t i = 0; i < pl.segs.size(); ++i)
         if (pl.segs[i].list == li) {
             pl.segs[i].flags |= SEG_RELMAT;
-            seg_of[pl.segs[i].prof * pl.L + pl.segs[i].layer] = (int)i;
+            rp.seg_of[pl.segs[i].prof * pl.L + pl.segs[i].layer] = (int)i;
         }
+    return true;
+}
+
+// The pole lists of every (profile, layer) that has a relmat segment.
+static void relmat_build(irs_ctx* ctx, const Plan& pl, const irs_fm_options& o, RelmatPlan& rp, bool jac) {
+    const RelmatHost& R = ctx->relmat;
+    const uint32_t iso_mask = rp.iso_mask;
+    const std::vector<int>& seg_of = rp.seg_of;
+    const int npl = pl.n_prof * pl.L;
     const int nv = jac ? 3 : 1;
     std::vector<std::vector<LmPole>> per((size_t)npl * nv);
     parallel_for(npl * nv, [&](int k) {
@@ -373,6 +384,11 @@ static bool relmat_plan(irs_ctx* ctx, Plan& pl, const irs_fm_options& o, RelmatP
     for (size_t k = 0; k < rows; ++k) rp.off[k + 1] = rp.off[k] + (long long)per[k].size();
     rp.poles.resize(rp.off[rows]);
     for (size_t k = 0; k < rows; ++k) std::copy(per[k].begin(), per[k].end(), rp.poles.begin() + rp.off[k]);
+}
+
+static bool relmat_plan(irs_ctx* ctx, Plan& pl, const irs_fm_options& o, RelmatPlan& rp, bool jac) {
+    if (!relmat_prepare(ctx, pl, o, rp)) return false;
+    relmat_build(ctx, pl, o, rp, jac);
     return true;
 }
 
@@ -439,30 +455,47 @@ static void forward_pass(irs_ctx* ctx, const irs_profile* profs, int n_prof, con
         workspace(ctx, "lrt", std::max<size_t>(lrt.size(), 1) * sizeof(LayerRT));
         workspace(ctx, "prt", std::max<size_t>(prt.size(), 1) * sizeof(ProfileRT));
     }
+    // relmat line mixing: the LM species' clamped sums go to their own rows while the
+    // host builds the poles (overlapping the line sum); the finish kernel then adds
+    // max(sum + d_sigma, 0) into the optical depths
     RelmatPlan rp;
-    const auto h0 = std::chrono::steady_clock::now();
-    const bool relmat = relmat_plan(ctx, pl, o, rp);
-    ctx->lm_host_pass = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
+    const bool relmat = relmat_prepare(ctx, pl, o, rp);
     ctx->lm_ev = relmat;
+    ctx->lm_host_pass = 0;
+    const long long pstride = ((n_nu + kPertAlign - 1) / kPertAlign) * kPertAlign;
+    std::vector<double> coef_pl;
     if (relmat) {
-        const long long ps = ((n_nu + kPertAlign - 1) / kPertAlign) * kPertAlign;
-        workspace(ctx, "lm_pert", (size_t)n_prof * L * ps * sizeof(double));
-        workspace(ctx, "lm_poles", std::max<size_t>(rp.poles.size(), 1) * sizeof(LmPole));
-        workspace(ctx, "lm_off", rp.off.size() * sizeof(long long));
+        coef_pl.assign((size_t)n_prof * L, 0.0);
+        for (size_t k = 0; k < rp.seg_of.size(); ++k)
+            if (rp.seg_of[k] >= 0) coef_pl[k] = pl.segs[rp.seg_of[k]].coef;
+        workspace(ctx, "lm_pert", (size_t)n_prof * L * pstride * sizeof(double));
+        workspace(ctx, "lm_sv", (size_t)n_prof * L * pstride * sizeof(double));
+        workspace(ctx, "lm_coef", coef_pl.size() * sizeof(double));
+        workspace(ctx, "lm_off", ((size_t)n_prof * L + 1) * sizeof(long long));
     }
     IRS_CUDA(cudaEventRecord(ctx->ev[0], st));
     double* d_grid = (double*)workspace(ctx, "grid", n_nu * sizeof(double));
     grid_values_kernel<<<(unsigned)((n_nu + 255) / 256), 256, 0, st>>>(to_dev(ig.g), d_grid);
     check_launch(ctx);
     if (o.with_ils) ensure_ils(ctx, ig.dnu_hi, s.opd_max, s.fwhm_gauss, o.apodization);
-    long long pstride = 0;
-    const double* d_pert = nullptr;
+    double* d_sv = relmat ? (double*)workspace(ctx, "lm_sv", (size_t)n_prof * L * pstride * sizeof(double)) : nullptr;
+    void* d_tau = run_linesum(ctx, pl, d_grid, n_nu, ig.g.at(0), ig.dnu_hi, o, 1, d_sv, pstride);
     if (relmat) {
+        const auto h0 = std::chrono::steady_clock::now();
+        relmat_build(ctx, pl, o, rp, false);  // host cores, while the GPU runs the line sum
+        ctx->lm_host_pass = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
         IRS_CUDA(cudaEventRecord(ctx->ev[7], st));
-        d_pert = relmat_launch(ctx, rp, d_grid, n_nu, o.lm_cutoff, o.x_far, pstride);
+        long long ps = 0;
+        const double* d_pert = relmat_launch(ctx, rp, d_grid, n_nu, o.lm_cutoff, o.x_far, ps);
+        const double* d_coef = upload(ctx, "lm_coef", coef_pl);
+        dim3 gf((unsigned)((n_nu + 255) / 256), n_prof * L);
+        if (o.precision != IRS_FP64)
+            relmat_finish_kernel<float><<<gf, 256, 0, st>>>((float*)d_tau, d_sv, d_pert, d_coef, n_nu, pstride);
+        else
+            relmat_finish_kernel<double><<<gf, 256, 0, st>>>((double*)d_tau, d_sv, d_pert, d_coef, n_nu, pstride);
+        check_launch(ctx);
         IRS_CUDA(cudaEventRecord(ctx->ev[8], st));
     }
-    void* d_tau = run_linesum(ctx, pl, d_grid, n_nu, ig.g.at(0), ig.dnu_hi, o, 1, d_pert, pstride);
     IRS_CUDA(cudaEventRecord(ctx->ev[2], st));
     LayerRT* d_lrt = upload(ctx, "lrt", lrt);
     ProfileRT* d_prt = upload(ctx, "prt", prt);

@@ -45,7 +45,7 @@ template <int METHOD>
 __global__ void __launch_bounds__(256) linesum_f64_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const int2* __restrict__ pl_segs,
     LpOutF64 lp, const double* __restrict__ grid, long long n_nu, double cutoff, double x_far,
-    double* __restrict__ tau, const double* __restrict__ pert, long long pstride) {
+    double* __restrict__ tau, double* __restrict__ pert, long long pstride) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int pl = blockIdx.y;
     if (i >= n_nu) return;
@@ -87,7 +87,10 @@ __global__ void __launch_bounds__(256) linesum_f64_kernel(
         }
         double sig = fmax(acc, 0.0);
         if (lm) sig = fmax(sig + accD, 0.0);
-        if (pert && (sg.flags & SEG_RELMAT)) sig = fmax(sig + pert[(size_t)pl * pstride + i], 0.0);
+        if (pert && (sg.flags & SEG_RELMAT)) {  // relmat line mixing: finished by relmat_finish_kernel
+            pert[(size_t)pl * pstride + i] = sig;
+            continue;
+        }
         tsum += sig * sg.coef;
     }
     tau[(size_t)pl * n_nu + i] = tsum;
@@ -236,7 +239,7 @@ template <int METHOD, bool LM, bool FAR>
 __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, const LpOutMixed& lp, long long wb,
                                              float cut, float cut2, int lane, WarpTile& T, const FarTable& FT,
                                              float xn, float* tsum, unsigned long long& work,
-                                             const double* __restrict__ prow) {
+                                             double* __restrict__ prow) {
     constexpr float kCentre = 0.5f * (kMxWarpPts - 1);
     constexpr float kHalf = 0.5f * kMxWarpPts + 0.5f;
     long long jlo, jhi;
@@ -507,14 +510,15 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             if (LM) kahan_add(sumD[q], compD[q], vd);
         }
     }
-    const bool rel = prow && (sg.flags & SEG_RELMAT);  // relmat line mixing: sigma = max(sigma_V + d_sigma, 0)
-    const float rc = (float)sg.coef;
+    // relmat line mixing: this species' clamped sum goes to its own row, and
+    // relmat_finish_kernel adds max(sum + d_sigma, 0) once the perturbation is known
+    const bool rel = prow && (sg.flags & SEG_RELMAT);
 #pragma unroll
     for (int q = 0; q < kMxQ; ++q) {
         float sig = fmaxf(sum[q], 0.f);
         if (LM) sig = fmaxf(sig + sumD[q], 0.f);
-        if (rel) sig = fmaxf(sig + rc * (float)prow[wb + 32 * q + lane], 0.f);
-        tsum[q] += sig;
+        if (rel) prow[wb + 32 * q + lane] = (double)sig;
+        else tsum[q] += sig;
     }
 }
 
@@ -567,14 +571,15 @@ __device__ __forceinline__ void warp_segment_pv(const SegDev& sg, long long cnt,
     for (int q = 0; q < kMxQ; ++q) tsum[q] += fmaxf(sum[q], 0.f);
 }
 
-// PERT: segments flagged SEG_RELMAT add the relaxation-matrix perturbation rows
-// pert[(profile, layer)][pstride] before their clamp (a separate instantiation, so the
-// kernels without it are unchanged).
+// PERT: segments flagged SEG_RELMAT write their clamped sums to the rows
+// pert[(profile, layer)][pstride] instead of the optical depth, for
+// relmat_finish_kernel (a separate instantiation, so the kernels without it are
+// unchanged).
 template <int METHOD, bool ANY_LM, bool FAR, bool PERT = false>
 __global__ void __launch_bounds__(kMxThreads, ANY_LM ? 2 : 3) linesum_mixed_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const int2* __restrict__ pl_segs,
     LpOutMixed lp, long long n_nu, float cut_g, float* __restrict__ tau, unsigned long long* __restrict__ evald,
-    const double* __restrict__ pert, long long pstride) {
+    double* __restrict__ pert, long long pstride) {
     __shared__ WarpTile tiles[kMxWarps];
     __shared__ FarTable ftab;
     if (FAR) {

@@ -62,4 +62,24 @@ __global__ void __launch_bounds__(256) lm_pert_kernel(const LmPoleDev* __restric
     out[(size_t)pl * stride + i] = acc;
 }
 
+// tau[pl][i] += the relmat species' cross section max(sigma_V + d_sigma, 0) times its
+// column amount (the clamp of compute_voigt_{lm,vpw}_cross_sections): sv holds the
+// line-sum's clamped Voigt part (already times the column amount for the FP32 path),
+// dsig the perturbation; coef[pl] = 0 where the species is absent.
+template <typename TT>
+__global__ void __launch_bounds__(256) relmat_finish_kernel(TT* __restrict__ tau, const double* __restrict__ sv,
+                                                            const double* __restrict__ dsig,
+                                                            const double* __restrict__ coef, long long n_nu,
+                                                            long long pstride) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int pl = blockIdx.y;
+    const double c = coef[pl];
+    if (i >= n_nu || c == 0.0) return;
+    const size_t k = (size_t)pl * pstride + i;
+    if (sizeof(TT) == sizeof(float))
+        tau[(size_t)pl * n_nu + i] += fmaxf((float)sv[k] + (float)c * (float)dsig[k], 0.f);
+    else
+        tau[(size_t)pl * n_nu + i] += fmax(sv[k] + dsig[k], 0.0) * c;
+}
+
 }  // namespace irs
