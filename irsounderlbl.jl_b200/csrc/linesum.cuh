@@ -297,11 +297,19 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             }
         }
         if (FAR && !LM && __all_sync(kFull, cls == 3 || cls == 0)) {  // far lines and lines out of reach
-            if (cls == 3) {
+            if (cls == 3) {  // nodes in pairs, packed: one reciprocal of the product per pair
+                const float2 u2 = make_float2(uh, uh), l2 = make_float2(ul, ul);
+                const float2 b2 = make_float2(a0.x, a0.x), aa = make_float2(a0.y, a0.y);
 #pragma unroll
-                for (int k = 0; k < kFarNodes; ++k) {
-                    const float d = (far_node_f(k) - uh) - ul;
-                    fnode[k] = fmaf(a0.y, rcp_fast(fmaf(d, d, a0.x)), fnode[k]);
+                for (int k = 0; k < kFarNodes; k += 2) {
+                    const float2 xs = make_float2(far_node_f(k + 1), far_node_f(k));  // swapped
+                    const float2 ds = __fadd2_rn(__fadd2_rn(xs, make_float2(-u2.x, -u2.y)),
+                                                 make_float2(-l2.x, -l2.y));
+                    const float2 es = __ffma2_rn(ds, ds, b2);                       // (e[k+1], e[k])
+                    const float R = rcp_fast(es.x * es.y);
+                    const float2 r = __fmul2_rn(es, make_float2(R, R));             // (1/e[k], 1/e[k+1])
+                    fnode[k] = fmaf(aa.x, r.x, fnode[k]);
+                    fnode[k + 1] = fmaf(aa.y, r.y, fnode[k + 1]);
                 }
             }
             kahan_add(PA, PAc, pa);
