@@ -258,8 +258,10 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
         dim3 g2((unsigned)((n_nu + kMxStrip - 1) / kMxStrip), npl);
         const float cut_g = (float)(o.cutoff / dnu_g);
         unsigned long long* d_eval = d_pairs + 2;
-#define IRS_MX(M, LMX, F, P) \
-    linesum_mixed_kernel<M, LMX, F, P><<<g2, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau, d_eval, d_pert, pstride)
+#define IRS_MX(M, LMX, F, P) do { \
+        IRS_CUDA(cudaFuncSetAttribute(linesum_mixed_kernel<M, LMX, F, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMxSmem)); \
+        linesum_mixed_kernel<M, LMX, F, P><<<g2, kMxThreads, kMxSmem, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau, d_eval, d_pert, pstride); \
+    } while (0)
         const bool far = o.precision == IRS_MIXED;
         if (o.method == 1) { if (far) IRS_MX(1, false, true, false); else IRS_MX(1, false, false, false); }
         else if (o.method == 2) IRS_MX(2, false, false, false);

@@ -145,6 +145,14 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
+// Inner points of a slow line: |x| + y < 15 (plus one point each side), where
+// faddeeva32 takes its CF4 or Weideman branch.  They span a few points of one or two
+// 32-point rows, so evaluating them inside the per-point loop leaves most lanes of
+// those rows idle; instead each tile evaluates the inner points of all its slow lines
+// lane-parallel into cw (up to kCoreBuf per tile; lines beyond it keep the per-point
+// evaluation) and the per-point loop reads them back.
+constexpr int kCoreBuf = 256;
+
 struct WarpTile {
     float4 fu[32];  // fast lines: uh, ul, b2, a               (PV: uh, ul, -, class)
     float4 su[32];  // slow lines: uh, ul, b2, a               (PV: gV2, aPV, c1, c0)
@@ -155,6 +163,8 @@ struct WarpTile {
     float ffg[32];  // far lines: g
     float4 eu[32];  // cutoff-edge lines (far field only): uh, ul, b2, a
     float4 ep[32];  // cutoff-edge lines: c1, c0, g, -
+    int4 sr[32];    // slow lines (FullFaddeeva): inner points [x, y] of the block, their offset z in cw
+    float2 cw[kCoreBuf];  // w(x + i y) at the inner points of the tile's slow lines, line after line
     // mid lines (far field only) share su/sp/sq with the slow lines, from the top
     // down (position 31 - k): su = (uh, ul, b2, a), sp = (c1, c0, fx, y),
     // sq = (An, g, Yw, dfar2)
@@ -319,6 +329,30 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             if (lane == 0) work += (unsigned long long)nfar * kFarNodes;
             continue;
         }
+        // FullFaddeeva slow lines: the inner points of the block, [plo, plo + nin - 1],
+        // and their offsets in cw by a warp scan; cfit = the points that fit (warp-uniform)
+        int nin = 0, plo = 1, coff = 0, cfit = 0;
+        if (METHOD == 3) {
+            if (cls == 2 && a1.w < 15.f) {
+                const float hw = (15.f - a1.w) / a1.z + 1.f;
+                const float c = uh + ul;
+                const float lo = fmaxf(c - hw, 0.f), hi = fminf(c + hw, (float)(kMxWarpPts - 1));
+                if (lo <= hi) {
+                    plo = (int)ceilf(lo);
+                    nin = max((int)floorf(hi) - plo + 1, 0);
+                }
+            }
+            int inc = nin;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int t = __shfl_up_sync(kFull, inc, d);
+                if (lane >= d) inc += t;
+            }
+            coff = inc - nin;
+            const unsigned ov = __ballot_sync(kFull, inc > kCoreBuf && nin > 0);
+            cfit = ov ? __shfl_sync(kFull, coff, __ffs(ov) - 1) : __shfl_sync(kFull, inc, 31);
+            if (inc > kCoreBuf) nin = 0;  // beyond the buffer: evaluated per point
+        }
         const unsigned fm = __ballot_sync(kFull, cls == 1), sm = __ballot_sync(kFull, cls == 2);
         const unsigned xm = FAR ? __ballot_sync(kFull, cls == 3) : 0u;
         const unsigned em = FAR ? __ballot_sync(kFull, cls == 4) : 0u;
@@ -346,6 +380,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             T.su[pos] = make_float4(uh, ul, a0.x, a0.y);
             T.sp[pos] = make_float4(a0.z, a0.w, a1.x, a1.y);
             T.sq[pos] = make_float4(a1.z, a1.w, a2.x, a2.y);
+            if (METHOD == 3) T.sr[pos] = make_int4(plo, plo + nin - 1, coff, 0);
         }
         float A = 0.f, B = 0.f, Cc = 0.f;
         if (FAR) {
@@ -377,6 +412,22 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             work += (unsigned long long)(nf + ns) * kMxWarpPts;
         }
         if (FAR && nf + ns + ne + nm == 0) continue;  // warp-uniform: nothing per point in this tile
+        if (METHOD == 3 && cfit > 0) {  // the inner points, one per lane: the slow line owning
+                                        // element e is the last one whose offset is <= e
+            for (int e = lane; e < cfit; e += 32) {
+                int lo = 0, hi = ns - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (T.sr[mid].z <= e) lo = mid;
+                    else hi = mid - 1;
+                }
+                const int4 r = T.sr[lo];
+                const float4 u = T.su[lo], w = T.sq[lo];
+                const float d = ((float)(r.x + (e - r.z)) - u.x) - u.y;  // as in the per-point loop
+                T.cw[e] = faddeeva32(d * w.x, w.y);
+            }
+            __syncwarp();
+        }
         float2 acc2[kMxQ / 2];
         float tdsp[kMxQ];
 #pragma unroll
@@ -456,6 +507,13 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             const float4 u = T.su[k];
             const float4 p = T.sp[k];
             const float4 w = T.sq[k];
+            int rlo = 1, rhi = 0, rb = 0;  // inner points held in cw: [rlo, rhi] at rb + point
+            if (METHOD == 3) {
+                const int4 r = T.sr[k];
+                rlo = r.x;
+                rhi = r.y;
+                rb = r.z - r.x;
+            }
 #pragma unroll
             for (int q = 0; q < kMxQ; ++q) {
                 const float d = ((pl0 + 32.f * q) - u.x) - u.y;
@@ -469,7 +527,8 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
                         v = fmaf(p.w, weideman24_32(x, w.y), ped);
                         vd = 0.f;
                     } else {
-                        const float2 fw = faddeeva32_fast(x, w.y);
+                        const int pt = lane + 32 * q;
+                        const float2 fw = (pt >= rlo && pt <= rhi) ? T.cw[rb + pt] : faddeeva32_fast(x, w.y);
                         v = fmaf(p.w, fw.x, ped);
                         vd = w.w * fw.y;
                     }
@@ -583,13 +642,17 @@ __device__ __forceinline__ void warp_segment_pv(const SegDev& sg, long long cnt,
 // pert[(profile, layer)][pstride] instead of the optical depth, for
 // relmat_finish_kernel (a separate instantiation, so the kernels without it are
 // unchanged).
+// dynamic shared memory of linesum_mixed_kernel: the warps' tiles, then the far table
+constexpr size_t kMxSmem = sizeof(WarpTile) * kMxWarps + sizeof(FarTable);
+
 template <int METHOD, bool ANY_LM, bool FAR, bool PERT = false>
 __global__ void __launch_bounds__(kMxThreads, ANY_LM ? 2 : 3) linesum_mixed_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const int2* __restrict__ pl_segs,
     LpOutMixed lp, long long n_nu, float cut_g, float* __restrict__ tau, unsigned long long* __restrict__ evald,
     double* __restrict__ pert, long long pstride) {
-    __shared__ WarpTile tiles[kMxWarps];
-    __shared__ FarTable ftab;
+    extern __shared__ __align__(16) unsigned char mx_smem[];
+    WarpTile* tiles = reinterpret_cast<WarpTile*>(mx_smem);
+    FarTable& ftab = *reinterpret_cast<FarTable*>(mx_smem + sizeof(WarpTile) * kMxWarps);
     if (FAR) {
         far_table_init(ftab);
         __syncthreads();
