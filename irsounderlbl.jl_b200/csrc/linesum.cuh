@@ -245,10 +245,23 @@ __device__ __forceinline__ void fast_pair(float2 d0s, float2 offs, float2 b2, fl
     acc = __ffma2_rn(a, r, acc);
 }
 
+// The optical-depth row of a warp's 256 points.  Each segment's clamped sums are
+// added to it in segment order (the first one stores), so no per-point total stays
+// in registers from one segment to the next.
+struct OutRow {
+    float* p;    // tau at the warp's first point
+    int n;       // the warp's points inside the grid
+    bool wrote;  // a segment has stored
+};
+__device__ __forceinline__ void out_add(OutRow& o, int q, int lane, float sig) {
+    const int i = 32 * q + lane;
+    if (i < o.n) o.p[i] = o.wrote ? o.p[i] + sig : sig;
+}
+
 template <int METHOD, bool LM, bool FAR>
 __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, const LpOutMixed& lp, long long wb,
                                              float cut, float cut2, int lane, WarpTile& T, const FarTable& FT,
-                                             float xn, float* tsum, unsigned long long& work,
+                                             float xn, OutRow& orow, unsigned long long& work,
                                              double* __restrict__ prow) {
     constexpr float kCentre = 0.5f * (kMxWarpPts - 1);
     constexpr float kHalf = 0.5f * kMxWarpPts + 0.5f;
@@ -262,14 +275,15 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
     float sum[kMxQ], comp[kMxQ], sumD[kMxQ], compD[kMxQ];
 #pragma unroll
     for (int q = 0; q < kMxQ; ++q) sum[q] = comp[q] = sumD[q] = compD[q] = 0.f;
-    // far-field node sums: lane l accumulates node l % 8 over every fourth far line
+    // with line mixing, far-field node sums of the staged far lines: lane l accumulates
+    // node l % 8 over every fourth far line
     float farS = 0.f, farC = 0.f, farDS = 0.f, farDC = 0.f;
     // with the far field, each lane accumulates its own lines' pedestal quadratics
     // (compensated) and the warp reduces them once per segment, so tiles holding only
     // far lines need no per-point work
     float PA = 0.f, PAc = 0.f, PB = 0.f, PBc = 0.f, PC = 0.f, PCc = 0.f;
-    // tiles whose lines are all far lines skip the staging: each lane evaluates its own
-    // line at the 8 nodes and accumulates them here (reduced across the warp once)
+    // without line mixing each lane evaluates its own far lines at the 8 nodes and
+    // accumulates them here (reduced across the warp once)
     float fnode[kFarNodes];
 #pragma unroll
     for (int k = 0; k < kFarNodes; ++k) fnode[k] = 0.f;
@@ -306,7 +320,10 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
                     cls = 5;
             }
         }
-        if (FAR && !LM && __all_sync(kFull, cls == 3 || cls == 0)) {  // far lines and lines out of reach
+        // without line mixing each lane evaluates its own far line at the 8 nodes (summed
+        // across the warp once per segment); tiles holding only far lines and lines out
+        // of reach then need nothing else
+        if (FAR && !LM) {
             if (cls == 3) {  // nodes in pairs, packed: one reciprocal of the product per pair
                 const float2 u2 = make_float2(uh, uh), l2 = make_float2(ul, ul);
                 const float2 b2 = make_float2(a0.x, a0.x), aa = make_float2(a0.y, a0.y);
@@ -322,12 +339,14 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
                     fnode[k + 1] = fmaf(aa.y, r.y, fnode[k + 1]);
                 }
             }
-            kahan_add(PA, PAc, pa);
-            kahan_add(PB, PBc, pb);
-            kahan_add(PC, PCc, pc);
             const unsigned nfar = __popc(__ballot_sync(kFull, cls == 3));
             if (lane == 0) work += (unsigned long long)nfar * kFarNodes;
-            continue;
+            if (__all_sync(kFull, cls == 3 || cls == 0)) {
+                kahan_add(PA, PAc, pa);
+                kahan_add(PB, PBc, pb);
+                kahan_add(PC, PCc, pc);
+                continue;
+            }
         }
         // FullFaddeeva slow lines: the inner points of the block, [plo, plo + nin - 1],
         // and their offsets in cw by a warp scan; cfit = the points that fit (warp-uniform)
@@ -354,7 +373,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             if (inc > kCoreBuf) nin = 0;  // beyond the buffer: evaluated per point
         }
         const unsigned fm = __ballot_sync(kFull, cls == 1), sm = __ballot_sync(kFull, cls == 2);
-        const unsigned xm = FAR ? __ballot_sync(kFull, cls == 3) : 0u;
+        const unsigned xm = (FAR && LM) ? __ballot_sync(kFull, cls == 3) : 0u;  // staged far lines
         const unsigned em = FAR ? __ballot_sync(kFull, cls == 4) : 0u;
         const unsigned mm = FAR ? __ballot_sync(kFull, cls == 5) : 0u;
         __syncwarp();
@@ -362,7 +381,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             const int pos = __popc(fm & lt);
             T.fu[pos] = make_float4(uh, ul, a0.x, a0.y);
             if (LM) T.fg[pos] = a2.x;
-        } else if (FAR && cls == 3) {
+        } else if (FAR && LM && cls == 3) {
             const int pos = __popc(xm & lt);
             T.ff[pos] = make_float4(uh, ul, a0.x, a0.y);
             if (LM) T.ffg[pos] = a2.x;
@@ -398,16 +417,18 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             const int nx = __popc(xm);
             if (lane == 0)
                 work += (unsigned long long)(nf + ns + ne + nm) * kMxWarpPts + (unsigned long long)nx * kFarNodes;
-            float ft = 0.f, fd = 0.f;
-            for (int k = lane >> 3; k < nx; k += 4) {
-                const float4 f = T.ff[k];
-                const float d = (xn - f.x) - f.y;
-                const float r = rcp_fast(fmaf(d, d, f.z));
-                ft = fmaf(f.w, r, ft);
-                if (LM) fd = fmaf(T.ffg[k] * d, r, fd);
+            if (LM) {  // staged far lines: lane l takes node l % 8 of every fourth one
+                float ft = 0.f, fd = 0.f;
+                for (int k = lane >> 3; k < nx; k += 4) {
+                    const float4 f = T.ff[k];
+                    const float d = (xn - f.x) - f.y;
+                    const float r = rcp_fast(fmaf(d, d, f.z));
+                    ft = fmaf(f.w, r, ft);
+                    fd = fmaf(T.ffg[k] * d, r, fd);
+                }
+                kahan_add(farS, farC, ft);
+                kahan_add(farDS, farDC, fd);
             }
-            kahan_add(farS, farC, ft);
-            if (LM) kahan_add(farDS, farDC, fd);
         } else if (lane == 0) {
             work += (unsigned long long)(nf + ns) * kMxWarpPts;
         }
@@ -548,18 +569,17 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             if (LM) kahan_add(sumD[q], compD[q], tdsp[q]);
         }
     }
-    if (FAR) {  // node totals (4 lanes per node), then the interpolant at this lane's points
-        farS += __shfl_xor_sync(kFull, farS, 8);
-        farS += __shfl_xor_sync(kFull, farS, 16);
-        if (LM) {
+    if (FAR) {  // node totals, then the interpolant at this lane's points
+        if (LM) {  // 4 lanes per node
+            farS += __shfl_xor_sync(kFull, farS, 8);
+            farS += __shfl_xor_sync(kFull, farS, 16);
             farDS += __shfl_xor_sync(kFull, farDS, 8);
             farDS += __shfl_xor_sync(kFull, farDS, 16);
         }
         float Fn[kFarNodes], Dn[kFarNodes];
 #pragma unroll
         for (int k = 0; k < kFarNodes; ++k) {
-            Fn[k] = __shfl_sync(kFull, farS, k);
-            if (!LM) Fn[k] += warp_sum(fnode[k]);
+            Fn[k] = LM ? __shfl_sync(kFull, farS, k) : warp_sum(fnode[k]);
             Dn[k] = LM ? __shfl_sync(kFull, farDS, k) : 0.f;
         }
         const float A = warp_sum(PA - PAc), B = warp_sum(PB - PBc), Cc = warp_sum(PC - PCc);
@@ -585,14 +605,15 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
         float sig = fmaxf(sum[q], 0.f);
         if (LM) sig = fmaxf(sig + sumD[q], 0.f);
         if (rel) prow[wb + 32 * q + lane] = (double)sig;
-        else tsum[q] += sig;
+        else out_add(orow, q, lane, sig);
     }
+    if (!rel) orow.wrote = true;
 }
 
 // PseudoVoigt (voigt.jl:281-313): no far-wing shortcut; p0 = (gV2, aPV, c1, c0),
 // p1 = (kPV, gPV, -, -): value = aPV/(d^2 + gV2) + gPV 2^(-kPV d^2) + c1 d^2 + c0.
 __device__ __forceinline__ void warp_segment_pv(const SegDev& sg, long long cnt, const LpOutMixed& lp, long long wb,
-                                                float cut, float cut2, int lane, WarpTile& T, float* tsum) {
+                                                float cut, float cut2, int lane, WarpTile& T, OutRow& orow) {
     constexpr float kCentre = 0.5f * (kMxWarpPts - 1);
     constexpr float kHalf = 0.5f * kMxWarpPts + 0.5f;
     long long jlo, jhi;
@@ -635,7 +656,8 @@ __device__ __forceinline__ void warp_segment_pv(const SegDev& sg, long long cnt,
         for (int q = 0; q < kMxQ; ++q) kahan_add(sum[q], comp[q], tacc[q]);
     }
 #pragma unroll
-    for (int q = 0; q < kMxQ; ++q) tsum[q] += fmaxf(sum[q], 0.f);
+    for (int q = 0; q < kMxQ; ++q) out_add(orow, q, lane, fmaxf(sum[q], 0.f));
+    orow.wrote = true;
 }
 
 // PERT: segments flagged SEG_RELMAT write their clamped sums to the rows
@@ -665,27 +687,23 @@ __global__ void __launch_bounds__(kMxThreads, ANY_LM ? 2 : 3) linesum_mixed_kern
     unsigned long long work = 0;
     const float cut2 = cut_g * cut_g;
     WarpTile& T = tiles[warp];
-    float tsum[kMxQ];
-#pragma unroll
-    for (int q = 0; q < kMxQ; ++q) tsum[q] = 0.f;
+    OutRow orow{tau + (size_t)pl * n_nu + wb, (int)min((long long)kMxWarpPts, n_nu - wb), false};
     const int2 rng = pl_segs[pl];
     for (int s = rng.x; s < rng.x + rng.y; ++s) {
         const SegDev sg = segs[s];
         const long long cnt = seg_count[s];
         if (METHOD == 2)
-            warp_segment_pv(sg, cnt, lp, wb, cut_g, cut2, lane, T, tsum);
+            warp_segment_pv(sg, cnt, lp, wb, cut_g, cut2, lane, T, orow);
         else if (ANY_LM && (sg.flags & 2))
-            warp_segment<METHOD, true, FAR>(sg, cnt, lp, wb, cut_g, cut2, lane, T, ftab, xn, tsum, work, nullptr);
+            warp_segment<METHOD, true, FAR>(sg, cnt, lp, wb, cut_g, cut2, lane, T, ftab, xn, orow, work, nullptr);
         else
-            warp_segment<METHOD, false, FAR>(sg, cnt, lp, wb, cut_g, cut2, lane, T, ftab, xn, tsum, work,
+            warp_segment<METHOD, false, FAR>(sg, cnt, lp, wb, cut_g, cut2, lane, T, ftab, xn, orow, work,
                                              PERT ? pert + (size_t)pl * pstride : nullptr);
     }
     if (evald && lane == 0 && work) atomicAdd(evald, work);
-    float* out = tau + (size_t)pl * n_nu;
+    if (!orow.wrote) {  // no segment stored: zero optical depth
 #pragma unroll
-    for (int q = 0; q < kMxQ; ++q) {
-        const long long i = wb + q * 32 + lane;
-        if (i < n_nu) out[i] = tsum[q];
+        for (int q = 0; q < kMxQ; ++q) out_add(orow, q, lane, 0.f);
     }
 }
 
