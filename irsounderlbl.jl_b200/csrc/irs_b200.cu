@@ -258,11 +258,30 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
         dim3 g2((unsigned)((n_nu + kMxStrip - 1) / kMxStrip), npl);
         const float cut_g = (float)(o.cutoff / dnu_g);
         unsigned long long* d_eval = d_pairs + 2;
+        const bool far = o.precision == IRS_MIXED;
+        const bool anylm = o.line_mixing == IRS_LM_PER_LINE_Y;
+        // strip far field (pre-pass): 272 bytes per (segment, strip), skipped past 2 GiB
+        float* d_sfar = nullptr;
+        int4* d_srng = nullptr;
+        const int n_strips = (int)g2.x;
+        const size_t cells = (size_t)nseg * n_strips;
+        if (far && o.method == 3 && cells * (kStripWords * sizeof(float) + sizeof(int4)) <= ((size_t)2 << 30)) {
+            char* b = (char*)workspace(ctx, "strip_far", cells * (kStripWords * sizeof(float) + sizeof(int4)));
+            d_sfar = (float*)b;
+            d_srng = (int4*)(b + cells * kStripWords * sizeof(float));
+            constexpr int nM = kMxWarps * kFarNodes * kCtaNodes;
+            float* d_M = (float*)workspace(ctx, "strip_M", nM * sizeof(float));
+            strip_table_kernel<<<(nM + 255) / 256, 256, 0, st>>>(d_M);
+            check_launch(ctx);
+            dim3 g3(n_strips, npl);
+            if (anylm) strip_far_kernel<true><<<g3, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, cut_g, n_strips, d_M, d_sfar, d_srng, d_eval);
+            else strip_far_kernel<false><<<g3, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, cut_g, n_strips, d_M, d_sfar, d_srng, d_eval);
+            check_launch(ctx);
+        }
 #define IRS_MX(M, LMX, F, P) do { \
         IRS_CUDA(cudaFuncSetAttribute(linesum_mixed_kernel<M, LMX, F, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMxSmem)); \
-        linesum_mixed_kernel<M, LMX, F, P><<<g2, kMxThreads, kMxSmem, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau, d_eval, d_pert, pstride); \
+        linesum_mixed_kernel<M, LMX, F, P><<<g2, kMxThreads, kMxSmem, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau, d_eval, d_pert, pstride, d_sfar, d_srng, n_strips); \
     } while (0)
-        const bool far = o.precision == IRS_MIXED;
         if (o.method == 1) { if (far) IRS_MX(1, false, true, false); else IRS_MX(1, false, false, false); }
         else if (o.method == 2) IRS_MX(2, false, false, false);
         else if (o.line_mixing == IRS_LM_PER_LINE_Y) { if (far) IRS_MX(3, true, true, false); else IRS_MX(3, true, false, false); }

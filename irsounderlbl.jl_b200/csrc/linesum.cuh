@@ -205,6 +205,32 @@ __device__ __forceinline__ void far_table_init(FarTable& F) {
     }
 }
 
+// Strip far field.  A line whose shifted centre lies kCtaR or more points from the
+// centre of a 2048-point strip (the 8 warps of a CTA), and whose cutoff covers the
+// whole strip, is a function of the point index analytic well beyond the strip: its
+// far wing is evaluated once per strip at kCtaNodes Chebyshev nodes (by
+// strip_far_kernel, the 8 warps sharing the lines) instead of once per warp, and the
+// degree-15 interpolant is taken to each warp's 8 nodes by the fixed matrix M, where
+// it joins the warp's own far field.  Worst error of one line's term: 1.6e-8 of its
+// largest value on the strip (poles at distance >= 2048 from its centre).  The
+// pedestals of these lines are quadratics summed exactly as for the warp's far lines
+// (compensated, then evaluated at the nodes, which interpolation reproduces).  The
+// lines are those with unshifted centre V in [c - rout, c - rin) or [c + rin, c + rout),
+// rin = kCtaR + margin, rout = cut - 1024 - margin (margin >= the pressure shift + 2
+// points): one index range each side, taken out of every warp's window.
+constexpr int kCtaNodes = 16;
+constexpr float kCtaR = 2048.f;
+constexpr double kCtaCentre = 0.5 * (kMxStrip - 1);  // 1023.5
+constexpr int kStripWords = kMxWarps * kFarNodes;    // per (segment, strip): the warps' node values
+// the nodes relative to the strip centre, 1023.5 cos((2k+1) pi / 32), rounded to FP32
+__device__ __forceinline__ float cta_node_f(int k) {
+    const int a = k < 8 ? k : 15 - k;
+    const float v = a == 0 ? 1.018571594e+03f : a == 1 ? 9.794284058e+02f : a == 2 ? 9.026464233e+02f
+                  : a == 3 ? 7.911762085e+02f : a == 4 ? 6.493015137e+02f : a == 5 ? 4.824745483e+02f
+                  : a == 6 ? 2.971063538e+02f : 1.003205414e+02f;
+    return k < 8 ? v : -v;
+}
+
 // First index i in [0, n) with a[i] >= v (n if none), found by the whole warp: each
 // round probes 32 evenly spaced positions and keeps the interval between the last
 // probe below v and the first one at or above it (32-ary search: 4 dependent loads
@@ -245,6 +271,149 @@ __device__ __forceinline__ void fast_pair(float2 d0s, float2 offs, float2 b2, fl
     acc = __ffma2_rn(a, r, acc);
 }
 
+// ------------------------------------------------------------ strip far field
+// M[w][j][k] = L_k(node j of warp w) for the strip nodes k, at the FP32 nodes the
+// kernel evaluates; one thread per entry, once per line sum
+__global__ void strip_table_kernel(float* __restrict__ M) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kMxWarps * kFarNodes * kCtaNodes) return;
+    const int w = i / (kFarNodes * kCtaNodes), j = (i / kCtaNodes) % kFarNodes, k = i % kCtaNodes;
+    const double x = (double)kMxWarpPts * w + far_node(j) - kCtaCentre;
+    const double xk = (double)cta_node_f(k);
+    double v = 1.0;
+    for (int l = 0; l < kCtaNodes; ++l)
+        if (l != k) v *= (x - (double)cta_node_f(l)) / (xk - (double)cta_node_f(l));
+    M[i] = (float)v;
+}
+
+constexpr int kStripSegs = 16;  // segments whose ranges are searched together
+constexpr int kStripUnroll = 4;  // tiles in flight per warp
+
+// One CTA per (strip, profile-layer).  The segments' index ranges are searched first,
+// spread over the warps (kStripSegs at a time); then per segment each warp takes
+// tiles warp, warp + 8, ... of the ranges' lines, kStripUnroll tiles per round with
+// their loads issued together, evaluates each line at the 16 nodes, and the warps'
+// node sums go through M to far[(segment, strip)][warp][node], the ranges to
+// ranges[(segment, strip)].  Segments with line mixing (when the line sum treats them
+// so) are left out; strips without such lines get empty ranges and zero values.
+template <bool ANY_LM>
+__global__ void __launch_bounds__(kMxThreads) strip_far_kernel(
+    const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const int2* __restrict__ pl_segs,
+    LpOutMixed lp, float cut_g, int n_strips, const float* __restrict__ M, float* __restrict__ far,
+    int4* __restrict__ ranges, unsigned long long* __restrict__ evald) {
+    __shared__ float slot[kMxWarps][kCtaNodes + 4];  // per warp: node sums, pedestal A, B, C
+    __shared__ int sj[kStripSegs][4];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int strip = blockIdx.x, pl = blockIdx.y;
+    const long long cb = (long long)strip * kMxStrip;
+    const double c = (double)cb + kCtaCentre;
+    unsigned long long work = 0;
+    const int2 rng = pl_segs[pl];
+    for (int s0 = rng.x; s0 < rng.x + rng.y; s0 += kStripSegs) {  // block-uniform
+        const int ns = min(kStripSegs, rng.x + rng.y - s0);
+        for (int i = warp; i < 4 * ns; i += kMxWarps) {  // search i: bound i % 4 of segment i / 4
+            const SegDev sg = segs[s0 + i / 4];
+            const double m = sg.margin_g, rin = (double)kCtaR + m, rout = (double)cut_g - 0.5 * kMxStrip - m;
+            int j = 0;
+            if (rout > rin && !(ANY_LM && (sg.flags & 2))) {
+                const int b = i % 4;
+                const double v = b == 0 ? c - rout : b == 1 ? c - rin : b == 2 ? c + rin : c + rout;
+                j = (int)warp_lower_bound(lp.V + sg.off, v, seg_count[s0 + i / 4], lane);
+            }
+            if (lane == 0) sj[i / 4][i % 4] = j;
+        }
+        __syncthreads();
+        for (int si = 0; si < ns; ++si) {
+            const int s = s0 + si;
+            const long long off = segs[s].off;
+            const int jA = sj[si][0], jB = sj[si][1], jC = sj[si][2], jD = sj[si][3];
+            const int nL = jB - jA, n = nL + (jD - jC);
+            float2 acc[kCtaNodes / 2];
+#pragma unroll
+            for (int h = 0; h < kCtaNodes / 2; ++h) acc[h] = make_float2(0.f, 0.f);
+            float PA = 0.f, PAc = 0.f, PB = 0.f, PBc = 0.f, PC = 0.f, PCc = 0.f;
+            for (int t0 = warp * 32; t0 < n; t0 += kStripUnroll * 32 * kMxWarps) {
+                float2 uf[kStripUnroll];
+                float4 a0[kStripUnroll];
+#pragma unroll
+                for (int u = 0; u < kStripUnroll; ++u) {  // the loads first
+                    const int t = t0 + u * 32 * kMxWarps + lane;
+                    if (t < n) {
+                        const long long q = off + (t < nL ? jA + t : jC + (t - nL));
+                        uf[u] = lp.U[q];
+                        a0[u] = lp.p0[q];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kStripUnroll; ++u) {
+                    const int t = t0 + u * 32 * kMxWarps + lane;
+                    float pa = 0.f, pb = 0.f, pc = 0.f;
+                    if (t < n) {
+                        const float uc = (uf[u].x - (float)cb) - (float)kCtaCentre;  // exact: see split_hi_lo
+                        const float ul = uf[u].y;
+                        const float2 b2 = make_float2(a0[u].x, a0[u].x), aa = make_float2(a0[u].y, a0[u].y);
+#pragma unroll
+                        for (int k = 0; k < kCtaNodes; k += 2) {  // pairs of nodes, one reciprocal per pair
+                            const float2 xs = make_float2(cta_node_f(k + 1), cta_node_f(k));  // swapped
+                            const float2 ds = __fadd2_rn(__fadd2_rn(xs, make_float2(-uc, -uc)), make_float2(-ul, -ul));
+                            const float2 es = __ffma2_rn(ds, ds, b2);                       // (e[k+1], e[k])
+                            const float R = rcp_fast(es.x * es.y);
+                            const float2 r = __fmul2_rn(es, make_float2(R, R));             // (1/e[k], 1/e[k+1])
+                            acc[k / 2] = __ffma2_rn(aa, r, acc[k / 2]);
+                        }
+                        // c1 (x - u)^2 + c0 = c1 x^2 - 2 c1 u x + (c1 u^2 + c0), x from the centre
+                        pa = a0[u].z;
+                        pb = a0[u].z * uc;
+                        pc = fmaf(pb, uc, a0[u].w);
+                    }
+                    kahan_add(PA, PAc, pa);
+                    kahan_add(PB, PBc, pb);
+                    kahan_add(PC, PCc, pc);
+                }
+                if (lane == 0) work += (unsigned long long)min(kStripUnroll * 32, n - t0) * kCtaNodes;
+            }
+#pragma unroll
+            for (int h = 0; h < kCtaNodes / 2; ++h) {
+                const float x = warp_sum(acc[h].x), y = warp_sum(acc[h].y);
+                if (lane == 0) {
+                    slot[warp][2 * h] = x;
+                    slot[warp][2 * h + 1] = y;
+                }
+            }
+            const float A = warp_sum(PA - PAc), B = warp_sum(PB - PBc), Cc = warp_sum(PC - PCc);
+            if (lane == 0) {
+                slot[warp][kCtaNodes] = A;
+                slot[warp][kCtaNodes + 1] = B;
+                slot[warp][kCtaNodes + 2] = Cc;
+            }
+            __syncthreads();
+            // the strip's node values (lane k < 16: node k, the warps in a fixed order,
+            // plus the pedestal quadratic), then this warp's 8 nodes through M
+            float fc = 0.f, SA = 0.f, SB = 0.f, SC = 0.f;
+#pragma unroll
+            for (int w = 0; w < kMxWarps; ++w) {
+                if (lane < kCtaNodes) fc += slot[w][lane];
+                SA += slot[w][kCtaNodes];
+                SB += slot[w][kCtaNodes + 1];
+                SC += slot[w][kCtaNodes + 2];
+            }
+            float xk = 0.f;
+#pragma unroll
+            for (int k = 0; k < kCtaNodes; ++k) xk = lane == k ? cta_node_f(k) : xk;
+            fc += fmaf(xk, fmaf(xk, SA, -2.f * SB), SC);
+            const float* Mw = M + ((size_t)warp * kFarNodes + (lane & (kFarNodes - 1))) * kCtaNodes;
+            float g = 0.f;
+#pragma unroll
+            for (int k = 0; k < kCtaNodes; ++k) g = fmaf(__ldg(Mw + k), __shfl_sync(kFull, fc, k), g);
+            const size_t cell = (size_t)s * n_strips + strip;
+            if (lane < kFarNodes) far[cell * kStripWords + warp * kFarNodes + lane] = g;
+            if (threadIdx.x == 0) ranges[cell] = make_int4(jA, jB, jC, jD);
+            __syncthreads();  // the slots are reused by the next segment
+        }
+    }
+    if (evald && lane == 0 && work) atomicAdd(evald, work);
+}
+
 // The optical-depth row of a warp's 256 points.  Each segment's clamped sums are
 // added to it in segment order (the first one stores), so no per-point total stays
 // in registers from one segment to the next.
@@ -258,11 +427,17 @@ __device__ __forceinline__ void out_add(OutRow& o, int q, int lane, float sig) {
     if (i < o.n) o.p[i] = o.wrote ? o.p[i] + sig : sig;
 }
 
+// the next tile start: past the end a of the first range to b, past c to d
+__device__ __forceinline__ int skip_ranges(int t, int a, int b, int c, int d) {
+    t = t == a ? b : t;
+    return t == c ? d : t;
+}
+
 template <int METHOD, bool LM, bool FAR>
 __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, const LpOutMixed& lp, long long wb,
                                              float cut, float cut2, int lane, WarpTile& T, const FarTable& FT,
                                              float xn, OutRow& orow, unsigned long long& work,
-                                             double* __restrict__ prow) {
+                                             double* __restrict__ prow, int4 sx, float gnode) {
     constexpr float kCentre = 0.5f * (kMxWarpPts - 1);
     constexpr float kHalf = 0.5f * kMxWarpPts + 0.5f;
     long long jlo, jhi;
@@ -288,8 +463,15 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
 #pragma unroll
     for (int k = 0; k < kFarNodes; ++k) fnode[k] = 0.f;
     const unsigned lt = (1u << lane) - 1u;
-    for (long long t0 = jlo; t0 < jhi; t0 += 32) {
-        const int nt = (int)min(32LL, jhi - t0);
+    // the window without the strip far field's ranges [sx.x, sx.y) and [sx.z, sx.w):
+    // [ilo, ra), [rb, rc) and [rd, ihi), walked in turn (indices within a segment fit
+    // in int: seg_count is an int)
+    const int ilo = (int)jlo, ihi = (int)jhi;
+    const int ra = min(max(sx.x, ilo), ihi), rb = min(max(sx.y, ilo), ihi);
+    const int rc = min(max(sx.z, ilo), ihi), rd = min(max(sx.w, ilo), ihi);
+    int nt = 0;
+    for (int t0 = skip_ranges(ilo, ra, rb, rc, rd); t0 < ihi; t0 = skip_ranges(t0 + nt, ra, rb, rc, rd)) {
+        nt = min(32, (t0 < ra ? ra : t0 < rc ? rc : ihi) - t0);
         float pa = 0.f, pb = 0.f, pc = 0.f;  // this line's pedestal quadratic (fast and far lines)
         int cls = 0;
         float4 a0, a1, a2;
@@ -579,7 +761,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
         float Fn[kFarNodes], Dn[kFarNodes];
 #pragma unroll
         for (int k = 0; k < kFarNodes; ++k) {
-            Fn[k] = LM ? __shfl_sync(kFull, farS, k) : warp_sum(fnode[k]);
+            Fn[k] = LM ? __shfl_sync(kFull, farS, k) : warp_sum(fnode[k]) + __shfl_sync(kFull, gnode, k);
             Dn[k] = LM ? __shfl_sync(kFull, farDS, k) : 0.f;
         }
         const float A = warp_sum(PA - PAc), B = warp_sum(PB - PBc), Cc = warp_sum(PC - PCc);
@@ -671,7 +853,8 @@ template <int METHOD, bool ANY_LM, bool FAR, bool PERT = false>
 __global__ void __launch_bounds__(kMxThreads, ANY_LM ? 2 : 3) linesum_mixed_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const int2* __restrict__ pl_segs,
     LpOutMixed lp, long long n_nu, float cut_g, float* __restrict__ tau, unsigned long long* __restrict__ evald,
-    double* __restrict__ pert, long long pstride) {
+    double* __restrict__ pert, long long pstride, const float* __restrict__ sfar, const int4* __restrict__ sranges,
+    int n_strips) {
     extern __shared__ __align__(16) unsigned char mx_smem[];
     WarpTile* tiles = reinterpret_cast<WarpTile*>(mx_smem);
     FarTable& ftab = *reinterpret_cast<FarTable*>(mx_smem + sizeof(WarpTile) * kMxWarps);
@@ -695,10 +878,19 @@ __global__ void __launch_bounds__(kMxThreads, ANY_LM ? 2 : 3) linesum_mixed_kern
         if (METHOD == 2)
             warp_segment_pv(sg, cnt, lp, wb, cut_g, cut2, lane, T, orow);
         else if (ANY_LM && (sg.flags & 2))
-            warp_segment<METHOD, true, FAR>(sg, cnt, lp, wb, cut_g, cut2, lane, T, ftab, xn, orow, work, nullptr);
-        else
+            warp_segment<METHOD, true, FAR>(sg, cnt, lp, wb, cut_g, cut2, lane, T, ftab, xn, orow, work, nullptr,
+                                            make_int4(0, 0, 0, 0), 0.f);
+        else {
+            int4 sx = make_int4(0, 0, 0, 0);  // no strip far field: the whole window
+            float gn = 0.f;
+            if (FAR && sfar) {
+                const size_t cell = (size_t)s * n_strips + blockIdx.x;
+                sx = sranges[cell];
+                gn = sfar[cell * kStripWords + warp * kFarNodes + (lane & (kFarNodes - 1))];
+            }
             warp_segment<METHOD, false, FAR>(sg, cnt, lp, wb, cut_g, cut2, lane, T, ftab, xn, orow, work,
-                                             PERT ? pert + (size_t)pl * pstride : nullptr);
+                                             PERT ? pert + (size_t)pl * pstride : nullptr, sx, gn);
+        }
     }
     if (evald && lane == 0 && work) atomicAdd(evald, work);
     if (!orow.wrote) {  // no segment stored: zero optical depth
