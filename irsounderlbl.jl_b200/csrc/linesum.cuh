@@ -290,18 +290,20 @@ constexpr int kStripSegs = 16;  // segments whose ranges are searched together
 constexpr int kStripUnroll = 4;  // tiles in flight per warp
 
 // One CTA per (strip, profile-layer).  The segments' index ranges are searched first,
-// spread over the warps (kStripSegs at a time); then per segment each warp takes
-// tiles warp, warp + 8, ... of the ranges' lines, kStripUnroll tiles per round with
-// their loads issued together, evaluates each line at the 16 nodes, and the warps'
-// node sums go through M to far[(segment, strip)][warp][node], the ranges to
-// ranges[(segment, strip)].  Segments with line mixing (when the line sum treats them
-// so) are left out; strips without such lines get empty ranges and zero values.
+// spread over the warps (kStripSegs segments at a time); then each warp walks every
+// segment's lines without waiting for the others (tiles warp, warp + 8, ... of the two
+// ranges, kStripUnroll tiles per round with their loads issued together; each line at
+// the 16 nodes) and leaves its node and pedestal sums in the segment's slot; after one
+// block barrier each warp combines the slots of every segment (the warps in a fixed
+// order) and takes them through M to its own 8 nodes: far[(segment, strip)][warp][node],
+// and ranges[(segment, strip)].  Segments with line mixing (when the line sum treats
+// them so) are left out; strips without such lines get empty ranges and zero values.
 template <bool ANY_LM>
-__global__ void __launch_bounds__(kMxThreads) strip_far_kernel(
+__global__ void __launch_bounds__(kMxThreads, 3) strip_far_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const int2* __restrict__ pl_segs,
     LpOutMixed lp, float cut_g, int n_strips, const float* __restrict__ M, float* __restrict__ far,
     int4* __restrict__ ranges, unsigned long long* __restrict__ evald) {
-    __shared__ float slot[kMxWarps][kCtaNodes + 4];  // per warp: node sums, pedestal A, B, C
+    __shared__ float slot[kStripSegs][kMxWarps][kCtaNodes + 4];  // node sums, pedestal A, B, C
     __shared__ int sj[kStripSegs][4];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int strip = blockIdx.x, pl = blockIdx.y;
@@ -324,8 +326,7 @@ __global__ void __launch_bounds__(kMxThreads) strip_far_kernel(
         }
         __syncthreads();
         for (int si = 0; si < ns; ++si) {
-            const int s = s0 + si;
-            const long long off = segs[s].off;
+            const long long off = segs[s0 + si].off;
             const int jA = sj[si][0], jB = sj[si][1], jC = sj[si][2], jD = sj[si][3];
             const int nL = jB - jA, n = nL + (jD - jC);
             float2 acc[kCtaNodes / 2];
@@ -372,44 +373,47 @@ __global__ void __launch_bounds__(kMxThreads) strip_far_kernel(
                 }
                 if (lane == 0) work += (unsigned long long)min(kStripUnroll * 32, n - t0) * kCtaNodes;
             }
+            float* sl = slot[si][warp];
 #pragma unroll
             for (int h = 0; h < kCtaNodes / 2; ++h) {
                 const float x = warp_sum(acc[h].x), y = warp_sum(acc[h].y);
                 if (lane == 0) {
-                    slot[warp][2 * h] = x;
-                    slot[warp][2 * h + 1] = y;
+                    sl[2 * h] = x;
+                    sl[2 * h + 1] = y;
                 }
             }
             const float A = warp_sum(PA - PAc), B = warp_sum(PB - PBc), Cc = warp_sum(PC - PCc);
             if (lane == 0) {
-                slot[warp][kCtaNodes] = A;
-                slot[warp][kCtaNodes + 1] = B;
-                slot[warp][kCtaNodes + 2] = Cc;
+                sl[kCtaNodes] = A;
+                sl[kCtaNodes + 1] = B;
+                sl[kCtaNodes + 2] = Cc;
             }
-            __syncthreads();
-            // the strip's node values (lane k < 16: node k, the warps in a fixed order,
-            // plus the pedestal quadratic), then this warp's 8 nodes through M
+        }
+        __syncthreads();
+        // per segment: the strip's node values (lane k < 16: node k, the warps in a fixed
+        // order, plus the pedestal quadratic), then this warp's 8 nodes through M
+        const float* Mw = M + ((size_t)warp * kFarNodes + (lane & (kFarNodes - 1))) * kCtaNodes;
+        float xk = 0.f;
+#pragma unroll
+        for (int k = 0; k < kCtaNodes; ++k) xk = lane == k ? cta_node_f(k) : xk;
+        for (int si = 0; si < ns; ++si) {
             float fc = 0.f, SA = 0.f, SB = 0.f, SC = 0.f;
 #pragma unroll
             for (int w = 0; w < kMxWarps; ++w) {
-                if (lane < kCtaNodes) fc += slot[w][lane];
-                SA += slot[w][kCtaNodes];
-                SB += slot[w][kCtaNodes + 1];
-                SC += slot[w][kCtaNodes + 2];
+                if (lane < kCtaNodes) fc += slot[si][w][lane];
+                SA += slot[si][w][kCtaNodes];
+                SB += slot[si][w][kCtaNodes + 1];
+                SC += slot[si][w][kCtaNodes + 2];
             }
-            float xk = 0.f;
-#pragma unroll
-            for (int k = 0; k < kCtaNodes; ++k) xk = lane == k ? cta_node_f(k) : xk;
             fc += fmaf(xk, fmaf(xk, SA, -2.f * SB), SC);
-            const float* Mw = M + ((size_t)warp * kFarNodes + (lane & (kFarNodes - 1))) * kCtaNodes;
             float g = 0.f;
 #pragma unroll
             for (int k = 0; k < kCtaNodes; ++k) g = fmaf(__ldg(Mw + k), __shfl_sync(kFull, fc, k), g);
-            const size_t cell = (size_t)s * n_strips + strip;
+            const size_t cell = (size_t)(s0 + si) * n_strips + strip;
             if (lane < kFarNodes) far[cell * kStripWords + warp * kFarNodes + lane] = g;
-            if (threadIdx.x == 0) ranges[cell] = make_int4(jA, jB, jC, jD);
-            __syncthreads();  // the slots are reused by the next segment
+            if (threadIdx.x == 0) ranges[cell] = make_int4(sj[si][0], sj[si][1], sj[si][2], sj[si][3]);
         }
+        if (s0 + kStripSegs < rng.x + rng.y) __syncthreads();  // slots and ranges reused by the next batch
     }
     if (evald && lane == 0 && work) atomicAdd(evald, work);
 }
