@@ -274,8 +274,8 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
             strip_table_kernel<<<(nM + 255) / 256, 256, 0, st>>>(d_M);
             check_launch(ctx);
             dim3 g3(n_strips, npl);
-            if (anylm) strip_far_kernel<true><<<g3, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, cut_g, n_strips, d_M, d_sfar, d_srng, d_eval);
-            else strip_far_kernel<false><<<g3, kMxThreads, 0, st>>>(d_segs, d_count, d_pl, om, cut_g, n_strips, d_M, d_sfar, d_srng, d_eval);
+            if (anylm) strip_far_kernel<true><<<g3, kStripThreads, 0, st>>>(d_segs, d_count, d_pl, om, cut_g, n_strips, d_M, d_sfar, d_srng, d_eval);
+            else strip_far_kernel<false><<<g3, kStripThreads, 0, st>>>(d_segs, d_count, d_pl, om, cut_g, n_strips, d_M, d_sfar, d_srng, d_eval);
             check_launch(ctx);
         }
 #define IRS_MX(M, LMX, F, P) do { \

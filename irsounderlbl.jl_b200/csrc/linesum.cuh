@@ -97,22 +97,22 @@ __global__ void __launch_bounds__(256) linesum_f64_kernel(
 }
 
 // ----------------------------------------------------------------- mixed
-// Each warp owns 256 consecutive grid points (8 per lane, point = 32 q + lane)
+// Each warp owns 128 consecutive grid points (4 per lane, point = 32 q + lane)
 // and walks its own window of lines in tiles of 32 staged in warp-private shared
 // memory (no block-wide barriers).  The staging lane of each line precomputes,
 // once per (warp, line): the FP32 position split u = uh + ul relative to the
 // warp, the class of the line for this warp (outside the cutoff / fast / slow),
 // and, for fast lines, the line's pedestal as a quadratic in the point index, so
 // the 32 pedestals of a tile reduce to three numbers.
-//   fast: inside the cutoff and in the Lorentz far wing (|x| > x_far) for all 256
+//   fast: inside the cutoff and in the Lorentz far wing (|x| > x_far) for all 128
 //         points: d by one FADD from a per-line origin, one MUFU reciprocal per
 //         two pairs, one FMA into the tile sum;
 //   slow: Faddeeva core or cutoff edge: per-pair tests.
 // Tile sums go into a Kahan-compensated FP32 accumulator per point.
-constexpr int kMxWarps = 8;
+constexpr int kMxWarps = 16;
 constexpr int kMxThreads = 32 * kMxWarps;
-constexpr int kMxQ = 8;                               // points per lane
-constexpr int kMxWarpPts = 32 * kMxQ;                 // 256 points per warp
+constexpr int kMxQ = 4;                               // points per lane
+constexpr int kMxWarpPts = 32 * kMxQ;                 // 128 points per warp
 constexpr int kMxStrip = kMxWarps * kMxWarpPts;       // 2048 points per CTA
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -151,7 +151,7 @@ __device__ __forceinline__ float warp_sum(float v) {
 // those rows idle; instead each tile evaluates the inner points of all its slow lines
 // lane-parallel into cw (up to kCoreBuf per tile; lines beyond it keep the per-point
 // evaluation) and the per-point loop reads them back.
-constexpr int kCoreBuf = 256;
+constexpr int kCoreBuf = 128;
 
 struct WarpTile {
     float4 fu[32];  // fast lines: uh, ul, b2, a               (PV: uh, ul, -, class)
@@ -172,27 +172,29 @@ struct WarpTile {
 
 
 // Far field.  A fast line whose centre lies kFarDist or more points from the centre
-// of a warp's 256-point block contributes a function of the point index that is
-// analytic well beyond the block (its poles sit at complex distance >= kFarDist - 128
+// of a warp's 128-point block contributes a function of the point index that is
+// analytic well beyond the block (its poles sit at complex distance >= kFarDist - 64
 // from it), so its far-wing sum over all such lines is evaluated at the 8 Chebyshev
-// nodes of the block and interpolated to the 256 points with the fixed Lagrange
-// weights L_k(i): 8 pairs per line instead of 256.  The interpolation error of one
+// nodes of the block and interpolated to the 128 points with the fixed Lagrange
+// weights L_k(i): 8 pairs per line instead of 128.  The interpolation error of one
 // line's term is at most 1.6e-7 of its largest value on the block (degree 7, nodes
-// on [0, 255], distance 640); pedestals stay exact (quadratic sums), as do the
-// near lines, the Faddeeva cores and the cutoff edges.
-constexpr float kFarDist = 640.f;
+// on [0, 127], distance 320 = 5 half-widths); pedestals stay exact (quadratic sums),
+// as do the near lines, the Faddeeva cores and the cutoff edges.
+constexpr float kFarDist = 2.5f * kMxWarpPts;
 constexpr int kFarNodes = 8;
 struct FarTable {
-    float L[kFarNodes][kMxWarpPts];  // L_k(i), i = 0..255
+    float L[kFarNodes][kMxWarpPts];  // L_k(i), i = 0..127
 };
 __device__ __forceinline__ double far_node(int k) {
-    return 127.5 + 127.5 * cos((2 * k + 1) * 3.14159265358979323846 / (2 * kFarNodes));
+    constexpr double h = 0.5 * (kMxWarpPts - 1);
+    return h + h * cos((2 * k + 1) * 3.14159265358979323846 / (2 * kFarNodes));
 }
 // the same nodes rounded to FP32, as literals for fully unrolled node loops
 __device__ __forceinline__ float far_node_f(int k) {
-    return k == 0 ? 2.525501251e+02f : k == 1 ? 2.335123749e+02f : k == 2 ? 1.983352051e+02f
-         : k == 3 ? 1.523740234e+02f : k == 4 ? 1.026259842e+02f : k == 5 ? 5.666479492e+01f
-         : k == 6 ? 2.148762512e+01f : 2.449876785e+00f;
+    static_assert(kMxWarpPts == 128, "far_node_f holds the nodes of a 128-point block");
+    return k == 0 ? 1.257798691e+02f : k == 1 ? 1.162983170e+02f : k == 2 ? 9.877870941e+01f
+         : k == 3 ? 7.588823700e+01f : k == 4 ? 5.111176300e+01f : k == 5 ? 2.822129059e+01f
+         : k == 6 ? 1.070167923e+01f : 1.220134735e+00f;
 }
 // whole block, before any early exit
 __device__ __forceinline__ void far_table_init(FarTable& F) {
@@ -251,7 +253,7 @@ __device__ __forceinline__ long long warp_lower_bound(const double* a, double v,
     return lo + __popc(below);
 }
 
-// window [jlo, jhi) of the lines that can reach this warp's points [wb, wb + 255]
+// window [jlo, jhi) of the lines that can reach this warp's points [wb, wb + kMxWarpPts - 1]
 __device__ __forceinline__ void warp_window(const LpOutMixed& lp, const SegDev& sg, long long cnt,
                                             long long wb, float cut, int lane, long long& jlo, long long& jhi) {
     const double* V = lp.V + sg.off;
@@ -288,6 +290,8 @@ __global__ void strip_table_kernel(float* __restrict__ M) {
 
 constexpr int kStripSegs = 16;  // segments whose ranges are searched together
 constexpr int kStripUnroll = 4;  // tiles in flight per warp
+constexpr int kStripWarps = 8;   // warps of strip_far_kernel (each serves kMxWarps / 8 line-sum warps)
+constexpr int kStripThreads = 32 * kStripWarps;
 
 // One CTA per (strip, profile-layer).  The segments' index ranges are searched first,
 // spread over the warps (kStripSegs segments at a time); then each warp walks every
@@ -299,11 +303,11 @@ constexpr int kStripUnroll = 4;  // tiles in flight per warp
 // and ranges[(segment, strip)].  Segments with line mixing (when the line sum treats
 // them so) are left out; strips without such lines get empty ranges and zero values.
 template <bool ANY_LM>
-__global__ void __launch_bounds__(kMxThreads, 3) strip_far_kernel(
+__global__ void __launch_bounds__(kStripThreads, 3) strip_far_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const int2* __restrict__ pl_segs,
     LpOutMixed lp, float cut_g, int n_strips, const float* __restrict__ M, float* __restrict__ far,
     int4* __restrict__ ranges, unsigned long long* __restrict__ evald) {
-    __shared__ float slot[kStripSegs][kMxWarps][kCtaNodes + 4];  // node sums, pedestal A, B, C
+    __shared__ float slot[kStripSegs][kStripWarps][kCtaNodes + 4];  // node sums, pedestal A, B, C
     __shared__ int sj[kStripSegs][4];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int strip = blockIdx.x, pl = blockIdx.y;
@@ -313,7 +317,7 @@ __global__ void __launch_bounds__(kMxThreads, 3) strip_far_kernel(
     const int2 rng = pl_segs[pl];
     for (int s0 = rng.x; s0 < rng.x + rng.y; s0 += kStripSegs) {  // block-uniform
         const int ns = min(kStripSegs, rng.x + rng.y - s0);
-        for (int i = warp; i < 4 * ns; i += kMxWarps) {  // search i: bound i % 4 of segment i / 4
+        for (int i = warp; i < 4 * ns; i += kStripWarps) {  // search i: bound i % 4 of segment i / 4
             const SegDev sg = segs[s0 + i / 4];
             const double m = sg.margin_g, rin = (double)kCtaR + m, rout = (double)cut_g - 0.5 * kMxStrip - m;
             int j = 0;
@@ -333,12 +337,12 @@ __global__ void __launch_bounds__(kMxThreads, 3) strip_far_kernel(
 #pragma unroll
             for (int h = 0; h < kCtaNodes / 2; ++h) acc[h] = make_float2(0.f, 0.f);
             float PA = 0.f, PAc = 0.f, PB = 0.f, PBc = 0.f, PC = 0.f, PCc = 0.f;
-            for (int t0 = warp * 32; t0 < n; t0 += kStripUnroll * 32 * kMxWarps) {
+            for (int t0 = warp * 32; t0 < n; t0 += kStripUnroll * 32 * kStripWarps) {
                 float2 uf[kStripUnroll];
                 float4 a0[kStripUnroll];
 #pragma unroll
                 for (int u = 0; u < kStripUnroll; ++u) {  // the loads first
-                    const int t = t0 + u * 32 * kMxWarps + lane;
+                    const int t = t0 + u * 32 * kStripWarps + lane;
                     if (t < n) {
                         const long long q = off + (t < nL ? jA + t : jC + (t - nL));
                         uf[u] = lp.U[q];
@@ -347,7 +351,7 @@ __global__ void __launch_bounds__(kMxThreads, 3) strip_far_kernel(
                 }
 #pragma unroll
                 for (int u = 0; u < kStripUnroll; ++u) {
-                    const int t = t0 + u * 32 * kMxWarps + lane;
+                    const int t = t0 + u * 32 * kStripWarps + lane;
                     float pa = 0.f, pb = 0.f, pc = 0.f;
                     if (t < n) {
                         const float uc = (uf[u].x - (float)cb) - (float)kCtaCentre;  // exact: see split_hi_lo
@@ -391,26 +395,29 @@ __global__ void __launch_bounds__(kMxThreads, 3) strip_far_kernel(
         }
         __syncthreads();
         // per segment: the strip's node values (lane k < 16: node k, the warps in a fixed
-        // order, plus the pedestal quadratic), then this warp's 8 nodes through M
-        const float* Mw = M + ((size_t)warp * kFarNodes + (lane & (kFarNodes - 1))) * kCtaNodes;
+        // order, plus the pedestal quadratic), then through M to the 8 nodes of the
+        // line-sum warps this warp serves
         float xk = 0.f;
 #pragma unroll
         for (int k = 0; k < kCtaNodes; ++k) xk = lane == k ? cta_node_f(k) : xk;
         for (int si = 0; si < ns; ++si) {
             float fc = 0.f, SA = 0.f, SB = 0.f, SC = 0.f;
 #pragma unroll
-            for (int w = 0; w < kMxWarps; ++w) {
+            for (int w = 0; w < kStripWarps; ++w) {
                 if (lane < kCtaNodes) fc += slot[si][w][lane];
                 SA += slot[si][w][kCtaNodes];
                 SB += slot[si][w][kCtaNodes + 1];
                 SC += slot[si][w][kCtaNodes + 2];
             }
             fc += fmaf(xk, fmaf(xk, SA, -2.f * SB), SC);
-            float g = 0.f;
-#pragma unroll
-            for (int k = 0; k < kCtaNodes; ++k) g = fmaf(__ldg(Mw + k), __shfl_sync(kFull, fc, k), g);
             const size_t cell = (size_t)(s0 + si) * n_strips + strip;
-            if (lane < kFarNodes) far[cell * kStripWords + warp * kFarNodes + lane] = g;
+            for (int mw = warp; mw < kMxWarps; mw += kStripWarps) {
+                const float* Mw = M + ((size_t)mw * kFarNodes + (lane & (kFarNodes - 1))) * kCtaNodes;
+                float g = 0.f;
+#pragma unroll
+                for (int k = 0; k < kCtaNodes; ++k) g = fmaf(__ldg(Mw + k), __shfl_sync(kFull, fc, k), g);
+                if (lane < kFarNodes) far[cell * kStripWords + mw * kFarNodes + lane] = g;
+            }
             if (threadIdx.x == 0) ranges[cell] = make_int4(sj[si][0], sj[si][1], sj[si][2], sj[si][3]);
         }
         if (s0 + kStripSegs < rng.x + rng.y) __syncthreads();  // slots and ranges reused by the next batch
@@ -418,7 +425,7 @@ __global__ void __launch_bounds__(kMxThreads, 3) strip_far_kernel(
     if (evald && lane == 0 && work) atomicAdd(evald, work);
 }
 
-// The optical-depth row of a warp's 256 points.  Each segment's clamped sums are
+// The optical-depth row of a warp's 128 points.  Each segment's clamped sums are
 // added to it in segment order (the first one stores), so no per-point total stays
 // in registers from one segment to the next.
 struct OutRow {
@@ -854,7 +861,7 @@ __device__ __forceinline__ void warp_segment_pv(const SegDev& sg, long long cnt,
 constexpr size_t kMxSmem = sizeof(WarpTile) * kMxWarps + sizeof(FarTable);
 
 template <int METHOD, bool ANY_LM, bool FAR, bool PERT = false>
-__global__ void __launch_bounds__(kMxThreads, ANY_LM ? 2 : 3) linesum_mixed_kernel(
+__global__ void __launch_bounds__(kMxThreads, ANY_LM ? 1 : 2) linesum_mixed_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const int2* __restrict__ pl_segs,
     LpOutMixed lp, long long n_nu, float cut_g, float* __restrict__ tau, unsigned long long* __restrict__ evald,
     double* __restrict__ pert, long long pstride, const float* __restrict__ sfar, const int4* __restrict__ sranges,
