@@ -544,7 +544,8 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
         // FullFaddeeva slow lines: the inner points of the block, [plo, plo + nin - 1],
         // and their offsets in cw by a warp scan; cfit = the points that fit (warp-uniform)
         int nin = 0, plo = 1, coff = 0, cfit = 0;
-        if (METHOD == 3) {
+        const unsigned sm = __ballot_sync(kFull, cls == 2);
+        if (METHOD == 3 && sm) {  // (warp-uniform)
             if (cls == 2 && a1.w < 15.f) {
                 const float hw = (15.f - a1.w) / a1.z + 1.f;
                 const float c = uh + ul;
@@ -565,7 +566,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
             cfit = ov ? __shfl_sync(kFull, coff, __ffs(ov) - 1) : __shfl_sync(kFull, inc, 31);
             if (inc > kCoreBuf) nin = 0;  // beyond the buffer: evaluated per point
         }
-        const unsigned fm = __ballot_sync(kFull, cls == 1), sm = __ballot_sync(kFull, cls == 2);
+        const unsigned fm = __ballot_sync(kFull, cls == 1);
         const unsigned xm = (FAR && LM) ? __ballot_sync(kFull, cls == 3) : 0u;  // staged far lines
         const unsigned em = FAR ? __ballot_sync(kFull, cls == 4) : 0u;
         const unsigned mm = FAR ? __ballot_sync(kFull, cls == 5) : 0u;
