@@ -260,7 +260,7 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
         unsigned long long* d_eval = d_pairs + 2;
         const bool far = o.precision == IRS_MIXED;
         const bool anylm = o.line_mixing == IRS_LM_PER_LINE_Y;
-        // strip far field (pre-pass): 272 bytes per (segment, strip), skipped past 2 GiB
+        // strip far field (pre-pass): 528 bytes per (segment, strip), skipped past 2 GiB
         float* d_sfar = nullptr;
         int4* d_srng = nullptr;
         const int n_strips = (int)g2.x;
