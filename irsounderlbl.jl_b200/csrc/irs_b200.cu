@@ -232,16 +232,20 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
         o64.nu0 = base; o64.f = base + S; o64.y = base + 2 * S; o64.Sn = base + 3 * S;
         o64.Hc = base + 4 * S; o64.YSn = base + 5 * S;
         lp_write_kernel<0><<<g1, kLpThreads, 0, st>>>(d_segs, d_lists, tp, cfg, d_keep, d_chunk, n_chunks,
-                                                      d_count, o64, om, d_pairs);
-    } else {
+                                                      d_count, o64, om, d_pairs, nullptr);
+    }
+    unsigned* d_reach = nullptr;  // per segment: the largest Faddeeva-core half-width, grid units
+    if (mixed) {
         char* base = (char*)workspace(ctx, "lpmx", S * (8 + 8 + 16 + 16 + 16));
         om.V = (double*)base;
         om.U = (float2*)(base + S * 8);
         om.p0 = (float4*)(base + S * 16);
         om.p1 = (float4*)(base + S * 32);
         om.p2 = (float4*)(base + S * 48);
+        d_reach = (unsigned*)workspace(ctx, "core_reach", sizeof(unsigned) * std::max(nseg, 1));
+        IRS_CUDA(cudaMemsetAsync(d_reach, 0, sizeof(unsigned) * std::max(nseg, 1), st));
         lp_write_kernel<1><<<g1, kLpThreads, 0, st>>>(d_segs, d_lists, tp, cfg, d_keep, d_chunk, n_chunks,
-                                                      d_count, o64, om, d_pairs);
+                                                      d_count, o64, om, d_pairs, d_reach);
     }
     check_launch(ctx);
     IRS_CUDA(cudaEventRecord(ctx->ev[ev_mid], st));
@@ -274,8 +278,8 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
             strip_table_kernel<<<(nM + 255) / 256, 256, 0, st>>>(d_M);
             check_launch(ctx);
             dim3 g3(n_strips, npl);
-            if (anylm) strip_far_kernel<true><<<g3, kStripThreads, 0, st>>>(d_segs, d_count, d_pl, om, cut_g, n_strips, d_M, d_sfar, d_srng, d_eval);
-            else strip_far_kernel<false><<<g3, kStripThreads, 0, st>>>(d_segs, d_count, d_pl, om, cut_g, n_strips, d_M, d_sfar, d_srng, d_eval);
+            if (anylm) strip_far_kernel<true><<<g3, kStripThreads, 0, st>>>(d_segs, d_count, d_reach, d_pl, om, cut_g, n_strips, d_M, d_sfar, d_srng, d_eval);
+            else strip_far_kernel<false><<<g3, kStripThreads, 0, st>>>(d_segs, d_count, d_reach, d_pl, om, cut_g, n_strips, d_M, d_sfar, d_srng, d_eval);
             check_launch(ctx);
         }
 #define IRS_MX(M, LMX, F, P) do { \

@@ -149,7 +149,8 @@ template <int PREC>
 __global__ void __launch_bounds__(kLpThreads) lp_write_kernel(
     const SegDev* __restrict__ segs, const ListDev* __restrict__ lists, TipsDev tp, LpConfig cfg,
     const unsigned char* __restrict__ keep, const int* __restrict__ chunk_count, int n_chunks_max,
-    int* __restrict__ seg_count, LpOutF64 o64, LpOutMixed om, unsigned long long* __restrict__ pair_counts) {
+    int* __restrict__ seg_count, LpOutF64 o64, LpOutMixed om, unsigned long long* __restrict__ pair_counts,
+    unsigned* __restrict__ seg_core_reach) {
     const SegDev sg = segs[blockIdx.y];
     const ListDev L = lists[sg.list];
     const long long base = (long long)blockIdx.x * kLpChunk;
@@ -157,6 +158,7 @@ __global__ void __launch_bounds__(kLpThreads) lp_write_kernel(
     __shared__ int s_warp[kLpThreads / 32];
     __shared__ long long s_off;
     __shared__ unsigned long long s_pairs[2];
+    __shared__ unsigned s_reach;  // largest core reach of the chunk's lines (FP32 bits, >= 0)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x < 32) {  // offset of this chunk = kept lines of the earlier chunks
         long long s = 0;
@@ -165,6 +167,7 @@ __global__ void __launch_bounds__(kLpThreads) lp_write_kernel(
         if (lane == 0) {
             s_off = s;
             s_pairs[0] = s_pairs[1] = 0;
+            s_reach = 0u;
             if (blockIdx.x == gridDim.x - 1 || base + kLpChunk >= L.n) {
                 // last chunk of the segment publishes the segment's kept count
                 const long long last = (L.n - 1) / kLpChunk;
@@ -176,6 +179,7 @@ __global__ void __launch_bounds__(kLpThreads) lp_write_kernel(
     __syncthreads();
     long long run = s_off;
     unsigned long long pairs = 0, core = 0;
+    float reach = 0.f;  // x_far / fx in grid units: the Faddeeva core's half-width
     const double isp = kInvSqrtPi;
     for (int r = 0; r < kLpPerThread; ++r) {
         const long long j = base + r * kLpThreads + threadIdx.x;
@@ -260,6 +264,7 @@ __global__ void __launch_bounds__(kLpThreads) lp_write_kernel(
                     // denominators stay normal in FP32 even at p -> 0
                     const double b2 = fmax((y / fx) * (y / fx), 1e-12);
                     const double dfar = cfg.x_far / fx;
+                    reach = fmaxf(reach, (float)fmin(dfar, 1.0e30));
                     const double c1 = P * (dg / c) * (dg / c);
                     om.p0[slot] = make_float4((float)b2, (float)(An * y * isp / (fx * fx)), (float)c1,
                                               (float)(-2.0 * P));
@@ -275,15 +280,18 @@ __global__ void __launch_bounds__(kLpThreads) lp_write_kernel(
         pairs += __shfl_down_sync(0xffffffffu, pairs, d);
         core += __shfl_down_sync(0xffffffffu, core, d);
     }
+    for (int d = 16; d; d >>= 1) reach = fmaxf(reach, __shfl_xor_sync(0xffffffffu, reach, d));
     if (lane == 0) {
         atomicAdd(&s_pairs[0], pairs);
         atomicAdd(&s_pairs[1], core);
+        atomicMax(&s_reach, __float_as_uint(reach));  // non-negative floats order as their bits
     }
     __syncthreads();
     if (threadIdx.x == 0 && pair_counts) {
         atomicAdd(&pair_counts[0], s_pairs[0]);
         atomicAdd(&pair_counts[1], s_pairs[1]);
     }
+    if (threadIdx.x == 0 && seg_core_reach) atomicMax(&seg_core_reach[blockIdx.y], s_reach);
 }
 
 }  // namespace irs

@@ -218,8 +218,10 @@ __device__ __forceinline__ void far_table_init(FarTable& F) {
 // pedestals of these lines are quadratics summed exactly as for the warp's far lines
 // (compensated, then evaluated at the nodes, which interpolation reproduces).  The
 // lines are those with unshifted centre V in [c - rout, c - rin) or [c + rin, c + rout),
-// rin = kCtaR + margin, rout = cut - 1024 - margin (margin >= the pressure shift + 2
-// points): one index range each side, taken out of every warp's window.
+// rin = max(kCtaR, core reach + 1025) + margin, rout = cut - 1024 - margin (margin >= the
+// pressure shift + 2 points; core reach = the segment's largest x_far / fx, so no line
+// of the ranges has its Faddeeva core on the strip): one index range each side, taken
+// out of every warp's window.
 constexpr int kCtaNodes = 16;
 constexpr float kCtaR = 2048.f;
 constexpr double kCtaCentre = 0.5 * (kMxStrip - 1);  // 1023.5
@@ -304,9 +306,9 @@ constexpr int kStripThreads = 32 * kStripWarps;
 // them so) are left out; strips without such lines get empty ranges and zero values.
 template <bool ANY_LM>
 __global__ void __launch_bounds__(kStripThreads, 3) strip_far_kernel(
-    const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const int2* __restrict__ pl_segs,
-    LpOutMixed lp, float cut_g, int n_strips, const float* __restrict__ M, float* __restrict__ far,
-    int4* __restrict__ ranges, unsigned long long* __restrict__ evald) {
+    const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const unsigned* __restrict__ core_reach,
+    const int2* __restrict__ pl_segs, LpOutMixed lp, float cut_g, int n_strips, const float* __restrict__ M,
+    float* __restrict__ far, int4* __restrict__ ranges, unsigned long long* __restrict__ evald) {
     __shared__ float slot[kStripSegs][kStripWarps][kCtaNodes + 4];  // node sums, pedestal A, B, C
     __shared__ int sj[kStripSegs][4];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -319,7 +321,11 @@ __global__ void __launch_bounds__(kStripThreads, 3) strip_far_kernel(
         const int ns = min(kStripSegs, rng.x + rng.y - s0);
         for (int i = warp; i < 4 * ns; i += kStripWarps) {  // search i: bound i % 4 of segment i / 4
             const SegDev sg = segs[s0 + i / 4];
-            const double m = sg.margin_g, rin = (double)kCtaR + m, rout = (double)cut_g - 0.5 * kMxStrip - m;
+            // rin: the interpolation distance, and every line's Faddeeva core (|x| <= x_far)
+            // off the strip
+            const double reach = (double)__uint_as_float(core_reach[s0 + i / 4]);
+            const double m = sg.margin_g, rin = fmax((double)kCtaR, reach + 0.5 * kMxStrip + 1.0) + m;
+            const double rout = (double)cut_g - 0.5 * kMxStrip - m;
             int j = 0;
             if (rout > rin && !(ANY_LM && (sg.flags & 2))) {
                 const int b = i % 4;
