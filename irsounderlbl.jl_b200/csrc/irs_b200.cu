@@ -700,18 +700,37 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
             LpConfig cfg;
             cfg.cutoff = o.cutoff; cfg.x_far = o.x_far; cfg.dptmn = 0.0; cfg.grid0 = ig.g.at(0); cfg.u_gran = 1.0 / 16.0;
             cfg.dnu_g = ig.dnu_hi; cfg.method = o.method; cfg.n_nu = n_nu;
-            jg_params_kernel<<<dim3((unsigned)((max_list + 255) / 256), nseg), 256, 0, st>>>(d_segs, d_lists, tips_dev(ctx), cfg, go);
+            unsigned* d_reach = (unsigned*)workspace(ctx, "jg_reach", sizeof(unsigned) * nseg);
+            IRS_CUDA(cudaMemsetAsync(d_reach, 0, sizeof(unsigned) * nseg, st));
+            jg_params_kernel<<<dim3((unsigned)((max_list + 255) / 256), nseg), 256, 0, st>>>(d_segs, d_lists, tips_dev(ctx), cfg, go, d_reach);
             check_launch(ctx);
             const dim3 g2((unsigned)((n_nu + kJgStrip - 1) / kJgStrip), np * L);
             const float cut_g = (float)(o.cutoff / ig.dnu_hi);
             const bool lm = o.line_mixing == 1;
+            // strip far field (pre-pass): 1808 bytes per (segment, strip), skipped past 2 GiB
+            float* d_sfar = nullptr;
+            int4* d_srng = nullptr;
+            const int n_strips = (int)g2.x;
+            const size_t cells = (size_t)nseg * n_strips;
+            if (o.method == 3 && cells * (kJgStripWords * sizeof(float) + sizeof(int4)) <= ((size_t)2 << 30)) {
+                char* b = (char*)workspace(ctx, "jg_strip", cells * (kJgStripWords * sizeof(float) + sizeof(int4)));
+                d_sfar = (float*)b;
+                d_srng = (int4*)(b + cells * kJgStripWords * sizeof(float));
+                constexpr int nM = kJgWarps * kJgFarNodes * kJgStripNodes;
+                float* d_M = (float*)workspace(ctx, "jg_strip_M", nM * sizeof(float));
+                jg_strip_table_kernel<<<(nM + 255) / 256, 256, 0, st>>>(d_M);
+                check_launch(ctx);
+                if (lm) jg_strip_kernel<true><<<g2, kJgWarps * 32, 0, st>>>(d_segs, d_sn, d_reach, d_pl, go, cut_g, n_strips, d_M, d_sfar, d_srng);
+                else jg_strip_kernel<false><<<g2, kJgWarps * 32, 0, st>>>(d_segs, d_sn, d_reach, d_pl, go, cut_g, n_strips, d_M, d_sfar, d_srng);
+                check_launch(ctx);
+            }
 #define IRS_JG(NO)                                                                                          \
     do {                                                                                                    \
         const size_t sm = jg_smem_bytes(NO);                                                                \
         IRS_CUDA(cudaFuncSetAttribute(jg_linesum_kernel<true, NO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
         IRS_CUDA(cudaFuncSetAttribute(jg_linesum_kernel<false, NO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
-        if (lm) jg_linesum_kernel<true, NO><<<g2, kJgWarps * 32, sm, st>>>(d_segs, d_sn, d_sw, d_pl, go, n_nu, cut_g, d_out, d_pert, pstride); \
-        else jg_linesum_kernel<false, NO><<<g2, kJgWarps * 32, sm, st>>>(d_segs, d_sn, d_sw, d_pl, go, n_nu, cut_g, d_out, d_pert, pstride); \
+        if (lm) jg_linesum_kernel<true, NO><<<g2, kJgWarps * 32, sm, st>>>(d_segs, d_sn, d_sw, d_pl, go, n_nu, cut_g, d_out, d_pert, pstride, d_sfar, d_srng, n_strips); \
+        else jg_linesum_kernel<false, NO><<<g2, kJgWarps * 32, sm, st>>>(d_segs, d_sn, d_sw, d_pl, go, n_nu, cut_g, d_out, d_pert, pstride, d_sfar, d_srng, n_strips); \
     } while (0)
             switch (n_out) {
                 case 3: IRS_JG(3); break;

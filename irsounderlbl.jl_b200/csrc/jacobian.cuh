@@ -58,7 +58,7 @@ __device__ __forceinline__ double tips_slope(const TipsDev& t, int idx, double T
 // vmr_jacobian.jl:188-201).  cross_section_jacobian.jl:198-236.
 __global__ void __launch_bounds__(256) jg_params_kernel(const SegDev* __restrict__ segs,
                                                         const ListDev* __restrict__ lists, TipsDev tp,
-                                                        LpConfig cfg, JgOut o) {
+                                                        LpConfig cfg, JgOut o, unsigned* __restrict__ core_reach) {
     const SegDev sg = segs[blockIdx.y];
     const ListDev L = lists[sg.list];
     const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -118,6 +118,11 @@ __global__ void __launch_bounds__(256) jg_params_kernel(const SegDev* __restrict
     o.q2[slot] = make_float4((float)dyp, (float)(dn0p / dg), (float)dHcp, (float)fmin(cfg.x_far / (f * dg), 1.0e30));
     o.q3[slot] = make_float4((float)dyv, (float)(dn0v / dg), (float)dHcv, 0.f);
     o.q4[slot] = make_float4((float)Yw, (float)YwT, (float)Ywp, 0.f);
+    if (core_reach) {  // the segment's largest core half-width (non-negative floats order as their bits)
+        const unsigned mask = __activemask();
+        const unsigned r = __reduce_max_sync(mask, __float_as_uint((float)fmin(cfg.x_far / (f * dg), 1.0e30)));
+        if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) atomicMax(&core_reach[blockIdx.y], r);
+    }
 }
 
 // ------------------------------------------------------------------ line sum
@@ -199,6 +204,56 @@ struct JgTile {
     float4 q0[32], q1[32], q2[32], q3[32], q4[32];  // slow: per-line primitives
 };
 
+// The far-wing coefficients of one line (the JgTile fast-line layout; fu = (-, -, b2,
+// a_s)) and its pedestal scales P[o] (value, d/dT, d/dp, d/dv) of -P pf,
+// pf = 2 - (i - u)^2 / c^2 (pf also moves with the centre for d/dp and d/dv).
+template <bool LM>
+__device__ __forceinline__ void jg_wing_coeffs(const float4& a0, const float4& a1, const float4& a2,
+                                               const float4& a3, const float4& a4, float4& fu, float4& fT,
+                                               float4& fp, float4& fL0, float4& fL1, float P[4]) {
+    constexpr float k = (float)kInvSqrtPi;
+    const float An = a0.x, fx = a0.y, y = a0.z, Hc = a0.w;
+    const float AnT = a1.x, fxT = a1.y, yT = a1.z, HcT = a1.w;
+    const float yp = a2.x, up = a2.y, Hcp = a2.z, yv = a3.x, uv = a3.y, Hcv = a3.z;
+    const float gg = 1.f / (fx * fx), b2 = y * y * gg, Aky = An * k * y;
+    fu = make_float4(0.f, 0.f, b2, Aky * gg);
+    const float r_fx = fxT / fx;
+    fT = make_float4(gg * k * (AnT * y + An * yT) - 2.f * Aky * r_fx * gg,
+                     2.f * Aky * b2 * r_fx * gg - 2.f * An * k * yT * b2 * gg, An * k * yp * gg,
+                     -2.f * An * k * yp * b2 * gg);
+    fp = make_float4(2.f * Aky * up * gg, An * k * yv * gg, -2.f * An * k * yv * b2 * gg, 2.f * Aky * uv * gg);
+    if (LM) {
+        const float Yw = a4.x, YwT = a4.y, Ywp = a4.z;
+        fL0 = make_float4(Yw * k / fx, YwT * k / fx - Yw * k * gg * fxT,
+                          2.f * Yw * k * gg * fxT * b2 - 2.f * Yw * k * y * fx * yT * gg * gg, Ywp * k / fx);
+        fL1 = make_float4(Yw * k * up / fx, -2.f * Yw * k * up * b2 / fx, -2.f * Yw * k * y * fx * yp * gg * gg, 0.f);
+    }
+    // pedestals: -P0 pf, -PT pf, -An Hc pf_p - An Hc_p pf, ... with pf = 2 - (i - u)^2 / c^2
+    P[0] = An * Hc;
+    P[1] = AnT * Hc + An * HcT;
+    P[2] = An * Hcp;
+    P[3] = An * Hcv;
+}
+
+// A line's pedestals as quadratics in the point index i (value A + B i + C i^2, the
+// centre u in the same coordinates as i)
+__device__ __forceinline__ void jg_pedestal_quadratics(const float P[4], const float4& a0, const float4& a2,
+                                                       const float4& a3, float u, float icut2, float pA[4],
+                                                       float pB[4], float pC[4]) {
+    const float e0 = 2.f - u * u * icut2, e1 = 2.f * u * icut2;
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+        pA[o] = -P[o] * e0;
+        pB[o] = -P[o] * e1;
+        pC[o] = P[o] * icut2;
+    }
+    const float shp = 2.f * a0.x * a0.w * icut2;  // pf_p = 2 (i - u) u_p / c^2
+    pA[2] += shp * a2.y * u;
+    pB[2] -= shp * a2.y;
+    pA[3] += shp * a3.y * u;
+    pB[3] -= shp * a3.y;
+}
+
 // Far field of the Jacobian sums: as in the forward line sum, the fast lines whose
 // centres lie kJgFarDist or more points from the centre of the warp's 128-point block
 // are summed at the 8 Chebyshev nodes of the block (all seven sums: s, s_T, s_p, s_v
@@ -222,9 +277,203 @@ __device__ __forceinline__ void jg_far_table_init(JgFarTable& F) {
     }
 }
 
+// ---------------------------------------------------------- strip far field
+// As for the forward line sum (strip_far_kernel): a line whose shifted centre lies
+// kJgStripR or more points from the centre of a 1024-point strip (the 8 warps of a CTA),
+// whose cutoff covers the strip and whose Faddeeva core stays off it, is evaluated once
+// per strip at 16 Chebyshev nodes, for the four sums (seven with VP_Y on the segment),
+// pedestals included (quadratics, reproduced by the interpolation); the degree-15
+// interpolants go to each warp's 8 nodes through the fixed matrix M and join the
+// warp's own far field.  Worst error of one line's term: 1.6e-8 of its largest value
+// on the strip (poles 2 half-widths or more from its centre).  Its lines are two index
+// ranges per (segment, strip), taken out of every warp's window.
+constexpr float kJgStripR = 1024.f;
+constexpr double kJgStripCentre = 0.5 * (kJgStrip - 1);  // 511.5
+constexpr int kJgStripNodes = 16;
+constexpr int kJgStripOut = 7;                                       // s, s_T, s_p, s_v, D, D_T, D_p
+constexpr int kJgStripWords = kJgWarps * kJgStripOut * kJgFarNodes;  // per (segment, strip)
+constexpr int kJgStripSegs = 4;                                      // segments per block-wide exchange
+// the nodes relative to the strip centre, 511.5 cos((2k+1) pi / 32), rounded to FP32
+__device__ __forceinline__ float jg_strip_node_f(int k) {
+    const int a = k < 8 ? k : 15 - k;
+    const float v = a == 0 ? 5.090369873e+02f : a == 1 ? 4.894749756e+02f : a == 2 ? 4.511027222e+02f
+                  : a == 3 ? 3.953948364e+02f : a == 4 ? 3.244921570e+02f : a == 5 ? 2.411194305e+02f
+                  : a == 6 ? 1.484806061e+02f : 5.013576889e+01f;
+    return k < 8 ? v : -v;
+}
+
+// M[w][j][k] = L_k(node j of warp w) for the strip nodes k; one thread per entry
+__global__ void jg_strip_table_kernel(float* __restrict__ M) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kJgWarps * kJgFarNodes * kJgStripNodes) return;
+    const int w = i / (kJgFarNodes * kJgStripNodes), j = (i / kJgStripNodes) % kJgFarNodes, k = i % kJgStripNodes;
+    const double x = (double)kJgWarpPts * w + jg_far_node(j) - kJgStripCentre;
+    const double xk = (double)jg_strip_node_f(k);
+    double v = 1.0;
+    for (int l = 0; l < kJgStripNodes; ++l)
+        if (l != k) v *= (x - (double)jg_strip_node_f(l)) / (xk - (double)jg_strip_node_f(l));
+    M[i] = (float)v;
+}
+
+// One CTA per (strip, profile-layer).  Per batch of segments: the index ranges
+// (rin = max(kJgStripR, core reach + 513) + margin, rout = cut - 512 - margin), then
+// each warp takes tiles warp, warp + 8, ... of the ranges' lines: the lanes stage their
+// lines' far-wing coefficients and sum their pedestal quadratics (the centre as offset
+// from the strip centre), and lane l evaluates node l % 16 over every other staged line;
+// the warps' node and pedestal sums meet in shared memory, and each warp takes them
+// (the warps in a fixed order, pedestals evaluated at the nodes) through M to its own
+// line-sum warp's 8 nodes: far[(segment, strip)][warp][sum][node], and the ranges.
+template <bool ANY_LM>
+__global__ void __launch_bounds__(kJgWarps * 32, 2) jg_strip_kernel(
+    const SegDev* __restrict__ segs, const int* __restrict__ seg_n, const unsigned* __restrict__ core_reach,
+    const int2* __restrict__ pl_segs, JgOut g, float cut_g, int n_strips, const float* __restrict__ M,
+    float* __restrict__ far, int4* __restrict__ ranges) {
+    constexpr int NC = ANY_LM ? 7 : 4;            // sums
+    constexpr int kSlot = kJgStripOut * kJgStripNodes + 12;  // node sums, then A, B, C of the 4 pedestals
+    __shared__ float4 sfu[kJgWarps][32], sfT[kJgWarps][32], sfp[kJgWarps][32];
+    __shared__ float4 sL0[ANY_LM ? kJgWarps : 1][32], sL1[ANY_LM ? kJgWarps : 1][32];
+    __shared__ float slot[kJgStripSegs][kJgWarps][kSlot];
+    __shared__ int sj[kJgStripSegs][4];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int strip = blockIdx.x, pl = blockIdx.y;
+    const double c = (double)strip * kJgStrip + kJgStripCentre;
+    const float icut2 = 1.f / (cut_g * cut_g);
+    const float xk = jg_strip_node_f(lane & (kJgStripNodes - 1));  // this lane's node
+    const int2 rng = pl_segs[pl];
+    for (int s0 = rng.x; s0 < rng.x + rng.y; s0 += kJgStripSegs) {  // block-uniform
+        const int ns = min(kJgStripSegs, rng.x + rng.y - s0);
+        for (int i = warp; i < 4 * ns; i += kJgWarps) {  // search i: bound i % 4 of segment i / 4
+            const SegDev sg = segs[s0 + i / 4];
+            const double reach = (double)__uint_as_float(core_reach[s0 + i / 4]);
+            const double m = sg.margin_g, rin = fmax((double)kJgStripR, reach + 0.5 * kJgStrip + 1.0) + m;
+            const double rout = (double)cut_g - 0.5 * kJgStrip - m;
+            int j = 0;
+            if (rout > rin) {
+                const int b = i % 4;
+                const double v = b == 0 ? c - rout : b == 1 ? c - rin : b == 2 ? c + rin : c + rout;
+                j = (int)warp_lower_bound(g.V + sg.off, v, seg_n[s0 + i / 4], lane);
+            }
+            if (lane == 0) sj[i / 4][i % 4] = j;
+        }
+        __syncthreads();
+        for (int si = 0; si < ns; ++si) {
+            const SegDev sg = segs[s0 + si];
+            const bool lm = ANY_LM && (sg.flags & SEG_LM);
+            const int jA = sj[si][0], jB = sj[si][1], jC = sj[si][2], jD = sj[si][3];
+            const int nL = jB - jA, n = nL + (jD - jC);
+            float v[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            float QA[4] = {0.f, 0.f, 0.f, 0.f}, QB[4] = {0.f, 0.f, 0.f, 0.f}, QC[4] = {0.f, 0.f, 0.f, 0.f};
+            float QAc = 0.f, QBc = 0.f, QCc = 0.f;
+            for (int t0 = warp * 32; t0 < n; t0 += 32 * kJgWarps) {
+                const int t = t0 + lane, nt = min(32, n - t0);
+                float pA[4] = {0.f, 0.f, 0.f, 0.f}, pB[4] = {0.f, 0.f, 0.f, 0.f}, pC[4] = {0.f, 0.f, 0.f, 0.f};
+                if (t < n) {
+                    const long long q = sg.off + (t < nL ? jA + t : jC + (t - nL));
+                    const double u = g.U[q] - c;
+                    const float uh = (float)u, ul = (float)(u - (double)uh);
+                    const float4 a0 = g.q0[q], a1 = g.q1[q], a2 = g.q2[q], a3 = g.q3[q];
+                    const float4 a4 = lm ? g.q4[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    float4 fu, fT, fp, fL0, fL1;
+                    float P[4];
+                    jg_wing_coeffs<ANY_LM>(a0, a1, a2, a3, a4, fu, fT, fp, fL0, fL1, P);
+                    sfu[warp][lane] = make_float4(uh, ul, fu.z, fu.w);
+                    sfT[warp][lane] = fT;
+                    sfp[warp][lane] = fp;
+                    if (ANY_LM) {
+                        sL0[warp][lane] = fL0;
+                        sL1[warp][lane] = fL1;
+                    }
+                    jg_pedestal_quadratics(P, a0, a2, a3, uh, icut2, pA, pB, pC);
+                }
+                kahan_add(QA[0], QAc, pA[0]);
+                kahan_add(QB[0], QBc, pB[0]);
+                kahan_add(QC[0], QCc, pC[0]);
+#pragma unroll
+                for (int o = 1; o < 4; ++o) {
+                    QA[o] += pA[o];
+                    QB[o] += pB[o];
+                    QC[o] += pC[o];
+                }
+                __syncwarp();
+                for (int kk = lane >> 4; kk < nt; kk += 2) {
+                    const float4 f0 = sfu[warp][kk], f1 = sfT[warp][kk], f2 = sfp[warp][kk];
+                    const float d = (xk - f0.x) - f0.y;
+                    const float rho = rcp_fast(fmaf(d, d, f0.z));
+                    const float rho2 = rho * rho, drho2 = d * rho2;
+                    v[0] = fmaf(f0.w, rho, v[0]);
+                    v[1] = fmaf(f1.x, rho, fmaf(f1.y, rho2, v[1]));
+                    v[2] = fmaf(f1.z, rho, fmaf(f1.w, rho2, fmaf(f2.x, drho2, v[2])));
+                    v[3] = fmaf(f2.y, rho, fmaf(f2.z, rho2, fmaf(f2.w, drho2, v[3])));
+                    if (ANY_LM) {
+                        const float4 l0 = sL0[warp][kk], l1 = sL1[warp][kk];
+                        const float drho = d * rho;
+                        v[4] = fmaf(l0.x, drho, v[4]);
+                        v[5] = fmaf(l0.y, drho, fmaf(l0.z, drho2, v[5]));
+                        v[6] = fmaf(l0.w, drho, fmaf(l1.x, rho, fmaf(l1.y, rho2, fmaf(l1.z, drho2, v[6]))));
+                    }
+                }
+                __syncwarp();
+            }
+            float* sl = slot[si][warp];
+#pragma unroll
+            for (int cc = 0; cc < NC; ++cc) {
+                const float x = v[cc] + __shfl_xor_sync(kFull, v[cc], 16);  // the two halves of the lines
+                if (lane < kJgStripNodes) sl[cc * kJgStripNodes + lane] = x;
+            }
+            float wA[4], wB[4], wC[4];
+            wA[0] = warp_sum(QA[0] - QAc);
+            wB[0] = warp_sum(QB[0] - QBc);
+            wC[0] = warp_sum(QC[0] - QCc);
+#pragma unroll
+            for (int o = 1; o < 4; ++o) {
+                wA[o] = warp_sum(QA[o]);
+                wB[o] = warp_sum(QB[o]);
+                wC[o] = warp_sum(QC[o]);
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int o = 0; o < 4; ++o) {
+                    sl[kJgStripOut * kJgStripNodes + 3 * o] = wA[o];
+                    sl[kJgStripOut * kJgStripNodes + 3 * o + 1] = wB[o];
+                    sl[kJgStripOut * kJgStripNodes + 3 * o + 2] = wC[o];
+                }
+            }
+        }
+        __syncthreads();
+        const float* Mw = M + ((size_t)warp * kJgFarNodes + (lane & (kJgFarNodes - 1))) * kJgStripNodes;
+        for (int si = 0; si < ns; ++si) {
+            const size_t cell = (size_t)(s0 + si) * n_strips + strip;
+            const bool lm = ANY_LM && (segs[s0 + si].flags & SEG_LM);
+#pragma unroll
+            for (int cc = 0; cc < NC; ++cc) {
+                if (cc >= 4 && !lm) break;
+                float fc = 0.f;  // lane k < 16: node k of sum cc, the warps in a fixed order
+                float A = 0.f, B = 0.f, C = 0.f;
+#pragma unroll
+                for (int w = 0; w < kJgWarps; ++w) {
+                    fc += slot[si][w][cc * kJgStripNodes + (lane & (kJgStripNodes - 1))];
+                    if (cc < 4) {
+                        A += slot[si][w][kJgStripOut * kJgStripNodes + 3 * cc];
+                        B += slot[si][w][kJgStripOut * kJgStripNodes + 3 * cc + 1];
+                        C += slot[si][w][kJgStripOut * kJgStripNodes + 3 * cc + 2];
+                    }
+                }
+                if (cc < 4) fc += fmaf(xk, fmaf(xk, C, B), A);
+                float gv = 0.f;
+#pragma unroll
+                for (int k = 0; k < kJgStripNodes; ++k) gv = fmaf(__ldg(Mw + k), __shfl_sync(kFull, fc, k), gv);
+                if (lane < kJgFarNodes) far[cell * kJgStripWords + (warp * kJgStripOut + cc) * kJgFarNodes + lane] = gv;
+            }
+            if (threadIdx.x == 0) ranges[cell] = make_int4(sj[si][0], sj[si][1], sj[si][2], sj[si][3]);
+        }
+        if (s0 + kJgStripSegs < rng.x + rng.y) __syncthreads();  // slots and ranges reused by the next batch
+    }
+}
+
 template <bool LM>
 __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long long wb, float cut, int lane,
-                           JgTile& T, const JgFarTable& FT, float xn, float sum[4][kJgQ], float dsum[3][kJgQ]) {
+                           JgTile& T, const JgFarTable& FT, float xn, float sum[4][kJgQ], float dsum[3][kJgQ],
+                           int4 sx, const float* __restrict__ gfar) {
     constexpr float kCentre = 0.5f * (kJgWarpPts - 1);
     constexpr float kHalf = 0.5f * kJgWarpPts + 0.5f;
     constexpr float k = (float)kInvSqrtPi;
@@ -254,8 +503,14 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
     // reduced over the warp once per segment
     float QA[4] = {0.f, 0.f, 0.f, 0.f}, QB[4] = {0.f, 0.f, 0.f, 0.f}, QC[4] = {0.f, 0.f, 0.f, 0.f};
     float QAc = 0.f, QBc = 0.f, QCc = 0.f;
-    for (long long t0 = jlo; t0 < jhi; t0 += 32) {
-        const int nt = (int)min(32LL, jhi - t0);
+    // the window without the strip far field's ranges [sx.x, sx.y) and [sx.z, sx.w):
+    // [ilo, ra), [rb, rc) and [rd, ihi), walked in turn (indices within a segment fit in int)
+    const int ilo = (int)jlo, ihi = (int)jhi;
+    const int ra = min(max(sx.x, ilo), ihi), rb = min(max(sx.y, ilo), ihi);
+    const int rc = min(max(sx.z, ilo), ihi), rd = min(max(sx.w, ilo), ihi);
+    int nt = 0;
+    for (int t0 = skip_ranges(ilo, ra, rb, rc, rd); t0 < ihi; t0 = skip_ranges(t0 + nt, ra, rb, rc, rd)) {
+        nt = min(32, (t0 < ra ? ra : t0 < rc ? rc : ihi) - t0);
         int cls = 0;
         float uh = 0.f, ul = 0.f;
         float4 a0, a1, a2, a3, a4;
@@ -282,43 +537,21 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
         __syncwarp();
         if (cls == 1 || cls == 3 || cls == 4) {  // fast lines first, far lines after them, edge lines from the top
             const int pos = cls == 1 ? __popc(fm & lt) : (cls == 3 ? __popc(fm) + __popc(xm & lt) : 31 - __popc(em & lt));
-            const float An = a0.x, fx = a0.y, y = a0.z, Hc = a0.w;
-            const float AnT = a1.x, fxT = a1.y, yT = a1.z, HcT = a1.w;
-            const float yp = a2.x, up = a2.y, Hcp = a2.z, yv = a3.x, uv = a3.y, Hcv = a3.z;
-            const float gg = 1.f / (fx * fx), b2 = y * y * gg, Aky = An * k * y;
-            T.fu[pos] = make_float4(uh, ul, b2, Aky * gg);
-            const float r_fx = fxT / fx;
-            T.fT[pos] = make_float4(gg * k * (AnT * y + An * yT) - 2.f * Aky * r_fx * gg,
-                                    2.f * Aky * b2 * r_fx * gg - 2.f * An * k * yT * b2 * gg, An * k * yp * gg,
-                                    -2.f * An * k * yp * b2 * gg);
-            T.fp[pos] = make_float4(2.f * Aky * up * gg, An * k * yv * gg, -2.f * An * k * yv * b2 * gg,
-                                    2.f * Aky * uv * gg);
+            float4 fu, fT, fp, fL0, fL1;
+            float P[4];
+            jg_wing_coeffs<LM>(a0, a1, a2, a3, a4, fu, fT, fp, fL0, fL1, P);
+            T.fu[pos] = make_float4(uh, ul, fu.z, fu.w);
+            T.fT[pos] = fT;
+            T.fp[pos] = fp;
             if (LM) {
-                const float Yw = a4.x, YwT = a4.y, Ywp = a4.z;
-                T.fL0[pos] = make_float4(Yw * k / fx, YwT * k / fx - Yw * k * gg * fxT,
-                                         2.f * Yw * k * gg * fxT * b2 - 2.f * Yw * k * y * fx * yT * gg * gg,
-                                         Ywp * k / fx);
-                T.fL1[pos] = make_float4(Yw * k * up / fx, -2.f * Yw * k * up * b2 / fx,
-                                         -2.f * Yw * k * y * fx * yp * gg * gg, 0.f);
+                T.fL0[pos] = fL0;
+                T.fL1[pos] = fL1;
             }
-            // pedestals: -P0 pf, -PT pf, -An Hc pf_p - An Hc_p pf, ... with pf = 2 - (i - u)^2 / c^2
-            const float P[4] = {An * Hc, AnT * Hc + An * HcT, An * Hcp, An * Hcv};
             if (cls == 4) {  // edge lines: pedestals per point (masked by the cutoff), in the slow arrays' top
                 T.q0[pos] = make_float4(P[0], P[1], P[2], P[3]);
-                T.q1[pos] = make_float4(2.f * up * icut2 * P[0], 2.f * uv * icut2 * P[0], 0.f, 0.f);
+                T.q1[pos] = make_float4(2.f * a2.y * icut2 * P[0], 2.f * a3.y * icut2 * P[0], 0.f, 0.f);
             } else {
-                const float e0 = 2.f - uh * uh * icut2, e1 = 2.f * uh * icut2;
-#pragma unroll
-                for (int o = 0; o < 4; ++o) {
-                    pA[o] = -P[o] * e0;
-                    pB[o] = -P[o] * e1;
-                    pC[o] = P[o] * icut2;
-            }
-                const float shp = 2.f * An * Hc * icut2;  // pf_p = 2 (i - u) u_p / c^2
-                pA[2] += shp * up * uh;
-                pB[2] -= shp * up;
-                pA[3] += shp * uv * uh;
-                pB[3] -= shp * uv;
+                jg_pedestal_quadratics(P, a0, a2, a3, uh, icut2, pA, pB, pC);
             }
         } else if (cls == 2) {
             const int pos = __popc(sm & lt);
@@ -506,6 +739,7 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
             if (!LM && c >= 4) continue;
             v[c] += __shfl_xor_sync(kFull, v[c], 8);
             v[c] += __shfl_xor_sync(kFull, v[c], 16);
+            if (gfar) v[c] += gfar[c * kJgFarNodes + (lane & (kJgFarNodes - 1))];  // the strip far field
         }
         float it[7][kJgQ];
 #pragma unroll
@@ -567,7 +801,8 @@ template <bool ANY_LM, int NOUT>
 __global__ void __launch_bounds__(kJgWarps * 32, 2) jg_linesum_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_n, const SegW* __restrict__ wts,
     const int2* __restrict__ pl_segs, JgOut g, long long n_nu, float cut_g, float* __restrict__ out,
-    const double* __restrict__ pert, long long pstride) {
+    const double* __restrict__ pert, long long pstride, const float* __restrict__ sfar,
+    const int4* __restrict__ sranges, int n_strips) {
     extern __shared__ float4 jg_sh[];
     JgTile* tiles = (JgTile*)jg_sh;
     JgFarTable& ftab = *(JgFarTable*)((float*)(tiles + kJgWarps) + (size_t)kJgWarps * NOUT * kJgWarpPts);
@@ -588,10 +823,17 @@ __global__ void __launch_bounds__(kJgWarps * 32, 2) jg_linesum_kernel(
         float s[4][kJgQ], ds[3][kJgQ];
         const long long nl = seg_n[si];
         const bool lm = ANY_LM && (sg.flags & SEG_LM);
+        int4 sx = make_int4(0, 0, 0, 0);  // no strip far field: the whole window
+        const float* gf = nullptr;
+        if (sfar) {
+            const size_t cell = (size_t)si * n_strips + blockIdx.x;
+            sx = sranges[cell];
+            gf = sfar + cell * kJgStripWords + (size_t)warp * kJgStripOut * kJgFarNodes;
+        }
         if (lm)
-            jg_segment<true>(sg, nl, g, wb, cut_g, lane, tiles[warp], ftab, xn, s, ds);
+            jg_segment<true>(sg, nl, g, wb, cut_g, lane, tiles[warp], ftab, xn, s, ds, sx, gf);
         else
-            jg_segment<false>(sg, nl, g, wb, cut_g, lane, tiles[warp], ftab, xn, s, ds);
+            jg_segment<false>(sg, nl, g, wb, cut_g, lane, tiles[warp], ftab, xn, s, ds, sx, gf);
         // clamps (voigt.jl:276, line_mixing.jl:1368, cross_section_jacobian.jl:107-113, :312-319)
         const SegW& W = wts[si];
         // relaxation-matrix line mixing: rows (perturbation, d/dT, d/dp) x column amount
