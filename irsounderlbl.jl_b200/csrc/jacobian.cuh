@@ -319,7 +319,8 @@ __global__ void jg_strip_table_kernel(float* __restrict__ M) {
 // (rin = max(kJgStripR, core reach + 513) + margin, rout = cut - 512 - margin), then
 // each warp takes tiles warp, warp + 8, ... of the ranges' lines: the lanes stage their
 // lines' far-wing coefficients and sum their pedestal quadratics (the centre as offset
-// from the strip centre), and lane l evaluates node l % 16 over every other staged line;
+// from the strip centre), and lane l evaluates nodes l % 8 and l % 8 + 8 (packed) over
+// every fourth staged line;
 // the warps' node and pedestal sums meet in shared memory, and each warp takes them
 // (the warps in a fixed order, pedestals evaluated at the nodes) through M to its own
 // line-sum warp's 8 nodes: far[(segment, strip)][warp][sum][node], and the ranges.
@@ -338,7 +339,10 @@ __global__ void __launch_bounds__(kJgWarps * 32, 2) jg_strip_kernel(
     const int strip = blockIdx.x, pl = blockIdx.y;
     const double c = (double)strip * kJgStrip + kJgStripCentre;
     const float icut2 = 1.f / (cut_g * cut_g);
-    const float xk = jg_strip_node_f(lane & (kJgStripNodes - 1));  // this lane's node
+    const float xk = jg_strip_node_f(lane & (kJgStripNodes - 1));  // this lane's node (combining)
+    // this lane's node pair (np, np + 8), np = lane % 8, for the line evaluations
+    const float2 xp = make_float2(jg_strip_node_f(lane & 7), jg_strip_node_f((lane & 7) + 8));
+    const float2 xps = make_float2(xp.y, xp.x);
     const int2 rng = pl_segs[pl];
     for (int s0 = rng.x; s0 < rng.x + rng.y; s0 += kJgStripSegs) {  // block-uniform
         const int ns = min(kJgStripSegs, rng.x + rng.y - s0);
@@ -361,7 +365,9 @@ __global__ void __launch_bounds__(kJgWarps * 32, 2) jg_strip_kernel(
             const bool lm = ANY_LM && (sg.flags & SEG_LM);
             const int jA = sj[si][0], jB = sj[si][1], jC = sj[si][2], jD = sj[si][3];
             const int nL = jB - jA, n = nL + (jD - jC);
-            float v[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            float2 v[7];  // this lane's node pair (np, np + 8), np = lane % 8, over lines lane / 8 + 4 i
+#pragma unroll
+            for (int cc = 0; cc < 7; ++cc) v[cc] = make_float2(0.f, 0.f);
             float QA[4] = {0.f, 0.f, 0.f, 0.f}, QB[4] = {0.f, 0.f, 0.f, 0.f}, QC[4] = {0.f, 0.f, 0.f, 0.f};
             float QAc = 0.f, QBc = 0.f, QCc = 0.f;
             for (int t0 = warp * 32; t0 < n; t0 += 32 * kJgWarps) {
@@ -395,30 +401,48 @@ __global__ void __launch_bounds__(kJgWarps * 32, 2) jg_strip_kernel(
                     QC[o] += pC[o];
                 }
                 __syncwarp();
-                for (int kk = lane >> 4; kk < nt; kk += 2) {
+                for (int kk = lane >> 3; kk < nt; kk += 4) {  // packed: one reciprocal per node pair
                     const float4 f0 = sfu[warp][kk], f1 = sfT[warp][kk], f2 = sfp[warp][kk];
-                    const float d = (xk - f0.x) - f0.y;
-                    const float rho = rcp_fast(fmaf(d, d, f0.z));
-                    const float rho2 = rho * rho, drho2 = d * rho2;
-                    v[0] = fmaf(f0.w, rho, v[0]);
-                    v[1] = fmaf(f1.x, rho, fmaf(f1.y, rho2, v[1]));
-                    v[2] = fmaf(f1.z, rho, fmaf(f1.w, rho2, fmaf(f2.x, drho2, v[2])));
-                    v[3] = fmaf(f2.y, rho, fmaf(f2.z, rho2, fmaf(f2.w, drho2, v[3])));
+                    const float2 nu_ = make_float2(-f0.x, -f0.x), nl = make_float2(-f0.y, -f0.y);
+                    const float2 dn = __fadd2_rn(__fadd2_rn(xp, nu_), nl);     // (d_a, d_b)
+                    const float2 dsw = __fadd2_rn(__fadd2_rn(xps, nu_), nl);   // (d_b, d_a)
+                    const float2 es = __ffma2_rn(dsw, dsw, make_float2(f0.z, f0.z));  // (e_b, e_a)
+                    const float R = rcp_fast(es.x * es.y);
+                    const float2 rho = __fmul2_rn(es, make_float2(R, R));     // (1/e_a, 1/e_b)
+                    const float2 rho2 = __fmul2_rn(rho, rho), drho2 = __fmul2_rn(dn, rho2);
+                    v[0] = __ffma2_rn(make_float2(f0.w, f0.w), rho, v[0]);
+                    v[1] = __ffma2_rn(make_float2(f1.x, f1.x), rho, __ffma2_rn(make_float2(f1.y, f1.y), rho2, v[1]));
+                    v[2] = __ffma2_rn(make_float2(f1.z, f1.z), rho,
+                                      __ffma2_rn(make_float2(f1.w, f1.w), rho2,
+                                                 __ffma2_rn(make_float2(f2.x, f2.x), drho2, v[2])));
+                    v[3] = __ffma2_rn(make_float2(f2.y, f2.y), rho,
+                                      __ffma2_rn(make_float2(f2.z, f2.z), rho2,
+                                                 __ffma2_rn(make_float2(f2.w, f2.w), drho2, v[3])));
                     if (ANY_LM) {
                         const float4 l0 = sL0[warp][kk], l1 = sL1[warp][kk];
-                        const float drho = d * rho;
-                        v[4] = fmaf(l0.x, drho, v[4]);
-                        v[5] = fmaf(l0.y, drho, fmaf(l0.z, drho2, v[5]));
-                        v[6] = fmaf(l0.w, drho, fmaf(l1.x, rho, fmaf(l1.y, rho2, fmaf(l1.z, drho2, v[6]))));
+                        const float2 drho = __fmul2_rn(dn, rho);
+                        v[4] = __ffma2_rn(make_float2(l0.x, l0.x), drho, v[4]);
+                        v[5] = __ffma2_rn(make_float2(l0.y, l0.y), drho, __ffma2_rn(make_float2(l0.z, l0.z), drho2, v[5]));
+                        v[6] = __ffma2_rn(make_float2(l0.w, l0.w), drho,
+                                          __ffma2_rn(make_float2(l1.x, l1.x), rho,
+                                                     __ffma2_rn(make_float2(l1.y, l1.y), rho2,
+                                                                __ffma2_rn(make_float2(l1.z, l1.z), drho2, v[6]))));
                     }
                 }
                 __syncwarp();
             }
             float* sl = slot[si][warp];
 #pragma unroll
-            for (int cc = 0; cc < NC; ++cc) {
-                const float x = v[cc] + __shfl_xor_sync(kFull, v[cc], 16);  // the two halves of the lines
-                if (lane < kJgStripNodes) sl[cc * kJgStripNodes + lane] = x;
+            for (int cc = 0; cc < NC; ++cc) {  // the four line groups, then node np and np + 8
+                float2 x = v[cc];
+                x.x += __shfl_xor_sync(kFull, x.x, 8);
+                x.y += __shfl_xor_sync(kFull, x.y, 8);
+                x.x += __shfl_xor_sync(kFull, x.x, 16);
+                x.y += __shfl_xor_sync(kFull, x.y, 16);
+                if (lane < 8) {
+                    sl[cc * kJgStripNodes + lane] = x.x;
+                    sl[cc * kJgStripNodes + lane + 8] = x.y;
+                }
             }
             float wA[4], wB[4], wC[4];
             wA[0] = warp_sum(QA[0] - QAc);
