@@ -278,3 +278,18 @@ def test_iasi_400k_far_field_vs_direct(pkg, ctx, iasi_lists):
             assert st.evaluated_pairs < 0.3 * st.pairs
     d = out["mixed"] - out["mixed_direct"]
     assert np.max(np.abs(d)) < 1e-3
+
+
+def test_far_field_fine_grid_core_reach(pkg, ctx):
+    """A grid fine enough (and x_far large enough) that the Faddeeva cores reach
+    thousands of points: the strip far field starts beyond every line's core reach, and
+    IRS_MIXED still agrees with the direct FP32 sum (IRS_MIXED_DIRECT) to 1e-3 K."""
+    lists = pkg.synthetic.lists_5k_co2()
+    snd = pkg.Sounder.make(660.0, 664.0, 0.25, opd_max=2.0, fwhm_gauss=0.5)
+    prof = pkg.afgl_atmosphere("us_standard")
+    out = {}
+    for prec in ("mixed_direct", "mixed"):
+        _, _, out[prec] = pkg.forward_model(prof, lists, sounder=snd, backend=ctx, internal_dnu=5e-5,
+                                            x_far=400.0, precision=prec)
+    assert np.all(np.isfinite(out["mixed"])) and np.all(out["mixed"] > 150)
+    assert np.max(np.abs(out["mixed"] - out["mixed_direct"])) < 1e-3
