@@ -264,33 +264,58 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
         unsigned long long* d_eval = d_pairs + 2;
         const bool far = o.precision == IRS_MIXED;
         const bool anylm = o.line_mixing == IRS_LM_PER_LINE_Y;
-        // strip far field (pre-pass): 528 bytes per (segment, strip), skipped past 2 GiB
-        float* d_sfar = nullptr;
-        int4* d_srng = nullptr;
+        // strip far field (pre-pass): 528 bytes per (segment, strip) in a buffer of at most
+        // ctx->strip_buf_max; larger batches run in groups of profile-layers (their segments
+        // are contiguous) whose cells fit it
         const int n_strips = (int)g2.x;
-        const size_t cells = (size_t)nseg * n_strips;
-        if (far && o.method == 3 && cells * (kStripWords * sizeof(float) + sizeof(int4)) <= ((size_t)2 << 30)) {
-            char* b = (char*)workspace(ctx, "strip_far", cells * (kStripWords * sizeof(float) + sizeof(int4)));
-            d_sfar = (float*)b;
-            d_srng = (int4*)(b + cells * kStripWords * sizeof(float));
+        const size_t cell_bytes = kStripWords * sizeof(float) + sizeof(int4);
+        const bool strip = far && o.method == 3;
+        float* d_M = nullptr;
+        char* d_sbuf = nullptr;
+        size_t max_cells = 0;
+        if (strip) {
+            max_cells = std::min((size_t)nseg * n_strips, ctx->strip_buf_max / cell_bytes);
+            d_sbuf = (char*)workspace(ctx, "strip_far", max_cells * cell_bytes);
             constexpr int nM = kMxWarps * kFarNodes * kCtaNodes;
-            float* d_M = (float*)workspace(ctx, "strip_M", nM * sizeof(float));
+            d_M = (float*)workspace(ctx, "strip_M", nM * sizeof(float));
             strip_table_kernel<<<(nM + 255) / 256, 256, 0, st>>>(d_M);
             check_launch(ctx);
-            dim3 g3(n_strips, npl);
-            if (anylm) strip_far_kernel<true><<<g3, kStripThreads, 0, st>>>(d_segs, d_count, d_reach, d_pl, om, cut_g, n_strips, d_M, d_sfar, d_srng, d_eval);
-            else strip_far_kernel<false><<<g3, kStripThreads, 0, st>>>(d_segs, d_count, d_reach, d_pl, om, cut_g, n_strips, d_M, d_sfar, d_srng, d_eval);
-            check_launch(ctx);
         }
+        std::vector<int> first(npl + 1, 0);  // first segment of each profile-layer (emitted in order)
+        for (int q = 0; q < npl; ++q) first[q + 1] = first[q] + pl.pl_segs[q].y;
+        for (int pa = 0; pa < npl;) {
+            // this launch: profile-layers [pa, pb) and their segments [s_a, first[pb])
+            int pb = npl;
+            const int s_a = first[pa];
+            float* d_sfar = nullptr;
+            int4* d_srng = nullptr;
+            if (strip) {
+                pb = pa;
+                while (pb < npl && (size_t)(first[pb + 1] - s_a) * n_strips <= max_cells) ++pb;
+                if (pb == pa) pb = pa + 1;  // one profile-layer beyond the buffer: no strip far field
+                const size_t cells = (size_t)(first[pb] - s_a) * n_strips;
+                if (cells <= max_cells) {
+                    d_sfar = (float*)d_sbuf;
+                    d_srng = (int4*)(d_sbuf + cells * kStripWords * sizeof(float));
+                    dim3 g3(n_strips, pb - pa);
+                    if (anylm) strip_far_kernel<true><<<g3, kStripThreads, 0, st>>>(d_segs, d_count, d_reach, d_pl, om, cut_g, n_strips, d_M, d_sfar, d_srng, d_eval, pa, s_a);
+                    else strip_far_kernel<false><<<g3, kStripThreads, 0, st>>>(d_segs, d_count, d_reach, d_pl, om, cut_g, n_strips, d_M, d_sfar, d_srng, d_eval, pa, s_a);
+                    check_launch(ctx);
+                }
+            }
+            const dim3 g2c(g2.x, pb - pa);
 #define IRS_MX(M, LMX, F, P) do { \
         IRS_CUDA(cudaFuncSetAttribute(linesum_mixed_kernel<M, LMX, F, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMxSmem)); \
-        linesum_mixed_kernel<M, LMX, F, P><<<g2, kMxThreads, kMxSmem, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau, d_eval, d_pert, pstride, d_sfar, d_srng, n_strips); \
+        linesum_mixed_kernel<M, LMX, F, P><<<g2c, kMxThreads, kMxSmem, st>>>(d_segs, d_count, d_pl, om, n_nu, cut_g, (float*)d_tau, d_eval, d_pert, pstride, d_sfar, d_srng, n_strips, pa, s_a); \
     } while (0)
-        if (o.method == 1) { if (far) IRS_MX(1, false, true, false); else IRS_MX(1, false, false, false); }
-        else if (o.method == 2) IRS_MX(2, false, false, false);
-        else if (o.line_mixing == IRS_LM_PER_LINE_Y) { if (far) IRS_MX(3, true, true, false); else IRS_MX(3, true, false, false); }
-        else if (d_pert) { if (far) IRS_MX(3, false, true, true); else IRS_MX(3, false, false, true); }
-        else { if (far) IRS_MX(3, false, true, false); else IRS_MX(3, false, false, false); }
+            if (o.method == 1) { if (far) IRS_MX(1, false, true, false); else IRS_MX(1, false, false, false); }
+            else if (o.method == 2) IRS_MX(2, false, false, false);
+            else if (o.line_mixing == IRS_LM_PER_LINE_Y) { if (far) IRS_MX(3, true, true, false); else IRS_MX(3, true, false, false); }
+            else if (d_pert) { if (far) IRS_MX(3, false, true, true); else IRS_MX(3, false, false, true); }
+            else { if (far) IRS_MX(3, false, true, false); else IRS_MX(3, false, false, false); }
+            check_launch(ctx);
+            pa = pb;
+        }
 #undef IRS_MX
     }
     check_launch(ctx);
@@ -477,6 +502,13 @@ static void forward_pass(irs_ctx* ctx, const irs_profile* profs, int n_prof, con
             workspace(ctx, "chunk_count", sizeof(int) * (size_t)nseg * ((max_list + kLpChunk - 1) / kLpChunk));
         }
         workspace(ctx, "seg_count", sizeof(int) * nseg);
+        if (o.precision == IRS_MIXED && o.method == 3) {  // the strip far field's buffers
+            const size_t n_strips = (size_t)((n_nu + kMxStrip - 1) / kMxStrip);
+            const size_t cb = kStripWords * sizeof(float) + sizeof(int4);
+            workspace(ctx, "strip_far", std::min((size_t)nseg * n_strips, ctx->strip_buf_max / cb) * cb);
+            workspace(ctx, "strip_M", sizeof(float) * kMxWarps * kFarNodes * kCtaNodes);
+        }
+        if (mixed) workspace(ctx, "core_reach", sizeof(unsigned) * nseg);
         workspace(ctx, "lrt", std::max<size_t>(lrt.size(), 1) * sizeof(LayerRT));
         workspace(ctx, "prt", std::max<size_t>(prt.size(), 1) * sizeof(ProfileRT));
     }
@@ -1202,6 +1234,11 @@ int irs_create(int device, irs_ctx** out) {
     IRS_CUDA(cudaSetDevice(device));
     std::unique_ptr<irs_ctx> c(new irs_ctx);
     c->device = device;
+    if (const char* e = std::getenv("IRS_STRIP_BUFFER_BYTES")) {
+        const long long v = std::atoll(e);
+        IRS_REQUIRE(v > 0, "IRS_STRIP_BUFFER_BYTES must be a positive byte count");
+        c->strip_buf_max = (size_t)v;
+    }
     IRS_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     for (auto& e : c->ev) IRS_CUDA(cudaEventCreate(&e));
     FaddeevaConsts fc;

@@ -191,6 +191,9 @@ struct irs_ctx {
     // cached ILS kernel
     double ils_key[4] = {-1, -1, -1, -1};
     int64_t ils_n = 0;
+    // bytes of the strip far field's node values per line-sum launch (larger batches run
+    // in groups of profile-layers); IRS_STRIP_BUFFER_BYTES at context creation sets it
+    size_t strip_buf_max = (size_t)2 << 30;
 };
 
 namespace irs {

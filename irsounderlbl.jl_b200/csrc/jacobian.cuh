@@ -500,7 +500,6 @@ __device__ void jg_segment(const SegDev& sg, long long cnt, const JgOut& g, long
                            int4 sx, const float* __restrict__ gfar) {
     constexpr float kCentre = 0.5f * (kJgWarpPts - 1);
     constexpr float kHalf = 0.5f * kJgWarpPts + 0.5f;
-    constexpr float k = (float)kInvSqrtPi;
     const float cut2 = cut * cut, icut2 = 1.f / cut2;
     const long long jlo = warp_lower_bound(g.V + sg.off, (double)wb - cut - sg.margin_g, cnt, lane);
     const long long jhi =

@@ -308,11 +308,11 @@ template <bool ANY_LM>
 __global__ void __launch_bounds__(kStripThreads, 3) strip_far_kernel(
     const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const unsigned* __restrict__ core_reach,
     const int2* __restrict__ pl_segs, LpOutMixed lp, float cut_g, int n_strips, const float* __restrict__ M,
-    float* __restrict__ far, int4* __restrict__ ranges, unsigned long long* __restrict__ evald) {
+    float* __restrict__ far, int4* __restrict__ ranges, unsigned long long* __restrict__ evald, int pl0, int seg0) {
     __shared__ float slot[kStripSegs][kStripWarps][kCtaNodes + 4];  // node sums, pedestal A, B, C
     __shared__ int sj[kStripSegs][4];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int strip = blockIdx.x, pl = blockIdx.y;
+    const int strip = blockIdx.x, pl = pl0 + (int)blockIdx.y;  // cells counted from segment seg0
     const long long cb = (long long)strip * kMxStrip;
     const double c = (double)cb + kCtaCentre;
     unsigned long long work = 0;
@@ -416,7 +416,7 @@ __global__ void __launch_bounds__(kStripThreads, 3) strip_far_kernel(
                 SC += slot[si][w][kCtaNodes + 2];
             }
             fc += fmaf(xk, fmaf(xk, SA, -2.f * SB), SC);
-            const size_t cell = (size_t)(s0 + si) * n_strips + strip;
+            const size_t cell = (size_t)(s0 + si - seg0) * n_strips + strip;
             for (int mw = warp; mw < kMxWarps; mw += kStripWarps) {
                 const float* Mw = M + ((size_t)mw * kFarNodes + (lane & (kFarNodes - 1))) * kCtaNodes;
                 float g = 0.f;
@@ -872,7 +872,7 @@ __global__ void __launch_bounds__(kMxThreads, ANY_LM ? 1 : 2) linesum_mixed_kern
     const SegDev* __restrict__ segs, const int* __restrict__ seg_count, const int2* __restrict__ pl_segs,
     LpOutMixed lp, long long n_nu, float cut_g, float* __restrict__ tau, unsigned long long* __restrict__ evald,
     double* __restrict__ pert, long long pstride, const float* __restrict__ sfar, const int4* __restrict__ sranges,
-    int n_strips) {
+    int n_strips, int pl0, int seg0) {
     extern __shared__ __align__(16) unsigned char mx_smem[];
     WarpTile* tiles = reinterpret_cast<WarpTile*>(mx_smem);
     FarTable& ftab = *reinterpret_cast<FarTable*>(mx_smem + sizeof(WarpTile) * kMxWarps);
@@ -881,7 +881,7 @@ __global__ void __launch_bounds__(kMxThreads, ANY_LM ? 1 : 2) linesum_mixed_kern
         __syncthreads();
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int pl = blockIdx.y;
+    const int pl = pl0 + (int)blockIdx.y;  // the launch's profile-layers start at pl0, its strip cells at seg0
     const long long wb = (long long)blockIdx.x * kMxStrip + (long long)warp * kMxWarpPts;
     if (wb >= n_nu) return;  // no block-wide barriers below: whole warps may leave
     const float xn = FAR ? (float)far_node(lane & (kFarNodes - 1)) : 0.f;
@@ -902,7 +902,7 @@ __global__ void __launch_bounds__(kMxThreads, ANY_LM ? 1 : 2) linesum_mixed_kern
             int4 sx = make_int4(0, 0, 0, 0);  // no strip far field: the whole window
             float gn = 0.f;
             if (FAR && sfar) {
-                const size_t cell = (size_t)s * n_strips + blockIdx.x;
+                const size_t cell = (size_t)(s - seg0) * n_strips + blockIdx.x;
                 sx = sranges[cell];
                 gn = sfar[cell * kStripWords + warp * kFarNodes + (lane & (kFarNodes - 1))];
             }

@@ -293,3 +293,26 @@ def test_far_field_fine_grid_core_reach(pkg, ctx):
                                             x_far=400.0, precision=prec)
     assert np.all(np.isfinite(out["mixed"])) and np.all(out["mixed"] > 150)
     assert np.max(np.abs(out["mixed"] - out["mixed_direct"])) < 1e-3
+
+
+def test_strip_far_field_batch_groups(pkg, ctx, monkeypatch):
+    """The strip far field keeps its node values in a buffer of bounded size
+    (IRS_STRIP_BUFFER_BYTES at context creation); a batch whose (segment, strip) cells
+    exceed it runs the line sum in groups of profile-layers, with the same brightness
+    temperatures as one launch.  A buffer too small for one profile-layer leaves the
+    strip far field out (the warps take their whole windows): within 1e-3 K."""
+    lists = pkg.synthetic.lists_5k_co2()
+    snd = pkg.Sounder.make(660.0, 680.0, 0.25, opd_max=2.0, fwhm_gauss=0.5)
+    profs, _ = pkg.synthetic.perturbed_profiles(3)
+    kw = dict(sounder=snd, internal_dnu=0.0025, precision="mixed")
+    _, _, bt1 = pkg.forward_model_batch(profs, lists, backend=ctx, **kw)
+    out = {}
+    for limit in (5 * 30 * 528, 100):  # a few profile-layers of at most 30 strips; less than one
+        monkeypatch.setenv("IRS_STRIP_BUFFER_BYTES", str(limit))
+        c2 = pkg.B200Context()
+        try:
+            _, _, out[limit] = pkg.forward_model_batch(profs, lists, backend=c2, **kw)
+        finally:
+            c2.close()
+    assert np.array_equal(out[5 * 30 * 528], bt1)
+    assert np.max(np.abs(out[100] - bt1)) < 1e-3
