@@ -638,7 +638,14 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
     for (auto& l : ctx->lists) total_lines += l.n;
     const size_t per_prof = (size_t)L * total_lines * 96 + (size_t)n_out * L * n_nu * 4 + (size_t)n_state * n_nu * 4 +
                             (size_t)n_nu * 8 + (size_t)n_state * n_ch * 4;
-    const int chunk = profiles_per_pass(ctx, n_prof, L, per_prof);
+    int chunk = profiles_per_pass(ctx, n_prof, L, per_prof);
+    if (o.method == 3) {  // the strip far field's node values of a pass fit its buffer
+        int n_lists = 0;
+        for (auto& l : ctx->lists) n_lists += l.n > 0 ? 1 : 0;
+        const size_t strip_prof = (size_t)L * std::max(n_lists, 1) * (size_t)((n_nu + kJgStrip - 1) / kJgStrip) *
+                                  (kJgStripWords * sizeof(float) + sizeof(int4));
+        chunk = std::max(1, std::min<int>(chunk, (int)std::min<size_t>(ctx->strip_buf_max / strip_prof, n_prof)));
+    }
     std::vector<float> Kf;
     for (int p0 = 0; p0 < n_prof; p0 += chunk) {
         const int np = std::min(chunk, n_prof - p0);
@@ -739,12 +746,13 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
             const dim3 g2((unsigned)((n_nu + kJgStrip - 1) / kJgStrip), np * L);
             const float cut_g = (float)(o.cutoff / ig.dnu_hi);
             const bool lm = o.line_mixing == 1;
-            // strip far field (pre-pass): 1808 bytes per (segment, strip), skipped past 2 GiB
+            // strip far field (pre-pass): 1808 bytes per (segment, strip); the profile passes
+            // are sized so a pass fits ctx->strip_buf_max (a single profile beyond it runs without)
             float* d_sfar = nullptr;
             int4* d_srng = nullptr;
             const int n_strips = (int)g2.x;
             const size_t cells = (size_t)nseg * n_strips;
-            if (o.method == 3 && cells * (kJgStripWords * sizeof(float) + sizeof(int4)) <= ((size_t)2 << 30)) {
+            if (o.method == 3 && cells * (kJgStripWords * sizeof(float) + sizeof(int4)) <= ctx->strip_buf_max) {
                 char* b = (char*)workspace(ctx, "jg_strip", cells * (kJgStripWords * sizeof(float) + sizeof(int4)));
                 d_sfar = (float*)b;
                 d_srng = (int4*)(b + cells * kJgStripWords * sizeof(float));
