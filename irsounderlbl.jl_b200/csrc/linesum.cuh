@@ -471,14 +471,16 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
     // node l % 8 over every fourth far line
     float farS = 0.f, farC = 0.f, farDS = 0.f, farDC = 0.f;
     // with the far field, each lane accumulates its own lines' pedestal quadratics
-    // (compensated) and the warp reduces them once per segment, so tiles holding only
-    // far lines need no per-point work
+    // A p^2 - 2 B p + C and the warp reduces them once per segment, so tiles holding only
+    // far lines need no per-point work.  B and C are compensated; A is a plain sum: with
+    // c1 = P / cut^2 and c0 = -2 P, A p^2 is below p^2 / (2 cut^2) of C at the block's
+    // points, so its rounding does not reach the result
     float PA = 0.f, PAc = 0.f, PB = 0.f, PBc = 0.f, PC = 0.f, PCc = 0.f;
     // without line mixing each lane evaluates its own far lines at the 8 nodes and
     // accumulates them here (reduced across the warp once)
-    float fnode[kFarNodes];
+    float2 fnode[kFarNodes / 2];  // nodes (2h, 2h + 1)
 #pragma unroll
-    for (int k = 0; k < kFarNodes; ++k) fnode[k] = 0.f;
+    for (int h = 0; h < kFarNodes / 2; ++h) fnode[h] = make_float2(0.f, 0.f);
     const unsigned lt = (1u << lane) - 1u;
     // the window without the strip far field's ranges [sx.x, sx.y) and [sx.z, sx.w):
     // [ilo, ra), [rb, rc) and [rd, ihi), walked in turn (indices within a segment fit
@@ -534,14 +536,13 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
                     const float2 es = __ffma2_rn(ds, ds, b2);                       // (e[k+1], e[k])
                     const float R = rcp_fast(es.x * es.y);
                     const float2 r = __fmul2_rn(es, make_float2(R, R));             // (1/e[k], 1/e[k+1])
-                    fnode[k] = fmaf(aa.x, r.x, fnode[k]);
-                    fnode[k + 1] = fmaf(aa.y, r.y, fnode[k + 1]);
+                    fnode[k / 2] = __ffma2_rn(aa, r, fnode[k / 2]);
                 }
             }
             const unsigned nfar = __popc(__ballot_sync(kFull, cls == 3));
             if (lane == 0) work += (unsigned long long)nfar * kFarNodes;
             if (__all_sync(kFull, cls == 3 || cls == 0)) {
-                kahan_add(PA, PAc, pa);
+                PA += pa;
                 kahan_add(PB, PBc, pb);
                 kahan_add(PC, PCc, pc);
                 continue;
@@ -603,7 +604,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
         }
         float A = 0.f, B = 0.f, Cc = 0.f;
         if (FAR) {
-            kahan_add(PA, PAc, pa);
+            PA += pa;
             kahan_add(PB, PBc, pb);
             kahan_add(PC, PCc, pc);
         } else {
@@ -779,7 +780,8 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
         float Fn[kFarNodes], Dn[kFarNodes];
 #pragma unroll
         for (int k = 0; k < kFarNodes; ++k) {
-            Fn[k] = LM ? __shfl_sync(kFull, farS, k) : warp_sum(fnode[k]) + __shfl_sync(kFull, gnode, k);
+            Fn[k] = LM ? __shfl_sync(kFull, farS, k)
+                       : warp_sum((k & 1) ? fnode[k / 2].y : fnode[k / 2].x) + __shfl_sync(kFull, gnode, k);
             Dn[k] = LM ? __shfl_sync(kFull, farDS, k) : 0.f;
         }
         const float A = warp_sum(PA - PAc), B = warp_sum(PB - PBc), Cc = warp_sum(PC - PCc);
