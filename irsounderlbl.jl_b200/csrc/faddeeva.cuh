@@ -128,7 +128,7 @@ __device__ __forceinline__ float2 cmul32(float2 a, float2 b) {
     return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 
-static __device__ __noinline__ float2 faddeeva32(float x, float y) {
+__device__ __forceinline__ float2 faddeeva32_inline(float x, float y) {
     const float s = fabsf(x) + y;
     const float2 z = make_float2(x, y);
     if (s >= 8.0f) {
@@ -153,6 +153,8 @@ static __device__ __noinline__ float2 faddeeva32(float x, float y) {
     const float2 t2 = cdiv32(make_float2((float)kInvSqrtPi, 0.0f), den);
     return make_float2(t1.x + t2.x, t1.y + t2.y);
 }
+// the same as a call (per-point loops, where inlining it would cost registers)
+static __device__ __noinline__ float2 faddeeva32(float x, float y) { return faddeeva32_inline(x, y); }
 
 // 1/x by the MUFU approximation (about 1 ulp); x > 0 and finite where it is used
 __device__ __forceinline__ float rcp_approx32(float x) {

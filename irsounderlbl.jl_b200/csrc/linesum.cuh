@@ -646,7 +646,7 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
                 const int4 r = T.sr[lo];
                 const float4 u = T.su[lo], w = T.sq[lo];
                 const float d = ((float)(r.x + (e - r.z)) - u.x) - u.y;  // as in the per-point loop
-                T.cw[e] = faddeeva32(d * w.x, w.y);
+                T.cw[e] = faddeeva32_inline(d * w.x, w.y);
             }
             __syncwarp();
         }
