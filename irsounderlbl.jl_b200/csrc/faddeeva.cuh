@@ -81,12 +81,16 @@ static __device__ __noinline__ double2 faddeeva64(double x, double y) {
 }
 
 // erfcx(y) = w(i y) for real y >= 0 (the DPTMIN peak, voigt.jl:345); the same two
-// methods as faddeeva64 restricted to the imaginary axis, in real arithmetic.
+// methods as faddeeva64 restricted to the imaginary axis, in real arithmetic.  The
+// continued fraction converges faster as y grows: 12 levels for y >= 8, 8 for y >= 15,
+// 6 for y >= 26, 5 for y >= 40 and 4 for y >= 60 agree with 24 levels to within an
+// ulp (checked in double precision over y in [8, 1e6]).
 static __device__ double erfcx64(double y) {
     if (y >= 8.0) {
+        const int K = y >= 60.0 ? 4 : y >= 40.0 ? 5 : y >= 26.0 ? 6 : y >= 15.0 ? 8 : 12;
         double rho = 0.0;
 #pragma unroll 1
-        for (int k = 24; k >= 1; --k) rho = -(0.5 * k) / (y - rho);
+        for (int k = K; k >= 1; --k) rho = -(0.5 * k) / (y - rho);
         return kInvSqrtPi / (y - rho);
     }
     const double L = c_fad.w64_L;
