@@ -215,18 +215,21 @@ __device__ __forceinline__ void jg_wing_coeffs(const float4& a0, const float4& a
     const float An = a0.x, fx = a0.y, y = a0.z, Hc = a0.w;
     const float AnT = a1.x, fxT = a1.y, yT = a1.z, HcT = a1.w;
     const float yp = a2.x, up = a2.y, Hcp = a2.z, yv = a3.x, uv = a3.y, Hcv = a3.z;
-    const float gg = 1.f / (fx * fx), b2 = y * y * gg, Aky = An * k * y;
+    // 1/fx by the MUFU reciprocal (about 1 ulp) instead of IEEE divisions: these are
+    // far-wing coefficients of an FP32 sum
+    const float ifx = rcp_fast(fx);
+    const float gg = ifx * ifx, b2 = y * y * gg, Aky = An * k * y;
     fu = make_float4(0.f, 0.f, b2, Aky * gg);
-    const float r_fx = fxT / fx;
+    const float r_fx = fxT * ifx;
     fT = make_float4(gg * k * (AnT * y + An * yT) - 2.f * Aky * r_fx * gg,
                      2.f * Aky * b2 * r_fx * gg - 2.f * An * k * yT * b2 * gg, An * k * yp * gg,
                      -2.f * An * k * yp * b2 * gg);
     fp = make_float4(2.f * Aky * up * gg, An * k * yv * gg, -2.f * An * k * yv * b2 * gg, 2.f * Aky * uv * gg);
     if (LM) {
         const float Yw = a4.x, YwT = a4.y, Ywp = a4.z;
-        fL0 = make_float4(Yw * k / fx, YwT * k / fx - Yw * k * gg * fxT,
-                          2.f * Yw * k * gg * fxT * b2 - 2.f * Yw * k * y * fx * yT * gg * gg, Ywp * k / fx);
-        fL1 = make_float4(Yw * k * up / fx, -2.f * Yw * k * up * b2 / fx, -2.f * Yw * k * y * fx * yp * gg * gg, 0.f);
+        fL0 = make_float4(Yw * k * ifx, YwT * k * ifx - Yw * k * gg * fxT,
+                          2.f * Yw * k * gg * fxT * b2 - 2.f * Yw * k * y * fx * yT * gg * gg, Ywp * k * ifx);
+        fL1 = make_float4(Yw * k * up * ifx, -2.f * Yw * k * up * b2 * ifx, -2.f * Yw * k * y * fx * yp * gg * gg, 0.f);
     }
     // pedestals: -P0 pf, -PT pf, -An Hc pf_p - An Hc_p pf, ... with pf = 2 - (i - u)^2 / c^2
     P[0] = An * Hc;
