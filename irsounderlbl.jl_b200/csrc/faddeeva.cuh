@@ -12,7 +12,9 @@
 //         Weideman (1994, SIAM J. Numer. Anal. 31:1497) rational series, N = 40.
 //   FP32: continued fraction with 2 levels for |x| + y >= 15, 4 levels for
 //         8 <= |x| + y < 15, else the Weideman series with N = 16.  Worst error
-//         against scipy.special.wofz is ~4e-7 of the line-centre value H(0, y).
+//         against scipy.special.wofz is ~4e-7 of the line-centre value H(0, y); on a
+//         B200 against faddeeva64 over x in [-20, 20], y in [1e-4, 30]: 4.5e-7, the
+//         same with the MUFU reciprocals in cdiv32 as with correctly rounded ones.
 // The series coefficients are the DFT of exp(-t^2)(L^2 + t^2) at
 // t = L tan(theta/2), computed once on the host (irs_host.cpp) and held in
 // constant memory.
@@ -124,8 +126,16 @@ __device__ __forceinline__ double hcore64(double x, double y) {
 }
 
 // ---------------------------------------------------------------- FP32
+// 1/x by the MUFU approximation (about 1 ulp); x > 0 and finite where it is used
+__device__ __forceinline__ float rcp_approx32(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// a / b; |b|^2 is a normal FP32 number wherever it is used (|b| between about 1 and 30)
 __device__ __forceinline__ float2 cdiv32(float2 a, float2 b) {
-    const float inv = __frcp_rn(b.x * b.x + b.y * b.y);
+    const float inv = rcp_approx32(b.x * b.x + b.y * b.y);
     return make_float2((a.x * b.x + a.y * b.y) * inv, (a.y * b.x - a.x * b.y) * inv);
 }
 __device__ __forceinline__ float2 cmul32(float2 a, float2 b) {
@@ -160,12 +170,6 @@ __device__ __forceinline__ float2 faddeeva32_inline(float x, float y) {
 // the same as a call (per-point loops, where inlining it would cost registers)
 static __device__ __noinline__ float2 faddeeva32(float x, float y) { return faddeeva32_inline(x, y); }
 
-// 1/x by the MUFU approximation (about 1 ulp); x > 0 and finite where it is used
-__device__ __forceinline__ float rcp_approx32(float x) {
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
 
 // Faddeeva w(z) for |x| + y >= 15 by the two-level Laplace continued fraction of
 // faddeeva32 (w = i/sqrt(pi) / (z - 1/2 / (z - 1/z))), written out in real arithmetic

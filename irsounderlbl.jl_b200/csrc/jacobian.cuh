@@ -155,7 +155,7 @@ __device__ __forceinline__ void jg_pair(float d, bool core, const float4& q0, co
         }
     } else {
         const float e = fmaf(x, x, y * y);
-        const float r = __frcp_rn(e);
+        const float r = rcp_approx32(e);
         const float r2 = r * r;
         const float k = (float)kInvSqrtPi;
         H = y * k * r;
