@@ -363,16 +363,20 @@ int irs_last_stage_times(irs_ctx* ctx, irs_stage_times* out);
 /* No counterpart in the reference.  compute_voigt_cross_sections in FP64 for callers
  * that cannot allocate device memory (hosts whose allocator already owns the device,
  * such as a CUDA.jl memory pool, or hosts that forbid allocation after start-up):
- * it allocates nothing.  d_lines (56-byte records sorted by wavenumber), d_tips_q
- * (Q(T) at 1 K from tips_t_min, or NULL for Q proportional to T), d_grid and d_sigma
- * are device pointers owned by the caller; the work is queued on `stream`.  At most
- * 131072 lines (IRS_E_ARG beyond).  Its per-line scratch is one file-scope device
- * array shared by all calls, so calls that overlap on the GPU race; the first call
- * on each device does a one-time set-up and should come before any stream capture. */
+ * it allocates nothing.  d_lines (56-byte records sorted by wavenumber), d_tips_q,
+ * d_grid and d_sigma are device pointers owned by the caller; the work is queued on
+ * `stream`.  d_tips_q holds n_tips TIPS tables packed one after another, each Q(T) at
+ * tips_n temperatures 1 K apart from tips_t_min; tips_keys (host) gives the (mol, iso)
+ * of table k at [2k], [2k + 1].  Each line takes the table of its own (mol, iso)
+ * (Q_ratio, partition.jl:41-47) and Q proportional to T when none matches or d_tips_q
+ * is NULL.  At most 131072 lines and 64 tables (IRS_E_ARG beyond).  Its per-line
+ * scratch is one file-scope device array shared by all calls, so calls that overlap on
+ * the GPU race; the first call in each CUDA context does a one-time set-up and should
+ * come before any stream capture; after cudaDeviceReset reload the library. */
 int irs_cross_sections_noalloc(const irs_line* d_lines, int64_t n_lines, const double* d_tips_q,
-                               int tips_t_min, int tips_n, const double* d_grid, int64_t n_nu,
-                               double T, double p_atm, double vmr_self, double cutoff, int method,
-                               double x_far, double* d_sigma, void* stream);
+                               const int32_t* tips_keys, int n_tips, int tips_t_min, int tips_n,
+                               const double* d_grid, int64_t n_nu, double T, double p_atm, double vmr_self,
+                               double cutoff, int method, double x_far, double* d_sigma, void* stream);
 
 /* ------------------------------------------------------------------------------
  * MLP surrogate of forward_model.  No counterpart in the reference: it maps a

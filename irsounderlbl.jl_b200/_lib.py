@@ -116,9 +116,9 @@ SIGNATURES = {
                       C.POINTER(C.c_int32), C.POINTER(C.c_int32), _PD], C.c_int),
     "irs_synchronize": ([_P], C.c_int),
     "irs_last_stage_times": ([_P, C.POINTER(StageTimes)], C.c_int),
-    "irs_cross_sections_noalloc": ([_P, C.c_int64, _P, C.c_int, C.c_int, _P, C.c_int64, C.c_double,
-                                    C.c_double, C.c_double, C.c_double, C.c_int, C.c_double, _P, _P],
-                                   C.c_int),
+    "irs_cross_sections_noalloc": ([_P, C.c_int64, _P, C.POINTER(C.c_int32), C.c_int, C.c_int, C.c_int, _P,
+                                    C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                    C.c_double, _P, _P], C.c_int),
     "irs_surrogate_create": ([_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)],
                              C.c_int),
     "irs_surrogate_destroy": ([_P], C.c_int),

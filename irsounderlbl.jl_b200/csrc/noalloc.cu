@@ -6,17 +6,25 @@
 // whose CUDA.jl memory pool owns the device and hands this library only the input and
 // output buffers), real-time or embedded hosts that forbid allocation after start-up,
 // and plug-ins that may not grow a process's device footprint.  The caller passes the
-// line list, the TIPS table, the grid and the output as device pointers; the per-line
+// line list, the TIPS tables, the grid and the output as device pointers; the per-line
 // parameters go to the file-scope array below instead of a context workspace.
+//
+// TIPS: the caller passes up to kNoAllocMaxTips tables packed one after another on the
+// device (all on the same 1 K temperature grid) and, on the host, the (mol, iso) of
+// each.  Every line takes the table of its own (mol, iso), as Q_ratio does
+// (partition.jl:41-47); a line whose (mol, iso) has no table takes Q proportional to T,
+// the reference's fallback.
 //
 // The array is sized for kNoAllocMaxLines lines (5 doubles each, about 5.2 MB) and
 // every GPU that loads this library holds it until the process exits.  Every call
 // shares it, so calls that overlap on the GPU (concurrent streams, or host threads
 // using different streams) race on it: serialise them.  Its contents persist between
-// calls; each call rewrites all the entries it reads.  The first call on each device
-// performs a one-time set-up (it looks up the array's device address with
+// calls; each call rewrites all the entries it reads.  The first call in each CUDA
+// context performs a one-time set-up (it looks up the array's device address with
 // cudaGetSymbolAddress and uploads the Faddeeva constants); make that first call
-// before any stream capture.
+// before any stream capture.  The set-up is remembered per context: after
+// cudaDeviceReset (which destroys the context and the array's contents with it) the
+// process must reload this library before calling it again.
 #include <cuda_runtime.h>
 
 #include <map>
@@ -28,6 +36,13 @@
 namespace irs {
 
 constexpr long long kNoAllocMaxLines = 1LL << 17;  // 131,072 lines
+constexpr int kNoAllocMaxTips = 64;                // TIPS tables per call
+
+// the (mol, iso) of each packed TIPS table, by value in the kernel's parameters
+struct NoAllocTips {
+    int mol[kNoAllocMaxTips], iso[kNoAllocMaxTips];
+    int n_tab, tmin, n;
+};
 
 struct NoAllocScratch {
     double nu0[kNoAllocMaxLines];
@@ -56,7 +71,7 @@ __device__ double na_mass(int mol) {  // broadening.jl:131-148
 
 // per-line parameters (voigt.jl:402-454) from the caller's 56-byte line records
 __global__ void na_params_kernel(const irs_line* __restrict__ lines, long long n, const double* __restrict__ q,
-                                 int tmin, int nq, double T, double p, double vs, double cutoff, int method,
+                                 NoAllocTips tt, double T, double p, double vs, double cutoff, int method,
                                  double x_far, NoAllocScratch* __restrict__ s) {
     const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
@@ -69,7 +84,11 @@ __global__ void na_params_kernel(const irs_line* __restrict__ lines, long long n
     const double gl = pow(tr, n_air) * (double)l.air_broad * (1.0 - vs) * p +
                       pow(tr, n_self) * (double)l.self_broad * vs * p;
     const double gd = fmax(l.wavenumber * 3.58126e-7 * sqrt(T / na_mass(mol)), 1e-10);
-    const double Qr = q ? na_tips(q, tmin, nq, 296.0) / na_tips(q, tmin, nq, T) : 296.0 / T;
+    int tab = -1;  // this line's (mol, iso) table, partition.jl:41-47
+    for (int k = 0; q && k < tt.n_tab; ++k)
+        if (tt.mol[k] == mol && tt.iso[k] == (int)l.iso_id) { tab = k; break; }
+    const double* qt = tab >= 0 ? q + (size_t)tab * tt.n : nullptr;
+    const double Qr = qt ? na_tips(qt, tt.tmin, tt.n, 296.0) / na_tips(qt, tt.tmin, tt.n, T) : 296.0 / T;
     const double c2 = 1.4387752;
     const double S = l.intensity * Qr * exp(-c2 * l.lower_energy * (1.0 / T - 1.0 / 296.0)) *
                      (1.0 - exp(-c2 * l.wavenumber / T)) / (1.0 - exp(-c2 * l.wavenumber / 296.0));
@@ -133,22 +152,41 @@ __global__ void na_sum_kernel(const NoAllocScratch* __restrict__ s, long long n,
     sigma[i] = fmax(acc, 0.0);
 }
 
-// Device address of the scratch array and the Faddeeva constants, once per device.
+// Device address of the scratch array and the Faddeeva constants, once per CUDA
+// context (the current one, as the driver reports it).
 std::mutex g_mu;
-std::map<int, NoAllocScratch*> g_addr;
+std::map<void*, NoAllocScratch*> g_addr;
 
-NoAllocScratch* scratch_for_current_device() {
-    int dev = 0;
+void* current_context() {
+    typedef int (*GetCtx)(void**);  // CUresult cuCtxGetCurrent(CUcontext*)
+    static GetCtx fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult r;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &r) != cudaSuccess ||
+            r != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return (GetCtx)p;
+    }();
+    if (!fn) throw Error{IRS_E_CUDA, "cuCtxGetCurrent is not available from the driver"};
+    int dev = 0;  // cudaSetDevice makes the device's primary context current
     IRS_CUDA(cudaGetDevice(&dev));
+    IRS_CUDA(cudaSetDevice(dev));
+    void* c = nullptr;
+    if (fn(&c) != 0 || !c) throw Error{IRS_E_CUDA, "no current CUDA context"};
+    return c;
+}
+
+NoAllocScratch* scratch_for_current_context() {
+    void* cx = current_context();
     std::lock_guard<std::mutex> lock(g_mu);
-    auto it = g_addr.find(dev);
+    auto it = g_addr.find(cx);
     if (it != g_addr.end()) return it->second;
     void* ptr = nullptr;
     IRS_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
     FaddeevaConsts fc;
     compute_faddeeva_consts(&fc);
     IRS_CUDA(cudaMemcpyToSymbol(c_fad, &fc, sizeof fc));
-    g_addr[dev] = (NoAllocScratch*)ptr;
+    g_addr[cx] = (NoAllocScratch*)ptr;
     return (NoAllocScratch*)ptr;
 }
 
@@ -156,9 +194,10 @@ NoAllocScratch* scratch_for_current_device() {
 }  // namespace irs
 
 extern "C" int irs_cross_sections_noalloc(const irs_line* d_lines, int64_t n_lines, const double* d_tips_q,
-                                          int tips_t_min, int tips_n, const double* d_grid, int64_t n_nu,
-                                          double T, double p_atm, double vmr_self, double cutoff, int method,
-                                          double x_far, double* d_sigma, void* stream) {
+                                          const int32_t* tips_keys, int n_tips, int tips_t_min, int tips_n,
+                                          const double* d_grid, int64_t n_nu, double T, double p_atm,
+                                          double vmr_self, double cutoff, int method, double x_far,
+                                          double* d_sigma, void* stream) {
     using namespace irs;
     try {
         IRS_REQUIRE(n_lines >= 0 && n_lines <= kNoAllocMaxLines,
@@ -166,12 +205,23 @@ extern "C" int irs_cross_sections_noalloc(const irs_line* d_lines, int64_t n_lin
         IRS_REQUIRE(n_nu >= 1 && d_grid && d_sigma && (n_lines == 0 || d_lines), "invalid arguments");
         IRS_REQUIRE(method >= 1 && method <= 3, "method must be 1 (Weideman), 2 (PseudoVoigt) or 3 (FullFaddeeva)");
         IRS_REQUIRE(T > 0.0 && p_atm >= 0.0 && cutoff > 0.0, "T and cutoff must be positive, p_atm non-negative");
-        IRS_REQUIRE(!d_tips_q || tips_n >= 2, "the TIPS table needs at least two points");
-        NoAllocScratch* s = scratch_for_current_device();
+        IRS_REQUIRE(n_tips >= 0 && n_tips <= kNoAllocMaxTips,
+                    "irs_cross_sections_noalloc: at most 64 TIPS tables per call");
+        IRS_REQUIRE(!d_tips_q || n_tips == 0 || (tips_keys && tips_n >= 2),
+                    "the TIPS tables need their (mol, iso) keys and at least two points each");
+        NoAllocTips tt{};
+        tt.n_tab = d_tips_q ? n_tips : 0;
+        tt.tmin = tips_t_min;
+        tt.n = tips_n;
+        for (int k = 0; k < tt.n_tab; ++k) {
+            tt.mol[k] = tips_keys[2 * k];
+            tt.iso[k] = tips_keys[2 * k + 1];
+        }
+        NoAllocScratch* s = scratch_for_current_context();
         cudaStream_t st = (cudaStream_t)stream;
         if (n_lines > 0)
             na_params_kernel<<<(unsigned)((n_lines + 255) / 256), 256, 0, st>>>(
-                d_lines, n_lines, d_tips_q, tips_t_min, tips_n, T, p_atm, vmr_self, cutoff, method, x_far, s);
+                d_lines, n_lines, d_tips_q, tt, T, p_atm, vmr_self, cutoff, method, x_far, s);
         const unsigned g = (unsigned)((n_nu + 255) / 256);
         if (method == 1) na_sum_kernel<1><<<g, 256, 0, st>>>(s, n_lines, d_grid, n_nu, cutoff, x_far, d_sigma);
         else if (method == 2) na_sum_kernel<2><<<g, 256, 0, st>>>(s, n_lines, d_grid, n_nu, cutoff, x_far, d_sigma);
