@@ -1,6 +1,6 @@
 """Regenerate the bundled physical tables in this folder from an IRSounderLBL.jl checkout.
 
-Usage:  python extract_tables.py /root/reference
+Usage:  python extract_tables.py <path of an IRSounderLBL.jl checkout>
 
 What it writes (next to this script):
 
@@ -48,4 +48,6 @@ def main(ref: Path):
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python extract_tables.py <path of an IRSounderLBL.jl checkout>")
+    main(Path(sys.argv[1]))
