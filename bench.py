@@ -45,6 +45,18 @@ def _package():
     return ge._package()
 
 
+# metric, unit and workload description shared by both arms (the driver compares the
+# two lines only when they agree)
+METRIC = "IASI spectra/s (line-by-line forward_model, 400k lines)"
+
+
+def workload_config():
+    return {"workload": "iasi-400k", "lines": 400000, "species": 6, "grid_dnu": 0.0025, "n_nu": 858801,
+            "layers": 49, "channels": 8461, "profiles": "the 6 AFGL 50-level profiles", "method": "FullFaddeeva",
+            "cutoff": 25.0, "dptmn": 1e-6, "continua": "h2o,co2",
+            "l2": "working set (line parameters ~4 GB, tau 1 GB) >> L2"}
+
+
 def _workload_kw():
     return dict(internal_dnu=0.0025, cutoff=25.0, dptmn=1e-6, apply_continuum=True,
                 with_ils=True, apodization="gaussian", T_method="logp_at_pcg",
@@ -170,12 +182,11 @@ def reference_arm(args, rank):
     t = sum(ts) / len(ts)
     v = n_pts / n_full / t
     line = {
-        "impl": "reference", "metric": "IASI spectra/s (line-by-line forward_model, 400k lines)",
+        "impl": "reference", "metric": METRIC,
         "value": v, "unit": "spectra/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded line lists, AFGL profiles)",
-        "config": {"workload": "iasi-400k", "lines": 400000, "species": 6, "grid_dnu": 0.0025,
-                   "n_nu": n_full, "layers": 49, "profiles_per_step": 1, "method": "FullFaddeeva"},
+        "config": workload_config(),
         "cpu_baseline": {"value": v, "unit": "spectra/s", "cores": cores, "kind": "port",
                          "sample": f"one AFGL profile, channels {c0}..{c0 + n_ch - 1} ({n_pts} internal grid "
                                    f"points of {n_full}), scaled by grid points"},
@@ -542,37 +553,48 @@ def main():
     far_max = float(dd.abs().max().item())
 
     if rank == 0:
+        plain_d = {"value": plain, "unit": "spectra/s", "ms_per_step": ms64, "mixed_over_plain": value / plain}
+        direct_d = {"value": world * N_PROF / (ms_d / 1e3), "unit": "spectra/s", "ms_per_step": ms_d,
+                    "bt_far_field_vs_direct_max_K": far_max}
         line = {
-            "metric": "IASI spectra/s (line-by-line forward_model, 400k lines, mixed FP32+Kahan, "
-                      "far wings interpolated from Chebyshev nodes)",
+            "metric": METRIC,
             "value": value, "unit": "spectra/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32+kahan (fp64 transmittance/RTE)",
+            "vs_baseline": None, "dtype": "f32+kahan (fp64 cumulative optical depth and transmittance)",
             "data": "synthetic (seeded line lists, AFGL profiles)",
-            "config": {"workload": "iasi-400k", "lines": 400000, "species": 6, "grid_dnu": 0.0025,
-                       "n_nu": 858801, "layers": 49, "channels": nch, "profiles_per_step_per_gpu": N_PROF,
-                       "method": "FullFaddeeva", "cutoff": 25.0, "dptmn": 1e-6,
-                       "continua": "h2o,co2", "l2": "working set (line parameters ~4 GB, tau 1 GB) >> L2"},
-            "plain_fp64": {"value": plain, "unit": "spectra/s", "ms_per_step": ms64,
-                           "mixed_over_plain": value / plain},
-            "bt_mixed_vs_fp64_K": {"rms": bt_rms, "max": bt_max},
-            "mixed_direct": {"value": world * N_PROF / (ms_d / 1e3), "unit": "spectra/s", "ms_per_step": ms_d,
-                             "bt_far_field_vs_direct_max_K": far_max},
-            "stages_ms": acc,
+            "config": workload_config(),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "linesum_mixed_kernel<3>",
-                         "work": {"pairs": pairs, "evaluated_pairs": evald, "core_pairs": core,
-                                  "far_flops": FAR_PAIR_FLOPS, "core_flops": CORE_PAIR_FLOPS,
-                                  "algorithmic_pairs_per_s": pairs / t_ls},
+                         "algorithmic_pairs_per_s": pairs / t_ls,
                          "peak_source": "148 SMs x 128 FP32 lanes x 2 FLOP x median sampled SM clock "
-                                        "(MEASURED_PEAKS.json has no FP32 figure)"},
+                                        "(MEASURED_PEAKS.json has no FP32 figure)",
+                         # the comparators of the headline, as scalars
+                         "plain_fp64_spectra_per_s": plain, "mixed_over_plain_fp64": value / plain,
+                         "mixed_direct_spectra_per_s": direct_d["value"],
+                         "bt_rms_mixed_vs_fp64_K": bt_rms, "bt_max_mixed_vs_fp64_K": bt_max,
+                         "bt_max_far_field_vs_direct_K": far_max,
+                         "work": {"pairs": pairs, "evaluated_pairs": evald, "core_pairs": core,
+                                  "far_flops": FAR_PAIR_FLOPS, "core_flops": CORE_PAIR_FLOPS}},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": clocks,
+            "stages_ms": acc,
+            "profiles_per_step_per_gpu": N_PROF,
         }
+        # the RTE kernel against HBM: it reads the FP32 optical depths once and writes I
+        rte_bytes = N_PROF * 49 * 858801 * 4 + N_PROF * 858801 * 8
+        peaks, psrc = _peaks()
+        line["rte"] = {"kernel": "rte_mixed_kernel", "ms_per_step": acc["rte_ms"], "bytes_per_step": rte_bytes,
+                       "achieved_gbs": rte_bytes / (acc["rte_ms"] / 1e3) / 1e9, "peak_gbs": peaks["hbm_gbs"],
+                       "frac": rte_bytes / (acc["rte_ms"] / 1e3) / 1e9 / peaks["hbm_gbs"],
+                       "peak_source": f"{psrc} hbm_gbs"}
         line.update(extras)
+        # last, so that a cut-off log still shows them
+        line["plain_fp64"] = plain_d
+        line["mixed_direct"] = direct_d
+        line["bt_mixed_vs_fp64_K"] = {"rms": bt_rms, "max": bt_max}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:

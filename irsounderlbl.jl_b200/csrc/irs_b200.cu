@@ -563,12 +563,19 @@ static void forward_pass(irs_ctx* ctx, const irs_profile* profs, int n_prof, con
         if ((o.continua & 2) && ctx->n_co2 > 1) cd.mask |= 2;
     }
     dim3 g3((unsigned)((n_nu + 255) / 256), n_prof);
-    if (o.precision != IRS_FP64)
-        if (cd.mask & kCiaMask)
-            rte_kernel<float, true><<<g3, 256, 0, st>>>((const float*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
-        else
-            rte_kernel<float><<<g3, 256, 0, st>>>((const float*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
-    else
+    if (o.precision != IRS_FP64) {
+        const size_t sm = (size_t)L * sizeof(RteLayerF);
+        IRS_REQUIRE(sm <= 200 * 1024, "too many layers for the RTE kernel (at most 4266)");
+        if (cd.mask & kCiaMask) {
+            if (sm > 48 * 1024)
+                IRS_CUDA(cudaFuncSetAttribute(rte_mixed_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            rte_mixed_kernel<true><<<g3, 256, sm, st>>>((const float*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
+        } else {
+            if (sm > 48 * 1024)
+                IRS_CUDA(cudaFuncSetAttribute(rte_mixed_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            rte_mixed_kernel<false><<<g3, 256, sm, st>>>((const float*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
+        }
+    } else
         if (cd.mask & kCiaMask)
             rte_kernel<double, true><<<g3, 256, 0, st>>>((const double*)d_tau, d_lrt, d_prt, L, d_grid, n_nu, o.source_function, cd, d_I);
         else

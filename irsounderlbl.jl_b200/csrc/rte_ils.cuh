@@ -8,8 +8,10 @@
 //    schwarzschild_rte, :cim and :toon sources    src/Solver/schwarzschild.jl:130-209
 //    add_reflected_downwelling! when eps < 1      schwarzschild.jl:228-274
 //    planck_radiance                              src/Solver/planck.jl:22-24
-//  The per-layer tau is FP32 (mixed) or FP64 (plain); the cumulative transmittance
-//  product and the radiance sum are FP64.
+//  for the plain FP64 path: FP64 throughout.
+//  rte_mixed_kernel is the same for the FP32 optical depths of the mixed path: FP64
+//  only in the cumulative optical depth and the transmittances, FP32 (Kahan-summed
+//  radiance) elsewhere.
 //
 //  ils_bt_kernel (one warp per channel and profile) restates apply_ils
 //  (src/Sensor/ils.jl:131-153) evaluated at the grid nodes that the linear channel
@@ -130,6 +132,14 @@ __device__ __forceinline__ double cia_tau(const ContDev& c, const CiaPoint& cp, 
         k += cia_sigma_at(c.cia, cp, 2, nu, T) * o2 * o2;
     }
     return k * dz;
+}
+
+// compensated FP32 sum: the value is s - c
+__device__ __forceinline__ void kahan_add32(float& s, float& c, float v) {
+    const float y = v - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
 }
 
 __global__ void grid_values_kernel(GridDev g, double* out) {
@@ -266,6 +276,174 @@ __global__ void __launch_bounds__(256) rte_kernel(const TT* __restrict__ tau, co
             g *= exp(-s);
         }
         Iv += (1.0 - pr.eps) * Id * Tr0;
+    }
+    I[(size_t)p * n_nu + i] = Iv;
+}
+
+// ------------------------------------------------------- RTE, mixed precision
+// rte_mixed_kernel: the same radiative transfer as rte_kernel for the FP32 optical
+// depths of the mixed path, with FP64 kept only where the result needs it: the
+// cumulative layer-to-space optical depth and the transmittances exp(-OD) (and the
+// surface-to-layer transmittance of the reflected term).  Planck radiances, the CIM /
+// Toon corrections and the MT-CKD continua are FP32, and the radiance is summed in
+// FP32 with Kahan compensation.  Per (grid point, layer) it reads the FP32 tau once.
+//
+// Per-layer FP32 constants, computed once per CTA from LayerRT into shared memory:
+struct RteLayerF {
+    float c2_ave, c2_top, c2_bot, c2_mid;  // c2 / T
+    float h2o_self, h2o_for, l2_296, co2;  // continuum column factors, log2(296/T_mid)
+    float l2_246, pad0, pad1, pad2;        // log2(T_mid / 246)
+};
+constexpr float kC1 = 1.191042953e-5f, kC2 = 1.4387769f;
+
+// planck_radiance (planck.jl:22-24) with c1 nu^3 and c2/T given: c1 nu^3 / expm1(c2 nu / T);
+// above x = 0.5 exp(x) - 1 loses under one bit, so the cheaper expf serves there
+__device__ __forceinline__ float planck32(float c1nu3, float nu, float c2T) {
+    const float x = nu * c2T;
+    return c1nu3 * __frcp_rn(x > 0.5f ? expf(x) - 1.0f : expm1f(x));
+}
+// _cim_correction (schwarzschild.jl:59-63): s/6 below 0.06 as the reference, then the
+// series 1 - 2 (1/s - 1/(e^s - 1)) = s/6 - s^3/360 + s^5/15120 - ... (next term below
+// 2e-7 of the value for s < 0.5, where the direct form loses digits in FP32), then the
+// direct form
+__device__ __forceinline__ float cim_corr32(float s) {
+    if (s < 0.06f) return s * (1.0f / 6.0f);
+    if (s < 0.5f) {
+        const float s2 = s * s;
+        return s * fmaf(s2, fmaf(s2, 1.0f / 15120.0f, -1.0f / 360.0f), 1.0f / 6.0f);
+    }
+    return 1.0f - 2.0f * (1.0f / s - 1.0f / expm1f(s));
+}
+// _lit_correction (schwarzschild.jl:43-47): (1 - e^-s)/s - e^-s; the reference's series
+// below 1e-4, continued to s^5 below 0.1 (next term s^6/840), then the direct form
+__device__ __forceinline__ float lit_corr32(float s) {
+    if (s < 1e-4f) return s * (0.5f - s * (1.0f / 3.0f - s * 0.125f));
+    if (s < 0.1f)
+        return s * fmaf(s, fmaf(s, fmaf(s, fmaf(s, 1.0f / 144.0f, -1.0f / 30.0f), 0.125f), -1.0f / 3.0f), 0.5f);
+    const float e = __expf(-s);
+    return -expm1f(-s) / s - e;
+}
+// radfn (continuum.jl:169-174) with c2/T given
+__device__ __forceinline__ float radfn32(float nu, float c2T) {
+    const float x = nu * c2T;
+    if (x <= 0.01f) return 0.5f * x * nu;
+    if (x <= 10.0f) {
+        const float e = __expf(-x);
+        return nu * (1.0f - e) / (1.0f + e);
+    }
+    return nu;
+}
+
+template <bool CIA>
+__global__ void __launch_bounds__(256) rte_mixed_kernel(const float* __restrict__ tau, const LayerRT* __restrict__ lrt,
+                                                        const ProfileRT* __restrict__ prt, int L,
+                                                        const double* __restrict__ grid, long long n_nu, int src,
+                                                        ContDev cont, double* __restrict__ I) {
+    extern __shared__ __align__(16) unsigned char rte_smem[];
+    RteLayerF* lc = reinterpret_cast<RteLayerF*>(rte_smem);
+    const int p = blockIdx.y;
+    const LayerRT* lr = lrt + (size_t)p * L;
+    for (int k = threadIdx.x; k < L; k += blockDim.x) {  // layer constants (FP64 -> FP32)
+        const LayerRT r = lr[k];
+        RteLayerF c;
+        c.c2_ave = (float)(1.4387769 / r.T_ave);
+        c.c2_top = (float)(1.4387769 / r.T_top);
+        c.c2_bot = (float)(1.4387769 / r.T_bot);
+        c.c2_mid = (float)(1.4387769 / r.T_mid);
+        const double rho = (r.p_mid / 1013.0) * (296.0 / r.T_mid);
+        const double nh = r.vmr_h2o * r.p_mid * 100.0 / (1.380649e-23 * r.T_mid) * 1e-6;
+        const double nc = r.vmr_co2 * r.p_mid * 100.0 / (1.380649e-23 * r.T_mid) * 1e-6;
+        c.h2o_self = (float)(r.vmr_h2o * rho * nh * r.dz_cm);
+        c.h2o_for = (float)((1.0 - r.vmr_h2o) * rho * nh * r.dz_cm);
+        c.l2_296 = (float)log2(296.0 / r.T_mid);
+        c.co2 = (float)(1e-20 * nc * rho * r.dz_cm);
+        c.l2_246 = (float)log2(r.T_mid / 246.0);
+        c.pad0 = c.pad1 = c.pad2 = 0.f;
+        lc[k] = c;
+    }
+    __syncthreads();
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_nu) return;
+    const double nud = grid[i];
+    const float nu = (float)nud;
+    const float c1nu3 = kC1 * nu * nu * nu;
+    float Cs = 0.f, Cf = 0.f, te = 0.f, Se = 0.f, td = 0.f;
+    if (cont.mask & 1) {
+        const Lerp l = lerp_at(cont.h2o, cont.n_h2o, nud);
+        Cs = (float)lerp_val(cont.h2o + cont.n_h2o, l);
+        Cf = (float)lerp_val(cont.h2o + 2 * cont.n_h2o, l);
+        te = (float)lerp_val(cont.h2o + 3 * cont.n_h2o, l);
+    }
+    if (cont.mask & 2) {
+        const Lerp l = lerp_at(cont.co2, cont.n_co2, nud);
+        Se = (float)lerp_val(cont.co2 + cont.n_co2, l);
+        td = (float)lerp_val(cont.co2 + 2 * cont.n_co2, l);
+    }
+    CiaPoint cp;
+    if (CIA) cia_prepare(cont.cia, cont.mask, nud, cp);
+    const ProfileRT pr = prt[p];
+    const float imu = (float)(1.0 / pr.mu);
+    const float* tp = tau + (size_t)p * L * n_nu + i;
+    // the layer's optical depth along the path (FP32)
+    auto slant = [&](int k) -> float {
+        const RteLayerF& c = lc[k];
+        float t = tp[(size_t)k * n_nu];
+        if (CIA) {
+            const LayerRT r = lr[k];
+            t += (float)cia_tau(cont, cp, nud, r.vmr_h2o, r.vmr_co2, r.p_mid, r.T_mid, r.dz_cm);
+        }
+        if (cont.mask & 3) {
+            const float rad = radfn32(nu, c.c2_mid);
+            float k_c = 0.f;
+            if (cont.mask & 1) k_c = fmaf(Cs * exp2f(te * c.l2_296), c.h2o_self, Cf * c.h2o_for);
+            if (cont.mask & 2) k_c = fmaf(Se * (td == 0.f ? 1.f : exp2f(td * c.l2_246)), c.co2, k_c);
+            t = fmaf(k_c, rad, t);
+        }
+        return t * imu;
+    };
+    double od = 0.0;        // cumulative optical depth from the top of the atmosphere
+    double Tr_up = 1.0;     // transmittance of the level above
+    float Is = 0.f, Ic = 0.f;  // radiance, Kahan-compensated
+    float B_up = planck32(c1nu3, nu, lc[L - 1].c2_top);  // B at the top level of the current layer
+    for (int k = L - 1; k >= 0; --k) {
+        const RteLayerF& c = lc[k];
+        const float s = slant(k);
+        od += (double)s;
+        const double Tr_k = exp(-od);
+        const float dT = (float)(Tr_up - Tr_k);
+        const float B_bot = planck32(c1nu3, nu, c.c2_bot);
+        float v;
+        if (src == 0) {
+            const float Ba = planck32(c1nu3, nu, c.c2_ave);
+            v = fmaf(Ba, dT, (B_up - Ba) * (dT * cim_corr32(s)));
+        } else {
+            v = fmaf(B_up, dT, (B_bot - B_up) * ((float)Tr_up * lit_corr32(s)));
+        }
+        kahan_add32(Is, Ic, v);
+        B_up = B_bot;
+        Tr_up = Tr_k;
+    }
+    const double Tr0 = Tr_up;
+    double Iv = (double)(Is - Ic) + pr.eps * (double)planck32(c1nu3, nu, kC2 / (float)pr.T_sfc) * Tr0;
+    if (pr.eps < 1.0) {  // add_reflected_downwelling!: layers from the surface up
+        float Ds = 0.f, Dc = 0.f;
+        double od_s = 0.0;  // optical depth from the surface to the bottom of layer k
+        for (int k = 0; k < L; ++k) {
+            const RteLayerF& c = lc[k];
+            const float s = slant(k);
+            const float one_m = -expm1f(-s);
+            float em;
+            if (src == 0) {
+                const float Ba = planck32(c1nu3, nu, c.c2_ave), Bb = planck32(c1nu3, nu, c.c2_bot);
+                em = one_m * fmaf(Bb - Ba, cim_corr32(s), Ba);
+            } else {
+                const float Bb = planck32(c1nu3, nu, c.c2_bot), Bt = planck32(c1nu3, nu, c.c2_top);
+                em = fmaf(Bb, one_m, (Bt - Bb) * lit_corr32(s));
+            }
+            kahan_add32(Ds, Dc, (float)exp(-od_s) * em);
+            od_s += (double)s;
+        }
+        Iv += (1.0 - pr.eps) * (double)(Ds - Dc) * Tr0;
     }
     I[(size_t)p * n_nu + i] = Iv;
 }
