@@ -601,9 +601,14 @@ static int64_t state_size(const irs_state_spec& sp, int n_lev) {
 // vmr_jacobian.jl:152-505 for profiles [0, n_prof): K_h [n_prof][n_state][n_ch], y_h [n_prof][n_ch]
 // Outputs: host K_h/y_h (double), or with K_dev non-null the device K_dev (float
 // [n_prof][n_state][n_ch]) and host y_h.
+// With dx_h non-null it computes the pullback dx = K^T dy instead (dy_h [n_prof][n_ch]
+// host, dx_h [n_prof][n_state] host): the derivative line sum as above, then I, R and
+// BT, the radiance cotangent on the grid by the transposed ILS, and one adjoint RTE sweep
+// that contracts each derivative term with it on the device; neither D nor K is formed.
 static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder& s,
                             const irs_fm_options& o_in, const irs_state_spec& sp, double* K_h, double* y_h,
-                            float* K_dev = nullptr) {
+                            float* K_dev = nullptr, const double* dy_h = nullptr, double* dx_h = nullptr) {
+    const bool adjoint = dx_h != nullptr;
     IRS_REQUIRE(n_prof >= 1 && profs, "need at least one profile");
     IRS_REQUIRE(sp.n_retrieved >= 0 && sp.n_retrieved <= 4 && (sp.n_retrieved == 0 || sp.retrieved),
                 "at most 4 retrieved species");
@@ -723,11 +728,12 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
         go.q0 = (float4*)(base + S * 16); go.q1 = (float4*)(base + S * 32); go.q2 = (float4*)(base + S * 48);
         go.q3 = (float4*)(base + S * 64); go.q4 = (float4*)(base + S * 80);
         float* d_out = (float*)workspace(ctx, "jg_out", (size_t)np * L * n_out * n_nu * sizeof(float));
-        float* d_D = (float*)workspace(ctx, "jg_D", (size_t)np * n_state * n_nu * sizeof(float));
+        float* d_D = adjoint ? nullptr : (float*)workspace(ctx, "jg_D", (size_t)np * n_state * n_nu * sizeof(float));
         double* d_I = (double*)workspace(ctx, "I", (size_t)np * n_nu * sizeof(double));
         double* d_RB = (double*)workspace(ctx, "jg_RB", (size_t)2 * np * n_ch * sizeof(double));
-        float* d_K = K_dev ? K_dev + (size_t)p0 * n_state * n_ch
-                           : (float*)workspace(ctx, "jg_K", (size_t)np * n_state * n_ch * sizeof(float));
+        float* d_K = adjoint ? nullptr
+                     : K_dev ? K_dev + (size_t)p0 * n_state * n_ch
+                             : (float*)workspace(ctx, "jg_K", (size_t)np * n_state * n_ch * sizeof(float));
         SegDev* d_segs = upload(ctx, "segs", sd);
         SegW* d_sw = upload(ctx, "jg_w", sw);
         int* d_sn = upload(ctx, "jg_n", sn);
@@ -794,18 +800,58 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
             if ((o.continua & 1) && ctx->n_h2o > 1) cd.mask |= 1;
             if ((o.continua & 2) && ctx->n_co2 > 1) cd.mask |= 2;
         }
-        if (cd.mask & kCiaMask)
-            jg_rte_kernel<true><<<dim3((unsigned)((n_nu + 127) / 128), np), 128, 0, st>>>(
-                d_out, n_out, d_lrt, d_jl, d_prt, d_jp, d_vlev, L, d_grid, n_nu, o.source_function, cd, d_I, d_D);
-        else
-            jg_rte_kernel<<<dim3((unsigned)((n_nu + 127) / 128), np), 128, 0, st>>>(
-                d_out, n_out, d_lrt, d_jl, d_prt, d_jp, d_vlev, L, d_grid, n_nu, o.source_function, cd, d_I, d_D);
+        const dim3 gr((unsigned)((n_nu + 127) / 128), np);
+        const bool cia = (cd.mask & kCiaMask) != 0;
+        if (!adjoint) {
+            if (cia)
+                jg_rte_kernel<true><<<gr, 128, 0, st>>>(d_out, n_out, d_lrt, d_jl, d_prt, d_jp, d_vlev, L, d_grid, n_nu,
+                                                        o.source_function, cd, d_I, d_D);
+            else
+                jg_rte_kernel<<<gr, 128, 0, st>>>(d_out, n_out, d_lrt, d_jl, d_prt, d_jp, d_vlev, L, d_grid, n_nu,
+                                                  o.source_function, cd, d_I, d_D);
+        } else if (cia) {
+            jg_rte_kernel<true, 1><<<gr, 128, 0, st>>>(d_out, n_out, d_lrt, d_jl, d_prt, d_jp, d_vlev, L, d_grid, n_nu,
+                                                       o.source_function, cd, d_I, nullptr);
+        } else {
+            jg_rte_kernel<false, 1><<<gr, 128, 0, st>>>(d_out, n_out, d_lrt, d_jl, d_prt, d_jp, d_vlev, L, d_grid,
+                                                        n_nu, o.source_function, cd, d_I, nullptr);
+        }
         check_launch(ctx);
         const double* d_kern = o.with_ils ? (const double*)ctx->work["ils"].p : nullptr;
         const int64_t n_taps = o.with_ils ? ctx->ils_n : 0;
         ils_bt_kernel<<<dim3((unsigned)((n_ch * 32 + 255) / 256), np), 256, 0, st>>>(
             d_I, n_nu, d_kern, n_taps, ig.dnu_hi, to_dev(ig.g), to_dev(ch), o.with_ils, d_RB, d_RB + (size_t)np * n_ch);
         check_launch(ctx);
+        if (adjoint) {  // the pullback: radiance cotangent on the grid, then the adjoint sweep
+            double* d_dy = (double*)workspace(ctx, "vjp_dy", (size_t)np * n_ch * sizeof(double));
+            IRS_CUDA(cudaMemcpyAsync(d_dy, dy_h + (size_t)p0 * n_ch, (size_t)np * n_ch * sizeof(double),
+                                     cudaMemcpyHostToDevice, st));
+            ctx->n_h2d += (double)np * n_ch * sizeof(double);
+            ChanAdj* d_ca = (ChanAdj*)workspace(ctx, "vjp_chan", (size_t)np * n_ch * sizeof(ChanAdj));
+            vjp_channel_kernel<<<dim3((unsigned)((n_ch + 255) / 256), np), 256, 0, st>>>(
+                d_RB, d_dy, n_nu, ig.dnu_hi, to_dev(ig.g), to_dev(ch), sp.observable, d_ca);
+            check_launch(ctx);
+            double* d_ib = (double*)workspace(ctx, "vjp_Ibar", (size_t)np * n_nu * sizeof(double));
+            ils_adjoint_kernel<<<dim3((unsigned)((n_nu + 255) / 256), np), 256, 0, st>>>(
+                d_ca, n_ch, d_kern, n_taps, ig.dnu_hi, o.with_ils, n_nu, d_ib);
+            check_launch(ctx);
+            double* d_xb = (double*)workspace(ctx, "vjp_xbar", (size_t)np * n_state * sizeof(double));
+            IRS_CUDA(cudaMemsetAsync(d_xb, 0, (size_t)np * n_state * sizeof(double), st));
+            const size_t xsm = (size_t)n_state * sizeof(double);
+            if (cia)
+                jg_rte_kernel<true, 2><<<gr, 128, xsm, st>>>(d_out, n_out, d_lrt, d_jl, d_prt, d_jp, d_vlev, L, d_grid,
+                                                             n_nu, o.source_function, cd, d_I, nullptr, d_ib, d_xb);
+            else
+                jg_rte_kernel<false, 2><<<gr, 128, xsm, st>>>(d_out, n_out, d_lrt, d_jl, d_prt, d_jp, d_vlev, L, d_grid,
+                                                              n_nu, o.source_function, cd, d_I, nullptr, d_ib, d_xb);
+            check_launch(ctx);
+            IRS_CUDA(cudaMemcpyAsync(dx_h + (size_t)p0 * n_state, d_xb, (size_t)np * n_state * sizeof(double),
+                                     cudaMemcpyDeviceToHost, st));
+            IRS_CUDA(cudaMemcpyAsync(y_h + (size_t)p0 * n_ch, d_RB + (sp.observable == 0 ? (size_t)np * n_ch : 0),
+                                     (size_t)np * n_ch * sizeof(double), cudaMemcpyDeviceToHost, st));
+            IRS_CUDA(cudaStreamSynchronize(st));
+            continue;
+        }
         jg_channel_kernel<<<dim3((unsigned)((n_ch * 32 + 255) / 256), (unsigned)n_state, np), 256, 0, st>>>(
             d_D, n_nu, (int)n_state, d_kern, n_taps, ig.dnu_hi, to_dev(ig.g), to_dev(ch), o.with_ils, d_RB,
             sp.observable, d_K);
@@ -1575,18 +1621,8 @@ int irs_vjp_batch(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_
     IRS_API_BEGIN
     IRS_REQUIRE(ctx && s && o && spec && dy && dx && y && profs && n_prof >= 1, "invalid arguments");
     IRS_CUDA(cudaSetDevice(ctx->device));
-    const int64_t n_state = state_size(*spec, profs[0].n_lev);
-    const int64_t n_ch = make_grid(s->nu_min, s->nu_max, s->dnu).n;
-    std::vector<double> Kh((size_t)n_prof * n_state * n_ch);
-    jacobian_device(ctx, profs, n_prof, *s, *o, *spec, Kh.data(), y);
-    for (int p = 0; p < n_prof; ++p)
-        for (int64_t x = 0; x < n_state; ++x) {
-            const double* row = Kh.data() + ((size_t)p * n_state + x) * n_ch;
-            const double* d = dy + (size_t)p * n_ch;
-            double acc = 0.0;
-            for (int64_t c = 0; c < n_ch; ++c) acc += row[c] * d[c];
-            dx[(size_t)p * n_state + x] = acc;
-        }
+    IRS_REQUIRE(state_size(*spec, profs[0].n_lev) * sizeof(double) <= 48 * 1024, "state vector too long for the adjoint");
+    jacobian_device(ctx, profs, n_prof, *s, *o, *spec, nullptr, y, nullptr, dy, dx);
     IRS_API_END
 }
 
@@ -1662,6 +1698,22 @@ int irs_faddeeva(irs_ctx* ctx, const double* x, const double* y, int64_t n, doub
     double* d_y = dev_copy(ctx, "op_b", y, n);
     double* d_o = (double*)workspace(ctx, "op_out", 2 * (size_t)n * sizeof(double));
     faddeeva_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(d_x, d_y, n, d_o, d_o + n);
+    check_launch(ctx);
+    to_host(ctx, re, d_o, n);
+    to_host(ctx, im, d_o + n, n);
+    IRS_API_END
+}
+
+int irs_faddeeva32(irs_ctx* ctx, const double* x, const double* y, int64_t n, double* re, double* im) {
+    IRS_API_BEGIN
+    IRS_REQUIRE(ctx && x && y && re && im && n >= 0, "invalid arguments");
+    IRS_CUDA(cudaSetDevice(ctx->device));
+    if (n == 0) return IRS_OK;
+    for (int64_t i = 0; i < n; ++i) IRS_REQUIRE(y[i] >= 0.0, "w(x + iy) is evaluated for y >= 0");
+    double* d_x = dev_copy(ctx, "op_a", x, n);
+    double* d_y = dev_copy(ctx, "op_b", y, n);
+    double* d_o = (double*)workspace(ctx, "op_out", 2 * (size_t)n * sizeof(double));
+    faddeeva32_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(d_x, d_y, n, d_o, d_o + n);
     check_launch(ctx);
     to_host(ctx, re, d_o, n);
     to_host(ctx, im, d_o + n, n);

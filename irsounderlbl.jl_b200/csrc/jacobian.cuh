@@ -952,15 +952,34 @@ __device__ __forceinline__ double cont_tau(double nu, const LayerRT& r, double d
 // schwarzschild_jacobian.jl:66-266 with the state chains of vmr_jacobian.jl:383-503.
 // Transmittances come from the FP64 cumulative optical depth: the top-of-layer
 // transmittance of layer m is exp(-(OD_total - OD_below_and_m)).
-template <bool CIA = false>
+//
+// MODE selects what the sweep leaves behind:
+//   0  D (forward mode, the columns of the monochromatic Jacobian) and I;
+//   1  I only (the derivative terms are not formed);
+//   2  the adjoint: with Ibar[profile][nu] = the radiance cotangent on the grid (the ILS
+//      and channel resampling transposed, applied to dy dBT/dR), each term D[x][nu] is
+//      multiplied by Ibar[nu] as it is formed and summed over the grid on the device
+//      (warp shuffles, then FP64 shared-memory and global atomics) into xbar[profile][x]
+//      = sum_nu Ibar D[x] = (K^T dy)[x].  D is never stored.  Dynamic shared memory:
+//      n_state doubles.
+template <bool CIA = false, int MODE = 0>
 __global__ void __launch_bounds__(128) jg_rte_kernel(
     const float* __restrict__ jl, int n_out, const LayerRT* __restrict__ lrt, const JgLayer* __restrict__ jlay,
     const ProfileRT* __restrict__ prt, const JgProfile* __restrict__ jprof, const double* __restrict__ vlev,
     int L, const double* __restrict__ grid, long long n_nu, int src, ContDev cont, double* __restrict__ I,
-    float* __restrict__ D) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    float* __restrict__ D, const double* __restrict__ Ibar = nullptr, double* __restrict__ xbar = nullptr) {
+    extern __shared__ double jg_xsh[];
+    const long long i_raw = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int p = blockIdx.y;
-    if (i >= n_nu) return;
+    const bool valid = i_raw < n_nu;
+    if (MODE != 2 && !valid) return;
+    // the adjoint keeps every lane to the end (warp reductions); others are clamped
+    const long long i = valid ? i_raw : n_nu - 1;
+    if (MODE == 2) {
+        for (int x = threadIdx.x; x < jprof[p].n_state; x += blockDim.x) jg_xsh[x] = 0.0;
+        __syncthreads();
+    }
+    const double ib = MODE == 2 && valid ? Ibar[(size_t)p * n_nu + i] : 0.0;
     const double nu = grid[i];
     const ProfileRT pr = prt[p];
     const JgProfile jp = jprof[p];
@@ -1024,7 +1043,18 @@ __global__ void __launch_bounds__(128) jg_rte_kernel(
     double cum = 0.0, gdn = 1.0, Id_below = 0.0;
     double carryT = 0.0, carryV[4] = {0, 0, 0, 0};
     const size_t nn = (size_t)n_nu;
-    float* Dp = D + (size_t)p * jp.n_state * nn;
+    float* Dp = MODE == 0 ? D + (size_t)p * jp.n_state * nn : nullptr;
+    auto emit = [&](size_t x, double val) {  // D[x][nu] = val
+        if (MODE == 0) {
+            Dp[x * nn + i] = (float)val;
+        } else if (MODE == 2) {
+            double v = valid ? val * ib : 0.0;
+#pragma unroll
+            for (int d = 16; d; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+            if ((threadIdx.x & 31) == 0) atomicAdd(&jg_xsh[x], v);
+        }
+    };
+    constexpr bool DERIV = MODE != 1;
     for (int m = 0; m < L; ++m) {
         const LayerRT r = lr[m];
         const JgLayer jm = jy[m];
@@ -1073,7 +1103,7 @@ __global__ void __launch_bounds__(128) jg_rte_kernel(
         // continuum derivatives by central differences (vmr_jacobian.jl:322-344)
         const float* om = out + (size_t)m * n_out * nn;
         double cT = 0.0, cvh = 0.0, cvc = 0.0;
-        if (cont.mask) {
+        if (DERIV && cont.mask) {
             const double vh = r.vmr_h2o, vc = r.vmr_co2, Tm = r.T_mid;
             if (jp.include_T)
                 cT = (cont_tau<CIA>(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh, vc, Tm + 0.05, cp) -
@@ -1089,31 +1119,35 @@ __global__ void __launch_bounds__(128) jg_rte_kernel(
                        cont_tau<CIA>(nu, r, jm.dp, cont, Cs, Cf, te, Se, td, vh, vc - h, Tm, cp)) / (2 * h);
             }
         }
-        if (jp.include_T) {
+        if (DERIV && jp.include_T) {
             const double tlo = (double)om[1 * nn + i] + cT * (1.0 - jm.wM);
             const double thi = (double)om[2 * nn + i] + cT * jm.wM;
-            Dp[(size_t)m * nn + i] = (float)(carryT + dTl_lo + dIdtau * tlo);
+            emit((size_t)m, carryT + dTl_lo + dIdtau * tlo);
             carryT = dTl_hi + dIdtau * thi;
         }
-        for (int rr = 0; rr < jp.n_retr; ++rr) {
+        for (int rr = 0; DERIV && rr < jp.n_retr; ++rr) {
             const double cv = rr == jp.retr_h2o ? cvh : (rr == jp.retr_co2 ? cvc : 0.0);
             const double vlo = (double)om[(size_t)(3 + 2 * rr) * nn + i] + cv * (1.0 - jm.wM);
             const double vhi = (double)om[(size_t)(4 + 2 * rr) * nn + i] + cv * jm.wM;
             const double sc = jp.log_vmr ? vl[rr * (L + 1) + m] : 1.0;
-            Dp[(size_t)(nT + rr * (L + 1) + m) * nn + i] = (float)(sc * (carryV[rr] + dIdtau * vlo));
+            emit((size_t)(nT + rr * (L + 1) + m), sc * (carryV[rr] + dIdtau * vlo));
             carryV[rr] = dIdtau * vhi;
         }
     }
-    if (jp.include_T) Dp[(size_t)L * nn + i] = (float)carryT;
-    for (int rr = 0; rr < jp.n_retr; ++rr) {
+    if (DERIV && jp.include_T) emit((size_t)L, carryT);
+    for (int rr = 0; DERIV && rr < jp.n_retr; ++rr) {
         const double sc = jp.log_vmr ? vl[rr * (L + 1) + L] : 1.0;
-        Dp[(size_t)(nT + rr * (L + 1) + L) * nn + i] = (float)(sc * carryV[rr]);
+        if (DERIV) emit((size_t)(nT + rr * (L + 1) + L), sc * carryV[rr]);
     }
     int col = nT + jp.n_retr * (L + 1);
-    if (jp.include_tsfc) Dp[(size_t)(col++) * nn + i] = (float)dIdTs;
-    if (jp.include_eps) Dp[(size_t)(col++) * nn + i] = (float)dIde;
+    if (DERIV && jp.include_tsfc) emit((size_t)(col++), dIdTs);
+    if (DERIV && jp.include_eps) emit((size_t)(col++), dIde);
     if (eps < 1.0) Iv += refl * Id * Tr0;
-    I[(size_t)p * nn + i] = Iv;
+    if (MODE != 2 && valid) I[(size_t)p * nn + i] = Iv;
+    if (MODE == 2) {
+        __syncthreads();
+        for (int x = threadIdx.x; x < jp.n_state; x += blockDim.x) atomicAdd(&xbar[(size_t)p * jp.n_state + x], jg_xsh[x]);
+    }
 }
 
 // ------------------------------------------------------------------ channel tail
@@ -1166,6 +1200,84 @@ __global__ void __launch_bounds__(256) jg_channel_kernel(const float* __restrict
         }
         K[((size_t)p * n_state + x) * ch.n + wid] = (float)(v * scale);
     }
+}
+
+// ------------------------------------------------------------------ adjoint tail
+// The transpose of the channel tail for the pullback: per (profile, channel) the
+// cotangent of R, rbar = dy dBT/dR (vmr_jacobian.jl:120-125; dy itself for the radiance
+// observable), split onto the two grid nodes the linear resampling reads
+// (sounder.jl:372-377): a0 at node ci, a1 at node ci + 1.
+struct ChanAdj {
+    long long ci;
+    double a0, a1;
+};
+__global__ void __launch_bounds__(256) vjp_channel_kernel(const double* __restrict__ R, const double* __restrict__ dy,
+                                                          long long n_nu, double dnu_hi, GridDev g, GridDev ch,
+                                                          int observable, ChanAdj* __restrict__ out) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = blockIdx.y;
+    if (c >= ch.n) return;
+    const double nu = ch.at(c);
+    const size_t pc = (size_t)p * ch.n + c;
+    double scale = 1.0;
+    if (observable == 0) {
+        const double Rc = R[pc];
+        if (Rc <= 0.0) scale = 0.0;
+        else {
+            const double A = 1.191042953e-5 * (nu * nu * nu), Lg = log1p(A / Rc);
+            scale = 1.4387769 * nu * A / ((Lg * Lg) * Rc * (Rc + A));
+        }
+    }
+    const double rb = dy[pc] * scale;
+    ChanAdj a{0, 0.0, 0.0};
+    const double g0 = g.at(0), gl = g.at(n_nu - 1);
+    if (nu <= g0) { a.ci = 0; a.a0 = rb; }
+    else if (nu >= gl) { a.ci = n_nu - 1; a.a0 = rb; }
+    else {  // the node search of ils_bt_kernel
+        long long i = (long long)floor((nu - g0) / dnu_hi);
+        i = max(0LL, min(i, n_nu - 2));
+        while (i > 0 && g.at(i) > nu) --i;
+        while (i + 2 < n_nu && g.at(i + 1) <= nu) ++i;
+        const double lo = g.at(i), hi = g.at(i + 1), w = (nu - lo) / (hi - lo);
+        a.ci = i;
+        a.a0 = w == 0.0 ? rb : rb * (1.0 - w);
+        a.a1 = w == 0.0 ? 0.0 : rb * w;
+    }
+    out[pc] = a;
+}
+
+// Ibar[profile][j] = sum over channels of a0 K(j - ci) + a1 K(j - ci - 1), with K(k) =
+// dnu_hi kern[k + half] inside the taps (apply_ils, ils.jl:131-153, transposed; zero
+// outside the grid as the forward convolution) or the unit impulse without the ILS.
+// One thread per grid point; the channels reaching it are found by a binary search on
+// their (ascending) nodes.
+__global__ void __launch_bounds__(256) ils_adjoint_kernel(const ChanAdj* __restrict__ ca, long long n_ch,
+                                                          const double* __restrict__ kern, long long n_taps,
+                                                          double dnu_hi, int with_ils, long long n_nu,
+                                                          double* __restrict__ Ibar) {
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = blockIdx.y;
+    if (j >= n_nu) return;
+    const ChanAdj* c = ca + (size_t)p * n_ch;
+    const long long half = with_ils ? (n_taps - 1) / 2 : 0;
+    long long lo = 0, hi = n_ch;  // first channel with ci >= j - half - 1
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if (c[mid].ci < j - half - 1) lo = mid + 1; else hi = mid;
+    }
+    double acc = 0.0;
+    for (long long k = lo; k < n_ch && c[k].ci <= j + half; ++k) {
+        const ChanAdj a = c[k];
+        const long long d0 = j - a.ci, d1 = d0 - 1;
+        if (with_ils) {
+            if (d0 >= -half && d0 <= half) acc = fma(a.a0, kern[d0 + half], acc);
+            if (d1 >= -half && d1 <= half) acc = fma(a.a1, kern[d1 + half], acc);
+        } else {
+            if (d0 == 0) acc += a.a0;
+            if (d1 == 0) acc += a.a1;
+        }
+    }
+    Ibar[(size_t)p * n_nu + j] = with_ils ? acc * dnu_hi : acc;
 }
 
 }  // namespace irs

@@ -414,6 +414,39 @@ def analytic_jacobian_batch(profiles, linelists, spec: StateVectorSpec, *, sound
     return nu, K, y
 
 
+def vjp_batch(profiles, linelists, spec: StateVectorSpec, dy, *, sounder=None, geoms=None, T_sfcs=None,
+              eps_sfcs=None, observable="bt", vmr_coupling=True, backend=None, line_mixing=None, **kw):
+    """Pullbacks dx = K^T dy of a batch (irs_vjp_batch: reverse mode on the GPU, K is never
+    formed).  dy is [n_prof, n_ch]; returns (y[n_prof, n_ch], dx[n_prof, n_state])."""
+    from . import (IASIInstrument, _prepare, _ProfileBatch, default_context, fm_options, nadir_geometry,
+                   sounder_grid)
+    _check_observable(observable)
+    ctx = backend or default_context()
+    sounder = sounder or IASIInstrument()
+    n = len(profiles)
+    nu = sounder_grid(sounder)
+    dy = np.ascontiguousarray(np.broadcast_to(np.asarray(dy, dtype=np.float64), (n, len(nu))))
+    geoms = geoms or [nadir_geometry()] * n
+    T_sfcs = T_sfcs if T_sfcs is not None else [None] * n
+    eps_sfcs = eps_sfcs if eps_sfcs is not None else [1.0] * n
+    _prepare(ctx, linelists, line_mixing)
+    kw.pop("dptmn", None)
+    o = fm_options(line_mixing=line_mixing, dptmn=0.0, **kw)
+    reduced = any(b.basis is not None for b in spec.vmr_blocks)
+    cs, keep = _c_spec(spec, spec.log_vmr and not reduced, vmr_coupling, observable)
+    batch = _ProfileBatch(profiles, T_sfcs, [g.mu for g in geoms], eps_sfcs)
+    s = sounder.c_struct()
+    n_full = C.c_int64()
+    check(ctx.lib.irs_state_size(C.byref(cs), spec.n_levels, C.byref(n_full)))
+    dx = np.empty((n, n_full.value))
+    y = np.empty((n, len(nu)))
+    check(ctx.lib.irs_vjp_batch(ctx.h, batch.arr, n, C.byref(s), C.byref(o), C.byref(cs), dptr(dy), dptr(dx),
+                                dptr(y)))
+    if reduced:  # the reduced columns are linear maps of the full ones: the same map on dx
+        dx = _map_reduced(spec, dx[:, None, :], profiles)[:, 0, :]
+    return y, dx
+
+
 def analytic_jacobian(prof, linelists, spec: StateVectorSpec, *, sounder=None, iasi=None, geom=None,
                       T_sfc: Optional[float] = None, eps_sfc: float = 1.0, observable="bt",
                       vmr_coupling=True, backend=None, line_mixing=None, **kw) -> Jacobian:

@@ -193,7 +193,8 @@ def test_analytic_vs_gpu_finite_differences(pkg, ctx, orc_mod):
 
 
 def test_batch_and_vjp(pkg, ctx, orc_mod):
-    """A batch of profiles gives each profile's own Jacobian; the pullback is K^T dy;
+    """A batch of profiles gives each profile's own Jacobian; the pullback is K^T dy
+    (within FP32 rounding: it is computed without K);
     reduced VMR bases are the full log-VMR columns times the basis."""
     ll = {2: pkg.HITRANLinelist(mk(orc_mod, 2, [(700.5, 2.0e-21, 0.07, 0.08, 250.0, 0.75, -0.003),
                                                 (702.0, 8.0e-22, 0.07, 0.08, 600.0, 0.75, -0.003)])),
@@ -214,7 +215,9 @@ def test_batch_and_vjp(pkg, ctx, orc_mod):
     assert np.array_equal(y, yb[1])
     dy = np.random.default_rng(5).standard_normal(len(nu))
     dx = pb(dy)
-    assert np.allclose(dx, Kb[1].T @ dy, rtol=1e-12, atol=1e-12 * np.max(np.abs(Kb[1].T @ dy)))
+    # the pullback runs in reverse mode (FP64 sums) while K passes through FP32: agreement
+    # to 1e-5 of sum |K| |dy| per element
+    assert np.all(np.abs(dx - Kb[1].T @ dy) <= 1e-5 * (np.abs(Kb[1]).T @ np.abs(dy)))
     # ColumnScale for H2O and a 2-block PartialColumns for CO2
     B = pkg.partial_column_basis(7, [range(0, 3), range(3, 7)])
     spec_r = pkg.StateVectorSpec(7, [pkg.ColumnScale(pkg.H2O), pkg.PartialColumns(pkg.CO2, B)])
