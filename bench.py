@@ -3,20 +3,22 @@
 
 Workload ("iasi-400k"): 400,000 lines over H2O, CO2, O3, N2O, CO, CH4 in
 645-2760 cm^-1, IASI sounder (8461 channels, Gaussian apodization), 0.0025 cm^-1
-internal grid (858,801 points), the six AFGL 50-level profiles (49 layers) per
-step and per GPU, FullFaddeeva, 25 cm^-1 cutoff, DPTMIN 1e-6, :cim source,
+internal grid (858,801 points), the six AFGL 50-level profiles (49 layers),
+FullFaddeeva, 25 cm^-1 cutoff, DPTMIN 1e-6, :cim source,
 MT-CKD H2O and CO2 continua (CIA tables are not bundled and contribute zero, as
 in the reference without them).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One process per GPU (torchrun for N > 1); every rank computes its own six
-profiles per step (weak scaling, no data-path collective).  `value` is the mixed
-(FP32 + Kahan) path with line lists resident in HBM, device-timed with CUDA
-events; `e2e` goes through the host C-ABI call with host buffers; the plain FP64
-kernel's spectra/s is reported beside it.  `--impl reference` times the
-reference algorithm's CPU implementation (the FP64 C++ restatement under
-oracle/, all host threads) on a bounded sample of the same workload.
+One process per GPU (torchrun for N > 1).  A step is one global batch of 24 profiles
+(the six AFGL profiles x 4) split into contiguous shards over the ranks (strong
+scaling; no data-path collective); a weak-scaling line (the six profiles on every
+rank) is reported beside it.  `value` is the mixed (FP32 + Kahan) path with line
+lists resident in HBM, device-timed with CUDA events (max over ranks); `e2e` goes
+through the host C-ABI call with host buffers; the plain FP64 kernel's spectra/s is
+reported beside it.  `--impl reference` times the reference algorithm's CPU
+implementation (the FP64 C++ restatement under oracle/, all host threads) on a
+bounded sample of the same workload.
 """
 from __future__ import annotations
 
@@ -34,6 +36,7 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 N_PROF = 6
+GLOBAL_BATCH = 4 * N_PROF  # profiles per step over all GPUs: the six AFGL profiles x 4
 FAR_PAIR_FLOPS = 10     # d (2), d^2, d^2+b^2, rcp, pedestal FMA (2), value FMA (2), accumulate
 CORE_PAIR_FLOPS = 70    # far-pair ops + FP32 Faddeeva (continued fraction / Weideman-16 branch)
 FP32_LANES = 148 * 128  # B200: 148 SMs x 128 FP32 lanes
@@ -52,7 +55,8 @@ METRIC = "IASI spectra/s (line-by-line forward_model, 400k lines)"
 
 def workload_config():
     return {"workload": "iasi-400k", "lines": 400000, "species": 6, "grid_dnu": 0.0025, "n_nu": 858801,
-            "layers": 49, "channels": 8461, "profiles": "the 6 AFGL 50-level profiles", "method": "FullFaddeeva",
+            "layers": 49, "channels": 8461, "profiles": "the 6 AFGL 50-level profiles",
+            "batch": "24 profiles per step (the 6 AFGL profiles x 4), split over the GPUs", "method": "FullFaddeeva",
             "cutoff": 25.0, "dptmn": 1e-6, "continua": "h2o,co2",
             "l2": "working set (line parameters ~4 GB, tau 1 GB) >> L2"}
 
@@ -184,7 +188,7 @@ def reference_arm(args, rank):
     line = {
         "impl": "reference", "metric": METRIC,
         "value": v, "unit": "spectra/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded line lists, AFGL profiles)",
         "config": workload_config(),
         "cpu_baseline": {"value": v, "unit": "spectra/s", "cores": cores, "kind": "port",
@@ -276,10 +280,17 @@ def bench_extras(pkg, ctx, lists, snd, torch, stream):
     t0 = time.perf_counter()
     pkg.analytic_jacobian_batch(profs, lists, spec, sounder=snd, geoms=geoms, backend=ctx, line_mixing=lm, **kw)
     tj = time.perf_counter() - t0
+    dy = np.random.default_rng(1002).standard_normal((len(profs), 8461))
+    pkg.vjp_batch(profs, lists, spec, dy, sounder=snd, geoms=geoms, backend=ctx, line_mixing=lm, **kw)
+    t0 = time.perf_counter()
+    pkg.vjp_batch(profs, lists, spec, dy, sounder=snd, geoms=geoms, backend=ctx, line_mixing=lm, **kw)
+    tv = time.perf_counter() - t0
     out["jacobian"] = {
         "metric": "IASI Jacobians/s (analytic, state T + log H2O + log O3 + T_sfc = 151, with VP_Y)",
         "value": len(profs) / tj, "unit": "jacobians/s", "timing": "host wall clock around the C-ABI call, "
         "host buffers (K is 8461 x 151 FP64 per profile)",
+        "pullbacks_per_s": len(profs) / tv,
+        "pullback": "irs_vjp_batch: dx = K^T dy in reverse mode on the device (K not formed)",
         "config": {"workload": "iasi-400k-lm", "profiles": len(profs), "n_state": spec.n, "channels": 8461}}
     # ---- relaxation-matrix line mixing on the 400k-line IASI workload (6 AFGL profiles)
     relmat = pkg.synthetic.synthetic_relmat(n_bands=6, j_max=60)
@@ -342,6 +353,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--batch", type=int, default=GLOBAL_BATCH,
+                    help="profiles per step over all GPUs (split into contiguous shards per rank)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the surrogate, Jacobian and optimal-estimation measurements")
@@ -428,7 +441,12 @@ def main():
     pkg = _package()
     ctx = pkg.B200Context(local)
     lists = pkg.synthetic.lists_iasi_400k()
-    profs = [pkg.afgl_atmosphere(a) for a in pkg.synthetic.AFGL][:N_PROF]
+    afgl = [pkg.afgl_atmosphere(a) for a in pkg.synthetic.AFGL][:N_PROF]
+    # the global batch (strong scaling: fixed total work, contiguous shards per rank)
+    profs_all = [afgl[k % N_PROF] for k in range(args.batch)]
+    first, count = pkg.shard_range(args.batch, world, rank)
+    if count < 1:
+        raise SystemExit(f"a batch of {args.batch} profiles leaves rank {rank} of {world} without work")
     snd = pkg.IASIInstrument()
     pkg._prepare(ctx, lists, None)
     lib = ctx.lib
@@ -436,41 +454,62 @@ def main():
     def options(prec):
         return pkg.fm_options(precision=prec, method=pkg.FullFaddeeva, **_workload_kw())
 
-    batch = pkg._ProfileBatch(profs, [None] * N_PROF, [1.0] * N_PROF, [1.0] * N_PROF)
     s = snd.c_struct()
     nch = 8461
-    R = torch.empty((N_PROF, nch), dtype=torch.float64, device="cuda")
-    BT = torch.empty_like(R)
     # a real (non-default) stream: the library orders its own stream after this one
     # on entry and this one after its work on exit, so events here bracket the work
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
 
-    def step_device(opt):
-        pkg.check(lib.irs_forward_model_batch_device(ctx.h, batch.arr, N_PROF, C.byref(s), C.byref(opt),
-                                                     C.c_void_p(R.data_ptr()), C.c_void_p(BT.data_ptr()),
-                                                     C.c_void_p(stream.cuda_stream)))
+    class Batch:
+        def __init__(self, profs):
+            self.n = len(profs)
+            self.b = pkg._ProfileBatch(profs, [None] * self.n, [1.0] * self.n, [1.0] * self.n)
+            self.R = torch.empty((self.n, nch), dtype=torch.float64, device="cuda")
+            self.BT = torch.empty_like(self.R)
+
+        def step(self, opt):
+            pkg.check(lib.irs_forward_model_batch_device(ctx.h, self.b.arr, self.n, C.byref(s), C.byref(opt),
+                                                         C.c_void_p(self.R.data_ptr()),
+                                                         C.c_void_p(self.BT.data_ptr()),
+                                                         C.c_void_p(stream.cuda_stream)))
+
+    def device_ms(b, opt, steps, warm):
+        for _ in range(warm):
+            b.step(opt)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            b.step(opt)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / steps)
+
+    mine = Batch(profs_all[first:first + count])  # this rank's shard of the global batch
+    six = Batch(afgl)                              # the six AFGL profiles (per-rank lines)
 
     # ---------------- value: mixed path, inputs resident, CUDA events
     om = options("mixed")
     for _ in range(args.warmup):
-        step_device(om)
+        mine.step(om)
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(_physical_gpu(local)) as clk:
         e0.record(stream)
         for _ in range(args.steps):
-            step_device(om)
+            mine.step(om)
         e1.record(stream)
         torch.cuda.synchronize()
     barrier()
     ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
-    value = weak_scaling_value(world, N_PROF, ms)
+    value = args.batch / (ms / 1e3)
 
     # per-stage device times (library events on its launching stream), averaged
     acc = {"line_params_ms": 0.0, "line_sum_ms": 0.0, "rte_ms": 0.0, "ils_ms": 0.0}
     for _ in range(args.steps):
-        step_device(om)
+        mine.step(om)
         pkg.check(lib.irs_synchronize(ctx.h))
         st = ctx.stage_times()
         for k in acc:
@@ -487,45 +526,31 @@ def main():
     achieved = flops / t_ls / 1e12
     traffic = _traffic_from_profiles()
 
+    # ---------------- weak scaling: the six AFGL profiles on every rank
+    ms6 = device_ms(six, om, max(2, args.steps // 2), 1)
+    weak = {"value": weak_scaling_value(world, N_PROF, ms6), "unit": "spectra/s", "ms_per_step": ms6,
+            "profiles_per_rank": N_PROF, "scaling": "weak"}
+
     # ---------------- e2e: host C-ABI call, host buffers in and out
-    Rh = (C.c_double * (N_PROF * nch))()
-    BTh = (C.c_double * (N_PROF * nch))()
+    Rh = (C.c_double * (count * nch))()
+    BTh = (C.c_double * (count * nch))()
     for _ in range(2):
-        pkg.check(lib.irs_forward_model_batch(ctx.h, batch.arr, N_PROF, C.byref(s), C.byref(om), Rh, BTh))
+        pkg.check(lib.irs_forward_model_batch(ctx.h, mine.b.arr, count, C.byref(s), C.byref(om), Rh, BTh))
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        pkg.check(lib.irs_forward_model_batch(ctx.h, batch.arr, N_PROF, C.byref(s), C.byref(om), Rh, BTh))
+        pkg.check(lib.irs_forward_model_batch(ctx.h, mine.b.arr, count, C.byref(s), C.byref(om), Rh, BTh))
     t_e2e = max_over_ranks((time.perf_counter() - t0) / args.steps)
     st = ctx.stage_times()
-    e2e = {"value": world * N_PROF / t_e2e, "unit": "spectra/s",
+    e2e = {"value": args.batch / t_e2e, "unit": "spectra/s",
            "h2d_bytes_per_step": int(st.h2d_bytes), "d2h_bytes_per_step": int(st.d2h_bytes),
            "timing": "host wall clock around the synchronous C-ABI call, max over ranks"}
 
-    # ---------------- plain FP64 kernel on the same workload
-    op = options("fp64")
-    step_device(op)
-    barrier()
-    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    p0.record(stream)
-    for _ in range(args.plain_steps):
-        step_device(op)
-    p1.record(stream)
-    torch.cuda.synchronize()
-    ms64 = max_over_ranks(p0.elapsed_time(p1) / args.plain_steps)
+    # ---------------- plain FP64 and direct FP32 kernels on the six AFGL profiles
+    ms64 = device_ms(six, options("fp64"), args.plain_steps, 1)
     plain = world * N_PROF / (ms64 / 1e3)
-
-    # ---------------- the direct FP32 sum (every pair evaluated) on the same workload
-    od = options("mixed_direct")
-    step_device(od)
-    barrier()
-    p0.record(stream)
-    for _ in range(args.plain_steps):
-        step_device(od)
-    p1.record(stream)
-    torch.cuda.synchronize()
-    ms_d = max_over_ranks(p0.elapsed_time(p1) / args.plain_steps)
-    BTd = BT.clone()
+    ms_d = device_ms(six, options("mixed_direct"), args.plain_steps, 1)
+    BTd = six.BT.clone()
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -540,13 +565,13 @@ def main():
         extras = bench_extras(pkg, ctx, lists, snd, torch, stream)
         pkg._prepare(ctx, lists, None)
 
-    # consistency check of this run: mixed vs FP64 BT on the last batch
-    step_device(om)
+    # consistency check of this run: mixed vs FP64 BT on the six AFGL profiles
+    six.step(om)
     torch.cuda.synchronize()
-    BTm = BT.clone()
-    step_device(op)
+    BTm = six.BT.clone()
+    six.step(options("fp64"))
     torch.cuda.synchronize()
-    d = (BTm - BT)
+    d = (BTm - six.BT)
     bt_rms = float(torch.sqrt(torch.mean(d * d)).item())
     bt_max = float(d.abs().max().item())
     dd = BTm - BTd
@@ -559,7 +584,7 @@ def main():
         line = {
             "metric": METRIC,
             "value": value, "unit": "spectra/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32+kahan (fp64 cumulative optical depth and transmittance)",
             "data": "synthetic (seeded line lists, AFGL profiles)",
             "config": workload_config(),
@@ -581,10 +606,11 @@ def main():
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": clocks,
             "stages_ms": acc,
-            "profiles_per_step_per_gpu": N_PROF,
+            "profiles_per_step": args.batch, "profiles_this_rank": count,
+            "weak_scaling": weak,
         }
         # the RTE kernel against HBM: it reads the FP32 optical depths once and writes I
-        rte_bytes = N_PROF * 49 * 858801 * 4 + N_PROF * 858801 * 8
+        rte_bytes = count * 49 * 858801 * 4 + count * 858801 * 8
         peaks, psrc = _peaks()
         line["rte"] = {"kernel": "rte_mixed_kernel", "ms_per_step": acc["rte_ms"], "bytes_per_step": rte_bytes,
                        "achieved_gbs": rte_bytes / (acc["rte_ms"] / 1e3) / 1e9, "peak_gbs": peaks["hbm_gbs"],

@@ -209,9 +209,26 @@ int irs_state_size(const irs_state_spec* spec, int n_lev, int64_t* n_state);
 int irs_jacobian_batch(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder* s,
                        const irs_fm_options* o, const irs_state_spec* spec, double* K, double* y);
 
+/* forward_model for one batch spread over n_ctx contexts (one per GPU; every context
+ * must hold the same line lists and tables).  No counterpart in the reference, whose
+ * profile loop is sequential (sounder.jl:283-307): the batch is split into contiguous
+ * shards (irs_shard_range), each run by its own host thread through
+ * irs_forward_model_batch on its context, and the shards' R and BT are written to the
+ * caller's host buffers [n_prof][n_channels] at their offsets.  No collective. */
+int irs_forward_model_batch_multi(irs_ctx* const* ctxs, int n_ctx, const irs_profile* profs, int n_prof,
+                                  const irs_sounder* s, const irs_fm_options* o, double* R, double* BT);
+/* The shard of n items that shard `shard` of n_shards takes: [*first, *first + *count),
+ * contiguous and balanced (the first n % n_shards shards take one more).  Host only. */
+int irs_shard_range(int64_t n, int n_shards, int shard, int64_t* first, int64_t* count);
+
 /* Vector-Jacobian product dx = K^T dy for each profile (the pullback behind the
  * ChainRulesCore.rrule of forward_model): dy is [n_prof][n_channels], dx is
- * [n_prof][n_state]; y receives the observable. */
+ * [n_prof][n_state]; y receives the observable.  Reverse mode on the device (the
+ * reference forms K first, vmr_jacobian.jl:152-505): the derivative line sum, the
+ * forward RTE, the radiance cotangent dy dBT/dR taken back through the channel
+ * resampling and the ILS to the grid, and one adjoint RTE sweep
+ * (schwarzschild_jacobian.jl:66-167 per grid point) that contracts every derivative term
+ * with it; K is never formed.  At most 6144 state elements. */
 int irs_vjp_batch(irs_ctx* ctx, const irs_profile* profs, int n_prof, const irs_sounder* s,
                   const irs_fm_options* o, const irs_state_spec* spec, const double* dy, double* dx,
                   double* y);
@@ -340,6 +357,10 @@ int irs_voigt_profile(irs_ctx* ctx, const double* nu, int64_t n, double nu0, dou
                       int method, double* out);
 /* w(x + iy) = erfcx(y - ix) for y >= 0 (faddeeva_voigt = Re w, voigt.jl:152-160). */
 int irs_faddeeva(irs_ctx* ctx, const double* x, const double* y, int64_t n, double* re, double* im);
+/* w(x + iy) by the FP32 evaluator of the mixed-precision line sums (no counterpart in
+ * the reference, which evaluates FullFaddeeva in FP64 only): for checking its
+ * accuracy against irs_faddeeva / erfcx.  Inputs are rounded to FP32. */
+int irs_faddeeva32(irs_ctx* ctx, const double* x, const double* y, int64_t n, double* re, double* im);
 /* ils_kernel(Δν, opd_max, fwhm; apodization) (ils.jl:80-115): the area-normalised taps
  * at k Δν, k = -n_half..n_half, n_taps = 2 ceil(16/Δν) + 1. */
 int irs_ils_kernel(irs_ctx* ctx, double dnu, double opd_max, double fwhm_gauss, int apodization, int64_t n_taps,
@@ -408,6 +429,18 @@ int irs_surrogate_train(irs_surrogate* s, const float* X, const float* Y, int64_
 /* loss and its gradient (same layout as the parameters) on one batch, no update */
 int irs_surrogate_gradients(irs_surrogate* s, const float* X, const float* Y, int64_t n, float* grads,
                             double* loss);
+/* Data-parallel training, split at the gradient so that it can be reduced across GPUs
+ * between the halves.  irs_surrogate_grad_size: the length of the flat gradient (the
+ * parameters in a padded device layout).  irs_surrogate_grad_device: the loss and
+ * gradient of 0.5 mean((y' - t')^2) over rows idx_dev[0..n) (NULL: rows 0..n) of the
+ * device arrays X_dev [rows][n_in], Y_dev [rows][n_out], written to g_dev (device, the
+ * flat layout); loss (host, nullable) waits for the result.  irs_surrogate_apply_device:
+ * one Adam step (as irs_surrogate_train's) from the gradient in g_dev with learning rate
+ * lr.  Both are ordered after and before the work on `stream` (a cudaStream_t). */
+int irs_surrogate_grad_size(irs_surrogate* s, int64_t* n);
+int irs_surrogate_grad_device(irs_surrogate* s, const float* X_dev, const float* Y_dev, const int32_t* idx_dev,
+                              int64_t n, float* g_dev, double* loss, void* stream);
+int irs_surrogate_apply_device(irs_surrogate* s, const float* g_dev, float lr, void* stream);
 /* predictions [n][n_out] and OOD scores [n] (ood nullable) */
 int irs_surrogate_infer(irs_surrogate* s, const float* X, int64_t n, float* out, float* ood);
 /* same with device buffers; ordered after and before the work on `stream` (a cudaStream_t) */

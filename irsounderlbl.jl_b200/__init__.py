@@ -395,6 +395,82 @@ def forward_model_batch(profiles: Sequence[AtmosphericProfile], linelists, *, so
     return nu_out, R, BT
 
 
+def shard_range(n: int, n_shards: int, shard: int):
+    """(first, count) of the contiguous, balanced shard `shard` of n items over n_shards
+    (irs_shard_range: the first n % n_shards shards take one more).  Host only."""
+    first, count = C.c_int64(), C.c_int64()
+    check(_lib.load().irs_shard_range(int(n), int(n_shards), int(shard), C.byref(first), C.byref(count)))
+    return first.value, count.value
+
+
+def forward_model_batch_multi(profiles: Sequence[AtmosphericProfile], linelists, *, backends: Sequence,
+                              sounder: Sounder = None, geoms: Optional[Sequence[ViewingGeometry]] = None,
+                              T_sfcs=None, eps_sfcs=None, line_mixing: Optional[VPYLineMixing] = None, **kw):
+    """forward_model_batch spread over several contexts (one per GPU): contiguous shards
+    of the batch, one host thread per context, gathered in batch order
+    (irs_forward_model_batch_multi).  Returns (nu_out, R[n_prof, n_ch], BT[n_prof, n_ch])."""
+    if not backends:
+        raise IRSError("forward_model_batch_multi needs at least one context")
+    sounder = sounder or IASIInstrument()
+    n = len(profiles)
+    geoms = geoms or [nadir_geometry()] * n
+    T_sfcs = T_sfcs if T_sfcs is not None else [None] * n
+    eps_sfcs = eps_sfcs if eps_sfcs is not None else [1.0] * n
+    for ctx in backends:
+        _prepare(ctx, linelists, line_mixing)
+    o = fm_options(line_mixing=line_mixing, **kw)
+    batch = _ProfileBatch(profiles, T_sfcs, [g.mu for g in geoms], eps_sfcs)
+    s = sounder.c_struct()
+    nu_out = sounder_grid(sounder)
+    R = np.empty((n, len(nu_out)))
+    BT = np.empty((n, len(nu_out)))
+    hs = (C.c_void_p * len(backends))(*[ctx.h.value for ctx in backends])
+    check(backends[0].lib.irs_forward_model_batch_multi(hs, len(backends), batch.arr, n, C.byref(s), C.byref(o),
+                                                        dptr(R), dptr(BT)))
+    return nu_out, R, BT
+
+
+def distributed_batch(compute, n: int, dist=None):
+    """Run a batch of n independent items over the ranks of a torch.distributed group:
+    rank r computes its contiguous shard (shard_range) as compute(first, count) -> a tuple
+    of arrays with the shard's items along axis 0, and every rank receives the arrays of
+    the whole batch in batch order (an all-gather of the shards).  `dist` None: one
+    process computes everything.  The only exchange is that gather."""
+    if dist is None:
+        return compute(0, n)
+    world, rank = dist.get_world_size(), dist.get_rank()
+    first, count = shard_range(n, world, rank)
+    local = compute(first, count) if count else None
+    parts = [None] * world
+    dist.all_gather_object(parts, local)
+    parts = [p for p in parts if p is not None]
+    return tuple(np.concatenate([p[k] for p in parts], axis=0) for k in range(len(parts[0])))
+
+
+def forward_model_batch_distributed(profiles: Sequence[AtmosphericProfile], linelists, *, dist=None,
+                                    backend=None, sounder: Sounder = None,
+                                    geoms: Optional[Sequence[ViewingGeometry]] = None, T_sfcs=None, eps_sfcs=None,
+                                    line_mixing: Optional[VPYLineMixing] = None, **kw):
+    """forward_model_batch over the ranks of a process group, one GPU (context) per rank:
+    each rank runs its contiguous shard of the profiles and all ranks receive R and BT of
+    the whole batch in batch order.  Returns (nu_out, R[n_prof, n_ch], BT[n_prof, n_ch])."""
+    n = len(profiles)
+    sounder = sounder or IASIInstrument()
+
+    def pick(v, a, b):
+        return None if v is None else list(v)[a:a + b]
+
+    def compute(first, count):
+        _, R, BT = forward_model_batch(profiles[first:first + count], linelists, sounder=sounder,
+                                       geoms=pick(geoms, first, count), T_sfcs=pick(T_sfcs, first, count),
+                                       eps_sfcs=pick(eps_sfcs, first, count), backend=backend,
+                                       line_mixing=line_mixing, **kw)
+        return R, BT
+
+    R, BT = distributed_batch(compute, n, dist)
+    return sounder_grid(sounder), R, BT
+
+
 def forward_model(prof: AtmosphericProfile, linelists, *, sounder: Sounder = None,
                   iasi: Sounder = None, geom: ViewingGeometry = None, T_sfc: Optional[float] = None,
                   eps_sfc: float = 1.0, backend=None, line_mixing: Optional[VPYLineMixing] = None, **kw):
@@ -410,7 +486,7 @@ iasi_forward_model = forward_model
 
 from .synthetic import afgl_atmosphere, synthetic_linelist  # noqa: E402,F401
 from .estimation import (ColumnScale, FullProfile, Jacobian, PartialColumns, StateVectorSpec,  # noqa: E402,F401
-                         analytic_jacobian, analytic_jacobian_batch, column, default_fd_steps, dfs_partition,
+                         analytic_jacobian, analytic_jacobian_batch, vjp_batch, column, default_fd_steps, dfs_partition,
                          finite_difference_jacobian, forward_model_rrule, pack_state, partial_column_basis,
                          state_labels, unpack_state, vmr_range, build_sa, scene_nedt, exclude_channels,
                          apodized_measurement_covariance, scene_measurement_covariance,

@@ -114,6 +114,9 @@ SIGNATURES = {
     "irs_oe_batch": ([_P, C.POINTER(Profile), C.c_int, C.POINTER(Sounder), C.POINTER(FMOptions),
                       C.POINTER(StateSpec), _PD, _PD, _PD, _PD, _PD, C.POINTER(OEParams), _PD, _PD, _PD,
                       C.POINTER(C.c_int32), C.POINTER(C.c_int32), _PD], C.c_int),
+    "irs_forward_model_batch_multi": ([C.POINTER(C.c_void_p), C.c_int, C.POINTER(Profile), C.c_int,
+                                       C.POINTER(Sounder), C.POINTER(FMOptions), _PD, _PD], C.c_int),
+    "irs_shard_range": ([C.c_int64, C.c_int, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
     "irs_synchronize": ([_P], C.c_int),
     "irs_last_stage_times": ([_P, C.POINTER(StageTimes)], C.c_int),
     "irs_cross_sections_noalloc": ([_P, C.c_int64, _P, C.POINTER(C.c_int32), C.c_int, C.c_int, C.c_int, _P,
@@ -122,6 +125,10 @@ SIGNATURES = {
     "irs_surrogate_create": ([_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)],
                              C.c_int),
     "irs_surrogate_destroy": ([_P], C.c_int),
+    "irs_surrogate_grad_size": ([_P, C.POINTER(C.c_int64)], C.c_int),
+    "irs_surrogate_grad_device": ([_P, _P, _P, C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_float),
+                                   C.POINTER(C.c_double), _P], C.c_int),
+    "irs_surrogate_apply_device": ([_P, C.POINTER(C.c_float), C.c_float, _P], C.c_int),
     "irs_surrogate_param_count": ([_P, C.POINTER(C.c_int64)], C.c_int),
     "irs_surrogate_get_params": ([_P, _PF], C.c_int),
     "irs_surrogate_set_params": ([_P, _PF], C.c_int),
@@ -138,6 +145,7 @@ SIGNATURES = {
                             C.c_int),
     "irs_voigt_profile": ([_P, _PD, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_int, _PD], C.c_int),
     "irs_faddeeva": ([_P, _PD, _PD, C.c_int64, _PD, _PD], C.c_int),
+    "irs_faddeeva32": ([_P, _PD, _PD, C.c_int64, _PD, _PD], C.c_int),
     "irs_ils_kernel": ([_P, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int64, _PD], C.c_int),
     "irs_apply_ils": ([_P, _PD, C.c_int64, C.c_double, _PD, C.c_int64, _PD], C.c_int),
     "irs_schwarzschild_rte": ([_P, _PD, C.c_int64, C.c_int, _PD, _PD, C.c_double, C.c_double, C.c_double, C.c_int,

@@ -15,7 +15,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 SO = HERE / "libirs_b200.so"
 SOURCES = [HERE / "csrc" / "irs_b200.cu", HERE / "csrc" / "noalloc.cu", HERE / "csrc" / "surrogate.cu",
-           HERE / "csrc" / "irs_host.cpp", HERE / "csrc" / "relmat.cpp"]
+           HERE / "csrc" / "irs_host.cpp", HERE / "csrc" / "relmat.cpp", HERE / "csrc" / "shard.cpp"]
 DEPS = SOURCES + sorted((HERE / "csrc").glob("*.cuh")) + sorted((HERE / "csrc").glob("*.h")) + \
     [HERE.parent / "include" / "irs_b200.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -575,6 +575,76 @@ int irs_surrogate_gradients(irs_surrogate* s, const float* X, const float* Yt, i
     SG_END
 }
 
+// ---------------------------------------------------- data-parallel training steps
+// A training step split so that the gradient can cross devices between its halves:
+// irs_surrogate_grad_device leaves the flat gradient (the padded layout of
+// irs_surrogate_grad_size) in the caller's device buffer, the caller reduces it over its
+// ranks (an NCCL all-reduce), and irs_surrogate_apply_device takes one Adam step from it.
+// Both order the library's stream after `stream` on entry and `stream` after their work.
+struct StreamJoin {
+    cudaEvent_t ev = nullptr;
+    cudaStream_t caller = nullptr, own = nullptr;
+    StreamJoin(cudaStream_t c, cudaStream_t o) : caller(c), own(o) {
+        if (!caller) return;
+        IRS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        IRS_CUDA(cudaEventRecord(ev, caller));
+        IRS_CUDA(cudaStreamWaitEvent(own, ev, 0));
+    }
+    void done() {
+        if (!caller) return;
+        IRS_CUDA(cudaEventRecord(ev, own));
+        IRS_CUDA(cudaStreamWaitEvent(caller, ev, 0));
+    }
+    ~StreamJoin() {
+        if (ev) cudaEventDestroy(ev);
+    }
+};
+
+int irs_surrogate_grad_size(irs_surrogate* s, int64_t* n) {
+    SG_BEGIN
+    IRS_REQUIRE(s && n, "invalid arguments");
+    *n = s->n_par;
+    SG_END
+}
+
+int irs_surrogate_grad_device(irs_surrogate* s, const float* X_dev, const float* Y_dev, const int32_t* idx_dev,
+                              int64_t n, float* g_dev, double* loss, void* stream) {
+    SG_BEGIN
+    IRS_REQUIRE(s && X_dev && Y_dev && g_dev && n >= 1 && n <= (1 << 20), "invalid arguments");
+    IRS_CUDA(cudaSetDevice(s->device));
+    const cudaStream_t st = s->stream;
+    StreamJoin j((cudaStream_t)stream, st);
+    ensure_batch(s, (int)n);
+    IRS_CUDA(cudaMemsetAsync(s->loss, 0, sizeof(double), st));
+    prep_input_kernel<<<(int)n, 256, 0, st>>>(X_dev, idx_dev, s->n_in, s->pin[0], (int)n, s->xmean, s->xsd,
+                                               s->act[0]);
+    forward(s, (int)n);
+    backward(s, (int)n, Y_dev, idx_dev);
+    IRS_CUDA(cudaMemcpyAsync(g_dev, s->g, (size_t)s->n_par * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    if (loss) {
+        IRS_CUDA(cudaMemcpyAsync(loss, s->loss, sizeof(double), cudaMemcpyDeviceToHost, st));
+        check_err(s);
+    }
+    j.done();
+    SG_END
+}
+
+int irs_surrogate_apply_device(irs_surrogate* s, const float* g_dev, float lr, void* stream) {
+    SG_BEGIN
+    IRS_REQUIRE(s && g_dev && lr > 0.f, "invalid arguments");
+    IRS_CUDA(cudaSetDevice(s->device));
+    const cudaStream_t st = s->stream;
+    StreamJoin j((cudaStream_t)stream, st);
+    s->t_step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, (float)s->t_step), c2 = 1.f - std::pow(b2, (float)s->t_step);
+    adam_kernel<<<(unsigned)((s->n_par + 255) / 256), 256, 0, st>>>(s->w, s->m, s->v, g_dev, s->n_par, lr, b1, b2,
+                                                                     1e-8f, c1, c2);
+    refresh_bf16(s);
+    j.done();
+    SG_END
+}
+
 // inference of n samples already on the device; out [n][n_out] BTs, ood [n] (nullable)
 static void infer_device(irs_surrogate* s, const float* dX, int64_t n, float* dOut, float* dOod) {
     const cudaStream_t st = s->stream;

@@ -155,6 +155,113 @@ class Surrogate:
             pass
 
 
+# ------------------------------------------------------------------ data parallel
+def cosine_lr(lr: float, epoch: int, epochs: int) -> float:
+    """The learning-rate schedule of irs_surrogate_train: cosine from lr down to lr/100."""
+    if epochs <= 1:
+        return float(lr)
+    lo = 0.01 * lr
+    return float(lo + 0.5 * (lr - lo) * (1.0 + np.cos(np.pi * epoch / (epochs - 1))))
+
+
+def dp_rows(n_local: int, batch: int, epoch: int, step: int, seed: int, rank: int) -> np.ndarray:
+    """Local rows of mini-batch `step` of `epoch` on `rank`: a permutation of the rank's
+    own samples seeded by (seed, epoch, rank), cut into full batches.  The global
+    mini-batch is the concatenation of every rank's rows."""
+    perm = np.random.Generator(np.random.PCG64([int(seed), int(epoch), int(rank)])).permutation(n_local)
+    return np.ascontiguousarray(perm[step * batch:(step + 1) * batch], dtype=np.int32)
+
+
+def train_data_parallel(grad_fn, apply_fn, n_local: int, *, batch: int, epochs: int, lr: float, seed: int,
+                        rank: int, world: int, all_reduce, steps_per_epoch: int = None):
+    """Data-parallel Adam over `world` ranks, one model replica per rank.
+
+    Each step every rank takes `batch` rows of its own samples (dp_rows), grad_fn(rows)
+    returns the gradient of 0.5 mean((y' - t')^2) over them (a tensor, any device) and
+    the local loss, the gradients are averaged over the ranks by all_reduce (an in-place
+    sum: NCCL on GPUs, gloo in tests; equal local batches make the average the gradient
+    of the concatenated global batch) and apply_fn(gradient, lr) takes one Adam step on
+    the replica.  Every rank takes the same number of steps (collectives stay matched):
+    steps_per_epoch, or n_local // batch, which must then agree on every rank.
+
+    Returns the loss per epoch (the mean over steps of the global-batch loss)."""
+    import torch
+    n_steps = steps_per_epoch if steps_per_epoch is not None else n_local // batch
+    if n_steps < 1 or n_steps * batch > n_local:
+        raise IRSError(f"{n_local} local samples do not fill {n_steps} batches of {batch}")
+    losses = np.zeros(epochs)
+    for ep in range(epochs):
+        lr_ep = cosine_lr(lr, ep, epochs)
+        tot = 0.0
+        for st in range(n_steps):
+            g, loss = grad_fn(dp_rows(n_local, batch, ep, st, seed, rank))
+            g.mul_(1.0 / world)
+            all_reduce(g)
+            apply_fn(g, lr_ep)
+            tot += float(loss)
+        t = torch.tensor([tot / n_steps / world], dtype=torch.float64)
+        all_reduce(t)
+        losses[ep] = float(t.item())
+    return losses
+
+
+class DataParallelSurrogate:
+    """One Surrogate replica per rank of a torch.distributed process group (NCCL, one
+    GPU per rank): its training data stays resident on the rank's device and each step
+    all-reduces the flat gradient in place before the Adam update, through
+    irs_surrogate_grad_device / irs_surrogate_apply_device on the current torch stream.
+    Peer memory is reached only by NCCL."""
+
+    def __init__(self, sur: Surrogate, dist=None):
+        import torch
+        self.sur, self.dist = sur, dist
+        self.torch = torch
+        n = C.c_int64()
+        check(sur.lib.irs_surrogate_grad_size(sur.h, C.byref(n)))
+        self.grad = torch.zeros(n.value, dtype=torch.float32, device="cuda")
+        self.world = dist.get_world_size() if dist is not None else 1
+        self.rank = dist.get_rank() if dist is not None else 0
+
+    def _all_reduce(self, t):
+        if self.dist is None:
+            return
+        if t.device.type == "cpu":  # the loss scalar
+            g = t.to("cuda")
+            self.dist.all_reduce(g)
+            t.copy_(g.cpu())
+        else:
+            self.dist.all_reduce(t)
+
+    def train(self, X_local: np.ndarray, Y_local: np.ndarray, *, epochs: int, batch: int, lr: float = 1e-3,
+              seed: int = 1003, steps_per_epoch: int = None) -> np.ndarray:
+        torch = self.torch
+        sur = self.sur
+        X = torch.from_numpy(np.ascontiguousarray(X_local, dtype=np.float32)).to("cuda")
+        Y = torch.from_numpy(np.ascontiguousarray(Y_local, dtype=np.float32)).to("cuda")
+        sur._check(X_local, Y_local)
+        idx = torch.empty(batch, dtype=torch.int32, device="cuda")
+        loss = C.c_double()
+
+        def grad_fn(rows):
+            idx.copy_(torch.from_numpy(rows))
+            st = torch.cuda.current_stream().cuda_stream
+            check(sur.lib.irs_surrogate_grad_device(sur.h, C.c_void_p(X.data_ptr()), C.c_void_p(Y.data_ptr()),
+                                                    C.cast(C.c_void_p(idx.data_ptr()), C.POINTER(C.c_int32)),
+                                                    len(rows), C.cast(C.c_void_p(self.grad.data_ptr()),
+                                                                      C.POINTER(C.c_float)),
+                                                    C.byref(loss), C.c_void_p(st)))
+            return self.grad, loss.value
+
+        def apply_fn(g, lr_ep):
+            st = torch.cuda.current_stream().cuda_stream
+            check(sur.lib.irs_surrogate_apply_device(sur.h, C.cast(C.c_void_p(g.data_ptr()), C.POINTER(C.c_float)),
+                                                     C.c_float(lr_ep), C.c_void_p(st)))
+
+        return train_data_parallel(grad_fn, apply_fn, len(X_local), batch=batch, epochs=epochs, lr=lr, seed=seed,
+                                   rank=self.rank, world=self.world, all_reduce=self._all_reduce,
+                                   steps_per_epoch=steps_per_epoch)
+
+
 def surrogate_forward_batch(sur: Surrogate, profiles: Sequence, scan_angles, linelists, *, sounder=None,
                             T_sfcs=None, holdout: float = 0.01, seed: int = 0, backend=None, **lbl_kw):
     """Brightness temperatures of a batch from the surrogate, with the line-by-line path
