@@ -11,10 +11,8 @@
 //   FP64: Laplace continued fraction (24 levels) for |x| + y >= 8, else the
 //         Weideman (1994, SIAM J. Numer. Anal. 31:1497) rational series, N = 40.
 //   FP32: continued fraction with 2 levels for |x| + y >= 15, 4 levels for
-//         8 <= |x| + y < 15, else the Weideman series with N = 16.  Worst error
-//         against scipy.special.wofz is ~4e-7 of the line-centre value H(0, y); on a
-//         B200 against faddeeva64 over x in [-20, 20], y in [1e-4, 30]: 4.5e-7, the
-//         same with the MUFU reciprocals in cdiv32 as with correctly rounded ones.
+//         8 <= |x| + y < 15, else the Weideman series with N = 16, each written as
+//         one rational function with a single MUFU reciprocal.
 // The series coefficients are the DFT of exp(-t^2)(L^2 + t^2) at
 // t = L tan(theta/2), computed once on the host (irs_host.cpp) and held in
 // constant memory.
@@ -142,46 +140,61 @@ __device__ __forceinline__ float2 cmul32(float2 a, float2 b) {
     return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 
+// The continued fractions of the FP32 evaluator folded into rational functions, so
+// that each branch takes a single reciprocal (the MUFU pipe runs at an eighth of the
+// FMA rate, and chained reciprocals were the cost of the core pairs):
+//   2 levels, i/sqrt(pi) / (z - 1/2 / (z - 1/z))
+//       = (i/sqrt(pi)) (z^2 - 1) / (z (z^2 - 3/2))
+//   4 levels, i/sqrt(pi) / (z - 1/2 / (z - 1 / (z - 3/2 / (z - 2/z))))
+//       = (i/sqrt(pi)) (u^2 - 9/2 u + 2) / (z (u^2 - 5 u + 15/4)),  u = z^2
+// Over their regions (|z| >= 10.6, resp. 5.6 <= |z| < 15) the polynomials' roots
+// (|u| <= 4.1) are far away, so no cancellation; |den|^2 stays below 3e38 for
+// |z| < 2.6e6.  The Weideman branch shares the reciprocal of |L - i z|^2 between its
+// two divisions.
+
+// w = (i/sqrt(pi)) N / D as (Re, Im), for N = (nr, ni), D = (dr, di)
+__device__ __forceinline__ float2 wz_ratio32(float nr, float ni, float dr, float di) {
+    const float s = (float)kInvSqrtPi * rcp_approx32(fmaf(dr, dr, di * di));
+    return make_float2((nr * di - ni * dr) * s, fmaf(nr, dr, ni * di) * s);
+}
+
+// Faddeeva w(z) for |x| + y >= 15 (two levels); y2 = y^2
+__device__ __forceinline__ float2 faddeeva_cf2(float x, float y, float y2) {
+    const float ur = fmaf(x, x, -y2), ui = 2.f * x * y;              // u = z^2
+    const float cr = ur - 1.5f;                                       // u - 3/2
+    return wz_ratio32(ur - 1.f, ui, fmaf(x, cr, -y * ui), fmaf(x, ui, y * cr));
+}
+
 __device__ __forceinline__ float2 faddeeva32_inline(float x, float y) {
     const float s = fabsf(x) + y;
-    const float2 z = make_float2(x, y);
-    if (s >= 8.0f) {
-        float2 r = make_float2(0.0f, 0.0f);
-        const int K = s >= 15.0f ? 2 : 4;
-        for (int k = K; k >= 1; --k)
-            r = cdiv32(make_float2(0.5f * k, 0.0f), make_float2(z.x - r.x, z.y - r.y));
-        return cdiv32(make_float2(0.0f, (float)kInvSqrtPi), make_float2(z.x - r.x, z.y - r.y));
+    if (s >= 15.0f) return faddeeva_cf2(x, y, y * y);
+    if (s >= 8.0f) {  // four levels
+        const float ur = fmaf(x, x, -y * y), ui = 2.f * x * y;
+        const float ar = ur - 4.5f, br = ur - 5.f;
+        const float nr = fmaf(ur, ar, fmaf(-ui, ui, 2.f)), ni = ui * (ar + ur);        // u (u - 9/2) + 2
+        const float mr = fmaf(ur, br, fmaf(-ui, ui, 3.75f)), mi = ui * (br + ur);      // u (u - 5) + 15/4
+        return wz_ratio32(nr, ni, fmaf(x, mr, -y * mi), fmaf(x, mi, y * mr));          // z m
     }
     const float L = c_fad.w32_L;
-    const float2 den = make_float2(L + y, -x);
-    const float2 num = make_float2(L - y, x);
-    const float2 Z = cdiv32(num, den);
+    const float er = L + y;  // den = L - i z = (er, -x), num = L + i z = (L - y, x)
+    const float inv = rcp_approx32(fmaf(er, er, x * x));
+    const float nr = L - y;
+    // Z = num conj(den) / |den|^2
+    const float2 Z = make_float2(fmaf(nr, er, -x * x) * inv, fmaf(x, er, nr * x) * inv);
     float2 p = make_float2(c_fad.w32_a[0], 0.0f);
 #pragma unroll
     for (int n = 1; n < kW32N; ++n) {
         p = cmul32(p, Z);
         p.x += c_fad.w32_a[n];
     }
-    const float2 d2 = cmul32(den, den);
-    const float2 t1 = cdiv32(make_float2(2.0f * p.x, 2.0f * p.y), d2);
-    const float2 t2 = cdiv32(make_float2((float)kInvSqrtPi, 0.0f), den);
-    return make_float2(t1.x + t2.x, t1.y + t2.y);
+    // w = 2 p / den^2 + (1/sqrt(pi)) / den = (2 p + den / sqrt(pi)) conj(den)^2 / |den|^4
+    const float qr = fmaf(2.f, p.x, er * (float)kInvSqrtPi), qi = fmaf(2.f, p.y, -x * (float)kInvSqrtPi);
+    const float cr = fmaf(er, er, -x * x), ci = 2.f * x * er;  // conj(den)^2
+    const float i2 = inv * inv;
+    return make_float2(fmaf(qr, cr, -qi * ci) * i2, fmaf(qr, ci, qi * cr) * i2);
 }
 // the same as a call (per-point loops, where inlining it would cost registers)
 static __device__ __noinline__ float2 faddeeva32(float x, float y) { return faddeeva32_inline(x, y); }
-
-
-// Faddeeva w(z) for |x| + y >= 15 by the two-level Laplace continued fraction of
-// faddeeva32 (w = i/sqrt(pi) / (z - 1/2 / (z - 1/z))), written out in real arithmetic
-// with three MUFU reciprocals; returns (Re w, Im w)
-__device__ __forceinline__ float2 faddeeva_cf2(float x, float y, float y2) {
-    const float iz = rcp_approx32(fmaf(x, x, y2));                 // 1/|z|^2
-    const float q1x = fmaf(-x, iz, x), q1y = fmaf(y, iz, y);   // z - 1/z
-    const float i1 = 0.5f * rcp_approx32(fmaf(q1x, q1x, q1y * q1y));
-    const float qx = fmaf(-q1x, i1, x), qy = fmaf(q1y, i1, y); // z - (1/2)/(z - 1/z)
-    const float iq = (float)kInvSqrtPi * rcp_approx32(fmaf(qx, qx, qy * qy));
-    return make_float2(qy * iq, qx * iq);
-}
 
 
 // faddeeva32 with its |x| + y >= 15 branch (the two-level continued fraction) inlined

@@ -736,6 +736,36 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
                 rhi = r.y;
                 rb = r.z - r.x;
             }
+            if (METHOD == 3) {
+                // every row: the far wing; rows holding a core point (warp-uniform): the
+                // two-level continued fraction (one reciprocal) at every lane, the inner
+                // points from cw, and an inner point beyond cw through faddeeva32
+                const float y2 = w.y * w.y;
+#pragma unroll
+                for (int q = 0; q < kMxQ; ++q) {
+                    const float d = ((pl0 + 32.f * q) - u.x) - u.y;
+                    const float d2 = d * d;
+                    const float ped = fmaf(p.x, d2, p.y);
+                    const float r = rcp_fast(d2 + u.z);
+                    float v = fmaf(u.w, r, ped), vd = w.z * d * r;
+                    const bool core = d2 <= p.z;  // |x| <= x_far
+                    if (__any_sync(kFull, core)) {
+                        const float x = d * w.x;
+                        const int pt = lane + 32 * q;
+                        float2 fw = faddeeva_cf2(x, w.y, y2);
+                        if (pt >= rlo && pt <= rhi) fw = T.cw[rb + pt];
+                        else if (core && fabsf(x) + w.y < 15.f) fw = faddeeva32(x, w.y);
+                        if (core) {
+                            v = fmaf(p.w, fw.x, ped);
+                            vd = w.w * fw.y;
+                        }
+                    }
+                    if (d2 > cut2) v = vd = 0.f;
+                    tacc[q] += v;
+                    if (LM) tdsp[q] += vd;
+                }
+                continue;
+            }
 #pragma unroll
             for (int q = 0; q < kMxQ; ++q) {
                 const float d = ((pl0 + 32.f * q) - u.x) - u.y;
@@ -743,17 +773,9 @@ __device__ __forceinline__ void warp_segment(const SegDev& sg, long long cnt, co
                 if (d2 > cut2) continue;
                 const float ped = fmaf(p.x, d2, p.y);
                 float v, vd;
-                if (d2 <= p.z) {  // |x| <= x_far: Faddeeva core
-                    const float x = d * w.x;
-                    if (METHOD == 1) {
-                        v = fmaf(p.w, weideman24_32(x, w.y), ped);
-                        vd = 0.f;
-                    } else {
-                        const int pt = lane + 32 * q;
-                        const float2 fw = (pt >= rlo && pt <= rhi) ? T.cw[rb + pt] : faddeeva32_fast(x, w.y);
-                        v = fmaf(p.w, fw.x, ped);
-                        vd = w.w * fw.y;
-                    }
+                if (d2 <= p.z) {  // |x| <= x_far: Faddeeva core (Weideman-24)
+                    v = fmaf(p.w, weideman24_32(d * w.x, w.y), ped);
+                    vd = 0.f;
                 } else {
                     const float r = rcp_fast(d2 + u.z);
                     v = fmaf(u.w, r, ped);

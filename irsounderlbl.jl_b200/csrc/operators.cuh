@@ -36,6 +36,17 @@ __global__ void __launch_bounds__(256) voigt_profile_kernel(const double* __rest
     out[i] = f * H * kInvSqrtPi;
 }
 
+// w(x + i y) with the FP32 evaluator of the mixed line sums (faddeeva32: the rational
+// continued fractions and the Weideman N = 16 series), for checking it on its own
+__global__ void __launch_bounds__(256) faddeeva32_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                                                         long long n, double* __restrict__ re, double* __restrict__ im) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float2 w = faddeeva32_inline((float)x[i], (float)y[i]);
+    re[i] = (double)w.x;
+    im[i] = (double)w.y;
+}
+
 // w(x + i y) = erfcx(y - i x), FP64
 __global__ void __launch_bounds__(256) faddeeva_kernel(const double* __restrict__ x, const double* __restrict__ y,
                                                        long long n, double* __restrict__ re, double* __restrict__ im) {

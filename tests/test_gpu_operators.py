@@ -43,6 +43,29 @@ def test_faddeeva(pkg, ctx, oracle):
         pkg.faddeeva(1.0, -1.0, backend=ctx)
 
 
+def test_faddeeva32_against_wofz(pkg, ctx, golden):
+    """The FP32 evaluator of the mixed line sums (rational continued fractions with one
+    reciprocal, Weideman N = 16) against scipy's wofz on the golden grid: every point
+    within 2e-6 of the line-centre value Re w(i y) (the FP32 accuracy the mixed path's
+    0.01 K budget rests on; ~5e-7 expected), on each side of the region switches."""
+    import ctypes as C
+    d = golden["wofz"]
+    x, y = np.ascontiguousarray(d["x"]), np.ascontiguousarray(d["y"])
+    keep = (np.abs(x) <= 122.0) & (y <= 100.0)  # the Faddeeva core of the line sums
+    x, y = np.ascontiguousarray(x[keep]), np.ascontiguousarray(y[keep])
+    re, im = np.empty(len(x)), np.empty(len(x))
+    pkg.check(ctx.lib.irs_faddeeva32(ctx.h, pkg._lib.dptr(x), pkg._lib.dptr(y), len(x), pkg._lib.dptr(re),
+                                     pkg._lib.dptr(im)))
+    from scipy.special import erfcx
+    centre = erfcx(y)  # Re w(i y)
+    err = np.maximum(np.abs(re - d["re"][keep]), np.abs(im - d["im"][keep])) / centre
+    s = np.abs(x) + y
+    for lo, hi in ((0, 8), (8, 15), (15, np.inf)):
+        m = (s >= lo) & (s < hi)
+        assert m.sum() > 100, (lo, hi)
+        assert err[m].max() < 2e-6, (lo, hi, err[m].max())
+
+
 @pytest.mark.parametrize("apod", ["gaussian", "norton_beer_weak", "norton_beer_medium", "norton_beer_strong"])
 def test_ils_kernel_and_apply(pkg, ctx, oracle, apod):
     d, k = pkg.ils_kernel(0.01, 2.0, 0.5, apod, backend=ctx)
