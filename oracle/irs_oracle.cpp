@@ -843,6 +843,20 @@ void species_grad(const orc_line* ll, long nL, const double* y0, bool lm, const 
 }  // namespace
 
 // =================================================================== C ABI
+// The lines of a list (sorted by wavenumber) that can reach grid [lo, hi]: centres
+// within the cutoff plus 1 cm^-1 (more than any pressure shift) of it.  Lines beyond
+// contribute nothing to the window, so leaving them out of a windowed run changes no
+// result; an unsorted list is used whole.
+static void reach_range(const orc_line* ll, long nL, double lo, double hi, double reach, long& a, long& b) {
+    a = 0;
+    b = nL;
+    for (long j = 1; j < nL; ++j)
+        if (ll[j].wavenumber < ll[j - 1].wavenumber) return;
+    const double vlo = lo - reach - 1.0, vhi = hi + reach + 1.0;
+    a = (long)(std::lower_bound(ll, ll + nL, vlo, [](const orc_line& l, double v) { return l.wavenumber < v; }) - ll);
+    b = (long)(std::upper_bound(ll, ll + nL, vhi, [](double v, const orc_line& l) { return v < l.wavenumber; }) - ll);
+}
+
 extern "C" {
 
 const char* orc_last_error(void) { return g_err.c_str(); }
@@ -1069,8 +1083,12 @@ int orc_forward_model(int n_lev, const double* p_lev, const double* T_lev, int n
             const double Tcg = o->T_method == 1 ? T_mass[k] : Ti(pcg);
             const double vs = sp == 1 ? vmr : 0.0;
             const double coef = vmr * dp[k] * NAIR_PER_VMR;
-            const orc_line* ll = lines + loff[li];
-            const long nL = (long)(loff[li + 1] - loff[li]);
+            long ja = 0, jb = 0;
+            reach_range(lines + loff[li], (long)(loff[li + 1] - loff[li]), grid.front(), grid.back(),
+                        std::max(o->cutoff, o->lm_cutoff), ja, jb);
+            const orc_line* ll = lines + loff[li] + ja;
+            const long nL = jb - ja;
+            const double* y0l = y0 ? y0 + loff[li] + ja : nullptr;
             // sounder.jl:294-300: DPTMIN is skipped for CO2 under any line-mixing model
             const bool lm_co2 = sp == 2 && o->line_mixing == 1;
             const bool no_dpt = sp == 2 && o->line_mixing != 0;
@@ -1088,7 +1106,7 @@ int orc_forward_model(int n_lev, const double* p_lev, const double* T_lev, int n
             if (lm_co2) {
                 voigt_xsec(use, nuse, grid.data(), nw, Tcg, p_atm, 0.0, o->cutoff, 3, o->x_far, sig.data());
                 if (y0) {
-                    lm_dispersive(use, nuse, y0 + loff[li], grid.data(), nw, Tcg, p_atm, o->lm_cutoff, o->x_far, ds.data());
+                    lm_dispersive(use, nuse, y0l, grid.data(), nw, Tcg, p_atm, o->lm_cutoff, o->x_far, ds.data());
                     for (long i = 0; i < nw; ++i) sig[i] = std::max(sig[i] + ds[i], 0.0);
                 }
             } else if (relmat) {  // compute_voigt_{lm,vpw}_cross_sections, line_mixing.jl:1093-1110, 1351-1369
@@ -1243,11 +1261,14 @@ int orc_analytic_jacobian(int n_lev, const double* p_lev, const double* T_lev, i
             const double Tcg = o->T_method == 1 ? T_ave[k] : Ti(pcg);
             const double vs = sp == 1 ? vmr : 0.0;
             const double coef = vmr * dp[k] * NAIR_PER_VMR;
-            const orc_line* ll = lines + loff[li];
-            const long nL = (long)(loff[li + 1] - loff[li]);
+            long ja = 0, jb = 0;
+            reach_range(lines + loff[li], (long)(loff[li + 1] - loff[li]), grid.front(), grid.back(),
+                        std::max(o->cutoff, o->lm_cutoff), ja, jb);
+            const orc_line* ll = lines + loff[li] + ja;
+            const long nL = jb - ja;
             const bool lm = sp == 2 && o->line_mixing == 1;
             Grad g;
-            species_grad(ll, nL, y0 ? y0 + loff[li] : nullptr, lm, grid.data(), nw, Tcg, p_atm, vs, o->cutoff,
+            species_grad(ll, nL, y0 ? y0 + loff[li] + ja : nullptr, lm, grid.data(), nw, Tcg, p_atm, vs, o->cutoff,
                          o->lm_cutoff, o->x_far, g);
             const size_t base = (size_t)k * nw;
             if (include_T) {
