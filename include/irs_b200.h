@@ -250,7 +250,7 @@ typedef struct {
  * Arrays: base [n_scene]; y_obs, se_inv, y_fit [n_scene][n_channels]; xa, x0, x_out
  * [n_scene][n_state]; Sa_inv [n_state][n_state] (shared); M_out [n_scene][n_state]
  * [n_state] = K^T Se^-1 K at the solution; n_iter, converged, cost [n_scene].
- * At most 127 state elements. */
+ * At most 160 state elements. */
 int irs_oe_batch(irs_ctx* ctx, const irs_profile* base, int n_scene, const irs_sounder* s,
                  const irs_fm_options* o, const irs_state_spec* spec, const double* y_obs,
                  const double* se_inv, const double* xa, const double* Sa_inv, const double* x0,

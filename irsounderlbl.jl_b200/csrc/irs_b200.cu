@@ -1004,21 +1004,25 @@ static void launch_oe_normal(irs_ctx* ctx, const int* d_list, int n_list, int n,
     const size_t smem = (size_t)(2 * kOeTile * n + kOeTile) * sizeof(double);
     static bool attr = false;
     if (!attr) {
-        IRS_CUDA(cudaFuncSetAttribute(oe_normal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        IRS_CUDA(cudaFuncSetAttribute(oe_normal_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        IRS_CUDA(cudaFuncSetAttribute(oe_normal_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         attr = true;
     }
     const int grid = std::min(n_list, 148 * 4);
-    oe_normal_kernel<<<grid, kOeThreads, smem, ctx->stream>>>(d_list, n_list, n, n_ch, K, w, r, M, b);
+    if (n * (n + 1) / 2 <= 256 * kOePairsPerThread)
+        oe_normal_kernel<256><<<grid, 256, smem, ctx->stream>>>(d_list, n_list, n, n_ch, K, w, r, M, b);
+    else
+        oe_normal_kernel<512><<<grid, 512, smem, ctx->stream>>>(d_list, n_list, n, n_ch, K, w, r, M, b);
     check_launch(ctx);
 }
 
 static void launch_oe_solve(irs_ctx* ctx, const int* d_list, int n_list, int n, const double* M, const double* b,
                             const double* Sa_inv, const double* x, const double* xa, const double* gamma, double* dx,
                             double* d2, int* ok) {
-    const size_t smem = ((size_t)n * n + 4 * (size_t)n) * sizeof(double);
+    const size_t smem = ((size_t)n * n + 4 * (size_t)n) * sizeof(double);  // 210 KB at n = 160
     static bool attr = false;
     if (!attr) {
-        IRS_CUDA(cudaFuncSetAttribute(oe_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        IRS_CUDA(cudaFuncSetAttribute(oe_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
         attr = true;
     }
     const int grid = std::min(n_list, 148);
@@ -1047,7 +1051,7 @@ static void oe_batch(irs_ctx* ctx, const irs_profile* base, int n_scene, const i
     IRS_REQUIRE(prm.method == 0 || prm.method == 1, "method must be 0 (levenberg_marquardt) or 1 (gauss_newton)");
     IRS_REQUIRE(prm.max_iter >= 1 && prm.max_linesearch >= 1, "max_iter and max_linesearch must be positive");
     const int n = (int)state_size(sp, base[0].n_lev);
-    IRS_REQUIRE(n >= 1 && n <= kOeMaxState, "the state vector must have 1 to 127 elements on this path");
+    IRS_REQUIRE(n >= 1 && n <= kOeMaxState, "the state vector must have 1 to 160 elements on this path");
     const int64_t n_ch = make_grid(s.nu_min, s.nu_max, s.dnu).n;
     irs_fm_options o = o_in;
     o.dptmn = 0.0;  // frozen line set for F as for K (optimal_estimation.jl:193-198)

@@ -12,35 +12,36 @@
 
 namespace irs {
 
-constexpr int kOeThreads = 256;
-constexpr int kOeMaxState = 127;  // n (n + 1) / 2 pairs <= 32 per thread
-constexpr int kOePairsPerThread = 32;
+constexpr int kOeThreads = 256;   // oe_solve_kernel; oe_normal_kernel takes 256 or 512
+constexpr int kOeMaxState = 160;  // the Cholesky's n x n FP64 matrix in shared memory (200 KB)
+constexpr int kOePairsPerThread = 32;  // n (n + 1) / 2 pairs <= 32 per thread of oe_normal_kernel
 constexpr int kOeTile = 32;       // channels per shared-memory tile
 
-// shared memory: tile [kOeTile][n] of K and of K * w, plus w r per channel
-__global__ void __launch_bounds__(kOeThreads) oe_normal_kernel(const int* __restrict__ list, int n_list, int n,
-                                                               int n_ch, const float* __restrict__ K,
-                                                               const double* __restrict__ w,
-                                                               const double* __restrict__ r, double* __restrict__ M,
-                                                               double* __restrict__ b) {
+// shared memory: tile [kOeTile][n] of K and of K * w, plus w r per channel.  THREADS
+// x 32 pairs cover the upper triangle: 256 threads up to n = 127, 512 up to n = 180.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) oe_normal_kernel(const int* __restrict__ list, int n_list, int n,
+                                                            int n_ch, const float* __restrict__ K,
+                                                            const double* __restrict__ w,
+                                                            const double* __restrict__ r, double* __restrict__ M,
+                                                            double* __restrict__ b) {
     extern __shared__ double sh[];
     double* tk = sh;                       // [kOeTile][n]
     double* tw = sh + kOeTile * n;         // [kOeTile][n] (K w)
     double* wr = tw + kOeTile * n;         // [kOeTile]
     const int P = n * (n + 1) / 2;
-    int pi[kOePairsPerThread], pj[kOePairsPerThread];
+    int pij[kOePairsPerThread];            // (i << 8) | j, or -1
 #pragma unroll
     for (int k = 0; k < kOePairsPerThread; ++k) {
-        int p = threadIdx.x + k * kOeThreads, i = 0;
+        int p = threadIdx.x + k * THREADS, i = 0;
         if (p < P) {  // row-major upper triangle: row i holds n - i pairs
             while (p >= n - i) {
                 p -= n - i;
                 ++i;
             }
-            pi[k] = i;
-            pj[k] = i + p;
+            pij[k] = (i << 8) | (i + p);
         } else {
-            pi[k] = pj[k] = -1;
+            pij[k] = -1;
         }
     }
     for (int a = blockIdx.x; a < n_list; a += gridDim.x) {
@@ -54,14 +55,14 @@ __global__ void __launch_bounds__(kOeThreads) oe_normal_kernel(const int* __rest
         double bacc = 0.0;
         for (int c0 = 0; c0 < n_ch; c0 += kOeTile) {
             __syncthreads();
-            for (int idx = threadIdx.x; idx < n * kOeTile; idx += kOeThreads) {
+            for (int idx = threadIdx.x; idx < n * kOeTile; idx += THREADS) {
                 const int i = idx / kOeTile, c = idx % kOeTile;
                 const bool in = c0 + c < n_ch;
                 const double kv = in ? (double)Ks[(size_t)i * n_ch + c0 + c] : 0.0;
                 tk[c * n + i] = kv;
                 tw[c * n + i] = in ? kv * ws[c0 + c] : 0.0;
             }
-            for (int c = threadIdx.x; c < kOeTile; c += kOeThreads)
+            for (int c = threadIdx.x; c < kOeTile; c += THREADS)
                 wr[c] = c0 + c < n_ch ? ws[c0 + c] * rs[c0 + c] : 0.0;
             __syncthreads();
 #pragma unroll 4
@@ -70,16 +71,17 @@ __global__ void __launch_bounds__(kOeThreads) oe_normal_kernel(const int* __rest
                 const double* roww = tw + c * n;
 #pragma unroll
                 for (int k = 0; k < kOePairsPerThread; ++k)
-                    if (pi[k] >= 0) acc[k] = fma(rowk[pi[k]], roww[pj[k]], acc[k]);
+                    if (pij[k] >= 0) acc[k] = fma(rowk[pij[k] >> 8], roww[pij[k] & 255], acc[k]);
                 if (threadIdx.x < n) bacc = fma(rowk[threadIdx.x], wr[c], bacc);
             }
         }
         double* Ms = M + (size_t)s * n * n;
 #pragma unroll
         for (int k = 0; k < kOePairsPerThread; ++k)
-            if (pi[k] >= 0) {
-                Ms[(size_t)pi[k] * n + pj[k]] = acc[k];
-                Ms[(size_t)pj[k] * n + pi[k]] = acc[k];
+            if (pij[k] >= 0) {
+                const int i = pij[k] >> 8, j = pij[k] & 255;
+                Ms[(size_t)i * n + j] = acc[k];
+                Ms[(size_t)j * n + i] = acc[k];
             }
         if (threadIdx.x < n) b[(size_t)s * n + threadIdx.x] = bacc;
     }

@@ -183,3 +183,37 @@ def test_apodized_se_vs_oracle(pkg, ctx, oracle, orc_mod, masked):
     rd = pkg.optimal_estimation(y, spec, base, llp, xa=xa, Sa=Sa, Se=np.diag(Se), channel_mask=keep, sounder=snd,
                                 backend=ctx, fm_kwargs=KW)
     assert np.max(np.abs(rd.x - res.x) / sd) > 0.01
+
+
+def test_gauss_newton_step_151_elements(pkg, ctx, oracle, orc_mod):
+    """Config 2's state (T + log H2O + log O3 + T_sfc on 50 levels = 151 elements, above
+    the 127 that one 256-thread block of the normal equations covers): one Gauss-Newton
+    step against the oracle, within 0.02 posterior sigma."""
+    import oe_oracle
+    a = np.zeros(7, dtype=orc_mod.LINE_DTYPE)
+    spec_lines = [(2, 700.5, 2.0e-21, 250.0), (2, 702.0, 8.0e-22, 600.0), (2, 703.6, 1.5e-21, 400.0),
+                  (1, 701.1, 3.0e-21, 200.0), (1, 704.2, 1.0e-21, 900.0),
+                  (3, 699.8, 4.0e-21, 300.0), (3, 702.9, 2.0e-21, 150.0)]
+    for k, (mol, nu, S, E) in enumerate(spec_lines):
+        a[k] = (mol, 1, nu, S, 1.0, 0.07, 0.09, E, 0.75, -0.003)
+    ll = {m: a[a["mol_id"] == m] for m in (1, 2, 3)}
+    llp = {m: pkg.HITRANLinelist(v) for m, v in ll.items()}
+    base = pkg.afgl_atmosphere("midlatitude_summer")
+    spec = pkg.StateVectorSpec(50, [pkg.H2O, pkg.O3], include_emissivity=False)
+    assert spec.n == 151
+    xa = pkg.pack_state(spec, base)
+    Sa = pkg.build_sa(spec, base, sigma_T=2.0, sigma_vmr=0.2)
+    rng = np.random.default_rng(151)
+    xt = xa + np.linalg.cholesky(Sa) @ rng.standard_normal(spec.n)
+    snd = pkg.Sounder.make(**IASI_SUB)
+    prof, Ts, _ = pkg.unpack_state(spec, xt, base)
+    y = pkg.forward_model(prof, llp, sounder=snd, T_sfc=Ts, backend=ctx, dptmn=0.0, **KW)[2]
+    se = np.full(len(y), 0.2 ** 2)
+    r = pkg.optimal_estimation_batch(y[None], spec, [base], llp, xa=xa, Sa=Sa, Se=se, method="gauss_newton",
+                                     max_iter=1, sounder=snd, backend=ctx, fm_kwargs=KW)
+    fwd, fwd_jac = oracle_fns(pkg, oracle, orc_mod, spec, base, ll)
+    ro = oe_oracle.optimal_estimation(y, fwd, fwd_jac, xa, Sa, se, method="gauss_newton", max_iter=1)
+    sd = np.sqrt(np.diag(np.linalg.inv(np.linalg.inv(Sa) + ro["M"])))
+    assert r["n_iter"][0] == ro["n_iter"] == 1
+    assert np.max(np.abs(r["x"][0] - ro["x"]) / sd) < 0.02
+    assert np.allclose(r["M"][0], ro["M"], rtol=1e-3, atol=1e-4 * np.max(np.abs(ro["M"])))
