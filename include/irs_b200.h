@@ -214,7 +214,8 @@ int irs_jacobian_batch(irs_ctx* ctx, const irs_profile* profs, int n_prof, const
  * profile loop is sequential (sounder.jl:283-307): the batch is split into contiguous
  * shards (irs_shard_range), each run by its own host thread through
  * irs_forward_model_batch on its context, and the shards' R and BT are written to the
- * caller's host buffers [n_prof][n_channels] at their offsets.  No collective. */
+ * caller's host buffers [n_prof][n_channels] at their offsets.  No collective.  A
+ * context serves one host thread at a time, so each may appear once in ctxs. */
 int irs_forward_model_batch_multi(irs_ctx* const* ctxs, int n_ctx, const irs_profile* profs, int n_prof,
                                   const irs_sounder* s, const irs_fm_options* o, double* R, double* BT);
 /* The shard of n items that shard `shard` of n_shards takes: [*first, *first + *count),

@@ -39,11 +39,18 @@ extern "C" int irs_forward_model_batch_multi(irs_ctx* const* ctxs, int n_ctx, co
         irs::set_error("irs_forward_model_batch_multi: invalid arguments");
         return IRS_E_ARG;
     }
-    for (int k = 0; k < n_ctx; ++k)
+    for (int k = 0; k < n_ctx; ++k) {
         if (!ctxs[k]) {
             irs::set_error("irs_forward_model_batch_multi: context " + std::to_string(k) + " is NULL");
             return IRS_E_ARG;
         }
+        for (int j = 0; j < k; ++j)  // a context serves one host thread at a time
+            if (ctxs[j] == ctxs[k]) {
+                irs::set_error("irs_forward_model_batch_multi: context " + std::to_string(k) +
+                               " repeats context " + std::to_string(j) + " (each context may appear once)");
+                return IRS_E_ARG;
+            }
+    }
     const int64_t n_ch = irs::make_grid(s->nu_min, s->nu_max, s->dnu).n;  // as irs_forward_model_batch
     std::vector<int> rc(n_ctx, IRS_OK);
     std::vector<std::string> msg(n_ctx);

@@ -297,6 +297,55 @@ def surrogate_forward_batch(sur: Surrogate, profiles: Sequence, scan_angles, lin
     return res
 
 
+def _state_feature_columns(spec, n_in: int):
+    """The surrogate input column of every state element when the state is the
+    full-profile [T][log VMR H2O][log VMR O3][T_sfc][eps] layout the features share
+    (-1: no feature, as eps), else None."""
+    n_lev = spec.n_levels
+    if n_in != 3 * n_lev + 2:
+        return None
+    cols = np.full(spec.n, -1, dtype=np.int64)
+    if spec.include_temperature:
+        cols[spec.temp_range.start:spec.temp_range.stop] = np.arange(n_lev)
+    for b in spec.vmr_blocks:
+        if b.basis is not None or not spec.log_vmr or int(b.species) not in (1, 3):
+            return None
+        off = n_lev if int(b.species) == 1 else 2 * n_lev
+        cols[b.range.start:b.range.stop] = off + np.arange(n_lev)
+    if spec.tsfc_index >= 0:
+        cols[spec.tsfc_index] = 3 * n_lev
+    return cols
+
+
+def _first_guess_columns(sur, ys, spec, base_list, scan_angles, xa, Sa, Se, n_iter, step, cols):
+    """surrogate_first_guess when the state maps onto feature columns: the perturbed
+    inputs are the scene's features moved in one column, all scenes' 2 n + 1 samples go
+    to the network in one call and the Gauss-Newton systems are solved as one batch."""
+    from .estimation import unpack_state
+    S, n = ys.shape[0], spec.n
+    w = 1.0 / Se
+    Sa_inv = np.linalg.inv(Sa)
+    x = np.array(xa, dtype=np.float64)
+    has = cols >= 0
+    for _ in range(n_iter):
+        rows = [unpack_state(spec, x[s_], base_list[s_]) for s_ in range(S)]
+        F0 = surrogate_features([r[0] for r in rows], scan_angles, [r[1] for r in rows]).astype(np.float64)
+        Xp = np.repeat(F0[:, None, :], 2 * n + 1, axis=1)  # [S, 2n + 1, n_in]
+        j = np.flatnonzero(has)
+        Xp[:, 1 + 2 * j, cols[j]] += step
+        Xp[:, 2 + 2 * j, cols[j]] -= step
+        F, _ = sur.predict(np.ascontiguousarray(Xp.reshape(-1, Xp.shape[2]), dtype=np.float32))
+        F = F.astype(np.float64).reshape(S, 2 * n + 1, -1)
+        K = np.transpose((F[:, 1::2] - F[:, 2::2]) / (2 * step), (0, 2, 1))  # [S, n_ch, n]
+        K[:, :, ~has] = 0.0
+        KtW = np.transpose(K, (0, 2, 1)) * w[:, None, :]
+        H = Sa_inv[None] + KtW @ K
+        r = ys - F[:, 0] + np.einsum("sij,sj->si", K, x - xa)
+        g = np.einsum("sij,sj->si", KtW, r)
+        x = xa + np.linalg.solve(H, g[..., None])[..., 0]
+    return x
+
+
 def surrogate_first_guess(sur: Surrogate, ys, spec, base_profs, scan_angles, *, xa, Sa, Se, n_iter: int = 4,
                           step: float = 1e-2):
     """First guesses of a batched retrieval from the surrogate: Gauss-Newton MAP steps
@@ -310,6 +359,10 @@ def surrogate_first_guess(sur: Surrogate, ys, spec, base_profs, scan_angles, *, 
     S, n = len(ys), spec.n
     xa = np.broadcast_to(np.asarray(xa, dtype=np.float64), (S, n))
     Se = np.broadcast_to(np.asarray(Se, dtype=np.float64), ys.shape)
+    base_list = list(base_profs) if isinstance(base_profs, (list, tuple)) else [base_profs] * S
+    cols = _state_feature_columns(spec, sur.n_in)
+    if cols is not None:
+        return _first_guess_columns(sur, ys, spec, base_list, scan_angles, xa, Sa, Se, n_iter, step, cols)
     w = 1.0 / Se
     Sa_inv = np.linalg.inv(Sa)
     base_profs = list(base_profs) if isinstance(base_profs, (list, tuple)) else [base_profs] * S

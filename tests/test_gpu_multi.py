@@ -36,18 +36,21 @@ def _case(pkg, n):
 def test_multi_context_batch_equals_single(pkg):
     lists, profs, snd = _case(pkg, 5)
     kw = dict(internal_dnu=0.0025, apply_continuum=True, continua=("h2o", "co2"), precision="mixed")
-    a, b = pkg.B200Context(0), pkg.B200Context(0)
+    a, b, c = pkg.B200Context(0), pkg.B200Context(0), pkg.B200Context(0)
     try:
         _, R1, BT1 = pkg.forward_model_batch(profs, lists, sounder=snd, backend=a, **kw)
-        for ctxs in ([a, b], [a, b, a]):  # 3 + 2 and 2 + 2 + 1 profiles
+        for ctxs in ([a, b], [a, b, c]):  # 3 + 2 and 2 + 2 + 1 profiles
             _, R, BT = pkg.forward_model_batch_multi(profs, lists, backends=ctxs, sounder=snd, **kw)
             assert np.array_equal(BT, BT1) and np.array_equal(R, R1), len(ctxs)
+        with pytest.raises(pkg.IRSError, match="appear once"):  # one context is one host thread's
+            pkg.forward_model_batch_multi(profs, lists, backends=[a, b, a], sounder=snd, **kw)
         _, R, BT = pkg.forward_model_batch_distributed(profs, lists, dist=None, backend=a, sounder=snd, **kw)
         assert np.array_equal(BT, BT1)
         assert len(np.unique(BT1[:, 10])) == len(profs)
     finally:
         a.close()
         b.close()
+        c.close()
 
 
 def test_data_parallel_step_one_rank(pkg):

