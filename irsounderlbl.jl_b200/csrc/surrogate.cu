@@ -55,34 +55,58 @@ static CUtensorMap make_map(const void* ptr, int64_t rows, int64_t cols, int64_t
     return m;
 }
 
-// 128 x 128 tiles (two CTAs per SM, so one CTA's epilogue runs under the other's main
-// loop).  The 128 x 256 variant (one CTA per SM, half the B-operand traffic per FLOP)
-// measured slower on the 1024 -> 8461 output layer (261 vs 189 us per 4096 batch):
-// without a second CTA its epilogue is exposed.
+// SM count and "max dynamic shared memory" attribute per device (a process may drive
+// several devices, one host thread each)
+static int sm_count(int dev) {
+    static std::mutex mu;
+    static int cached[64] = {};
+    IRS_REQUIRE(dev >= 0 && dev < 64, "device index");
+    std::lock_guard<std::mutex> lk(mu);
+    if (!cached[dev]) IRS_CUDA(cudaDeviceGetAttribute(&cached[dev], cudaDevAttrMultiProcessorCount, dev));
+    return cached[dev];
+}
+
 template <int EPI, int TBN>
-static void gemm_tbn(cudaStream_t st, const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int M, int N, int K,
-                     umma::EpiArgs ep) {
+static void gemm_tbn(cudaStream_t st, int dev, int nsm, const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int M,
+                     int N, int K, umma::EpiArgs ep) {
     using Cfg = umma::TileCfg<TBN>;
-    static bool attr = false;
-    if (!attr) {
-        IRS_CUDA(cudaFuncSetAttribute(umma::umma_gemm_kernel<EPI, TBN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)Cfg::kSmemBytes));
-        attr = true;
+    static std::mutex mu;
+    static uint64_t attr_set = 0;  // bit d: attribute set on device d
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!(attr_set >> dev & 1u)) {
+            IRS_CUDA(cudaFuncSetAttribute(umma::umma_gemm_kernel<EPI, TBN>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::kSmemBytes));
+            attr_set |= (uint64_t)1 << dev;
+        }
     }
     const CUtensorMap ta = make_map(A, M, K, lda, umma::BM);
     const CUtensorMap tb = make_map(B, N, K, ldb, TBN);
     ep.M = M;
     ep.N = N;
-    const dim3 grid((unsigned)((N + TBN - 1) / TBN), (unsigned)((M + umma::BM - 1) / umma::BM));
+    const int64_t tiles = (int64_t)((M + umma::BM - 1) / umma::BM) * ((N + TBN - 1) / TBN);
+    const unsigned grid = (unsigned)std::min<int64_t>(tiles, nsm);  // persistent: one CTA per SM at most
     umma::umma_gemm_kernel<EPI, TBN><<<grid, umma::kThreads, Cfg::kSmemBytes, st>>>(ta, tb, K, ep);
 }
 
+// Tile width: 128 x 256 tiles halve the B-operand traffic per FLOP; 128 x 128 tiles are
+// taken when they spread a small problem over clearly more SMs (the makespan in units
+// of a 128 x 128 tile, rounds x tile cost, at least 25 % shorter).
 template <int EPI>
 static void gemm(cudaStream_t st, const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int M, int N, int K,
                  umma::EpiArgs ep) {
     const bool f32_out = EPI == umma::EPI_F32 || EPI == umma::EPI_BIAS_F32;
     IRS_REQUIRE(M >= 1 && N >= 1 && K >= 1 && ep.ldc >= N && (f32_out || ep.ldc % 8 == 0), "GEMM sizes");
-    gemm_tbn<EPI, 128>(st, A, lda, B, ldb, M, N, K, ep);
+    int dev = 0;
+    IRS_CUDA(cudaGetDevice(&dev));
+    const int nsm = sm_count(dev);
+    const int64_t mb = (M + umma::BM - 1) / umma::BM;
+    const int64_t t128 = mb * ((N + 127) / 128), t256 = mb * ((N + 255) / 256);
+    const int64_t cost128 = (t128 + nsm - 1) / nsm, cost256 = 2 * ((t256 + nsm - 1) / nsm);
+    if (4 * cost128 <= 3 * cost256)
+        gemm_tbn<EPI, 128>(st, dev, nsm, A, lda, B, ldb, M, N, K, ep);
+    else
+        gemm_tbn<EPI, 256>(st, dev, nsm, A, lda, B, ldb, M, N, K, ep);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) throw Error{IRS_E_CUDA, std::string("GEMM launch: ") + cudaGetErrorString(e)};
 }
@@ -283,7 +307,7 @@ static void forward(irs_surrogate* s, int B, float* yout = nullptr, int ldy = 0)
         ep.err = s->err;
         if (l < s->nl - 1) {
             ep.Cb = s->act[l + 1];
-            ep.Z = s->z[l];
+            ep.Z = yout ? nullptr : s->z[l];  // inference keeps no pre-activations
             ep.ldc = s->pout[l];
             gemm<umma::EPI_GELU_FWD>(st, s->act[l], s->pin[l], s->wb + s->woff[l], s->pin[l], B, s->pout[l], s->pin[l], ep);
         } else if (yout) {
