@@ -86,7 +86,19 @@ static void gemm_tbn(cudaStream_t st, int dev, int nsm, const bf16* A, int64_t l
     ep.N = N;
     const int64_t tiles = (int64_t)((M + umma::BM - 1) / umma::BM) * ((N + TBN - 1) / TBN);
     const unsigned grid = (unsigned)std::min<int64_t>(tiles, nsm);  // persistent: one CTA per SM at most
-    umma::umma_gemm_kernel<EPI, TBN><<<grid, umma::kThreads, Cfg::kSmemBytes, st>>>(ta, tb, K, ep);
+    // programmatic dependent launch: the kernel waits (griddepcontrol.wait) for the
+    // previous grid before touching global memory, so only its prologue overlaps
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(umma::kThreads);
+    cfg.dynamicSmemBytes = Cfg::kSmemBytes;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    IRS_CUDA(cudaLaunchKernelEx(&cfg, umma::umma_gemm_kernel<EPI, TBN>, ta, tb, K, ep));
 }
 
 // Tile width: 128 x 256 tiles halve the B-operand traffic per FLOP; 128 x 128 tiles are

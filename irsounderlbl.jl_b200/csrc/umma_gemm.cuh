@@ -419,6 +419,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int ntiles = mblocks * ((ep.N + BN - 1) / BN);
 
     if (threadIdx.x == 0) {
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmA) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmB) : "memory");
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
@@ -442,6 +444,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
+    // Launched with programmatic stream serialization: the next kernel in the stream may
+    // start its own prologue on idle SMs now, and this grid's reads and writes of global
+    // memory wait until the previous grid has completed (its outputs are our operands).
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 
     if (warp == 0) {
         if (lane == 0) {  // TMA producer
