@@ -295,7 +295,7 @@ def oe_config4(pkg, ctx, n_sc: int = 1024, n_train: int = 16384):
                    "scenes": "perturbed-AFGL sampler (seed 1004) on the US-standard pressure grid, scan angles"}}
 
 
-def surrogate_iasi_accuracy(pkg, ctx, lists, n_train: int = 4096, n_test: int = 256):
+def surrogate_iasi_accuracy(pkg, ctx, lists, n_train: int = 12288, n_test: int = 256, epochs: int = 200):
     """The config-3 network (152 -> 4 x 1024 GELU -> 8461) trained only on n_train GPU-LBL
     IASI spectra (400k lines, mixed precision, the perturbed-AFGL sampler with scan angles)
     and judged by LBL on n_test held-out spectra of the same sampler."""
@@ -310,7 +310,7 @@ def surrogate_iasi_accuracy(pkg, ctx, lists, n_train: int = 4096, n_test: int = 
     t0 = time.perf_counter()
     sur = pkg.Surrogate(ctx, n_in=X.shape[1], n_hidden=1024, n_layers=4, n_out=BT.shape[1], seed=3)
     sur.fit_scaling(X[tr], BT[tr])
-    sur.train(X[tr], BT[tr].astype(np.float32), epochs=300, batch=256, lr=1e-3, seed=4)
+    sur.train(X[tr], BT[tr].astype(np.float32), epochs=epochs, batch=256, lr=1e-3, seed=4)
     t_train = time.perf_counter() - t0
     P, ood = sur.predict(X[te])
     sur.close()
@@ -324,7 +324,7 @@ def surrogate_iasi_accuracy(pkg, ctx, lists, n_train: int = 4096, n_test: int = 
             "held_out_flagged_ood": int(np.sum(ood > sur.ood_threshold)),
             "lbl_spectra_s": t_lbl, "training_s": t_train,
             "config": {"workload": "mlp-152-4x1024-8461 on iasi-400k spectra", "train_spectra": n_train,
-                       "held_out_spectra": n_test, "epochs": 300, "batch": 256,
+                       "held_out_spectra": n_test, "epochs": epochs, "batch": 256,
                        "lr": "1e-3, cosine to 1e-5", "sampler": "perturbed AFGL (seed 2025), scan 0-48 deg"}}
 
 
