@@ -340,6 +340,162 @@ bool lu_solve(int n, std::vector<cd> X, std::vector<cd>& r) {
     return true;
 }
 
+// ------------------------------------------------------------ complex symmetric path
+// W satisfies detailed balance (W_ij rho_j = W_ji rho_i, build_w), so with D = diag(rho)
+// the matrix S = D^-1/2 M D^1/2 = diag(nu) + i p D^-1/2 W D^1/2 is complex symmetric and,
+// when diagonalizable, S = Q Lam Q^T with Q^T Q = I.  Then X = D^1/2 Q, and the two
+// amplitude vectors of band_modes, a = X^T d and b = X^-1 (rho d), are both
+// w = Q^T (sqrt(rho) d): A_k = w_k^2.  Q itself is never formed: every reflection of
+// the tridiagonal reduction and every rotation of the QL sweeps is applied to w only,
+// so the cost is the reduction's ~n^3 plus O(n^2), against ~15 n^3 for the Schur path.
+// Complex orthogonal transformations break down on (near-)isotropic vectors
+// (x^T x ~ 0 with x != 0); the functions below then return false and band_modes takes
+// the Schur path.
+
+// S (row-major, symmetric, overwritten) -> tridiagonal d (diagonal) and e (e[i] = the
+// (i+1, i) element, e[n-1] = 0) by reflections H = I - tau u u^T (H^T H = I), w := H w.
+bool csym_tridiag(int n, std::vector<cd>& S, std::vector<cd>& d, std::vector<cd>& e, std::vector<cd>& w) {
+    std::vector<cd> u(n), q(n);
+    for (int k = 0; k + 2 < n; ++k) {
+        const int m = n - k - 1;
+        double xn2 = 0.0, tail = 0.0;
+        cd sig = 0.0;
+        for (int i = 0; i < m; ++i) {
+            const cd x = S[(size_t)(k + 1 + i) * n + k];
+            xn2 += std::norm(x);
+            if (i > 0) tail += std::norm(x);
+            sig += x * x;
+        }
+        if (tail == 0.0) continue;                     // already tridiagonal in this column
+        if (std::abs(sig) <= 1e-10 * xn2) return false;  // (near-)isotropic column
+        const cd x0 = S[(size_t)(k + 1) * n + k];
+        cd alpha = std::sqrt(sig);
+        if (std::real(std::conj(x0) * alpha) > 0.0) alpha = -alpha;  // x0 - alpha without cancellation
+        const cd utu = 2.0 * alpha * (alpha - x0);   // u^T u for u = x - alpha e1
+        if (std::abs(utu) <= 1e-12 * xn2) return false;
+        const cd tau = 2.0 / utu;
+        for (int i = 0; i < m; ++i) u[i] = S[(size_t)(k + 1 + i) * n + k];
+        u[0] -= alpha;
+        // trailing block A: H A H = A - u q^T - q u^T, q = p - K u, p = tau A u, K = tau u^T p / 2
+        cd K = 0.0;
+        for (int i = 0; i < m; ++i) {
+            const cd* row = &S[(size_t)(k + 1 + i) * n + k + 1];
+            cd t = 0.0;
+            for (int j = 0; j < m; ++j) t += row[j] * u[j];
+            q[i] = tau * t;
+            K += u[i] * q[i];
+        }
+        K *= 0.5 * tau;
+        for (int i = 0; i < m; ++i) q[i] -= K * u[i];
+        for (int i = 0; i < m; ++i) {
+            cd* row = &S[(size_t)(k + 1 + i) * n + k + 1];
+            const cd ui = u[i], qi = q[i];
+            for (int j = 0; j < m; ++j) row[j] -= ui * q[j] + qi * u[j];
+        }
+        S[(size_t)(k + 1) * n + k] = S[(size_t)k * n + k + 1] = alpha;
+        for (int i = 1; i < m; ++i) S[(size_t)(k + 1 + i) * n + k] = S[(size_t)k * n + k + 1 + i] = 0.0;
+        cd t = 0.0;
+        for (int i = 0; i < m; ++i) t += u[i] * w[k + 1 + i];
+        t *= tau;
+        for (int i = 0; i < m; ++i) w[k + 1 + i] -= t * u[i];
+    }
+    d.resize(n);
+    e.assign(n, cd(0.0));
+    for (int i = 0; i < n; ++i) d[i] = S[(size_t)i * n + i];
+    for (int i = 0; i + 1 < n; ++i) e[i] = S[(size_t)(i + 1) * n + i];
+    return true;
+}
+
+// Eigenvalues of the complex symmetric tridiagonal (d, e) by QL sweeps with implicit
+// shifts (the order of EISPACK's tql2, in complex arithmetic: r = sqrt(p^2 + 1) and
+// sqrt(p^2 + e^2) with complex square roots, rotations c^2 + s^2 = 1), each rotation
+// applied to w.  On return d holds the eigenvalues, w[k] pairs with d[k].
+bool csym_ql(int n, std::vector<cd>& d, std::vector<cd>& e, std::vector<cd>& w) {
+    const double eps = DBL_EPSILON;
+    double tst1 = 0.0;
+    cd f = 0.0;
+    for (int l = 0; l < n; ++l) {
+        tst1 = std::max(tst1, std::abs(d[l]) + std::abs(e[l]));
+        int m = l;
+        while (m < n - 1 && std::abs(e[m]) > eps * tst1) ++m;  // e[n-1] = 0 ends the search
+        int iter = 0;
+        while (m > l) {
+            if (++iter > 60) return false;
+            cd g = d[l];
+            cd p = (d[l + 1] - g) / (2.0 * e[l]);
+            cd r = std::sqrt(p * p + 1.0);
+            if (std::real(std::conj(p) * r) < 0.0) r = -r;  // |p + r| >= |p - r|
+            if (std::abs(p + r) == 0.0) return false;
+            d[l] = e[l] / (p + r);
+            d[l + 1] = e[l] * (p + r);
+            const cd dl1 = d[l + 1];
+            cd h = g - d[l];
+            for (int i = l + 2; i < n; ++i) d[i] -= h;
+            f += h;
+            p = d[m];
+            cd c = 1.0, c2 = 1.0, c3 = 1.0, sn = 0.0, s2 = 0.0;
+            const cd el1 = e[l + 1];
+            for (int i = m - 1; i >= l; --i) {
+                c3 = c2;
+                c2 = c;
+                s2 = sn;
+                g = c * e[i];
+                h = c * p;
+                r = std::sqrt(p * p + e[i] * e[i]);
+                if (!(std::abs(r) > 1e-12 * (std::abs(p) + std::abs(e[i])))) return false;  // breakdown
+                e[i + 1] = sn * r;
+                sn = e[i] / r;
+                c = p / r;
+                p = c * d[i] - sn * g;
+                d[i + 1] = h + sn * (c * g + sn * d[i]);
+                const cd w1 = w[i + 1];
+                w[i + 1] = sn * w[i] + c * w1;
+                w[i] = c * w[i] - sn * w1;
+            }
+            p = -sn * s2 * c3 * el1 * e[l] / dl1;
+            e[l] = sn * p;
+            d[l] = c * p;
+            if (std::abs(e[l]) <= eps * tst1) break;
+        }
+        d[l] += f;
+        e[l] = 0.0;
+    }
+    for (int i = 0; i < n; ++i)
+        if (!std::isfinite(d[i].real()) || !std::isfinite(d[i].imag()) || !std::isfinite(w[i].real()) ||
+            !std::isfinite(w[i].imag()))
+            return false;
+    return true;
+}
+
+// Eigenvalues lam and amplitudes A_k = w_k^2 of M = diag(nu) + i p W through S;
+// false (nothing usable) when W is not in detailed balance with rho or the complex
+// orthogonal reduction breaks down.
+bool csym_modes(int n, const std::vector<double>& nu, const std::vector<double>& W, const std::vector<double>& rho,
+                const std::vector<cd>& d0, double p_atm, std::vector<cd>& lam, std::vector<cd>& A) {
+    std::vector<double> sr(n);
+    for (int i = 0; i < n; ++i) {
+        if (!(rho[i] > 0.0) || !std::isfinite(rho[i])) return false;
+        sr[i] = std::sqrt(rho[i]);
+    }
+    std::vector<cd> S((size_t)n * n), w(n);
+    for (int i = 0; i < n; ++i) {
+        S[(size_t)i * n + i] = cd(nu[i], p_atm * W[(size_t)i * n + i]);
+        w[i] = sr[i] * d0[i];
+        for (int j = 0; j < i; ++j) {
+            const double wij = W[(size_t)i * n + j] * rho[j], wji = W[(size_t)j * n + i] * rho[i];
+            if (std::fabs(wij - wji) > 1e-10 * std::max(std::fabs(wij), std::fabs(wji))) return false;
+            const cd v(0.0, p_atm * W[(size_t)i * n + j] * (sr[j] / sr[i]));  // i p W_ij sqrt(rho_j / rho_i)
+            S[(size_t)i * n + j] = S[(size_t)j * n + i] = v;
+        }
+    }
+    std::vector<cd> d, e;
+    if (!csym_tridiag(n, S, d, e, w) || !csym_ql(n, d, e, w)) return false;
+    lam = d;
+    A.resize(n);
+    for (int k = 0; k < n; ++k) A[k] = w[k] * w[k];
+    return true;
+}
+
 // band_modes (:892-955): kept poles and amplitudes, and the band Doppler factor.
 void band_modes(const RelmatBandHost& b, double T, double p_atm, double q_ratio, double keep_threshold,
                 std::vector<cd>& poles, std::vector<cd>& amps, double& f) {
@@ -358,16 +514,21 @@ void band_modes(const RelmatBandHost& b, double T, double p_atm, double q_ratio,
         d[i] = b.lines[i].dipo_t * std::sqrt(nu * (1.0 - std::exp(-kCT * nu / T)));
         for (int j = 0; j < n; ++j) M[(size_t)i * n + j] = cd(i == j ? nu : 0.0, p_atm * W[(size_t)i * n + j]);
     }
-    std::vector<cd> lam, X;
-    if (!eig(n, M, lam, X)) throw Error{IRS_E_ARG, "band_modes: the QR iteration did not converge"};
-    std::vector<cd> bvec(n);
-    for (int i = 0; i < n; ++i) bvec[i] = rho[i] * d[i];
-    if (!lu_solve(n, X, bvec)) throw Error{IRS_E_ARG, "band_modes: singular eigenvector matrix"};
-    std::vector<cd> A(n);
-    for (int k = 0; k < n; ++k) {
-        cd a = 0.0;
-        for (int i = 0; i < n; ++i) a += X[(size_t)i * n + k] * d[i];
-        A[k] = a * bvec[k];
+    std::vector<cd> lam, A;
+    std::vector<double> nus(n);
+    for (int i = 0; i < n; ++i) nus[i] = b.lines[i].nu;
+    if (!csym_modes(n, nus, W, rho, d, p_atm, lam, A)) {  // the general (Schur) path
+        std::vector<cd> X;
+        if (!eig(n, M, lam, X)) throw Error{IRS_E_ARG, "band_modes: the QR iteration did not converge"};
+        std::vector<cd> bvec(n);
+        for (int i = 0; i < n; ++i) bvec[i] = rho[i] * d[i];
+        if (!lu_solve(n, X, bvec)) throw Error{IRS_E_ARG, "band_modes: singular eigenvector matrix"};
+        A.resize(n);
+        for (int k = 0; k < n; ++k) {
+            cd a = 0.0;
+            for (int i = 0; i < n; ++i) a += X[(size_t)i * n + k] * d[i];
+            A[k] = a * bvec[k];
+        }
     }
     const int iso = b.isot;
     const double gD = kCtGamD * (nu_sum / n) * std::sqrt(T / mass_amu(b.molecule, iso));
