@@ -212,9 +212,11 @@ __device__ __forceinline__ void far_table_init(FarTable& F) {
 // whole strip, is a function of the point index analytic well beyond the strip: its
 // far wing is evaluated once per strip at kCtaNodes Chebyshev nodes (by
 // strip_far_kernel, the 8 warps sharing the lines) instead of once per warp, and the
-// degree-15 interpolant is taken to each warp's 8 nodes by the fixed matrix M, where
-// it joins the warp's own far field.  Worst error of one line's term: 1.6e-8 of its
-// largest value on the strip (poles at distance >= 2048 from its centre).  The
+// degree-23 interpolant is taken to each warp's 8 nodes by the fixed matrix M, where
+// it joins the warp's own far field.  Worst error of one line's term: 2.2e-9 of its
+// largest value on the strip (poles at distance >= 1536 from its centre; 16 nodes at
+// 2048, the earlier choice, gave 1.4e-8 and left a quarter more lines to every warp's
+// window).  The
 // pedestals of these lines are quadratics summed exactly as for the warp's far lines
 // (compensated, then evaluated at the nodes, which interpolation reproduces).  The
 // lines are those with unshifted centre V in [c - rout, c - rin) or [c + rin, c + rout),
@@ -222,17 +224,18 @@ __device__ __forceinline__ void far_table_init(FarTable& F) {
 // pressure shift + 2 points; core reach = the segment's largest x_far / fx, so no line
 // of the ranges has its Faddeeva core on the strip): one index range each side, taken
 // out of every warp's window.
-constexpr int kCtaNodes = 16;
-constexpr float kCtaR = 2048.f;
+constexpr int kCtaNodes = 24;
+constexpr float kCtaR = 1536.f;
 constexpr double kCtaCentre = 0.5 * (kMxStrip - 1);  // 1023.5
 constexpr int kStripWords = kMxWarps * kFarNodes;    // per (segment, strip): the warps' node values
-// the nodes relative to the strip centre, 1023.5 cos((2k+1) pi / 32), rounded to FP32
+// the nodes relative to the strip centre, 1023.5 cos((2k+1) pi / 48), rounded to FP32
 __device__ __forceinline__ float cta_node_f(int k) {
-    const int a = k < 8 ? k : 15 - k;
-    const float v = a == 0 ? 1.018571594e+03f : a == 1 ? 9.794284058e+02f : a == 2 ? 9.026464233e+02f
-                  : a == 3 ? 7.911762085e+02f : a == 4 ? 6.493015137e+02f : a == 5 ? 4.824745483e+02f
-                  : a == 6 ? 2.971063538e+02f : 1.003205414e+02f;
-    return k < 8 ? v : -v;
+    const int a = k < 12 ? k : 23 - k;
+    const float v = a == 0 ? 1.021308594e+03f : a == 1 ? 1.003833740e+03f : a == 2 ? 9.691829834e+02f
+                  : a == 3 ? 9.179492798e+02f : a == 4 ? 8.510091553e+02f : a == 5 ? 7.695080566e+02f
+                  : a == 6 ? 6.748404541e+02f : a == 7 ? 5.686261597e+02f : a == 8 ? 4.526824646e+02f
+                  : a == 9 ? 3.289932861e+02f : a == 10 ? 1.996749420e+02f : 6.694010162e+01f;
+    return k < 12 ? v : -v;
 }
 
 // First index i in [0, n) with a[i] >= v (n if none), found by the whole warp: each
