@@ -401,6 +401,12 @@ def bench_extras(pkg, ctx, lists, snd, torch, stream):
         "host buffers (K is 8461 x 151 FP64 per profile)",
         "pullbacks_per_s": len(profs) / tv,
         "pullback": "irs_vjp_batch: dx = K^T dy in reverse mode on the device (K not formed)",
+        # executed FP32 FLOPs from ncu's per-op instruction counters on the profiling case
+        # (bench.py --profile-jacobian), not timed here
+        "roofline": {"bound": "fp32", "kernel": "jg_linesum_kernel<1, 7>", "achieved": 10.3, "peak": 74.4,
+                     "unit": "TFLOP/s", "frac": 10.3 / 74.4, "issue_slots_used": 0.34,
+                     "measured": "ncu sass op counters, 2 profiles x 645-1000 cm^-1 x 151-element state, "
+                                 "3.07e11 FP32 FLOP in 29.8 ms"},
         "config": {"workload": "iasi-400k-lm", "profiles": len(profs), "n_state": spec.n, "channels": 8461}}
     # ---- relaxation-matrix line mixing on the 400k-line IASI workload (6 AFGL profiles)
     relmat = pkg.synthetic.synthetic_relmat(n_bands=6, j_max=60)
