@@ -79,6 +79,31 @@ def test_surrogate_gradients_vs_oracle(pkg, ctx):
     s.close()
 
 
+@pytest.mark.parametrize("n_out,batch,hid", [(8461, 4200, 128), (1001, 700, 256)])
+def test_predict_unaligned_rows_vs_oracle(pkg, ctx, n_out, batch, hid):
+    """Inference rows that are not 16-byte aligned (n_out odd) leave the GEMM through
+    the staged row-run epilogue with the output scale and shift per column: 8461 x 4200
+    runs 128 x 256 tiles, several per CTA, with a ragged last row tile; 1001 x 700 runs
+    ragged 128 x 128 tiles.  Against the oracle network with the GPU's BF16 roundings."""
+    import mlp_oracle as mo
+    n_in, nl = 152, 2
+    s = pkg.Surrogate(ctx, n_in=n_in, n_hidden=hid, n_layers=nl, n_out=n_out, seed=5)
+    rng = np.random.default_rng(7)
+    s.fit_scaling(rng.normal(0.3, 2.0, (64, n_in)), rng.normal(250.0, 20.0, (64, n_out)) + rng.normal(0, 5, n_out))
+    p = s.get_params()
+    p = p + rng.normal(0, 0.05, p.shape).astype(np.float32)
+    s.set_params(p)
+    X = rng.normal(0, 1, (batch, n_in)).astype(np.float32)
+    P, _ = s.predict(X)
+    dims = [n_in] + [hid] * nl + [n_out]
+    _, _, out = mo.forward_backward(p, dims, X, np.zeros((batch, n_out)), s.x_mean, s.x_sd, s.y_mean, s.y_sd,
+                                    bf16=True, need_grad=False)
+    assert P.shape == out.shape and np.isfinite(P).all()
+    scaled = (P.astype(np.float64) - s.y_mean) / s.y_sd
+    assert np.max(np.abs(scaled - out)) <= 5e-3 * np.max(np.abs(out))
+    s.close()
+
+
 def test_training_and_ood(pkg, ctx):
     rng = np.random.default_rng(5)
     n_in, n_out = 152, 300
