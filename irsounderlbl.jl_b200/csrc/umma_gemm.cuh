@@ -44,6 +44,8 @@ template <int TBN> struct TileCfg {
     static constexpr uint32_t kStgBytes = kEpiWarps * 8 * kStgStride * 4;
     static constexpr size_t kSmemBytes = STAGES * (kTileA + kTileB) + kStgBytes + 1024 + 256;
     static constexpr uint32_t kTmemCols = 2 * TBN;
+    static_assert(kSmemBytes <= 232448, "dynamic shared memory per CTA (227 KB)");
+    static_assert(kTmemCols <= 512, "tensor memory columns per SM");
 };
 constexpr uint32_t kMaxSpin = 1u << 22;
 
