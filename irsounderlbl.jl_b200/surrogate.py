@@ -134,12 +134,20 @@ class Surrogate:
             raise IRSError(f"targets have shape {Y.shape}, expected ({len(X)}, {self.n_out})")
 
     # -------------------------------------------------------------- inference
-    def predict(self, X: np.ndarray):
-        """(BT [n, n_out] float32, OOD score [n])."""
+    def predict(self, X: np.ndarray, out: np.ndarray | None = None, ood: np.ndarray | None = None):
+        """(BT [n, n_out] float32, OOD score [n]).  `out` and `ood`, when given, are
+        filled in place and returned: a serving loop that reuses them (page-locked, for
+        example numpy views of pinned torch tensors) skips the allocation, first-touch
+        page faults and pageable staging of a fresh 4 x n x n_out-byte result per call."""
         X = np.ascontiguousarray(X, dtype=np.float32)
         self._check(X)
-        out = np.empty((len(X), self.n_out), np.float32)
-        ood = np.empty(len(X), np.float32)
+        if out is None:
+            out = np.empty((len(X), self.n_out), np.float32)
+        if ood is None:
+            ood = np.empty(len(X), np.float32)
+        for a, shape in ((out, (len(X), self.n_out)), (ood, (len(X),))):
+            if a.shape != shape or a.dtype != np.float32 or not a.flags.c_contiguous or not a.flags.writeable:
+                raise ValueError(f"predict: output must be a writeable C-contiguous float32 array of shape {shape}")
         check(self.lib.irs_surrogate_infer(self.h, fptr(X), len(X), fptr(out), fptr(ood)))
         return out, ood
 

@@ -104,6 +104,27 @@ def test_predict_unaligned_rows_vs_oracle(pkg, ctx, n_out, batch, hid):
     s.close()
 
 
+def test_predict_into_caller_buffers(pkg, ctx):
+    """predict(out=, ood=) fills the caller's arrays in place (the serving-loop form) with
+    the values of a plain predict, and rejects arrays of the wrong shape or type."""
+    s = pkg.Surrogate(ctx, n_in=152, n_hidden=64, n_layers=2, n_out=221, seed=2)
+    X = np.random.default_rng(4).normal(0, 1, (300, 152)).astype(np.float32)
+    P0, O0 = s.predict(X)
+    P = np.full((300, 221), np.nan, np.float32)
+    O = np.full(300, np.nan, np.float32)
+    P1, O1 = s.predict(X, out=P, ood=O)
+    assert P1 is P and O1 is O
+    assert np.array_equal(P, P0)
+    # the OOD score is a row sum of squares accumulated with FP32 atomics from several
+    # warps and tiles, so its rounding order (not its value) varies between calls
+    np.testing.assert_allclose(O, O0, rtol=1e-5, atol=1e-6)
+    for bad in (np.empty((300, 220), np.float32), np.empty((300, 221), np.float64),
+                np.empty((221, 300), np.float32).T):
+        with pytest.raises(ValueError):
+            s.predict(X, out=bad)
+    s.close()
+
+
 def test_training_and_ood(pkg, ctx):
     rng = np.random.default_rng(5)
     n_in, n_out = 152, 300
