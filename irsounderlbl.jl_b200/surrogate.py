@@ -151,6 +151,22 @@ class Surrogate:
         check(self.lib.irs_surrogate_infer(self.h, fptr(X), len(X), fptr(out), fptr(ood)))
         return out, ood
 
+    def predict_device(self, X, out, ood, stream=None):
+        """Inference between device tensors (torch, float32, C-contiguous, on this
+        surrogate's device): X [n, n_in] -> out [n, n_out], ood [n], ordered on `stream`
+        (a torch.cuda.Stream; the current one when None)."""
+        import torch
+        n = X.shape[0]
+        for t, shape in ((X, (n, self.n_in)), (out, (n, self.n_out)), (ood, (n,))):
+            if (tuple(t.shape) != shape or t.dtype != torch.float32 or not t.is_cuda or not t.is_contiguous()
+                    or t.device.index != self.ctx.device):
+                raise ValueError(f"predict_device: need a contiguous float32 tensor of shape {shape} on cuda:"
+                                 f"{self.ctx.device}")
+        st = stream if stream is not None else torch.cuda.current_stream(X.device)
+        check(self.lib.irs_surrogate_infer_device(self.h, C.c_void_p(X.data_ptr()), n, C.c_void_p(out.data_ptr()),
+                                                  C.c_void_p(ood.data_ptr()), C.c_void_p(st.cuda_stream)))
+        return out, ood
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.irs_surrogate_destroy(self.h)
@@ -328,29 +344,45 @@ def _state_feature_columns(spec, n_in: int):
 def _first_guess_columns(sur, ys, spec, base_list, scan_angles, xa, Sa, Se, n_iter, step, cols):
     """surrogate_first_guess when the state maps onto feature columns: the perturbed
     inputs are the scene's features moved in one column, all scenes' 2 n + 1 samples go
-    to the network in one call and the Gauss-Newton systems are solved as one batch."""
+    to the network in one device-to-device call, and K, K^T W K and the Gauss-Newton
+    systems of all scenes are formed and solved as batched FP64 tensors on the
+    surrogate's device (only the state -> feature rows are built on the host)."""
+    import torch
     from .estimation import unpack_state
+    dev = torch.device("cuda", sur.ctx.device)
+    f64 = dict(dtype=torch.float64, device=dev)
     S, n = ys.shape[0], spec.n
-    w = 1.0 / Se
-    Sa_inv = np.linalg.inv(Sa)
-    x = np.array(xa, dtype=np.float64)
     has = cols >= 0
+    j = np.flatnonzero(has)
+    jt, cj = torch.as_tensor(j, device=dev), torch.as_tensor(cols[j], device=dev)
+    w = torch.as_tensor(np.ascontiguousarray(1.0 / np.asarray(Se, dtype=np.float64)), **f64)  # [S, n_ch]
+    Sa_inv = torch.as_tensor(np.linalg.inv(Sa), **f64)
+    ys_t = torch.as_tensor(np.ascontiguousarray(ys, dtype=np.float64), **f64)
+    xa_t = torch.as_tensor(np.ascontiguousarray(xa, dtype=np.float64), **f64)
+    x = np.array(xa, dtype=np.float64)
+    # one set of buffers for every iteration's batched inference (S (2 n + 1) rows); a
+    # perturbed input is the float64 sum rounded once to float32
+    Xp = torch.empty((S, 2 * n + 1, sur.n_in), dtype=torch.float32, device=dev)
+    out = torch.empty((S * (2 * n + 1), sur.n_out), dtype=torch.float32, device=dev)
+    ood = torch.empty(S * (2 * n + 1), dtype=torch.float32, device=dev)
     for _ in range(n_iter):
         rows = [unpack_state(spec, x[s_], base_list[s_]) for s_ in range(S)]
-        F0 = surrogate_features([r[0] for r in rows], scan_angles, [r[1] for r in rows]).astype(np.float64)
-        Xp = np.repeat(F0[:, None, :], 2 * n + 1, axis=1)  # [S, 2n + 1, n_in]
-        j = np.flatnonzero(has)
-        Xp[:, 1 + 2 * j, cols[j]] += step
-        Xp[:, 2 + 2 * j, cols[j]] -= step
-        F, _ = sur.predict(np.ascontiguousarray(Xp.reshape(-1, Xp.shape[2]), dtype=np.float32))
-        F = F.astype(np.float64).reshape(S, 2 * n + 1, -1)
-        K = np.transpose((F[:, 1::2] - F[:, 2::2]) / (2 * step), (0, 2, 1))  # [S, n_ch, n]
-        K[:, :, ~has] = 0.0
-        KtW = np.transpose(K, (0, 2, 1)) * w[:, None, :]
-        H = Sa_inv[None] + KtW @ K
-        r = ys - F[:, 0] + np.einsum("sij,sj->si", K, x - xa)
-        g = np.einsum("sij,sj->si", KtW, r)
-        x = xa + np.linalg.solve(H, g[..., None])[..., 0]
+        F0 = torch.as_tensor(surrogate_features([r[0] for r in rows], scan_angles, [r[1] for r in rows]),
+                             device=dev)  # float32 [S, n_in]
+        Xp.copy_(F0[:, None, :].expand(-1, 2 * n + 1, -1))
+        c64 = F0[:, cj].double()
+        Xp[:, 1 + 2 * jt, cj] = (c64 + step).float()
+        Xp[:, 2 + 2 * jt, cj] = (c64 - step).float()
+        sur.predict_device(Xp.view(-1, sur.n_in), out, ood)
+        F = out.view(S, 2 * n + 1, -1).double()
+        KT = (F[:, 1::2] - F[:, 2::2]) / (2 * step)  # K^T: [S, n, n_ch]
+        KT[:, torch.as_tensor(~has, device=dev)] = 0.0
+        KtW = KT * w[:, None, :]
+        H = Sa_inv + KtW @ KT.transpose(1, 2)
+        dx = torch.as_tensor(x, **f64) - xa_t
+        r = ys_t - F[:, 0] + torch.einsum("sjc,sj->sc", KT, dx)
+        g = torch.einsum("sjc,sc->sj", KtW, r)
+        x = (xa_t + torch.linalg.solve(H, g[..., None])[..., 0]).cpu().numpy()
     return x
 
 
