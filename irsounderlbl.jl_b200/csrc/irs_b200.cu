@@ -322,6 +322,11 @@ static void* run_linesum(irs_ctx* ctx, Plan& pl, const double* d_grid, int64_t n
     return d_tau;
 }
 
+__global__ void ils_float_kernel(const double* __restrict__ k, long long n, float* __restrict__ kf) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) kf[i] = (float)k[i];
+}
+
 static void ensure_ils(irs_ctx* ctx, double dnu, double opd, double fwhm, int apod) {
     const double key[4] = {dnu, opd, fwhm, (double)apod};
     if (std::memcmp(key, ctx->ils_key, sizeof key) == 0) return;
@@ -331,6 +336,10 @@ static void ensure_ils(irs_ctx* ctx, double dnu, double opd, double fwhm, int ap
     ils_taps_kernel<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(dnu, opd, fwhm, apod, n_half, k);
     check_launch(ctx);
     ils_normalise_kernel<<<1, 1024, 0, ctx->stream>>>(k, n, dnu);
+    check_launch(ctx);
+    // the same taps rounded to FP32 for the Jacobian's channel contraction (FP32 sums)
+    float* kf = (float*)workspace(ctx, "ils_f", n * sizeof(float));
+    ils_float_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(k, n, kf);
     check_launch(ctx);
     std::memcpy(ctx->ils_key, key, sizeof key);
     ctx->ils_n = n;
@@ -853,7 +862,8 @@ static void jacobian_device(irs_ctx* ctx, const irs_profile* profs, int n_prof, 
             continue;
         }
         jg_channel_kernel<<<dim3((unsigned)((n_ch * 32 + 255) / 256), (unsigned)n_state, np), 256, 0, st>>>(
-            d_D, n_nu, (int)n_state, d_kern, n_taps, ig.dnu_hi, to_dev(ig.g), to_dev(ch), o.with_ils, d_RB,
+            d_D, n_nu, (int)n_state, o.with_ils ? (const float*)ctx->work["ils_f"].p : nullptr, n_taps, ig.dnu_hi,
+            to_dev(ig.g), to_dev(ch), o.with_ils, d_RB,
             sp.observable, d_K);
         check_launch(ctx);
         if (!K_dev) {

@@ -1152,9 +1152,11 @@ __global__ void __launch_bounds__(128) jg_rte_kernel(
 
 // ------------------------------------------------------------------ channel tail
 // K[x][c] = dBT/dR_c * resample(ILS(D[x]))_c, vmr_jacobian.jl:359-380.  One warp per
-// (state element, channel); the ILS taps run over lanes (FP32 products, FP32 sums).
+// (state element, channel); the ILS taps (kernf: the normalised FP64 taps rounded to
+// FP32) run over lanes (FP32 products, FP32 sums).  A window that lies inside the grid,
+// as it does for every channel away from the padded ends, needs no per-tap bounds test.
 __global__ void __launch_bounds__(256) jg_channel_kernel(const float* __restrict__ D, long long n_nu, int n_state,
-                                                         const double* __restrict__ kern, long long n_taps,
+                                                         const float* __restrict__ kernf, long long n_taps,
                                                          double dnu_hi, GridDev g, GridDev ch, int with_ils,
                                                          const double* __restrict__ R, int observable,
                                                          float* __restrict__ K) {
@@ -1166,11 +1168,18 @@ __global__ void __launch_bounds__(256) jg_channel_kernel(const float* __restrict
     const float* Dx = D + ((size_t)p * n_state + x) * n_nu;
     auto value = [&](long long i) -> double {
         if (!with_ils) return (double)Dx[i];
-        const long long half = (n_taps - 1) / 2;
+        const long long half = (n_taps - 1) / 2, j0 = i - half;
+        const int nt = (int)n_taps;
         float acc = 0.f;
-        for (long long k = lane; k < n_taps; k += 32) {
-            const long long j = i + k - half;
-            if (j >= 0 && j < n_nu) acc = fmaf(Dx[j], (float)kern[k], acc);
+        if (j0 >= 0 && j0 + n_taps <= n_nu) {
+            const float* Dw = Dx + j0;
+#pragma unroll 4
+            for (int k = lane; k < nt; k += 32) acc = fmaf(Dw[k], kernf[k], acc);
+        } else {
+            for (int k = lane; k < nt; k += 32) {
+                const long long j = j0 + k;
+                if (j >= 0 && j < n_nu) acc = fmaf(Dx[j], kernf[k], acc);
+            }
         }
         for (int d = 16; d; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
         return (double)acc * dnu_hi;
